@@ -1,0 +1,34 @@
+#!/bin/sh
+# Builds oracle A: the unmodified feMorph reference sources, compiled where
+# they lie (read-only) with the project-written Boost/Armadillo shim in
+# oracle/shim, linked with oracle/refdrv.cpp (driver + full-precision state
+# hooks).  Outputs go to oracle/_ref/ only.  Needs the reference tree; the GPU
+# host only runs the prebuilt oracle/_ref/fm_refdrv.
+#   REF=<path to the reference project>  (default /root/reference)
+set -e
+HERE=$(cd "$(dirname "$0")" && pwd)
+SRC=${REF:-/root/reference}/src
+OUT=$HERE/_ref
+OBJ=$OUT/obj
+[ -d "$SRC" ] || { echo "reference sources not found at $SRC" >&2; exit 2; }
+mkdir -p "$OBJ"
+CXXFLAGS="-std=c++11 -O2 -w -DUSE_ARMADILLO -include unistd.h -I$HERE/shim -I$SRC"
+pids=""
+for f in "$SRC"/*.cpp; do
+  b=$(basename "$f" .cpp)
+  [ "$b" = main ] && continue
+  if [ ! -f "$OBJ/$b.o" ] || [ "$f" -nt "$OBJ/$b.o" ]; then
+    g++ $CXXFLAGS -c "$f" -o "$OBJ/$b.o" &
+    pids="$pids $!"
+  fi
+done
+for p in $pids; do wait $p; done
+# Hooked members: every call from the solvers to these two femModel members is
+# redirected (GNU ld --wrap) to oracle/refdrv.cpp, which forwards to the real one.
+EXPORT_SYM=$(nm "$OBJ/femVMSExplicitFluidSolver.o" | awk '/ U .*femModel.*ExportToVTKLegacy/ {print $2}')
+SETVEL_SYM=$(nm "$OBJ/femVMSExplicitFluidSolver.o" | awk '/ U .*femModel.*setNodeVelocity/ {print $2}')
+[ -n "$EXPORT_SYM" ] && [ -n "$SETVEL_SYM" ] || { echo "hook symbols not found" >&2; exit 3; }
+g++ $CXXFLAGS -DFM_EXPORT_SYM="\"$EXPORT_SYM\"" -DFM_SETVEL_SYM="\"$SETVEL_SYM\"" \
+  "$HERE/refdrv.cpp" "$OBJ"/*.o -o "$OUT/fm_refdrv" \
+  -Wl,--wrap="$EXPORT_SYM" -Wl,--wrap="$SETVEL_SYM"
+echo "built $OUT/fm_refdrv"
