@@ -1,0 +1,222 @@
+"""ctypes binding of the C ABI in include/femorph_b200.h.
+
+The library is loaded from this package folder (built in-tree by
+femorph_b200/build.py).  There is no fallback: if the shared library is
+missing or no CUDA device is present, the calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import mesh as _mesh
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfemorph_b200.so")
+
+FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_ERR_CUDA, FM_ERR_DIVERGED, FM_ERR_TIMEOUT, FM_ERR_TABLE, FM_ERR_IO, \
+    FM_ERR_NODEVICE = range(9)
+FM_FP64, FM_MIXED = 0, 1
+_GLOB = {"NONE": 0, "X": 1, "Y": 2, "Z": 4, "XY": 3, "YZ": 6, "XZ": 5}
+
+SYMBOLS = [
+    "fm_strerror", "fm_last_error_message", "fm_version", "fm_problem_create", "fm_problem_destroy",
+    "fm_problem_read_dat", "fm_problem_info", "fm_batch_create", "fm_batch_destroy", "fm_batch_step",
+    "fm_batch_sync", "fm_batch_step_ragged", "fm_problem_get_state", "fm_problem_write_vtk",
+    "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
+]
+
+
+class FmMesh(C.Structure):
+    _fields_ = [("elem_type", C.c_int32), ("n_nodes", C.c_int64), ("n_elems", C.c_int64),
+                ("coords", C.c_void_p), ("conn", C.c_void_p)]
+
+
+class FmBC(C.Structure):
+    _fields_ = [("n_vel_rows", C.c_int64), ("vel_node", C.c_void_p), ("vel_vals", C.c_void_p),
+                ("vel_dir", C.c_void_p), ("n_dir", C.c_int64), ("dir_node", C.c_void_p), ("dir_vals", C.c_void_p),
+                ("n_pres", C.c_int64), ("pres_node", C.c_void_p), ("pres_vals", C.c_void_p)]
+
+
+class FmParams(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("precision", C.c_int32), ("props", C.c_double * 5),
+                ("time_step", C.c_double), ("total_steps", C.c_int32), ("save_every", C.c_int32),
+                ("dual_step", C.c_double), ("tot_dual_steps", C.c_int32), ("ex_opts", C.c_int32 * 6),
+                ("glob_fixed", C.c_int32), ("exit_condition", C.c_double)]
+
+
+class FmTuning(C.Structure):
+    _fields_ = [("tile_elems", C.c_int32), ("tile_nodes", C.c_int32), ("threads", C.c_int32),
+                ("graph_steps", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class FmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Loads libfemorph_b200.so (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m femorph_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.fm_strerror.restype = C.c_char_p
+        L.fm_strerror.argtypes = [C.c_int]
+        L.fm_last_error_message.restype = C.c_char_p
+        L.fm_problem_create.argtypes = [P, P, P, P, P]
+        L.fm_problem_destroy.argtypes = [P]
+        L.fm_problem_read_dat.argtypes = [C.c_char_p, C.c_int32, C.c_int32, P]
+        L.fm_problem_info.argtypes = [P, P, P, P, P, P]
+        L.fm_batch_create.argtypes = [P, C.c_int32, P, C.c_int32, P]
+        L.fm_batch_destroy.argtypes = [P]
+        L.fm_batch_step.argtypes = [P, C.c_int32, P]
+        L.fm_batch_sync.argtypes = [P]
+        L.fm_batch_step_ragged.argtypes = [P, P, P]
+        L.fm_problem_get_state.argtypes = [P, P, P, P, P]
+        L.fm_problem_write_vtk.argtypes = [P, C.c_char_p]
+        L.fm_problem_get_mass.argtypes = [P, P]
+        L.fm_batch_last_timing.argtypes = [P, P, P]
+        L.fm_batch_estimate_bytes.argtypes = [P, C.c_int32, P, P]
+        L.fm_batch_layout.argtypes = [P, P, P, P, P]
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code != FM_OK:
+        L = lib()
+        raise FmError(code, f"{L.fm_strerror(code).decode()}: {L.fm_last_error_message().decode()}")
+
+
+def _p(a):
+    return None if a is None or a.size == 0 else a.ctypes.data
+
+
+class GpuProblem:
+    """A femorph_b200 problem built from a femorph_b200.mesh.Problem."""
+
+    def __init__(self, p: "_mesh.Problem", precision: int = FM_FP64):
+        L = lib()
+        self.src = p
+        keep = dict(
+            x=np.ascontiguousarray(p.coords, np.float64), conn=np.ascontiguousarray(p.conn, np.int32),
+            vn=np.ascontiguousarray(p.vel_node, np.int32), vv=np.ascontiguousarray(p.vel_vals, np.float64).reshape(-1, 4),
+            vd=np.ascontiguousarray(p.vel_dir, np.int32), dn=np.ascontiguousarray(p.dir_node, np.int32),
+            dv=np.ascontiguousarray(p.dir_vals, np.float64).reshape(-1, 3),
+            pn=np.ascontiguousarray(p.pres_node, np.int32), pv=np.ascontiguousarray(p.pres_vals, np.float64),
+            init=None if p.init_state is None else np.ascontiguousarray(p.init_state, np.float64))
+        m = FmMesh(p.elem_type, p.n_nodes, p.n_elems, _p(keep["x"]), _p(keep["conn"]))
+        bc = FmBC(len(keep["vn"]), _p(keep["vn"]), _p(keep["vv"]), _p(keep["vd"]), len(keep["dn"]), _p(keep["dn"]),
+                  _p(keep["dv"]), len(keep["pn"]), _p(keep["pn"]), _p(keep["pv"]))
+        prm = FmParams()
+        prm.solver = p.solver
+        prm.precision = precision
+        for i in range(5):
+            prm.props[i] = float(p.props[i])
+        prm.time_step = p.time_step
+        prm.total_steps = p.total_steps
+        prm.save_every = p.save_every
+        prm.dual_step = p.dual_step
+        prm.tot_dual_steps = p.tot_dual_steps
+        for i in range(6):
+            prm.ex_opts[i] = int(p.ex_opts[i])
+        prm.glob_fixed = _GLOB[p.glob_fixed]
+        prm.exit_condition = p.exit_condition
+        h = C.c_void_p()
+        check(L.fm_problem_create(C.byref(m), C.byref(bc), C.byref(prm), _p(keep["init"]) if keep["init"] is not None
+                                  else None, C.byref(h)))
+        self.h = h
+        self.n_nodes, self.n_elems, self.solver = p.n_nodes, p.n_elems, p.solver
+
+    def state(self):
+        """(u (N,3), p (N,) VMS | (E,) SUPG, elem (E,3) VMS | (E,2) SUPG, sdus (E,12) VMS | None)."""
+        N, E = self.n_nodes, self.n_elems
+        u = np.zeros((N, 3))
+        vms = self.solver == _mesh.VMS
+        p = np.zeros(N if vms else E)
+        el = np.zeros((E, 3 if vms else 2))
+        sd = np.zeros((E, 12)) if vms else None
+        check(lib().fm_problem_get_state(self.h, _p(u), _p(p), _p(el), _p(sd) if sd is not None else None))
+        return u, p, el, sd
+
+    def mass(self):
+        m = np.zeros(self.n_nodes if self.solver == _mesh.VMS else self.n_nodes * 3)
+        check(lib().fm_problem_get_mass(self.h, _p(m)))
+        return m
+
+    def write_vtk(self, path: str) -> None:
+        check(lib().fm_problem_write_vtk(self.h, path.encode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fm_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Device-resident batch of GpuProblems (all share solver and element type)."""
+
+    def __init__(self, problems, tile_elems=0, tile_nodes=0, threads=0, graph_steps=0, device=0):
+        L = lib()
+        self.problems = list(problems)
+        arr = (C.c_void_p * len(self.problems))(*[q.h.value for q in self.problems])
+        t = FmTuning(tile_elems, tile_nodes, threads, graph_steps)
+        h = C.c_void_p()
+        check(L.fm_batch_create(arr, len(self.problems), C.byref(t), device, C.byref(h)))
+        self.h = h
+
+    def step(self, n: int = 1, stream=None) -> None:
+        check(lib().fm_batch_step(self.h, int(n), stream))
+
+    def step_ragged(self, steps, stream=None) -> None:
+        a = np.ascontiguousarray(steps, np.int32)
+        check(lib().fm_batch_step_ragged(self.h, _p(a), stream))
+
+    def sync(self) -> None:
+        check(lib().fm_batch_sync(self.h))
+
+    def last_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        check(lib().fm_batch_last_timing(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def layout(self):
+        a, b, c, d = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()
+        check(lib().fm_batch_layout(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return dict(tiles=a.value, iface_nodes=b.value, max_colors=c.value, slots=d.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve(p: "_mesh.Problem", steps: int | None = None, precision: int = FM_FP64, **tuning):
+    """Convenience: one problem, `steps` time steps, returns GpuProblem + Batch."""
+    gp = GpuProblem(p, precision)
+    b = Batch([gp], **tuning)
+    b.step(p.steps if steps is None else steps)
+    b.sync()
+    return gp, b

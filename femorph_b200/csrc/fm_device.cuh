@@ -1,0 +1,123 @@
+// Device-side batch view and helpers shared by the VMS and SUPG kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fm_internal.hpp"
+
+namespace fm {
+
+// Pointers of one device-resident batch (all in batch numbering).
+struct DevBatch {
+  // nodes
+  const double *x, *y, *z;        // coordinates
+  double *su, *sv, *sw, *sp;      // state after BCs
+  double *pu, *pv, *pw, *pp;      // state before BCs (read only at BC nodes)
+  const double* mass;             // VMS nd_mass / SUPG row-sum mass (one per node)
+  const int32_t* node_bc;         // BC record or -1
+  const BCRec* recs;
+  const int32_t* tab_off;
+  const int32_t* tab_len;
+  const double* tab_rows;
+  // elements
+  const uint16_t* conn;           // local node ids, n_elems x npe
+  double* sdus;                   // VMS subscales [12][E] ; SUPG AB2 history [24][E]
+  float* sdus32;                  // VMS mixed: FP32 subscales [12][E]
+  double* el_lam;                 // SUPG per-element lambda / regime (diagnostics)
+  double* el_reg;
+  int64_t E;
+  // tiles
+  const TileMeta* tiles;
+  int32_t n_tiles;
+  const int32_t* tile_nodes;
+  const int32_t* tile_cols;
+  // interface
+  double *part0, *part1, *part2, *part3;
+  const int32_t* iface_node;
+  const int32_t* iface_slot_beg;
+  const int32_t* iface_slots;
+  const int32_t* iface_prob;
+  int32_t n_iface;
+  // problems
+  const DevProb* probs;
+  DevProbState* pstate;
+  const int32_t* target;         // [prob] iteration count to reach
+  double* q1p;                    // [prob][2][4] pre-BC pressures of nodes 0..3
+  int32_t n_probs;
+  unsigned int* done;             // block counter of the interface pass
+  const unsigned char* precise;   // mixed: per element flag, FP64 Jacobian inverse
+};
+
+// femUtils.cpp:830-871 (interpTableData) with femUtils.cpp:818-828
+// (interpVelocity).  Returns false when the time lies before the table.
+__device__ __forceinline__ bool interp_table(double t, const double* tab, int n, double v[3]) {
+  if (t >= tab[(n - 1) * 4 + 3]) {
+    v[0] = tab[(n - 1) * 4 + 0];
+    v[1] = tab[(n - 1) * 4 + 1];
+    v[2] = tab[(n - 1) * 4 + 2];
+    return true;
+  }
+  int count = 1;
+  bool found = false;
+  while (!found && count < n) {
+    found = (t >= tab[(count - 1) * 4 + 3]) && (t < tab[count * 4 + 3]);
+    if (!found) count++;
+  }
+  if (!found) return false;
+  double t1 = tab[(count - 1) * 4 + 3], t2 = tab[count * 4 + 3];
+  for (int c = 0; c < 3; ++c) {
+    double v1 = tab[(count - 1) * 4 + c], v2 = tab[count * 4 + c];
+    v[c] = __dadd_rn(v1, __dmul_rn(__ddiv_rn(__dsub_rn(v2, v1), __dsub_rn(t2, t1)), __dsub_rn(t, t1)));
+  }
+  return true;
+}
+
+// Applies a node's resolved BC to (u, v, w, p) at time t.
+__device__ __forceinline__ void apply_bc(const DevBatch& B, int32_t rec, double t, double s[4], int32_t* status) {
+  BCRec r = B.recs[rec];
+  if (r.tab >= 0) {
+    double v[3];
+    if (interp_table(t, B.tab_rows + (int64_t)B.tab_off[r.tab] * 4, B.tab_len[r.tab], v)) {
+      if (r.mask & BC_VX) s[0] = v[0];
+      if (r.mask & BC_VY) s[1] = v[1];
+      if (r.mask & BC_VZ) s[2] = v[2];
+    } else {
+      *status = FM_ERR_TABLE;
+    }
+  }
+  if (r.mask & BC_PRES) s[3] = r.p;
+  if (r.mask & BC_DIR) {
+    s[0] = r.d[0];
+    s[1] = r.d[1];
+    s[2] = r.d[2];
+  }
+}
+
+// Marks the end of one pass over the interface nodes.  The last block to
+// finish (counter pattern: fence, ticket, no waiting) advances every active
+// problem by one iteration and its time at the start of a new step.
+__device__ __forceinline__ void finish_iteration(const DevBatch& B) {
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int ticket = atomicAdd(B.done, 1u);
+    s_last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int p = threadIdx.x; p < B.n_probs; p += blockDim.x) {
+    DevProbState st = B.pstate[p];
+    if (st.iter < B.target[p]) {
+      const int per_step = B.probs[p].ndual + 1;
+      st.iter += 1;
+      if (st.iter % per_step == 0) st.time = st.time + B.probs[p].dt;
+      B.pstate[p].iter = st.iter;
+      B.pstate[p].time = st.time;
+    }
+  }
+  if (threadIdx.x == 0) *B.done = 0u;
+}
+
+}  // namespace fm

@@ -1,0 +1,424 @@
+// Host-side preparation: problem copies, boundary-condition resolution,
+// lumped masses and the tiled batch layout.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "fm_internal.hpp"
+
+namespace fm {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+const char* last_error() { return g_last_error.c_str(); }
+
+// NODEVEL direction code -> component mask (femModel.cpp:4593-4629).
+static int dir_mask(int32_t d) {
+  static const int m[7] = {BC_VX, BC_VY, BC_VZ, BC_VX | BC_VY, BC_VY | BC_VZ, BC_VX | BC_VZ, BC_VX | BC_VY | BC_VZ};
+  return (d >= 0 && d <= 6) ? m[d] : -1;
+}
+
+// Groups NODEVEL rows into per-node tables the way
+// femModel::postProcessNodeVelocities does (femModel.cpp:4549-4576): unique
+// sorted node ids (femUtils::MakeCompactList), each node's rows in file
+// order, and - reproducing the reference - the direction of the k-th input
+// row applied to the k-th unique node.  Then resolves, per node, the final
+// effect of setNodeVelocity -> apply_zeroTraction (VMS) -> setDirichletBC.
+int resolve_bcs(fm_problem* p) {
+  const int64_t N = p->N;
+  p->node_rec.assign(N, -1);
+  p->recs.clear();
+  p->tab_off.clear();
+  p->tab_len.clear();
+  p->tab_rows.clear();
+  const int64_t nv = (int64_t)p->vel_node.size();
+  std::vector<int32_t> uniq(p->vel_node);
+  std::sort(uniq.begin(), uniq.end());
+  uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+  std::vector<std::vector<int64_t>> rows(uniq.size());
+  for (int64_t r = 0; r < nv; ++r) {
+    int32_t n = p->vel_node[r];
+    if (n < 0 || n >= N) return fail(FM_ERR_INVALID, "NODEVEL node out of range");
+    size_t k = std::lower_bound(uniq.begin(), uniq.end(), n) - uniq.begin();
+    rows[k].push_back(r);
+  }
+  auto rec_of = [&](int32_t n) -> BCRec& {
+    if (p->node_rec[n] < 0) {
+      p->node_rec[n] = (int32_t)p->recs.size();
+      BCRec r;
+      r.tab = -1;
+      r.mask = 0;
+      r.p = 0.0;
+      r.d[0] = r.d[1] = r.d[2] = 0.0;
+      p->recs.push_back(r);
+    }
+    return p->recs[p->node_rec[n]];
+  };
+  for (size_t k = 0; k < uniq.size(); ++k) {
+    int m = dir_mask(p->vel_dir[k]);  // quirk: row k's direction for unique node k
+    if (m < 0) return fail(FM_ERR_INVALID, "ERROR: Invalid direction for node velocities.");
+    BCRec& r = rec_of(uniq[k]);
+    r.tab = (int32_t)p->tab_off.size();
+    r.mask |= m;
+    p->tab_off.push_back((int32_t)(p->tab_rows.size() / 4));
+    p->tab_len.push_back((int32_t)rows[k].size());
+    for (int64_t row : rows[k])
+      for (int c = 0; c < 4; ++c) p->tab_rows.push_back(p->vel_vals[row * 4 + c]);
+  }
+  if (p->params.solver == FM_SOLVER_VMS) {
+    for (size_t i = 0; i < p->pres_node.size(); ++i) {
+      int32_t n = p->pres_node[i];
+      if (n < 0 || n >= N) return fail(FM_ERR_INVALID, "NODEPRES node out of range");
+      BCRec& r = rec_of(n);
+      r.mask |= BC_PRES;
+      r.p = p->pres_vals[i];
+    }
+  }
+  for (size_t i = 0; i < p->dir_node.size(); ++i) {
+    int32_t n = p->dir_node[i];
+    if (n < 0 || n >= N) return fail(FM_ERR_INVALID, "NODEDIRBC node out of range");
+    BCRec& r = rec_of(n);
+    r.mask |= BC_DIR;
+    for (int c = 0; c < 3; ++c) r.d[c] = p->dir_vals[i * 3 + c];
+  }
+  return FM_OK;
+}
+
+// ---- lumped masses (one-time, host, reference operation order) ----
+
+// VMS: initial_assemble (femVMSExplicitFluidSolver.cpp:21-91):
+// nd_mass[n] += (detJ/6)/4 over elements in file order.
+static void vms_mass(fm_problem* p) {
+  p->mass.assign(p->N, 0.0);
+  const double* X = p->coords.data();
+  for (int64_t e = 0; e < p->E; ++e) {
+    const int32_t* c = &p->conn[e * 4];
+    double x[4][3], j[3][3];
+    for (int i = 0; i < 4; ++i)
+      for (int k = 0; k < 3; ++k) x[i][k] = X[(int64_t)c[i] * 3 + k];
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 3; ++k) j[i][k] = x[k + 1][i] - x[0][i];
+    double c00 = j[1][1] * j[2][2] - j[2][1] * j[1][2];
+    double c01 = j[2][0] * j[1][2] - j[1][0] * j[2][2];
+    double c02 = j[1][0] * j[2][1] - j[2][0] * j[1][1];
+    double det = j[0][0] * c00 + j[0][1] * c01 + j[0][2] * c02;
+    double V = det / 6.0;
+    for (int i = 0; i < 4; ++i) p->mass[c[i]] += V / 4.0;
+  }
+}
+
+// SUPG: form_lumped_mass (femSUPGExplicitFluidSolver.cpp:507-598).  The
+// row-sum of the consistent mass is the same for the three components of a
+// node, so one value per node is kept.
+static void supg_mass(fm_problem* p) {
+  const int npe = p->etype;
+  const double rho = p->params.props[0];
+  double gps[8][3], gpw[8];
+  int ngp;
+  if (npe == 4) {
+    const double a = 0.58541020, b = 0.13819660;
+    double t[4][3] = {{a, b, b}, {b, a, b}, {b, b, a}, {b, b, b}};
+    ngp = 4;
+    for (int g = 0; g < 4; ++g) {
+      for (int k = 0; k < 3; ++k) gps[g][k] = t[g][k];
+      gpw[g] = (1.0 / 6.0) * (1.0 / 4.0);
+    }
+  } else {
+    double s = 1.0 / std::sqrt(3.0);
+    double t[8][3] = {{-s, -s, s}, {s, -s, s}, {s, s, s}, {-s, s, s}, {-s, -s, -s}, {s, -s, -s}, {s, s, -s}, {-s, s, -s}};
+    ngp = 8;
+    for (int g = 0; g < 8; ++g) {
+      for (int k = 0; k < 3; ++k) gps[g][k] = t[g][k];
+      gpw[g] = 8.0 * (1.0 / 8.0);
+    }
+  }
+  static const double c1[8] = {-1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0, -1.0};
+  static const double c2[8] = {-1.0, -1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0};
+  static const double c3[8] = {-1.0, -1.0, -1.0, -1.0, 1.0, 1.0, 1.0, 1.0};
+  p->mass.assign(p->N, 0.0);
+  const double* X = p->coords.data();
+  for (int64_t e = 0; e < p->E; ++e) {
+    const int32_t* cn = &p->conn[e * npe];
+    double xe[8][3];
+    for (int a = 0; a < npe; ++a)
+      for (int k = 0; k < 3; ++k) xe[a][k] = X[(int64_t)cn[a] * 3 + k];
+    double M[8][8];
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) M[a][b] = 0.0;
+    for (int g = 0; g < ngp; ++g) {
+      const double* q = gps[g];
+      double Nf[8], dN[8][3];
+      if (npe == 4) {
+        Nf[0] = q[0]; Nf[1] = q[1]; Nf[2] = q[2]; Nf[3] = 1.0 - q[0] - q[1] - q[2];
+        static const double t[4][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}, {-1.0, -1.0, -1.0}};
+        for (int a = 0; a < 4; ++a)
+          for (int k = 0; k < 3; ++k) dN[a][k] = t[a][k];
+      } else {
+        for (int a = 0; a < 8; ++a) {
+          Nf[a] = (1.0 / 8.0) * (1.0 + q[0] * c1[a]) * (1.0 + q[1] * c2[a]) * (1.0 + q[2] * c3[a]);
+          dN[a][0] = (1.0 / 8.0) * c1[a] * (1.0 + q[1] * c2[a]) * (1.0 + q[2] * c3[a]);
+          dN[a][1] = (1.0 / 8.0) * c2[a] * (1.0 + q[0] * c1[a]) * (1.0 + q[2] * c3[a]);
+          dN[a][2] = (1.0 / 8.0) * c3[a] * (1.0 + q[0] * c1[a]) * (1.0 + q[1] * c2[a]);
+        }
+      }
+      double J[3][3];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          double t = 0.0;
+          for (int n = 0; n < npe; ++n) t += dN[n][a] * xe[n][b];
+          J[a][b] = t;
+        }
+      double detJ = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                    J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+      for (int a = 0; a < npe; ++a)
+        for (int b = 0; b < npe; ++b) M[a][b] += rho * Nf[a] * Nf[b] * detJ * gpw[g];
+    }
+    for (int a = 0; a < npe; ++a) {
+      double t = 0.0;
+      for (int b = 0; b < npe; ++b) t += M[a][b];
+      p->mass[cn[a]] += t;
+    }
+  }
+}
+
+void compute_mass(fm_problem* p) {
+  if (p->params.solver == FM_SOLVER_VMS)
+    vms_mass(p);
+  else
+    supg_mass(p);
+}
+
+// ---- tiled layout ----
+
+static inline uint64_t spread3(uint64_t v) {
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+// Builds the batch layout:
+//  1. elements of each problem sorted by the Morton code of their centroid;
+//  2. cut greedily into tiles of <= tile_elems elements and <= tile_nodes
+//     distinct nodes (tiles never span problems, so a problem's arithmetic
+//     does not depend on what else is in the batch);
+//  3. nodes touched by one tile are "interior" to it, the others are
+//     "interface" nodes; nodes are renumbered tile-major (each tile's
+//     interior nodes contiguous), interface nodes after them;
+//  4. inside a tile, elements are coloured greedily (no two elements of a
+//     colour share a node) and sorted by colour, which fixes the order in
+//     which contributions reach every node;
+//  5. each (tile, interface node) pair gets a partial-sum slot; the slots of
+//     an interface node are listed in tile order.
+int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
+  L = Layout();
+  L.node_new.resize(n);
+  L.elem_old.resize(n);
+  int64_t node_base = 0, elem_base = 0, slot_base = 0;
+  for (int pi = 0; pi < n; ++pi) {
+    fm_problem* p = probs[pi];
+    const int npe = p->etype;
+    const int64_t E = p->E, N = p->N;
+    L.node_begin.push_back(node_base);
+    L.elem_begin.push_back(elem_base);
+    // 1. Morton order
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = 0; i < N; ++i)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], p->coords[i * 3 + k]);
+        hi[k] = std::max(hi[k], p->coords[i * 3 + k]);
+      }
+    double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    if (!(span > 0)) span = 1.0;
+    std::vector<uint64_t> code(E);
+    for (int64_t e = 0; e < E; ++e) {
+      double c[3] = {0, 0, 0};
+      for (int a = 0; a < npe; ++a)
+        for (int k = 0; k < 3; ++k) c[k] += p->coords[(int64_t)p->conn[e * npe + a] * 3 + k];
+      uint64_t q[3];
+      for (int k = 0; k < 3; ++k) {
+        double t = (c[k] / npe - lo[k]) / span;
+        t = std::min(std::max(t, 0.0), 1.0);
+        q[k] = (uint64_t)(t * 2097151.0);
+      }
+      code[e] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+    }
+    std::vector<int64_t> order(E);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return code[a] < code[b]; });
+    // 2. greedy tiles
+    std::vector<int64_t> tile_start;
+    std::vector<int32_t> stamp(N, -1);
+    {
+      int64_t cur_nodes = 0, cur_elems = 0;
+      int32_t tid = 0;
+      tile_start.push_back(0);
+      for (int64_t oi = 0; oi < E; ++oi) {
+        const int32_t* c = &p->conn[order[oi] * npe];
+        int fresh = 0;
+        for (int a = 0; a < npe; ++a)
+          if (stamp[c[a]] != tid) {
+            bool dup = false;
+            for (int b = 0; b < a; ++b) dup |= (c[b] == c[a]);
+            if (!dup) ++fresh;
+          }
+        if (cur_elems > 0 && (cur_elems + 1 > TE || cur_nodes + fresh > TN)) {
+          ++tid;
+          tile_start.push_back(oi);
+          cur_nodes = 0;
+          cur_elems = 0;
+          fresh = 0;
+          for (int a = 0; a < npe; ++a) {
+            bool dup = false;
+            for (int b = 0; b < a; ++b) dup |= (c[b] == c[a]);
+            if (!dup) ++fresh;
+          }
+        }
+        for (int a = 0; a < npe; ++a) stamp[c[a]] = tid;
+        cur_nodes += fresh;
+        ++cur_elems;
+      }
+      tile_start.push_back(E);
+    }
+    const int ntile = (int)tile_start.size() - 1;
+    // 3. node tile counts and first tile
+    std::vector<int32_t> ntiles(N, 0), first_tile(N, -1), last(N, -1);
+    for (int t = 0; t < ntile; ++t)
+      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+        const int32_t* c = &p->conn[order[oi] * npe];
+        for (int a = 0; a < npe; ++a)
+          if (last[c[a]] != t) {
+            last[c[a]] = t;
+            if (ntiles[c[a]]++ == 0) first_tile[c[a]] = t;
+          }
+      }
+    std::vector<int32_t>& nn = L.node_new[pi];
+    nn.assign(N, -1);
+    int64_t next = 0;
+    std::vector<int64_t> int_begin(ntile + 1, 0);
+    for (int t = 0; t < ntile; ++t) {
+      int_begin[t] = next;
+      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+        const int32_t* c = &p->conn[order[oi] * npe];
+        for (int a = 0; a < npe; ++a)
+          if (ntiles[c[a]] == 1 && nn[c[a]] < 0) nn[c[a]] = (int32_t)(node_base + next++);
+      }
+    }
+    int_begin[ntile] = next;
+    const int64_t iface_begin = next;
+    for (int t = 0; t < ntile; ++t)
+      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+        const int32_t* c = &p->conn[order[oi] * npe];
+        for (int a = 0; a < npe; ++a)
+          if (ntiles[c[a]] > 1 && nn[c[a]] < 0) nn[c[a]] = (int32_t)(node_base + next++);
+      }
+    for (int64_t i = 0; i < N; ++i)
+      if (nn[i] < 0) nn[i] = (int32_t)(node_base + next++);  // isolated nodes
+    // 4./5. tiles: local nodes, colouring, local connectivity, slots
+    std::vector<int32_t>& eo = L.elem_old[pi];
+    eo.resize(E);
+    std::vector<int32_t> local(N, -1);
+    std::vector<std::vector<int32_t>> iface_lists(N - (iface_begin));
+    int64_t e_out = 0;
+    for (int t = 0; t < ntile; ++t) {
+      TileMeta tm;
+      memset(&tm, 0, sizeof(tm));
+      tm.problem = pi;
+      tm.elem_begin = (int32_t)(elem_base + e_out);
+      tm.n_elem = (int32_t)(tile_start[t + 1] - tile_start[t]);
+      tm.node_begin = (int32_t)L.tile_nodes.size();
+      // local nodes: interior (contiguous batch ids) then interface sorted by id
+      std::vector<int32_t> inter, ifc;
+      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+        const int32_t* c = &p->conn[order[oi] * npe];
+        for (int a = 0; a < npe; ++a)
+          if (local[c[a]] != -2 - t) {
+            local[c[a]] = -2 - t;
+            (ntiles[c[a]] == 1 ? inter : ifc).push_back(c[a]);
+          }
+      }
+      std::sort(inter.begin(), inter.end(), [&](int32_t a, int32_t b) { return nn[a] < nn[b]; });
+      std::sort(ifc.begin(), ifc.end(), [&](int32_t a, int32_t b) { return nn[a] < nn[b]; });
+      tm.n_int = (int32_t)inter.size();
+      tm.n_node = (int32_t)(inter.size() + ifc.size());
+      tm.slot_base = (int32_t)slot_base;
+      std::vector<int32_t> lid;  // old node -> local id via map below
+      int32_t li = 0;
+      for (int32_t v : inter) { local[v] = li++; L.tile_nodes.push_back(nn[v]); }
+      for (int32_t v : ifc) {
+        iface_lists[nn[v] - node_base - iface_begin].push_back((int32_t)(slot_base + (li - tm.n_int)));
+        local[v] = li++;
+        L.tile_nodes.push_back(nn[v]);
+      }
+      slot_base += (int64_t)ifc.size();
+      // colouring (greedy, up to 128 colours)
+      const int64_t ne = tm.n_elem;
+      std::vector<uint64_t> used(2 * tm.n_node, 0);
+      std::vector<int32_t> col(ne);
+      int ncol = 0;
+      for (int64_t i = 0; i < ne; ++i) {
+        const int32_t* c = &p->conn[order[tile_start[t] + i] * npe];
+        uint64_t m0 = 0, m1 = 0;
+        for (int a = 0; a < npe; ++a) {
+          m0 |= used[2 * local[c[a]]];
+          m1 |= used[2 * local[c[a]] + 1];
+        }
+        int k;
+        if (~m0) k = __builtin_ctzll(~m0);
+        else if (~m1) k = 64 + __builtin_ctzll(~m1);
+        else return fail(FM_ERR_INVALID, "element colouring needs more than 128 colours in one tile");
+        col[i] = k;
+        ncol = std::max(ncol, k + 1);
+        for (int a = 0; a < npe; ++a) used[2 * local[c[a]] + (k >> 6)] |= (1ULL << (k & 63));
+      }
+      std::vector<int64_t> idx(ne);
+      std::iota(idx.begin(), idx.end(), 0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
+      tm.col_begin = (int32_t)L.tile_cols.size();
+      tm.n_col = ncol;
+      {
+        std::vector<int32_t> cnt(ncol + 1, 0);
+        for (int64_t i = 0; i < ne; ++i) cnt[col[i] + 1]++;
+        for (int k = 0; k < ncol; ++k) cnt[k + 1] += cnt[k];
+        for (int k = 0; k <= ncol; ++k) L.tile_cols.push_back(cnt[k]);
+      }
+      L.max_colors = std::max(L.max_colors, ncol);
+      for (int64_t i = 0; i < ne; ++i) {
+        int64_t oe = order[tile_start[t] + idx[i]];
+        eo[e_out + i] = (int32_t)oe;
+        const int32_t* c = &p->conn[oe * npe];
+        for (int a = 0; a < npe; ++a) L.conn_local.push_back((uint16_t)local[c[a]]);
+      }
+      e_out += ne;
+      for (int32_t v : inter) local[v] = -1;
+      for (int32_t v : ifc) local[v] = -1;
+      L.tiles.push_back(tm);
+    }
+    for (int64_t k = 0; k < (int64_t)iface_lists.size(); ++k) {
+      L.iface_node.push_back((int32_t)(node_base + iface_begin + k));
+      L.iface_slot_beg.push_back((int32_t)L.iface_slots.size());
+      for (int32_t s : iface_lists[k]) L.iface_slots.push_back(s);
+      L.iface_prob.push_back(pi);
+    }
+    node_base += N;
+    elem_base += E;
+  }
+  L.iface_slot_beg.push_back((int32_t)L.iface_slots.size());
+  L.n_nodes = node_base;
+  L.n_elems = elem_base;
+  L.n_slots = slot_base;
+  if (node_base >= INT32_MAX || elem_base >= INT32_MAX || slot_base >= INT32_MAX)
+    return fail(FM_ERR_INVALID, "batch too large for 32-bit indices");
+  return FM_OK;
+}
+
+}  // namespace fm

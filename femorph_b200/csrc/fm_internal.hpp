@@ -1,0 +1,106 @@
+// Internal host/device data structures of femorph_b200.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/femorph_b200.h"
+
+namespace fm {
+
+// Resolved boundary condition of one node.  The reference applies, in this
+// order, setNodeVelocity (per NODEVEL node, table-interpolated components
+// selected by the direction code), apply_zeroTraction (NODEPRES, VMS only)
+// and setDirichletBC (NODEDIRBC, all three components); later rows of the
+// same list overwrite earlier ones (femModel.cpp:4581-4643,
+// femVMSExplicitFluidSolver.cpp:648-653).
+enum : int32_t { BC_VX = 1, BC_VY = 2, BC_VZ = 4, BC_PRES = 8, BC_DIR = 16 };
+struct BCRec {
+  int32_t tab;    // velocity table index, -1 if none
+  int32_t mask;   // BC_* bits
+  double p;       // NODEPRES value
+  double d[3];    // NODEDIRBC values
+};
+
+// Per-problem constants on the device.
+struct DevProb {
+  double nu, inv_eps, c1, c2, dt, ds, rho, mu, alpha, c_i, exit_cond;
+  int32_t ndual, solver, precision, npe;
+  int32_t ex_mask;     // SUPG: bit0 euler, bit1 B-bar, bit2..5 K1..K4
+  int32_t glob_fixed;  // SUPG FM_FIX_* mask
+  int32_t q1[4];       // VMS: batch ids of the problem's nodes 0..3 (-1 absent)
+  int64_t node_begin, n_nodes, elem_begin, n_elems;
+};
+
+// Per-problem progress on the device.  iter counts completed dual
+// iterations (VMS) or steps (SUPG); a pass only works on problems with
+// iter < target[p] (a separate array, set by the host per launch block).  time is the physical time of the step iter belongs to,
+// accumulated by repeated addition like the reference's currentTime.
+struct DevProbState {
+  int32_t iter;
+  int32_t status;   // FM_OK or an FM_ERR_* raised on the device
+  int32_t pad0, pad1;
+  double time;
+  double max_u2;    // max |u|^2 seen in the last node pass (SUPG EXITCOND)
+};
+
+// One tile = the elements one CTA owns, their distinct nodes (interior
+// nodes first), and the colour ranges of its elements.
+struct TileMeta {
+  int32_t elem_begin, n_elem;   // batch element range
+  int32_t node_begin, n_node;   // range in tile_nodes
+  int32_t n_int;                // first n_int local nodes are interior
+  int32_t slot_base;            // partial slot of local node n_int
+  int32_t col_begin, n_col;     // colour offsets in tile_cols[col_begin .. +n_col]
+  int32_t problem, pad;
+};
+
+struct HostProblem;
+
+}  // namespace fm
+
+struct fm_problem {
+  int32_t etype = 4;
+  int64_t N = 0, E = 0;
+  std::vector<double> coords;
+  std::vector<int32_t> conn;
+  fm_params params{};
+  std::vector<int32_t> vel_node, vel_dir, dir_node, pres_node;
+  std::vector<double> vel_vals, dir_vals, pres_vals;
+  std::vector<double> init;  // N*4 or empty
+  // Resolved BCs
+  std::vector<int32_t> node_rec;   // per node: -1 or record index
+  std::vector<fm::BCRec> recs;
+  std::vector<int32_t> tab_off, tab_len;
+  std::vector<double> tab_rows;    // rows x 4
+  // Lumped mass (problem numbering): VMS N, SUPG N*3
+  std::vector<double> mass;
+  // Batch membership
+  fm_batch* batch = nullptr;
+  int32_t index = -1;
+  int64_t steps_done = 0;
+};
+
+namespace fm {
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int resolve_bcs(fm_problem* p);
+void compute_mass(fm_problem* p);
+
+// Host-side layout of a batch (all arrays in batch numbering).
+struct Layout {
+  int64_t n_nodes = 0, n_elems = 0;
+  std::vector<TileMeta> tiles;
+  std::vector<int32_t> tile_nodes, tile_cols;
+  std::vector<uint16_t> conn_local;   // n_elems x npe
+  std::vector<int32_t> iface_node, iface_slot_beg, iface_slots, iface_prob;
+  int64_t n_slots = 0;
+  int32_t max_colors = 0;
+  // per problem: batch node id of each problem node, problem element of each batch element
+  std::vector<std::vector<int32_t>> node_new;   // [prob][old] -> batch id
+  std::vector<std::vector<int32_t>> elem_old;   // [prob][batch e - elem_begin] -> old element
+  std::vector<int64_t> node_begin, elem_begin;
+};
+
+int build_layout(fm_problem* const* probs, int n, int tile_elems, int tile_nodes, Layout& L);
+}  // namespace fm

@@ -1,0 +1,257 @@
+// SUPG explicit step kernels (tet4 and hexa8): supg_tile_kernel +
+// supg_iface_kernel per time step, and the output-only pressure pass.
+//
+// Same tile scheme as the VMS kernels: nodes staged in shared memory,
+// element forces added colour by colour (fixed order, no atomics), interior
+// nodes updated in place, interface nodes through per-tile partials.
+// Node update (src lines 1509-1521): u^{n+1} = u^n + (1/l_M) acc with
+// acc = sum of -dt K u_e (forward Euler, or 1.5 k^n - 0.5 k^{n-1} for AB2
+// after the first step), then setNodeVelocity and setDirichletBC.  Global
+// fixed dofs (src lines 1527-1561) are applied on read: the stored state
+// keeps the values compute_pressure sees (it runs before the zeroing).
+#include <cuda_runtime.h>
+
+#include "fm_device.cuh"
+#include "fm_supg.cuh"
+
+namespace fm {
+
+__device__ __forceinline__ void mask_fixed(int gf, double& u, double& v, double& w) {
+  if (gf & FM_FIX_X) u = 0.0;
+  if (gf & FM_FIX_Y) v = 0.0;
+  if (gf & FM_FIX_Z) w = 0.0;
+}
+
+__device__ __forceinline__ void supg_node_update(const DevBatch& B, const DevProb& P, double time, int64_t g,
+                                                 const double old[3], const double acc[3], int32_t* status,
+                                                 double* max_u2) {
+  const double im = 1.0 / B.mass[g];
+  double s[4] = {old[0] + im * acc[0], old[1] + im * acc[1], old[2] + im * acc[2], 0.0};
+  const int32_t rec = B.node_bc[g];
+  if (rec >= 0) apply_bc(B, rec, time, s, status);
+  B.su[g] = s[0];
+  B.sv[g] = s[1];
+  B.sw[g] = s[2];
+  mask_fixed(P.glob_fixed, s[0], s[1], s[2]);
+  const double u2 = s[0] * s[0] + s[1] * s[1] + s[2] * s[2];
+  if (!isfinite(u2)) *status = FM_ERR_DIVERGED;
+  if (u2 > *max_u2) *max_u2 = u2;
+}
+
+// get_solution_extrema + EXITCOND (src lines 1594-1643): max |u| above the
+// threshold stops the solve.
+__device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, int pidx, double max_u2, int32_t status) {
+  if (P.exit_cond > 0.0 && sqrt(max_u2) > P.exit_cond) status = FM_ERR_DIVERGED;
+  if (status != FM_OK) B.pstate[pidx].status = status;
+}
+
+template <int NPE, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int tn_max) {
+  extern __shared__ double sm[];
+  double* s_x = sm;
+  double* s_y = s_x + tn_max;
+  double* s_z = s_y + tn_max;
+  double* s_u = s_z + tn_max;
+  double* s_v = s_u + tn_max;
+  double* s_w = s_v + tn_max;
+  double* s_a0 = s_w + tn_max;
+  double* s_a1 = s_a0 + tn_max;
+  double* s_a2 = s_a1 + tn_max;
+  int32_t* s_col = (int32_t*)(s_a2 + tn_max);
+
+  const TileMeta tm = B.tiles[blockIdx.x];
+  const int pidx = tm.problem;
+  const DevProbState st = B.pstate[pidx];
+  if (st.iter >= B.target[pidx]) return;
+  const DevProb& P = B.probs[pidx];
+  const bool euler = (P.ex_mask & 1) || st.iter == 0;
+  const bool ab2 = !(P.ex_mask & 1);
+  const int tid = threadIdx.x;
+  for (int ln = tid; ln < tm.n_node; ln += THREADS) {
+    const int g = B.tile_nodes[tm.node_begin + ln];
+    s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
+    double u = B.su[g], v = B.sv[g], w = B.sw[g];
+    mask_fixed(P.glob_fixed, u, v, w);
+    s_u[ln] = u; s_v[ln] = v; s_w[ln] = w;
+    s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0;
+  }
+  for (int c = tid; c <= tm.n_col; c += THREADS) s_col[c] = B.tile_cols[tm.col_begin + c];
+  __syncthreads();
+  const int64_t E = B.E;
+  int c_lo = 0;
+  for (int base = 0; base < tm.n_elem; base += THREADS) {
+    const int le = base + tid;
+    const bool active = le < tm.n_elem;
+    double k[NPE][3];
+    int ln[NPE];
+    if (active) {
+      const int64_t e = tm.elem_begin + le;
+      if (NPE == 4) {
+        const uint2 cw = __ldg(reinterpret_cast<const uint2*>(B.conn) + e);
+        ln[0] = cw.x & 0xffff; ln[1] = cw.x >> 16; ln[2] = cw.y & 0xffff; ln[3] = cw.y >> 16;
+      } else {
+        const uint4 cw = __ldg(reinterpret_cast<const uint4*>(B.conn) + e);
+        ln[0] = cw.x & 0xffff; ln[1] = cw.x >> 16; ln[2] = cw.y & 0xffff; ln[3] = cw.y >> 16;
+        ln[4 % NPE] = cw.z & 0xffff; ln[5 % NPE] = cw.z >> 16; ln[6 % NPE] = cw.w & 0xffff; ln[7 % NPE] = cw.w >> 16;
+      }
+      double lam, reg;
+      supg_element<NPE>(P, s_x, s_y, s_z, s_u, s_v, s_w, ln, k, lam, reg);
+      B.el_lam[e] = lam;
+      B.el_reg[e] = reg;
+      if (ab2) {
+#pragma unroll
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double* h = B.sdus + (int64_t)(a * 3 + c) * E + e;
+            const double kp = k[a][c];
+            if (!euler) k[a][c] = (3.0 / 2.0) * kp - (1.0 / 2.0) * __ldcs(h);
+            __stcs(h, kp);
+          }
+      }
+    }
+    while (c_lo < tm.n_col && s_col[c_lo + 1] <= base) ++c_lo;
+    for (int c = c_lo; c < tm.n_col && s_col[c] < base + THREADS; ++c) {
+      if (active && le >= s_col[c] && le < s_col[c + 1]) {
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+          s_a0[ln[a]] += k[a][0];
+          s_a1[ln[a]] += k[a][1];
+          s_a2[ln[a]] += k[a][2];
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  int32_t status = FM_OK;
+  double max_u2 = 0.0;
+  for (int l2 = tid; l2 < tm.n_node; l2 += THREADS) {
+    const double acc[3] = {s_a0[l2], s_a1[l2], s_a2[l2]};
+    if (l2 < tm.n_int) {
+      const int g = B.tile_nodes[tm.node_begin + l2];
+      const double old[3] = {s_u[l2], s_v[l2], s_w[l2]};
+      supg_node_update(B, P, st.time, g, old, acc, &status, &max_u2);
+    } else {
+      const int s = tm.slot_base + (l2 - tm.n_int);
+      B.part0[s] = acc[0]; B.part1[s] = acc[1]; B.part2[s] = acc[2];
+    }
+  }
+  check_exit(B, P, pidx, max_u2, status);
+}
+
+__global__ void supg_iface_kernel(DevBatch B) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
+    const int pidx = B.iface_prob[i];
+    const DevProbState st = B.pstate[pidx];
+    if (st.iter >= B.target[pidx]) continue;
+    const DevProb& P = B.probs[pidx];
+    const int g = B.iface_node[i];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int kk = B.iface_slot_beg[i]; kk < B.iface_slot_beg[i + 1]; ++kk) {
+      const int s = B.iface_slots[kk];
+      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s];
+    }
+    double old[3] = {B.su[g], B.sv[g], B.sw[g]};
+    mask_fixed(P.glob_fixed, old[0], old[1], old[2]);
+    int32_t status = FM_OK;
+    double max_u2 = 0.0;
+    supg_node_update(B, P, st.time, g, old, acc, &status, &max_u2);
+    check_exit(B, P, pidx, max_u2, status);
+  }
+  finish_iteration(B);
+}
+
+// compute_pressure (src lines 446-501): p_e = -lambda_e * (int div u) / (int 1),
+// on the stored (pre-zeroing) state.  Output only.
+template <int NPE>
+__global__ void supg_pressure_kernel(DevBatch B, int tn_max, double* pres) {
+  extern __shared__ double sm[];
+  double* s_x = sm;
+  double* s_y = s_x + tn_max;
+  double* s_z = s_y + tn_max;
+  double* s_u = s_z + tn_max;
+  double* s_v = s_u + tn_max;
+  double* s_w = s_v + tn_max;
+  const TileMeta tm = B.tiles[blockIdx.x];
+  for (int ln = threadIdx.x; ln < tm.n_node; ln += blockDim.x) {
+    const int g = B.tile_nodes[tm.node_begin + ln];
+    s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
+    s_u[ln] = B.su[g]; s_v[ln] = B.sv[g]; s_w[ln] = B.sw[g];
+  }
+  __syncthreads();
+  for (int le = threadIdx.x; le < tm.n_elem; le += blockDim.x) {
+    const int64_t e = tm.elem_begin + le;
+    int ln[NPE];
+    for (int a = 0; a < NPE; ++a) ln[a] = B.conn[e * NPE + a];
+    double num = 0.0, den = 0.0;
+    for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+      double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
+      GaussRule<NPE>::point(g, q);
+      shape<NPE>(q, Nf, dN);
+      const double det = jacobian<NPE>(dN, s_x, s_y, s_z, ln, inv);
+      double div = 0.0;
+      for (int a = 0; a < NPE; ++a) {
+        const double ua[3] = {s_u[ln[a]], s_v[ln[a]], s_w[ln[a]]};
+        for (int c = 0; c < 3; ++c)
+          div += (inv[c][0] * dN[a][0] + inv[c][1] * dN[a][1] + inv[c][2] * dN[a][2]) * ua[c];
+      }
+      num += div * det * GaussRule<NPE>::weight();
+      den += det * GaussRule<NPE>::weight();
+    }
+    pres[e] = -B.el_lam[e] * (num / den);
+  }
+}
+
+size_t supg_smem_bytes(int tn_max, int npe) {
+  (void)npe;
+  return (size_t)tn_max * 9 * sizeof(double) + 130 * sizeof(int32_t);
+}
+
+cudaError_t supg_configure(size_t smem, int npe) {
+  cudaError_t e;
+  if (npe == 4) {
+    e = cudaFuncSetAttribute(supg_tile_kernel<4, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(supg_tile_kernel<4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(supg_pressure_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  } else {
+    e = cudaFuncSetAttribute(supg_tile_kernel<8, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(supg_tile_kernel<8, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(supg_pressure_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  return e;
+}
+
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool write_diag,
+                             cudaStream_t s) {
+  (void)write_diag;
+  const size_t smem = supg_smem_bytes(tn_max, npe);
+  if (npe == 4) {
+    if (threads == 256)
+      supg_tile_kernel<4, 256><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+    else
+      supg_tile_kernel<4, 128><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+  } else {
+    if (threads == 256)
+      supg_tile_kernel<8, 256><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+    else
+      supg_tile_kernel<8, 128><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+  }
+  supg_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s) {
+  const size_t smem = (size_t)tn_max * 6 * sizeof(double);
+  if (npe == 4)
+    supg_pressure_kernel<4><<<B.n_tiles, 128, smem, s>>>(B, tn_max, pres);
+  else
+    supg_pressure_kernel<8><<<B.n_tiles, 128, smem, s>>>(B, tn_max, pres);
+  return cudaGetLastError();
+}
+
+}  // namespace fm

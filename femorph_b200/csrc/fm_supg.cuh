@@ -1,0 +1,294 @@
+// SUPG quasi-compressible element arithmetic, matrix-free (one thread = one
+// element).
+//
+// Reference: src/femSUPGExplicitFluidSolver.cpp:1095-1498.  Per Gauss point
+// the reference builds L, U, S, US, B, D, DB, H and accumulates five 24x24
+// matrices (Mass, K1, K1+, K2, K3, K4), then forms k = -dt (K1+K2+K3+K4) u_e.
+// Here each K_i u_e is evaluated directly from the Gauss-point quantities:
+//   (K1 u)[a][c] += rho N_a (u.grad) u_c w                    (Bubnov convection)
+//   (K2 u)[a][c] += sum_r B[r][a,c] (D(lambda, mu) B u)_r w   (viscous + penalty)
+//   (K3 u)[a][c] += rho tau (u.grad N_a) (u.grad) u_c w       (SUPG)
+//   (K4 u)[a][c] += rho nu_C dN_a/dx_c (div u) w              (grad-div)
+// with w = detJ * weight, tau and nu_C from eval_stabilization (src lines
+// 336-377) and lambda from eval_bulk_modulus (src lines 382-441).  The Mass
+// and K1+ matrices do not reach the update (src lines 1325-1327, 806) and the
+// Frobenius norms of K are diagnostics; none of them is formed.
+#pragma once
+#include "fm_device.cuh"
+
+namespace fm {
+
+// irSecondOrder rule (src/femIntegrationRule.cpp): tet4 4 points, weight
+// (1/6)(1/4); hexa8 2x2x2 points at +-1/sqrt(3) in the reference's order,
+// weight 1.
+template <int NPE>
+struct GaussRule;
+template <>
+struct GaussRule<4> {
+  static constexpr int n = 4;
+  __device__ static void point(int g, double q[3]) {
+    const double a = 0.58541020, b = 0.13819660;
+    q[0] = (g == 0) ? a : b;
+    q[1] = (g == 1) ? a : b;
+    q[2] = (g == 2) ? a : b;
+  }
+  __device__ static double weight() { return (1.0 / 6.0) * (1.0 / 4.0); }
+};
+template <>
+struct GaussRule<8> {
+  static constexpr int n = 8;
+  __device__ static void point(int g, double q[3]) {
+    const double s = 0.57735026918962573;  // 1/sqrt(3), correctly rounded
+    const double sx[8] = {-s, s, s, -s, -s, s, s, -s};
+    const double sy[8] = {-s, -s, s, s, -s, -s, s, s};
+    const double sz[8] = {s, s, s, s, -s, -s, -s, -s};
+    q[0] = sx[g];
+    q[1] = sy[g];
+    q[2] = sz[g];
+  }
+  __device__ static double weight() { return 8.0 * (1.0 / 8.0); }
+};
+
+// Shape functions and local derivatives (femTetra4.cpp:295-330,
+// femHexa8.cpp:13-42).
+template <int NPE>
+__device__ __forceinline__ void shape(const double q[3], double N[NPE], double dN[NPE][3]) {
+  if (NPE == 4) {
+    N[0] = q[0]; N[1] = q[1]; N[2] = q[2]; N[3] = 1.0 - q[0] - q[1] - q[2];
+    dN[0][0] = 1.0; dN[0][1] = 0.0; dN[0][2] = 0.0;
+    dN[1][0] = 0.0; dN[1][1] = 1.0; dN[1][2] = 0.0;
+    dN[2][0] = 0.0; dN[2][1] = 0.0; dN[2][2] = 1.0;
+    dN[3][0] = -1.0; dN[3][1] = -1.0; dN[3][2] = -1.0;
+  } else {
+    const double c1[8] = {-1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0, -1.0};
+    const double c2[8] = {-1.0, -1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0};
+    const double c3[8] = {-1.0, -1.0, -1.0, -1.0, 1.0, 1.0, 1.0, 1.0};
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+      const double fx = 1.0 + q[0] * c1[a], fy = 1.0 + q[1] * c2[a], fz = 1.0 + q[2] * c3[a];
+      N[a] = 0.125 * fx * fy * fz;
+      dN[a][0] = 0.125 * c1[a] * fy * fz;
+      dN[a][1] = 0.125 * c2[a] * fx * fz;
+      dN[a][2] = 0.125 * c3[a] * fx * fy;
+    }
+  }
+}
+
+// Jacobian J[a][b] = sum_n dN[n][a] x[n][b] (femElement.cpp:104-127), its
+// cofactor inverse (femUtils.cpp:716-770), global derivatives
+// gd[n][b] = sum_c inv[b][c] dN[n][c] (femElement.cpp:345-352) and the
+// geometric matrix G[a][b] = sum_c inv[c][a] inv[c][b] (femElement.cpp:222-230).
+template <int NPE>
+__device__ __forceinline__ double jacobian(const double dN[NPE][3], const double* sx, const double* sy, const double* sz,
+                                           const int ln[NPE], double inv[3][3]) {
+  double J[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double j0 = 0.0, j1 = 0.0, j2 = 0.0;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) {
+      j0 += dN[n][a] * sx[ln[n]];
+      j1 += dN[n][a] * sy[ln[n]];
+      j2 += dN[n][a] * sz[ln[n]];
+    }
+    J[a][0] = j0; J[a][1] = j1; J[a][2] = j2;
+  }
+  const double m00 = J[0][0], m01 = J[0][1], m02 = J[0][2], m10 = J[1][0], m11 = J[1][1], m12 = J[1][2], m20 = J[2][0],
+               m21 = J[2][1], m22 = J[2][2];
+  const double det = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+  const double id = 1.0 / det;
+  inv[0][0] = (m11 * m22 - m21 * m12) * id;
+  inv[0][1] = (m02 * m21 - m01 * m22) * id;
+  inv[0][2] = (m01 * m12 - m02 * m11) * id;
+  inv[1][0] = (m12 * m20 - m10 * m22) * id;
+  inv[1][1] = (m00 * m22 - m02 * m20) * id;
+  inv[1][2] = (m10 * m02 - m00 * m12) * id;
+  inv[2][0] = (m10 * m21 - m20 * m11) * id;
+  inv[2][1] = (m20 * m01 - m00 * m21) * id;
+  inv[2][2] = (m00 * m11 - m10 * m01) * id;
+  return det;
+}
+
+// One element: k[a][c] = -dt (sum of the enabled K_i u_e)[a][c].  Coordinates
+// and velocities are read from the tile's shared-memory node arrays through
+// the local ids ln[].  Also returns the element's lambda (volume average) and
+// regime (average of the Gauss-point regimes) for output.
+template <int NPE>
+__device__ __forceinline__ void supg_element(const DevProb& P, const double* sx, const double* sy, const double* sz,
+                                             const double* su, const double* sv, const double* sw, const int ln[NPE],
+                                             double k[NPE][3], double& lam_el, double& reg_el) {
+  const double rho = P.rho, mu = P.mu, alpha = P.alpha, cI = P.c_i;
+  const double nu = mu / rho;
+  const bool bbar = (P.ex_mask & 2) != 0;
+  const bool iK1 = (P.ex_mask & 4) != 0, iK2 = (P.ex_mask & 8) != 0, iK3 = (P.ex_mask & 16) != 0,
+             iK4 = (P.ex_mask & 32) != 0;
+  const double wq = GaussRule<NPE>::weight();
+#pragma unroll
+  for (int a = 0; a < NPE; ++a) k[a][0] = k[a][1] = k[a][2] = 0.0;
+  // volume-averaged derivatives for B-bar (eval_avg_shapeDeriv, src lines 660-707)
+  double sd0[NPE][3];
+  if (NPE == 8 && bbar) {
+    double num[NPE][3], den = 0.0;
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) num[a][0] = num[a][1] = num[a][2] = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+      double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
+      GaussRule<NPE>::point(g, q);
+      shape<NPE>(q, Nf, dN);
+      const double det = jacobian<NPE>(dN, sx, sy, sz, ln, inv);
+      const double w = det * wq;
+      den += w;
+#pragma unroll
+      for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          num[a][b] += (inv[b][0] * dN[a][0] + inv[b][1] * dN[a][1] + inv[b][2] * dN[a][2]) * w;
+    }
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) sd0[a][b] = num[a][b] / den;
+  }
+  double vol = 0.0, lam_int = 0.0, reg = 0.0;
+#pragma unroll 1
+  for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+    double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
+    GaussRule<NPE>::point(g, q);
+    shape<NPE>(q, Nf, dN);
+    const double det = jacobian<NPE>(dN, sx, sy, sz, ln, inv);
+    double gd[NPE][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) gd[a][b] = inv[b][0] * dN[a][0] + inv[b][1] * dN[a][1] + inv[b][2] * dN[a][2];
+    double G[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
+    // velocity, gradient, divergence at the point
+    double u[3] = {0.0, 0.0, 0.0}, gr[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+      const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[c] += Nf[a] * ua[c];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gr[c][d] += gd[a][d] * ua[c];
+      }
+    }
+    const double div = gr[0][0] + gr[1][1] + gr[2][2];
+    // eval_stabilization (dt term removed in the reference)
+    const double trG = G[0][0] + G[1][1] + G[2][2];
+    double t2 = 0.0, t3 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
+      t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
+    }
+    t3 = t3 * nu * nu * cI;
+    const double tau = 1.0 / sqrt(t2 + t3);
+    const double nuC = 1.0 / (trG * tau);
+    // eval_bulk_modulus: lambda = alpha * max(mu/rho, sqrt(u^T G^-1 u))
+    double lam, regime;
+    {
+      const double m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
+                   m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
+      const double dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+      const double idg = 1.0 / dG;
+      const double i00 = (m11 * m22 - m21 * m12) * idg, i01 = (m02 * m21 - m01 * m22) * idg,
+                   i02 = (m01 * m12 - m02 * m11) * idg, i10 = (m12 * m20 - m10 * m22) * idg,
+                   i11 = (m00 * m22 - m02 * m20) * idg, i12 = (m10 * m02 - m00 * m12) * idg,
+                   i20 = (m10 * m21 - m20 * m11) * idg, i21 = (m20 * m01 - m00 * m21) * idg,
+                   i22 = (m00 * m11 - m10 * m01) * idg;
+      const double l2 = sqrt((i00 * u[0] + i01 * u[1] + i02 * u[2]) * u[0] + (i10 * u[0] + i11 * u[1] + i12 * u[2]) * u[1] +
+                             (i20 * u[0] + i21 * u[1] + i22 * u[2]) * u[2]);
+      const double l1 = nu;
+      lam = alpha * ((l1 < l2) ? l2 : l1);  // std::max(limit_1, limit_2)
+      regime = (l1 > l2) ? 1.0 : 2.0;
+    }
+    const double w = det * wq;
+    vol += w;
+    lam_int += lam * w;
+    reg += regime;
+    double conv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) conv[c] = u[0] * gr[c][0] + u[1] * gr[c][1] + u[2] * gr[c][2];
+    // strain (B u) and stress (D B u)
+    double eps[6];
+    double sdiv[3] = {0.0, 0.0, 0.0};  // B-bar volumetric parts
+    if (NPE == 8 && bbar) {
+      // rows 0-2 of the B-bar matrix (src lines 234-256)
+      double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+#pragma unroll
+      for (int a = 0; a < NPE; ++a) {
+        const double B1 = (1.0 / 3.0) * (sd0[a][0] - gd[a][0]), B2 = gd[a][0] - B1;
+        const double B3 = (1.0 / 3.0) * (sd0[a][1] - gd[a][1]), B4 = gd[a][1] - B3;
+        const double B5 = (1.0 / 3.0) * (sd0[a][2] - gd[a][2]), B6 = gd[a][2] - B5;
+        const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
+        e0 += B2 * ua[0] + B3 * ua[1] + B5 * ua[2];
+        e1 += B1 * ua[0] + B4 * ua[1] + B5 * ua[2];
+        e2 += B1 * ua[0] + B3 * ua[1] + B6 * ua[2];
+      }
+      eps[0] = e0; eps[1] = e1; eps[2] = e2;
+    } else {
+      eps[0] = gr[0][0]; eps[1] = gr[1][1]; eps[2] = gr[2][2];
+    }
+    eps[3] = gr[0][1] + gr[1][0];
+    eps[4] = gr[1][2] + gr[2][1];
+    eps[5] = gr[0][2] + gr[2][0];
+    (void)sdiv;
+    const double l2m = lam + 2 * mu;
+    const double sig[6] = {l2m * eps[0] + lam * eps[1] + lam * eps[2], lam * eps[0] + l2m * eps[1] + lam * eps[2],
+                           lam * eps[0] + lam * eps[1] + l2m * eps[2], mu * eps[3], mu * eps[4], mu * eps[5]};
+    const double c1w = rho * w, c3w = rho * tau * w, c4w = rho * nuC * div * w;
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+      const double Aa = u[0] * gd[a][0] + u[1] * gd[a][1] + u[2] * gd[a][2];
+      double f[3] = {0.0, 0.0, 0.0};
+      if (iK1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] += c1w * Nf[a] * conv[c];
+      }
+      if (iK3) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] += c3w * Aa * conv[c];
+      }
+      if (iK4) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] += c4w * gd[a][c];
+      }
+      if (iK2) {
+        double r0, r1, r2;  // sum_r B[r][a,c] sigma_r for rows 0-2
+        if (NPE == 8 && bbar) {
+          const double B1 = (1.0 / 3.0) * (sd0[a][0] - gd[a][0]), B2 = gd[a][0] - B1;
+          const double B3 = (1.0 / 3.0) * (sd0[a][1] - gd[a][1]), B4 = gd[a][1] - B3;
+          const double B5 = (1.0 / 3.0) * (sd0[a][2] - gd[a][2]), B6 = gd[a][2] - B5;
+          r0 = B2 * sig[0] + B1 * sig[1] + B1 * sig[2];
+          r1 = B3 * sig[0] + B4 * sig[1] + B3 * sig[2];
+          r2 = B5 * sig[0] + B5 * sig[1] + B6 * sig[2];
+        } else {
+          r0 = gd[a][0] * sig[0];
+          r1 = gd[a][1] * sig[1];
+          r2 = gd[a][2] * sig[2];
+        }
+        f[0] += (r0 + gd[a][1] * sig[3] + gd[a][2] * sig[5]) * w;
+        f[1] += (r1 + gd[a][0] * sig[3] + gd[a][2] * sig[4]) * w;
+        f[2] += (r2 + gd[a][1] * sig[4] + gd[a][0] * sig[5]) * w;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) k[a][c] += f[c];
+    }
+  }
+  const double mdt = -P.dt;
+#pragma unroll
+  for (int a = 0; a < NPE; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) k[a][c] *= mdt;
+  lam_el = lam_int / vol;
+  reg_el = reg / (double)GaussRule<NPE>::n;
+}
+
+}  // namespace fm

@@ -1,0 +1,193 @@
+// VMS tet4 element arithmetic (one thread = one element).
+//
+// Reference: src/femVMSExplicitFluidSolver.cpp.  The P1 structure is used to
+// evaluate the reference's Gauss-point loops in closed form: the velocity
+// gradient and the shape-function gradients are element constants, the
+// weights are all V/4, and the Gauss-point shape values lN[g][a] are
+// ALPHA on the diagonal and BETA elsewhere, so every sum over Gauss points of
+// lN[g][a] * f_g equals BETA * sum_g f_g + (ALPHA - BETA) * f_a.  The result
+// is the same algebraic expression as the reference; only the rounding order
+// differs.
+#pragma once
+#include "fm_device.cuh"
+
+namespace fm {
+
+#define FM_VA 0.58541020
+#define FM_VB 0.13819660
+
+// Element geometry: initial_assemble (src lines 21-91).  Products are
+// rounded individually (no FMA contraction) so DN and V are bit-identical to
+// the reference's.
+struct TetGeom {
+  double DN[3][4];
+  double V;
+};
+
+__device__ __forceinline__ void tet_geometry(const double X[4][3], TetGeom& g) {
+  double j[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) j[i][k] = X[k + 1][i] - X[0][i];
+  double c00 = __dsub_rn(__dmul_rn(j[1][1], j[2][2]), __dmul_rn(j[2][1], j[1][2]));
+  double c01 = __dsub_rn(__dmul_rn(j[2][0], j[1][2]), __dmul_rn(j[1][0], j[2][2]));
+  double c02 = __dsub_rn(__dmul_rn(j[1][0], j[2][1]), __dmul_rn(j[2][0], j[1][1]));
+  double c10 = __dsub_rn(__dmul_rn(j[2][1], j[0][2]), __dmul_rn(j[0][1], j[2][2]));
+  double c11 = __dsub_rn(__dmul_rn(j[0][0], j[2][2]), __dmul_rn(j[2][0], j[0][2]));
+  double c12 = __dsub_rn(__dmul_rn(j[2][0], j[0][1]), __dmul_rn(j[0][0], j[2][1]));
+  double c20 = __dsub_rn(__dmul_rn(j[0][1], j[1][2]), __dmul_rn(j[1][1], j[0][2]));
+  double c21 = __dsub_rn(__dmul_rn(j[1][0], j[0][2]), __dmul_rn(j[0][0], j[1][2]));
+  double c22 = __dsub_rn(__dmul_rn(j[0][0], j[1][1]), __dmul_rn(j[1][0], j[0][1]));
+  double det = __dadd_rn(__dadd_rn(__dmul_rn(j[0][0], c00), __dmul_rn(j[0][1], c01)), __dmul_rn(j[0][2], c02));
+  double id = 1.0 / det;
+  // invJac[i][k] = cof[k][i] / det ; DN[i][0] = -(inv[0][i]) - inv[1][i] - inv[2][i]
+  double inv[3][3];
+  inv[0][0] = __dmul_rn(c00, id); inv[0][1] = __dmul_rn(c10, id); inv[0][2] = __dmul_rn(c20, id);
+  inv[1][0] = __dmul_rn(c01, id); inv[1][1] = __dmul_rn(c11, id); inv[1][2] = __dmul_rn(c21, id);
+  inv[2][0] = __dmul_rn(c02, id); inv[2][1] = __dmul_rn(c12, id); inv[2][2] = __dmul_rn(c22, id);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    g.DN[i][0] = __dsub_rn(__dsub_rn(-inv[0][i], inv[1][i]), inv[2][i]);
+    g.DN[i][1] = inv[0][i];
+    g.DN[i][2] = inv[1][i];
+    g.DN[i][3] = inv[2][i];
+  }
+  g.V = det / 6.0;
+}
+
+// Pending subscale update of the previous dual iteration:
+// assemble_projRes_explicit (src lines 406-588) followed by
+// update_subscales_explicit (src lines 593-646), with include_sg_p = false
+// and the element-local projection (proj_res_at_nodes = false).
+//   U   : nodal velocity after the dual update, before BCs (src line 1134)
+//   pq  : pressures of the problem's nodes 0..3 (src line 489 reads
+//         sol_n[i][3] with the local index i)
+//   sdu : in = subscales at the 4 Gauss points, out = updated subscales
+template <typename T>
+__device__ __forceinline__ void vms_subscale_update(const TetGeom& geo, const T U[4][3], const T pq[4], T sdu[4][3],
+                                                    T inv_dt, T c1nu, T c2, T ih) {
+  const T A = (T)FM_VA, Bt = (T)FM_VB, AB = (T)(FM_VA - FM_VB);
+  T G[3][3], gp[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      G[i][j] = (T)geo.DN[j][0] * U[0][i] + (T)geo.DN[j][1] * U[1][i] + (T)geo.DN[j][2] * U[2][i] +
+                (T)geo.DN[j][3] * U[3][i];
+    gp[i] = (T)geo.DN[i][0] * pq[0] + (T)geo.DN[i][1] * pq[1] + (T)geo.DN[i][2] * pq[2] + (T)geo.DN[i][3] * pq[3];
+  }
+  T Us[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) Us[i] = (U[0][i] + U[1][i]) + (U[2][i] + U[3][i]);
+  T r[4][3];
+  T maxa2 = (T)0;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    T hah[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) hah[i] = Bt * Us[i] + AB * U[g][i] + sdu[g][i];
+    T a2 = hah[0] * hah[0] + hah[1] * hah[1] + hah[2] * hah[2];
+    maxa2 = a2 > maxa2 ? a2 : maxa2;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2] + gp[i];
+  }
+  // Element-local L2 projection of r onto P1: P_a = sum_g lN[g][a] r_g / sum_g lN[g][a],
+  // evaluated back at the Gauss points.
+  const T invS = (T)1 / (A + (T)3 * Bt);
+  T tau_u_inv = c1nu * ih * ih + c2 * sqrt(maxa2) * ih;
+  T tau1 = (T)1 / (inv_dt + tau_u_inv);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);
+    T Pa[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) Pa[a] = (Bt * R + AB * r[a][i]) * invS;
+    T Ps = (Pa[0] + Pa[1]) + (Pa[2] + Pa[3]);
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      T proj = Bt * Ps + AB * Pa[g];
+      sdu[g][i] = ((sdu[g][i] * inv_dt - r[g][i]) + proj) * tau1;
+    }
+  }
+}
+
+// Element residual: assemble_RHS (src lines 93-399) with hdu = U (current
+// dual state after BCs), u_prev = Up (previous dual state), forcing 0
+// (femNode::force is never set) and subgrid pressure 0 (include_sg_p =
+// false).  Writes the 16 nodal residual entries lRes[a][0..3].
+template <typename T, bool HAS_PREV>
+__device__ __forceinline__ void vms_residual(const TetGeom& geo, const T U[4][3], const T P[4], const T Up[4][3],
+                                             const T sdu[4][3], T nu4, T inv_eps, T inv_dt, double lRes[4][4]) {
+  const T Bt = (T)FM_VB, AB = (T)(FM_VA - FM_VB);
+  const T S = (T)FM_VA + (T)3 * Bt;
+  T G[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      G[i][j] = (T)geo.DN[j][0] * U[0][i] + (T)geo.DN[j][1] * U[1][i] + (T)geo.DN[j][2] * U[2][i] +
+                (T)geo.DN[j][3] * U[3][i];
+  const T tr = (G[0][0] + G[1][1]) + G[2][2];
+  T Us[3], Ups[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    Us[i] = (U[0][i] + U[1][i]) + (U[2][i] + U[3][i]);
+    if (HAS_PREV) Ups[i] = (Up[0][i] + Up[1][i]) + (Up[2][i] + Up[3][i]);
+  }
+  const T Psum = (P[0] + P[1]) + (P[2] + P[3]);
+  // X_g = (a_g . grad) u (+ acceleration); M2[i][k] = sum_g sdu_g[i] a_g[k]
+  T X[4][3], M2[3][3], Ssdu[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    Ssdu[i] = (T)0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) M2[i][k] = (T)0;
+  }
+  T Hs = (T)0;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    T ug[3], hah[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      ug[i] = Bt * Us[i] + AB * U[g][i];
+      hah[i] = ug[i] + sdu[g][i];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      X[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2];
+      if (HAS_PREV) {
+        T upg = Bt * Ups[i] + AB * Up[g][i];
+        X[g][i] += (ug[i] - upg) * inv_dt;
+      }
+      Ssdu[i] += sdu[g][i];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) M2[i][k] += sdu[g][i] * hah[k];
+    }
+    Hs += Bt * Psum + AB * P[g];
+  }
+  // K'[i][k] = 4 nu G[i][k] - M2[i][k] - Hs delta_ik ; lRes[a][i] = V/4 (lumped terms + K'.DN)
+  T Kp[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Kp[i][k] = nu4 * G[i][k] - M2[i][k] - (i == k ? Hs : (T)0);
+  const double w = geo.V * 0.25;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T Xs = (X[0][i] + X[1][i]) + (X[2][i] + X[3][i]);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      T v = Bt * Xs + AB * X[a][i] + Kp[i][0] * (T)geo.DN[0][a] + Kp[i][1] * (T)geo.DN[1][a] +
+            Kp[i][2] * (T)geo.DN[2][a];
+      lRes[a][i] = w * (double)v;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    T v = tr * S - (Ssdu[0] * (T)geo.DN[0][a] + Ssdu[1] * (T)geo.DN[1][a] + Ssdu[2] * (T)geo.DN[2][a]);
+    lRes[a][3] = w * (double)(inv_eps * v);
+  }
+}
+
+}  // namespace fm

@@ -1,0 +1,186 @@
+/* femorph_b200: B200-native explicit stabilised incompressible-flow step.
+ *
+ * C ABI of the library libfemorph_b200.so.  Plain structs of pointers and
+ * sizes, 0-based int32 connectivity, FP64 coordinates and state.  The caller
+ * owns every host buffer it passes; the library owns the device buffers.
+ * Every function returns FM_OK (0) or an FM_ERR_* code; no C++ exception
+ * crosses this boundary.  Handles are not thread-safe: one host thread per
+ * batch at a time.
+ *
+ * The entry points replace these reference interfaces (desResLab/feMorph):
+ *   femVMSExplicitFluidSolver::solve(femModel*)   src/femVMSExplicitFluidSolver.h:9-14,
+ *                                                 src/femVMSExplicitFluidSolver.cpp:842-1334
+ *   femSUPGExplicitFluidSolver::solve(femModel*)  src/femSUPGExplicitFluidSolver.h:9-14,
+ *                                                 src/femSUPGExplicitFluidSolver.cpp:794-1735
+ *   femModel public fields read by those solvers  src/femModel.h:24-108
+ *   femModel::ReadFromFEMTextFile                 src/femModel.cpp:3719-4213
+ *   femModel::ExportToVTKLegacy                   src/femModel.cpp:1294-1530
+ * The femSolver adapter classes that keep the reference's
+ * solve(femModel*) entry live in femorph_b200/adapter/.
+ */
+#ifndef FEMORPH_B200_H
+#define FEMORPH_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FM_API __attribute__((visibility("default")))
+#else
+#define FM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---- */
+enum {
+  FM_OK = 0,
+  FM_ERR_INVALID = 1,     /* bad argument, unsupported option or malformed input */
+  FM_ERR_OOM = 2,         /* device or host allocation failed */
+  FM_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  FM_ERR_DIVERGED = 4,    /* NaN/Inf in the state, or max |u| above EXITCOND */
+  FM_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  FM_ERR_TABLE = 6,       /* time outside a NODEVEL table (femUtils.cpp:852-860) */
+  FM_ERR_IO = 7,          /* file could not be read or written */
+  FM_ERR_NODEVICE = 8     /* no usable sm_100 device */
+};
+
+enum { FM_TET4 = 4, FM_HEXA8 = 8 };
+enum { FM_SOLVER_VMS = 0, FM_SOLVER_SUPG = 1 };
+enum { FM_FP64 = 0, FM_MIXED = 1 };
+/* NODEDOF global fixed dofs (femSUPGExplicitFluidSolver.cpp:1527-1561) */
+enum { FM_FIX_NONE = 0, FM_FIX_X = 1, FM_FIX_Y = 2, FM_FIX_Z = 4 };
+
+/* Mesh: femModel::nodeList / elementList (femModel.h:26-27). */
+typedef struct fm_mesh {
+  int32_t elem_type;      /* FM_TET4 or FM_HEXA8 (hexa8 only with SUPG) */
+  int64_t n_nodes;
+  int64_t n_elems;
+  const double* coords;   /* n_nodes x 3 */
+  const int32_t* conn;    /* n_elems x elem_type, 0-based */
+} fm_mesh;
+
+/* Boundary conditions exactly as the .dat rows define them
+ * (femModel.cpp:3941-4005): NODEVEL rows in file order (grouped into per-node
+ * time tables by femModel::postProcessNodeVelocities, femModel.cpp:4549-4576),
+ * NODEDIRBC rows, NODEPRES rows. */
+typedef struct fm_bc {
+  int64_t n_vel_rows;
+  const int32_t* vel_node;   /* node of each row */
+  const double* vel_vals;    /* rows x 4: vx, vy, vz, time */
+  const int32_t* vel_dir;    /* 0..6: X Y Z XY YZ XZ XYZ */
+  int64_t n_dir;
+  const int32_t* dir_node;
+  const double* dir_vals;    /* n_dir x 3 */
+  int64_t n_pres;
+  const int32_t* pres_node;
+  const double* pres_vals;
+} fm_bc;
+
+/* Solver parameters: femModel.h fields vmsProps, timeStep, totalSteps,
+ * saveEvery, dual_step, tot_dual_steps, exOpts, glob_fixed_dofs,
+ * exit_condition. */
+typedef struct fm_params {
+  int32_t solver;          /* FM_SOLVER_VMS or FM_SOLVER_SUPG */
+  int32_t precision;       /* FM_FP64 or FM_MIXED */
+  double props[5];         /* VMS: rho mu invEps c1 c2; SUPG: rho mu alpha cI - */
+  double time_step;
+  int32_t total_steps;     /* TIMESTEP: the reference runs total_steps-1 steps */
+  int32_t save_every;
+  double dual_step;        /* VMS DUALSTEP */
+  int32_t tot_dual_steps;  /* VMS: dual iterations per step = tot_dual_steps+1 */
+  int32_t ex_opts[6];      /* SUPG EXOPTS: euler, B-bar, K1, K2, K3, K4 */
+  int32_t glob_fixed;      /* SUPG FM_FIX_* mask */
+  double exit_condition;   /* SUPG EXITCOND (max |u|); <= 0 disables */
+} fm_params;
+
+/* Launch shape; zero fields take the built-in defaults (or the autotuned
+ * values when fm_batch_autotune has run). */
+typedef struct fm_tuning {
+  int32_t tile_elems;      /* elements per tile (one CTA owns one tile)  */
+  int32_t tile_nodes;      /* max distinct nodes per tile (shared memory) */
+  int32_t threads;         /* threads per CTA */
+  int32_t graph_steps;     /* time steps captured per CUDA graph (0: no graph) */
+  int32_t reserved[4];
+} fm_tuning;
+
+typedef struct fm_problem fm_problem;
+typedef struct fm_batch fm_batch;
+
+FM_API const char* fm_strerror(int code);
+FM_API const char* fm_last_error_message(void);
+FM_API int fm_version(void);
+
+/* Host-side problem description.  init_state (n_nodes x 4: u v w p, before
+ * BCs) may be NULL for a zero start.  The library copies what it needs. */
+FM_API int fm_problem_create(const fm_mesh* mesh, const fm_bc* bc, const fm_params* params,
+                      const double* init_state, fm_problem** out);
+FM_API int fm_problem_destroy(fm_problem* p);
+
+/* Reads a reference .dat keyword file (femModel::ReadFromFEMTextFile,
+ * femModel.cpp:3719-4213; NODE, ELEMENT TET4|HEXA8, NODEVEL, NODEDIRBC,
+ * NODEPRES, NODEDOF, TIMESTEP, DUALSTEP, VMSPROPS, EXOPTS, EXITCOND; other
+ * keywords are ignored).  solver and precision are taken from the optional
+ * keywords "SOLVER VMS|SUPG" and "PRECISION FP64|MIXED", else from the
+ * arguments. */
+FM_API int fm_problem_read_dat(const char* path, int32_t solver, int32_t precision, fm_problem** out);
+
+/* Sizes of a problem (any pointer may be NULL). */
+FM_API int fm_problem_info(const fm_problem* p, int64_t* n_nodes, int64_t* n_elems, int32_t* elem_type,
+                    int32_t* solver, int64_t* steps_done);
+
+/* Packs problems into one device-resident batch (one launch per time step
+ * for all of them).  device: CUDA ordinal.  The problems must outlive the
+ * batch. */
+FM_API int fm_batch_create(fm_problem* const* problems, int32_t n, const fm_tuning* tuning, int32_t device,
+                    fm_batch** out);
+FM_API int fm_batch_destroy(fm_batch* b);
+
+/* Advances every problem of the batch by nsteps time steps (VMS: each with
+ * tot_dual_steps+1 dual iterations) on the given cudaStream_t (NULL: the
+ * batch's own stream).  Asynchronous; fm_batch_sync waits and reports the
+ * first device-side error (FM_ERR_DIVERGED, FM_ERR_TABLE, FM_ERR_TIMEOUT). */
+FM_API int fm_batch_step(fm_batch* b, int32_t nsteps, void* stream);
+FM_API int fm_batch_sync(fm_batch* b);
+
+/* Per-problem step targets for ragged batches: problem i advances by
+ * nsteps[i] (0 = idle) in the next fm_batch_step_ragged call. */
+FM_API int fm_batch_step_ragged(fm_batch* b, const int32_t* nsteps, void* stream);
+
+/* Copies a problem's current state to host memory, in the problem's own
+ * node/element numbering.
+ *   u: n_nodes x 3 velocity;
+ *   p: VMS n_nodes nodal pressure, SUPG n_elems element pressure
+ *      (compute_pressure, femSUPGExplicitFluidSolver.cpp:446-501);
+ *   elem3: VMS n_elems x 3 centroid subgrid velocity (subgrid_u of the VTK
+ *      output), SUPG n_elems x 2 (lambda, regime);
+ *   sdus: VMS n_elems x 12 Gauss-point subscales [e][gp][c] (SUPG: unused).
+ * Any pointer may be NULL. */
+FM_API int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, double* sdus);
+
+/* Writes the problem's current state as legacy ASCII VTK in the layout of
+ * femModel::ExportToVTKLegacy (femModel.cpp:1294-1530). */
+FM_API int fm_problem_write_vtk(fm_problem* p, const char* path);
+
+/* Nodal lumped mass as the solver uses it, problem numbering: VMS n_nodes
+ * (initial_assemble, femVMSExplicitFluidSolver.cpp:87-89), SUPG n_nodes x 3
+ * (form_lumped_mass, femSUPGExplicitFluidSolver.cpp:507-598). */
+FM_API int fm_problem_get_mass(fm_problem* p, double* mass);
+
+/* Device time of the kernels launched by the last fm_batch_step: total
+ * milliseconds and the number of kernel launches (CUDA events on the batch
+ * stream; valid after fm_batch_sync). */
+FM_API int fm_batch_last_timing(fm_batch* b, double* ms, int64_t* launches);
+
+/* Bytes of device memory a batch of these problems needs (admission). */
+FM_API int fm_batch_estimate_bytes(fm_problem* const* problems, int32_t n, const fm_tuning* tuning, int64_t* bytes);
+
+/* Layout statistics: tiles, interface nodes, max colours per tile. */
+FM_API int fm_batch_layout(fm_batch* b, int64_t* n_tiles, int64_t* n_iface_nodes, int32_t* max_colors,
+                    int64_t* n_slots);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEMORPH_B200_H */

@@ -1,0 +1,104 @@
+"""CPU checks of the C ABI: the library loads, exports every symbol the header
+declares, validates inputs, and its host-side preparation (BC resolution,
+lumped masses, .dat reader) matches the oracle without touching a GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from femorph_b200 import api, mesh
+from oracle import oracle_b
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            names |= set(re.findall(r"FM_API\s+[\w\s\*]+?\b(fm_\w+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = api.lib()
+    syms = header_symbols()
+    assert len(syms) >= 18
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(api.SYMBOLS) <= syms
+
+
+def test_strerror_and_version():
+    L = api.lib()
+    assert L.fm_version() >= 100
+    assert L.fm_strerror(api.FM_ERR_TABLE).decode().startswith("Could not find time")
+
+
+def test_invalid_inputs_rejected():
+    p = mesh.cavity(2, seed=0, steps=1)
+    bad = mesh.cavity(2, seed=0, steps=1)
+    bad.conn = bad.conn.copy()
+    bad.conn[3, 2] = bad.n_nodes + 5
+    with pytest.raises(api.FmError) as ei:
+        api.GpuProblem(bad)
+    assert ei.value.code == api.FM_ERR_INVALID
+    hexa = mesh.channel(2, 2, 2, steps=1)
+    hexa.solver = mesh.VMS
+    with pytest.raises(api.FmError):
+        api.GpuProblem(hexa)  # VMS is tet4-only
+    tetb = mesh.cavity(2, seed=0, steps=1, solver=mesh.SUPG)
+    tetb.ex_opts = (1, 1, 1, 1, 1, 1)
+    with pytest.raises(api.FmError):
+        api.GpuProblem(tetb)  # B-bar on tet4 reads out of bounds in the reference
+    bd = mesh.cavity(2, seed=0, steps=1)
+    bd.vel_dir = bd.vel_dir.copy()
+    bd.vel_dir[0] = 9
+    with pytest.raises(api.FmError):
+        api.GpuProblem(bd)
+    api.GpuProblem(p).close()
+
+
+def test_masses_match_oracle_on_host():
+    p = mesh.cavity(4, seed=3, steps=1)
+    m = api.GpuProblem(p).mass()
+    x, c = p.coords, p.conn
+    V = np.linalg.det(np.stack([x[c[:, 1]] - x[c[:, 0]], x[c[:, 2]] - x[c[:, 0]], x[c[:, 3]] - x[c[:, 0]]], 1)) / 6
+    ref = np.zeros(p.n_nodes)
+    np.add.at(ref, c.ravel(), np.repeat(V / 4, 4))
+    assert np.max(np.abs(m - ref)) <= 1e-15 * ref.max()
+    q = mesh.channel(5, 3, 2, seed=1, steps=1)
+    mq = api.GpuProblem(q).mass().reshape(-1, 3)
+    _, _, lm, _ = oracle_b.OracleSolve(q).state()
+    assert np.array_equal(mq, lm)
+
+
+def test_dat_reader_round_trip(tmp_path):
+    p = mesh.cavity(3, seed=4, steps=2)
+    path = str(tmp_path / "m.dat")
+    mesh.write_dat(p, path)
+    h = C.c_void_p()
+    api.check(api.lib().fm_problem_read_dat(path.encode(), 0, 0, C.byref(h)))
+    nn, ne, et, sv = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+    api.check(api.lib().fm_problem_info(h, C.byref(nn), C.byref(ne), C.byref(et), C.byref(sv), None))
+    assert (nn.value, ne.value, et.value, sv.value) == (p.n_nodes, p.n_elems, 4, 0)
+    m = np.zeros(nn.value)
+    api.check(api.lib().fm_problem_get_mass(h, m.ctypes.data))
+    assert np.array_equal(m, api.GpuProblem(p).mass())
+    api.lib().fm_problem_destroy(h)
+
+
+def test_batch_without_device_fails_loudly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except Exception:
+        pass
+    g = api.GpuProblem(mesh.cavity(2, seed=0, steps=1))
+    with pytest.raises(api.FmError) as ei:
+        api.Batch([g])
+    assert ei.value.code == api.FM_ERR_NODEVICE

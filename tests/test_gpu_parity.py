@@ -1,0 +1,169 @@
+"""GPU parity: the CUDA path (through the C ABI) against oracle B, the plain-C
+restatement that is itself pinned bit-exact to the compiled reference.
+
+Tolerances (relative L2 over all nodes, FP64 path): <= 1e-12 per step and
+<= 1e-10 after 200 steps for velocity and pressure.  The GPU evaluates the
+same algebra in a different rounding order (closed-form Gauss sums, tiled
+deterministic accumulation), so results are not bit-identical.
+"""
+import numpy as np
+import pytest
+
+from femorph_b200 import api, mesh
+from oracle import oracle_b
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-12
+TOL_200 = 1e-10
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0))
+
+
+def run_pair(p, steps, check_every=1, **tuning):
+    g = api.GpuProblem(p)
+    b = api.Batch([g], **tuning)
+    o = oracle_b.OracleSolve(p)
+    worst = 0.0
+    for s in range(1, steps + 1):
+        b.step(1)
+        o.step(1)
+        if s % check_every == 0 or s == steps:
+            b.sync()
+            u, pr, el, _ = g.state()
+            st, oel, _, _ = o.state()
+            eu = rel(u, st[:, :3])
+            if p.solver == mesh.VMS:
+                ep = rel(pr, st[:, 3])
+                es = rel(el, oel)
+            else:
+                ep = rel(pr, oel[:, 0])
+                es = rel(el[:, 0], oel[:, 1])
+            worst = max(worst, eu, ep)
+            yield s, eu, ep, es
+    b.close()
+    g.close()
+
+
+def test_vms_cavity_per_step():
+    p = mesh.cavity(4, seed=1, steps=10)
+    for s, eu, ep, es in run_pair(p, 10):
+        assert eu <= TOL_STEP and ep <= TOL_STEP, (s, eu, ep)
+        assert es <= 1e-10, (s, es)
+
+
+def test_vms_cavity_small_tiles_many_interfaces():
+    p = mesh.cavity(6, seed=2, steps=6)
+    for s, eu, ep, es in run_pair(p, 6, tile_elems=48, tile_nodes=64, threads=128):
+        assert eu <= TOL_STEP and ep <= TOL_STEP, (s, eu, ep)
+
+
+def test_vms_dual_iterations_and_ramp_table():
+    p = mesh.cavity(4, seed=7, steps=5)
+    p.tot_dual_steps = 2
+    p.dual_step = 0.5 * p.time_step
+    n = p.vel_node.size
+    p.vel_node = np.concatenate([p.vel_node, p.vel_node]).astype(np.int32)
+    ramp = np.zeros((2 * n, 4))
+    ramp[n:, 0] = 1.0
+    ramp[n:, 3] = 3.0 * p.time_step
+    p.vel_vals = ramp
+    p.vel_dir = np.full(2 * n, 6, np.int32)
+    for s, eu, ep, es in run_pair(p, 5):
+        assert eu <= TOL_STEP and ep <= TOL_STEP, (s, eu, ep)
+
+
+def test_vms_config1_200_steps():
+    """16^3 Kuhn cavity (24,576 tets, 4,913 nodes), 200 steps."""
+    p = mesh.cavity(16, seed=0, steps=200)
+    last = None
+    for s, eu, ep, es in run_pair(p, 200, check_every=20):
+        assert eu <= TOL_STEP * 10 and ep <= TOL_STEP * 10, (s, eu, ep)
+        last = (eu, ep)
+    assert last[0] <= TOL_200 and last[1] <= TOL_200
+
+
+def test_vms_deterministic_and_batch_independent():
+    """Same problem twice -> bitwise identical; alone vs in a mixed batch ->
+    bitwise identical (tiles never span problems)."""
+    ps = [mesh.cavity(n, seed=10 + n, steps=4, lid=0.5 + 0.3 * n) for n in (3, 5, 4)]
+    alone = []
+    for p in ps:
+        g = api.GpuProblem(p)
+        b = api.Batch([g])
+        b.step(4)
+        b.sync()
+        alone.append(g.state()[0:2])
+        b.close()
+    gs = [api.GpuProblem(p) for p in ps]
+    b = api.Batch(gs)
+    b.step(4)
+    b.sync()
+    for g, (u0, p0) in zip(gs, alone):
+        u, pr, _, _ = g.state()
+        assert np.array_equal(u, u0) and np.array_equal(pr, p0)
+
+
+def test_vms_ragged_steps():
+    ps = [mesh.cavity(3, seed=s, steps=6) for s in (1, 2)]
+    gs = [api.GpuProblem(p) for p in ps]
+    b = api.Batch(gs)
+    b.step_ragged([2, 5])
+    b.step_ragged([4, 1])
+    b.sync()
+    for p, g in zip(ps, gs):
+        o = oracle_b.OracleSolve(p)
+        o.step(6)
+        st, _, _, _ = o.state()
+        assert rel(g.state()[0], st[:, :3]) <= TOL_STEP
+
+
+def test_supg_hexa_channel_per_step():
+    p = mesh.channel(8, 4, 4, seed=3, steps=8)
+    for s, eu, ep, es in run_pair(p, 8):
+        assert eu <= TOL_STEP, (s, eu)
+        assert ep <= 1e-11 and es <= 1e-11, (s, ep, es)
+
+
+def test_supg_hexa_ab2_bbar_fixed_dof():
+    p = mesh.channel(6, 3, 3, seed=4, steps=6, ex_opts=(0, 1, 1, 1, 1, 1))
+    p.glob_fixed = "Z"
+    for s, eu, ep, es in run_pair(p, 6, tile_elems=16, tile_nodes=96):
+        assert eu <= TOL_STEP, (s, eu)
+        assert ep <= 1e-11, (s, ep)
+
+
+def test_supg_tet_cavity():
+    p = mesh.cavity(4, seed=5, steps=6, solver=mesh.SUPG)
+    for s, eu, ep, es in run_pair(p, 6):
+        assert eu <= TOL_STEP, (s, eu)
+        assert ep <= 1e-11, (s, ep)
+
+
+def test_divergence_reported_not_hung():
+    """A hugely unstable dt ends with FM_ERR_DIVERGED from the device status
+    word; the kernels keep running to completion (no trap, no wait)."""
+    p = mesh.cavity(4, seed=1, steps=200, dt=0.5)
+    g = api.GpuProblem(p)
+    b = api.Batch([g])
+    b.step(200)
+    with pytest.raises(api.FmError) as ei:
+        b.sync()
+    assert ei.value.code == api.FM_ERR_DIVERGED
+
+
+def test_lumped_mass_kat_gpu_path():
+    """The mass the GPU solver divides by equals the reference KAT."""
+    import os
+    k = np.load(os.path.join(os.path.dirname(__file__), "golden", "lumped_mass_kat.npz"))
+    p = mesh.Problem(coords=k["coords"], conn=k["conn"], solver=mesh.SUPG,
+                     props=(float(k["rho"]), 0.01, 0.05, 4.0, 0.0), max_node_dofs=3)
+    g = api.GpuProblem(p)
+    b = api.Batch([g])
+    b.step(1)
+    b.sync()
+    m = g.mass().reshape(-1, 3)[k["check_nodes"]]
+    assert np.max(np.abs(m - k["lumped_mass"]) / k["lumped_mass"]) < 2e-7
