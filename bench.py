@@ -1,0 +1,284 @@
+"""Benchmark: VMS explicit step on the 96^3 Kuhn-tet lid-driven cavity.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 96] [--precision fp64|mixed|both]
+
+Workload (one GPU): unit cube, 96^3 cells x 6 Kuhn tets = 5,308,416 tet4 and
+912,673 nodes, interior jitter +-0.1h, lid u=(1,0,0), no-slip walls,
+rho=1, mu=0.01, invEps=400, c1=4, c2=2, dt = 0.2 h_min/(1+sqrt(invEps)),
+seeded +-1e-3 initial noise.  A "step" is one time step (one dual iteration)
+of femVMSExplicitFluidSolver over the whole mesh.  Inputs (5.3 M elements x
+96 B of subscales, ~0.5 GB) exceed the 126 MB L2, so no L2 flush is needed
+between steps.  With --gpus N each rank solves its own cavity (seed = rank):
+weak scaling, no data-path collective; value = element-steps/s summed over
+ranks with the time taken as the max over ranks.
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        self.out = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.out.name).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(E: int, N: int, precision: str) -> int:
+    """Compulsory HBM bytes of one VMS step: per element connectivity (4 x int32)
+    and the 12 Gauss-point subscales read and written; per node coordinates,
+    the 4-dof state read and written and the lumped mass.  Geometry (DN, V, h)
+    is recomputed from coordinates and not counted."""
+    sub = 48 if precision == "mixed" else 96
+    return E * (16 + 2 * sub) + N * (24 + 32 + 32 + 8)
+
+
+def make_problem(n: int, seed: int):
+    from femorph_b200 import mesh
+    return mesh.cavity(n, seed=seed, steps=200)
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    from femorph_b200 import api, mesh
+
+    prec = api.FM_MIXED if args.precision == "mixed" else api.FM_FP64
+    p = make_problem(args.n, seed=rank)
+    E, N = p.n_elems, p.n_nodes
+    g = api.GpuProblem(p, prec)
+    b = api.Batch([g], device=local_rank)
+    b.step(args.warmup)
+    b.sync()
+    if dist:
+        dist.barrier()
+    with ClockSampler(local_rank) as clk:
+        b.step(args.steps)
+        b.sync()
+    ms, launches = b.last_timing()
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # per-kernel profile (separate, shorter run)
+    kprof, klaunch = b.profile(min(args.steps, 50))
+    b.sync()
+    lay = b.layout()
+    b.close()
+    g.close()
+    res = dict(E=E, N=N, ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch, layout=lay)
+    # end to end through the C ABI: host buffers in, state out
+    if rank == 0:
+        t0 = time.perf_counter()
+        g2 = api.GpuProblem(p, prec)
+        b2 = api.Batch([g2], device=local_rank)
+        b2.step(args.steps)
+        b2.sync()
+        u, pr, _, _ = g2.state()
+        t1 = time.perf_counter()
+        b2.close()
+        g2.close()
+        res["e2e_s"] = t1 - t0
+        res["h2d"] = p.coords.nbytes + p.conn.nbytes + p.init_state.nbytes
+        res["d2h"] = u.nbytes + pr.nbytes
+    return res
+
+
+def cpu_baseline(n: int, steps: int = 1):
+    """Oracle B (plain-C restatement, single thread) on `steps` steps of the same mesh."""
+    from oracle import oracle_b
+    p = make_problem(n, seed=0)
+    o = oracle_b.OracleSolve(p)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": p.n_elems * steps / dt, "unit": "element-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} time step(s) of the {n}^3 cavity ({p.n_elems} tets) with the single-threaded C "
+                      f"restatement of femVMSExplicitFluidSolver, setup excluded"}
+
+
+def run_reference(args):
+    """The reference's own CPU solver (oracle A = the reference sources compiled
+    in this repository) on a bounded sample of the workload: the full mesh,
+    W warm-up + K timed time steps, parse and setup excluded."""
+    from oracle import ref
+    from femorph_b200 import mesh
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/fm_refdrv was not built (reference sources absent)"}
+    n = args.n
+    steps = max(1, min(args.steps, args.ref_steps))
+    warm = max(1, min(args.warmup, 1))
+    p = make_problem(n, seed=0)
+    p.total_steps = steps + warm + 1
+    p.save_every = 10 ** 9
+    wd = tempfile.mkdtemp(prefix="fm_refbench_")
+    out = ref.run(p, workdir=wd, timing=True, timeout=3600)
+    st = out["timing"]["stamps"]
+    # stamps: initial call (t=0) then one per step (after its element loops)
+    t = st[:, 0]
+    per = np.diff(t[1:])[warm - 1:] if len(t) > 2 else np.array([np.nan])
+    per = per[-steps:]
+    sec = float(np.sum(per))
+    val = p.n_elems * len(per) / sec
+    cores = 1
+    return {"impl": "reference", "metric": METRIC, "value": val, "unit": "element-steps/s", "n_gpus": args.gpus,
+            "steps": len(per), "warmup": warm, "ms_per_step": 1e3 * sec / len(per), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(n, p),
+            "cpu_baseline": {"value": val, "unit": "element-steps/s", "cores": cores, "kind": "reference",
+                             "sample": f"{len(per)} timed steps after {warm} warm-up of the {n}^3 cavity through "
+                                       f"femVMSExplicitFluidSolver::solve (reference sources, g++ -O2), "
+                                       f"parse/setup excluded; the reference is single-threaded"},
+            "e2e": {"value": val, "unit": "element-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+METRIC = "VMS element-steps/s (explicit step, 96^3 Kuhn-tet cavity)"
+
+
+def workload_config(n, p):
+    return {"workload": f"VMS tet4 lid-driven cavity {n}^3 cells x 6 Kuhn tets ({p.n_elems} tets, {p.n_nodes} nodes)"
+                        f", invEps=400, nu=0.01, CFL 0.2 on lid+sqrt(invEps)",
+            "elements": p.n_elems, "nodes": p.n_nodes, "l2": "inputs larger than L2 (no flush)",
+            "parallelism": "independent problem per GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=96)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ref-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+    r = run_ours(args, rank, world, local_rank, dist)
+    if rank == 0:
+        E, N = r["E"], r["N"]
+        sec = r["ms"] / 1e3
+        value = world * E * args.steps / sec
+        peak, peak_kind = hbm_peak()
+        ab = algorithmic_bytes(E, N, args.precision)
+        klaunch = max(1, r["klaunch"])
+        tile_ms = r["kprof"]["tile"] / klaunch
+        achieved = ab / (tile_ms * 1e-3) / 1e9
+        p = make_problem(args.n, seed=0) if False else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "element-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+            "config": {"workload": f"VMS tet4 lid-driven cavity {args.n}^3 cells x 6 Kuhn tets ({E} tets, {N} nodes), "
+                                   f"invEps=400, nu=0.01, dt from CFL 0.2 on lid+sqrt(invEps), {args.precision}",
+                       "elements": E, "nodes": N, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"{world} independent cavity solve(s), one per GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "kernel": "vms_tile_kernel", "algorithmic_bytes_per_launch": ab,
+                         "avg_launch_ms": tile_ms, "iface_kernel_avg_ms": r["kprof"]["iface"] / klaunch},
+            "gpu_launches": r["launches"], "clocks": r["clocks"], "layout": r["layout"],
+        }
+        if "e2e_s" in r:
+            line["e2e"] = {"value": E * args.steps / r["e2e_s"], "unit": "element-steps/s",
+                           "h2d_bytes_per_step": r["h2d"] / args.steps, "d2h_bytes_per_step": r["d2h"] / args.steps,
+                           "note": "problem create + batch create (host layout, H2D) + K steps + state readback, "
+                                   "wall clock"}
+        if world == 1 and not args.no_cpu:
+            try:
+                line["cpu_baseline"] = cpu_baseline(args.n, 1)
+            except Exception as e:  # the baseline is reported, not required
+                line["cpu_baseline"] = {"error": str(e)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -26,6 +26,7 @@ SYMBOLS = [
     "fm_problem_read_dat", "fm_problem_info", "fm_batch_create", "fm_batch_destroy", "fm_batch_step",
     "fm_batch_sync", "fm_batch_step_ragged", "fm_problem_get_state", "fm_problem_write_vtk",
     "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
+    "fm_batch_profile",
 ]
 
 
@@ -87,6 +88,7 @@ def lib():
         L.fm_batch_last_timing.argtypes = [P, P, P]
         L.fm_batch_estimate_bytes.argtypes = [P, C.c_int32, P, P]
         L.fm_batch_layout.argtypes = [P, P, P, P, P]
+        L.fm_batch_profile.argtypes = [P, C.c_int32, P, P]
         _lib = L
     return _lib
 
@@ -195,6 +197,13 @@ class Batch:
         n = C.c_int64()
         check(lib().fm_batch_last_timing(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def profile(self, n: int):
+        """Runs n steps with per-kernel CUDA events: ({'tile': ms, 'iface': ms}, launches per kernel)."""
+        ms = (C.c_double * 2)()
+        ln = (C.c_int64 * 2)()
+        check(lib().fm_batch_profile(self.h, int(n), ms, ln))
+        return {"tile": ms[0], "iface": ms[1]}, ln[0]
 
     def layout(self):
         a, b, c, d = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()

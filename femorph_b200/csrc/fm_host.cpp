@@ -325,11 +325,17 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
       if (nn[i] < 0) nn[i] = (int32_t)(node_base + next++);  // isolated nodes
     // 4./5. tiles: local nodes, colouring, local connectivity, slots
     std::vector<int32_t>& eo = L.elem_old[pi];
-    eo.resize(E);
+    eo.clear();
     std::vector<int32_t> local(N, -1);
     std::vector<std::vector<int32_t>> iface_lists(N - (iface_begin));
     int64_t e_out = 0;
     for (int t = 0; t < ntile; ++t) {
+      // every tile starts at a multiple of ELEM_ALIGN elements (padding slots
+      // in between are never processed), so each chunk of a tile's element
+      // arrays starts on a 16-byte (in fact 128-byte) boundary
+      e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
+      eo.resize(e_out, -1);
+      L.conn_local.resize((size_t)(elem_base + e_out) * npe, 0);
       TileMeta tm;
       memset(&tm, 0, sizeof(tm));
       tm.problem = pi;
@@ -392,6 +398,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         for (int k = 0; k <= ncol; ++k) L.tile_cols.push_back(cnt[k]);
       }
       L.max_colors = std::max(L.max_colors, ncol);
+      eo.resize(e_out + ne, -1);
       for (int64_t i = 0; i < ne; ++i) {
         int64_t oe = order[tile_start[t] + idx[i]];
         eo[e_out + i] = (int32_t)oe;
@@ -410,8 +417,14 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
       L.iface_prob.push_back(pi);
     }
     node_base += N;
-    elem_base += E;
+    e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
+    eo.resize(e_out, -1);
+    L.elem_count.push_back(e_out);
+    elem_base += e_out;
   }
+  // trailing padding: chunk copies round their length up to 16 bytes
+  elem_base += ELEM_ALIGN;
+  L.conn_local.resize((size_t)elem_base * (probs[0]->etype), 0);
   L.iface_slot_beg.push_back((int32_t)L.iface_slots.size());
   L.n_nodes = node_base;
   L.n_elems = elem_base;

@@ -100,7 +100,11 @@ struct Layout {
   std::vector<std::vector<int32_t>> node_new;   // [prob][old] -> batch id
   std::vector<std::vector<int32_t>> elem_old;   // [prob][batch e - elem_begin] -> old element
   std::vector<int64_t> node_begin, elem_begin;
+  std::vector<int64_t> elem_count;   // per problem: padded element slots (elem_old has this size, -1 = padding)
 };
+
+// Tiles start at multiples of this many element slots.
+constexpr int ELEM_ALIGN = 32;
 
 int build_layout(fm_problem* const* probs, int n, int tile_elems, int tile_nodes, Layout& L);
 }  // namespace fm

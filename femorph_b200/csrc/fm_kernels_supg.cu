@@ -226,10 +226,10 @@ cudaError_t supg_configure(size_t smem, int npe) {
   return e;
 }
 
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool write_diag,
-                             cudaStream_t s) {
-  (void)write_diag;
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, cudaStream_t s,
+                             cudaEvent_t* ev) {
   const size_t smem = supg_smem_bytes(tn_max, npe);
+  if (ev) cudaEventRecord(ev[0], s);
   if (npe == 4) {
     if (threads == 256)
       supg_tile_kernel<4, 256><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
@@ -241,7 +241,9 @@ cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int ifa
     else
       supg_tile_kernel<8, 128><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
   }
+  if (ev) cudaEventRecord(ev[1], s);
   supg_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  if (ev) cudaEventRecord(ev[2], s);
   return cudaGetLastError();
 }
 

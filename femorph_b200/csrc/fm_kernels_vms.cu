@@ -17,6 +17,8 @@
 // applies the same node update, then advances the problems' iteration.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "fm_device.cuh"
 #include "fm_vms.cuh"
 
@@ -51,9 +53,101 @@ __device__ __forceinline__ void vms_node_update(const DevBatch& B, const DevProb
   B.su[g] = s[0]; B.sv[g] = s[1]; B.sw[g] = s[2]; B.sp[g] = s[3];
 }
 
-template <int THREADS>
+// Per-element VMS work for one chunk slot: pending subscale update (written
+// back to global memory) and the element residual lres.  S: subscale storage
+// type (double, or float in the mixed form).
+template <bool MIXED, typename S>
+__device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P, int64_t e, const int ln[4],
+                                            const double* s_x, const double* s_y, const double* s_z,
+                                            const double* s_u, const double* s_v, const double* s_w,
+                                            const double* s_p, const double* s_qu, const double* s_qv,
+                                            const double* s_qw, const S sd_in[12], const double pq[4], bool pending,
+                                            bool first_dual, double inv_dt, double c1nu, double nu4,
+                                            double lres[4][4]) {
+  const int64_t E = B.E;
+  double X[4][3], U[4][3], Pn[4], Q[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    X[a][0] = s_x[ln[a]]; X[a][1] = s_y[ln[a]]; X[a][2] = s_z[ln[a]];
+    Q[a][0] = s_qu[ln[a]]; Q[a][1] = s_qv[ln[a]]; Q[a][2] = s_qw[ln[a]];
+  }
+  if constexpr (MIXED) {
+    TetGeomF geo;
+    tet_geometry_mixed(X, B.precise[e] != 0, geo);
+    const float ih = rcbrtf((float)(6.0 * geo.V));
+    float sdu[4][3];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) sdu[q / 3][q % 3] = sd_in[q];
+    if (pending) {
+      float Q0[3], Qd[4][3], pqd[4];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        Q0[i] = (float)Q[0][i];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) Qd[a][i] = (float)(Q[a][i] - Q[0][i]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) pqd[a] = (float)(pq[a] - pq[0]);
+      vms_subscale_update_mixed(geo, Q0, Qd, pqd, sdu, (float)inv_dt, (float)c1nu, (float)P.c2, ih);
+#pragma unroll
+      for (int q = 0; q < 12; ++q) __stcs(B.sdus32 + (int64_t)q * E + e, sdu[q / 3][q % 3]);
+    }
+    float U0[3], Ud[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      U[a][0] = s_u[ln[a]]; U[a][1] = s_v[ln[a]]; U[a][2] = s_w[ln[a]]; Pn[a] = s_p[ln[a]];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      U0[i] = (float)U[0][i];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) Ud[a][i] = (float)(U[a][i] - U[0][i]);
+    }
+    if (first_dual) {
+      vms_residual_mixed<false>(geo, U0, Ud, Pn, Ud, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, lres);
+    } else {
+      float Dacc[4][3];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) Dacc[a][i] = (float)(U[a][i] - Q[a][i]);
+      vms_residual_mixed<true>(geo, U0, Ud, Pn, Dacc, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, lres);
+    }
+  } else {
+    TetGeom geo;
+    tet_geometry(X, geo);
+    const double ih = rcbrt(6.0 * geo.V);
+    double sdu[4][3];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) sdu[q / 3][q % 3] = sd_in[q];
+    if (pending) {
+      vms_subscale_update<double>(geo, Q, pq, sdu, inv_dt, c1nu, P.c2, ih);
+#pragma unroll
+      for (int q = 0; q < 12; ++q) __stcs(B.sdus + (int64_t)q * E + e, sdu[q / 3][q % 3]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      U[a][0] = s_u[ln[a]]; U[a][1] = s_v[ln[a]]; U[a][2] = s_w[ln[a]]; Pn[a] = s_p[ln[a]];
+    }
+    if (first_dual)
+      vms_residual<double, false>(geo, U, Pn, U, sdu, nu4, P.inv_eps, inv_dt, lres);
+    else
+      vms_residual<double, true>(geo, U, Pn, Q, sdu, nu4, P.inv_eps, inv_dt, lres);
+  }
+}
+
+// Shared memory of one tile CTA: node arrays (14 x tn_max doubles), the
+// double-buffered chunk stage (2 x (12 subscale rows + 1 connectivity row) x
+// THREADS slots), colour offsets.
+template <int THREADS, bool MIXED>
+__host__ __device__ constexpr size_t vms_stage_bytes() {
+  return 2 * ((size_t)12 * THREADS * (MIXED ? sizeof(float) : sizeof(double)) + (size_t)THREADS * 8);
+}
+
+template <int THREADS, bool MIXED>
 __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn_max) {
-  extern __shared__ double sm[];
+  using S = typename std::conditional<MIXED, float, double>::type;
+  extern __shared__ __align__(16) double sm[];
   double* s_x = sm;
   double* s_y = s_x + tn_max;
   double* s_z = s_y + tn_max;
@@ -61,14 +155,18 @@ __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn
   double* s_v = s_u + tn_max;
   double* s_w = s_v + tn_max;
   double* s_p = s_w + tn_max;
-  double* s_qu = s_p + tn_max;   // pre-BC velocity
+  double* s_qu = s_p + tn_max;   // velocity before the last BCs
   double* s_qv = s_qu + tn_max;
   double* s_qw = s_qv + tn_max;
-  double* s_a0 = s_qw + tn_max;
+  double* s_a0 = s_qw + tn_max;  // residual accumulators
   double* s_a1 = s_a0 + tn_max;
   double* s_a2 = s_a1 + tn_max;
   double* s_a3 = s_a2 + tn_max;
-  int32_t* s_col = (int32_t*)(s_a3 + tn_max);   // colour offsets (<= 129)
+  S* stage_s = reinterpret_cast<S*>(s_a3 + tn_max);                 // [2][12][THREADS]
+  uint2* stage_c = reinterpret_cast<uint2*>(stage_s + 2 * 12 * THREADS);  // [2][THREADS]
+  int32_t* s_col = reinterpret_cast<int32_t*>(stage_c + 2 * THREADS);     // colour offsets (<= 129)
+  __shared__ uint64_t bars[2];
+  __shared__ int s_abort;
 
   const TileMeta tm = B.tiles[blockIdx.x];
   const int pidx = tm.problem;
@@ -79,7 +177,32 @@ __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn
   const bool first_dual = (st.iter % per_step) == 0;
   const bool pending = st.iter > 0;
   const int tid = threadIdx.x;
+  const int64_t E = B.E;
+  const S* sdus_g = MIXED ? reinterpret_cast<const S*>(B.sdus32) : reinterpret_cast<const S*>(B.sdus);
+  const uint2* conn_g = reinterpret_cast<const uint2*>(B.conn);
+  const int nchunks = (tm.n_elem + THREADS - 1) / THREADS;
 
+  // one thread issues the bulk copies of chunk k into stage buffer k & 1
+  auto issue = [&](int k) {
+    const int b = k & 1;
+    const int base = k * THREADS;
+    const int nch = min(THREADS, tm.n_elem - base);
+    const int64_t e0 = tm.elem_begin + base;  // multiple of 32 elements
+    const uint32_t rs = MIXED ? ((nch + 3) & ~3) : ((nch + 1) & ~1);  // 16-byte multiples
+    const uint32_t bytes_s = rs * (uint32_t)sizeof(S);
+    const uint32_t bytes_c = (uint32_t)((nch + 1) & ~1) * 8u;
+    mbar_arrive_expect_tx(&bars[b], 12u * bytes_s + bytes_c);
+#pragma unroll 1
+    for (int q = 0; q < 12; ++q) bulk_load(stage_s + (b * 12 + q) * THREADS, sdus_g + (int64_t)q * E + e0, bytes_s, &bars[b]);
+    bulk_load(stage_c + b * THREADS, conn_g + e0, bytes_c, &bars[b]);
+  };
+
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    s_abort = 0;
+  }
   for (int ln = tid; ln < tm.n_node; ln += THREADS) {
     const int g = B.tile_nodes[tm.node_begin + ln];
     s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
@@ -102,53 +225,33 @@ __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn
   const double c1nu = P.c1 * P.nu;
   const double nu4 = 4.0 * P.nu;
   __syncthreads();
+  if (tid == 0 && nchunks > 0) issue(0);
 
-  const int64_t E = B.E;
   int c_lo = 0;
-  for (int base = 0; base < tm.n_elem; base += THREADS) {
+  int k = 0;
+  for (; k < nchunks; ++k) {
+    if (tid == 0 && k + 1 < nchunks) {
+      fence_proxy_async_smem();  // buffer (k+1)&1 was last read before the previous barrier
+      issue(k + 1);
+    }
+    if (!mbar_wait_bounded(&bars[k & 1], (uint32_t)((k >> 1) & 1))) s_abort = 1;
+    __syncthreads();
+    if (s_abort) break;
+    const int base = k * THREADS;
     const int le = base + tid;
     const bool active = le < tm.n_elem;
     double lres[4][4];
     int ln[4];
     if (active) {
-      const int64_t e = tm.elem_begin + le;
-      const uint2 cw = __ldg(reinterpret_cast<const uint2*>(B.conn) + e);
+      const uint2 cw = stage_c[(k & 1) * THREADS + tid];
       ln[0] = cw.x & 0xffff; ln[1] = cw.x >> 16; ln[2] = cw.y & 0xffff; ln[3] = cw.y >> 16;
-      double X[4][3], U[4][3], Pn[4];
+      S sd_in[12];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        X[a][0] = s_x[ln[a]]; X[a][1] = s_y[ln[a]]; X[a][2] = s_z[ln[a]];
-      }
-      TetGeom geo;
-      tet_geometry(X, geo);
-      const double ih = rcbrt(6.0 * geo.V);
-      double sdu[4][3];
-#pragma unroll
-      for (int g = 0; g < 4; ++g)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) sdu[g][i] = __ldcs(B.sdus + (int64_t)(g * 3 + i) * E + e);
-      double Q[4][3];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        Q[a][0] = s_qu[ln[a]]; Q[a][1] = s_qv[ln[a]]; Q[a][2] = s_qw[ln[a]];
-      }
-      if (pending) {
-        vms_subscale_update<double>(geo, Q, pq, sdu, inv_dt, c1nu, P.c2, ih);
-#pragma unroll
-        for (int g = 0; g < 4; ++g)
-#pragma unroll
-          for (int i = 0; i < 3; ++i) __stcs(B.sdus + (int64_t)(g * 3 + i) * E + e, sdu[g][i]);
-      }
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        U[a][0] = s_u[ln[a]]; U[a][1] = s_v[ln[a]]; U[a][2] = s_w[ln[a]]; Pn[a] = s_p[ln[a]];
-      }
-      if (first_dual)
-        vms_residual<double, false>(geo, U, Pn, U, sdu, nu4, P.inv_eps, inv_dt, lres);
-      else
-        vms_residual<double, true>(geo, U, Pn, Q, sdu, nu4, P.inv_eps, inv_dt, lres);
+      for (int q = 0; q < 12; ++q) sd_in[q] = stage_s[((k & 1) * 12 + q) * THREADS + tid];
+      vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, s_x, s_y, s_z, s_u, s_v, s_w, s_p, s_qu, s_qv, s_qw,
+                            sd_in, pq, pending, first_dual, inv_dt, c1nu, nu4, lres);
     }
-    // colour rounds over this chunk
+    // colour rounds over this chunk: elements of one colour share no node
     while (c_lo < tm.n_col && s_col[c_lo + 1] <= base) ++c_lo;
     for (int c = c_lo; c < tm.n_col && s_col[c] < base + THREADS; ++c) {
       if (active && le >= s_col[c] && le < s_col[c + 1]) {
@@ -162,8 +265,17 @@ __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn
       }
       __syncthreads();
     }
+    __syncthreads();
   }
-  __syncthreads();
+  if (s_abort) {
+    // a copy never completed: wait (bounded) for the copies this CTA issued,
+    // report, and leave the tile's nodes untouched
+    if (tid == 0) {
+      for (int j = k; j < nchunks && j <= k + 1; ++j) mbar_wait_bounded(&bars[j & 1], (uint32_t)((j >> 1) & 1), 1u << 16);
+      B.pstate[pidx].status = FM_ERR_TIMEOUT;
+    }
+    return;
+  }
   int32_t status = FM_OK;
   for (int ln2 = tid; ln2 < tm.n_node; ln2 += THREADS) {
     const double acc[4] = {s_a0[ln2], s_a1[ln2], s_a2[ln2], s_a3[ln2]};
@@ -200,23 +312,39 @@ __global__ void vms_iface_kernel(DevBatch B) {
   finish_iteration(B);
 }
 
-size_t vms_smem_bytes(int tn_max) { return (size_t)tn_max * 14 * sizeof(double) + 130 * sizeof(int32_t); }
+size_t vms_smem_bytes(int tn_max) {
+  // node arrays + stage (sized for the largest variant: 256 threads, FP64) + colours
+  return (size_t)tn_max * 14 * sizeof(double) + vms_stage_bytes<256, false>() + 130 * sizeof(int32_t);
+}
 
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, cudaStream_t s) {
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, bool mixed,
+                                 cudaStream_t s, cudaEvent_t* ev) {
   const size_t smem = vms_smem_bytes(tn_max);
-  if (threads == 256) {
-    vms_tile_kernel<256><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+  if (ev) cudaEventRecord(ev[0], s);
+  if (mixed) {
+    if (threads == 256)
+      vms_tile_kernel<256, true><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+    else
+      vms_tile_kernel<128, true><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
   } else {
-    vms_tile_kernel<128><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+    if (threads == 256)
+      vms_tile_kernel<256, false><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+    else
+      vms_tile_kernel<128, false><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
   }
+  if (ev) cudaEventRecord(ev[1], s);
   vms_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  if (ev) cudaEventRecord(ev[2], s);
   return cudaGetLastError();
 }
 
 cudaError_t vms_configure(size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(vms_tile_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256, false>, a, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, false>, a, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<256, true>, a, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, true>, a, (int)smem);
+  return e;
 }
 
 }  // namespace fm

@@ -15,11 +15,51 @@ namespace fm {
 const char* last_error();
 size_t vms_smem_bytes(int tn_max);
 cudaError_t vms_configure(size_t smem);
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, cudaStream_t s);
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, bool mixed,
+                                 cudaStream_t s, cudaEvent_t* ev);
+
+// Aspect ratio h_max / (2 sqrt(6) r_in) of a tet (1 for the regular tet,
+// about 1.7 for a Kuhn tet); r_in = 3V / (sum of face areas).
+static double tet_aspect_ratio(const double* X, const int32_t* c) {
+  double p[4][3];
+  for (int a = 0; a < 4; ++a)
+    for (int k = 0; k < 3; ++k) p[a][k] = X[(int64_t)c[a] * 3 + k];
+  auto sub = [](const double* a, const double* b, double* r) {
+    for (int k = 0; k < 3; ++k) r[k] = a[k] - b[k];
+  };
+  auto cross_norm = [](const double* u, const double* v) {
+    double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2], z = u[0] * v[1] - u[1] * v[0];
+    return std::sqrt(x * x + y * y + z * z);
+  };
+  double hmax = 0.0;
+  for (int a = 0; a < 4; ++a)
+    for (int b2 = a + 1; b2 < 4; ++b2) {
+      double d[3];
+      sub(p[a], p[b2], d);
+      hmax = std::max(hmax, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+    }
+  double e1[3], e2[3], e3[3];
+  sub(p[1], p[0], e1);
+  sub(p[2], p[0], e2);
+  sub(p[3], p[0], e3);
+  const double vol6 = std::fabs(e1[0] * (e2[1] * e3[2] - e2[2] * e3[1]) - e1[1] * (e2[0] * e3[2] - e2[2] * e3[0]) +
+                                e1[2] * (e2[0] * e3[1] - e2[1] * e3[0]));
+  static const int f[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+  double area = 0.0;
+  for (int k = 0; k < 4; ++k) {
+    double u[3], v[3];
+    sub(p[f[k][1]], p[f[k][0]], u);
+    sub(p[f[k][2]], p[f[k][0]], v);
+    area += 0.5 * cross_norm(u, v);
+  }
+  if (!(vol6 > 0.0)) return 1e300;
+  const double r_in = 3.0 * (vol6 / 6.0) / area;
+  return hmax / (2.0 * std::sqrt(6.0) * r_in);
+}
 size_t supg_smem_bytes(int tn_max, int npe);
 cudaError_t supg_configure(size_t smem, int npe);
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool write_diag,
-                             cudaStream_t s);
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, cudaStream_t s,
+                             cudaEvent_t* ev);
 cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
 }  // namespace fm
 
@@ -399,8 +439,31 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
   UP(dconn, L.conn_local);
   D.conn = dconn;
   D.E = NE;
-  const int nhist = solver == FM_SOLVER_VMS ? 12 : 3 * npe;
-  {
+  // Per-element history: VMS subscales (12 per element, FP64 or FP32 in the
+  // mixed form); SUPG the previous step's element forces for AB2 (3*npe).
+  bool any_ab2 = false;
+  for (int pi = 0; pi < n; ++pi) any_ab2 |= (probs[pi]->params.ex_opts[0] == 0);
+  if (solver == FM_SOLVER_VMS && prec == FM_MIXED) {
+    r = dalloc(b, (void**)&D.sdus32, (size_t)NE * 12 * sizeof(float));
+    if (r) { release(b); delete b; return r; }
+    CK(cudaMemset(D.sdus32, 0, (size_t)NE * 12 * sizeof(float)));
+    // elements whose Jacobian inverse stays in FP64 (aspect ratio above the limit)
+    std::vector<unsigned char> hprec(NE, 0);
+    for (int pi = 0; pi < n; ++pi) {
+      fm_problem* p = probs[pi];
+      for (int64_t k = 0; k < L.elem_count[pi]; ++k) {
+        const int32_t oe = L.elem_old[pi][k];
+        if (oe >= 0)
+          hprec[L.elem_begin[pi] + k] =
+              tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT;
+      }
+    }
+    unsigned char* dprec;
+    r = upload(b, &dprec, hprec);
+    if (r) { release(b); delete b; return r; }
+    D.precise = dprec;
+  } else if (solver == FM_SOLVER_VMS || any_ab2) {
+    const int nhist = solver == FM_SOLVER_VMS ? 12 : 3 * npe;
     r = dalloc(b, (void**)&D.sdus, (size_t)NE * nhist * sizeof(double));
     if (r) { release(b); delete b; return r; }
     CK(cudaMemset(D.sdus, 0, (size_t)NE * nhist * sizeof(double)));
@@ -486,7 +549,10 @@ int fm_batch_destroy(fm_batch* b) {
 }
 
 // Sets per-problem targets (iterations) and launches enough iterations.
-static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cudaStream_t s) {
+// With prof != nullptr every kernel is bracketed by CUDA events and the
+// per-kernel device times are summed into prof[0] (element/tile kernel) and
+// prof[1] (interface kernel), in milliseconds.
+static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cudaStream_t s, double* prof = nullptr) {
   const int n = (int)b->probs.size();
   int32_t maxit = 0;
   for (int i = 0; i < n; ++i) maxit = std::max(maxit, add_iters[i]);
@@ -498,17 +564,35 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
   CK(cudaEventRecord(b->ev_tgt, s));
   CK(cudaEventRecord(b->ev0, s));
   int64_t launches = 0;
+  std::vector<cudaEvent_t> evs;
+  if (prof) {
+    evs.resize((size_t)maxit * 3);
+    for (auto& e : evs) CK(cudaEventCreate(&e));
+  }
   for (int it = 0; it < maxit; ++it) {
     cudaError_t e;
+    cudaEvent_t* ev = prof ? &evs[(size_t)it * 3] : nullptr;
     if (b->solver == FM_SOLVER_VMS) {
-      e = launch_vms_iteration(b->D, b->tn_max, b->threads, b->iface_blocks, s);
+      e = launch_vms_iteration(b->D, b->tn_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s, ev);
     } else {
-      e = launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, it == maxit - 1, s);
+      e = launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, s, ev);
     }
     if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     launches += 2;
   }
   CK(cudaEventRecord(b->ev1, s));
+  if (prof) {
+    CK(cudaEventSynchronize(b->ev1));
+    prof[0] = prof[1] = 0.0;
+    for (int it = 0; it < maxit; ++it) {
+      float a = 0.f, c = 0.f;
+      CK(cudaEventElapsedTime(&a, evs[it * 3], evs[it * 3 + 1]));
+      CK(cudaEventElapsedTime(&c, evs[it * 3 + 1], evs[it * 3 + 2]));
+      prof[0] += a;
+      prof[1] += c;
+    }
+    for (auto& e : evs) cudaEventDestroy(e);
+  }
   b->last_launches = launches;
   b->timed = true;
   for (int i = 0; i < n; ++i) b->iters[i] += add_iters[i];
@@ -529,6 +613,32 @@ int fm_batch_step_ragged(fm_batch* b, const int32_t* nsteps, void* stream) {
   int r = run_iterations(b, add, s);
   if (r) return r;
   for (int i = 0; i < n; ++i) b->probs[i]->steps_done += nsteps[i];
+  return FM_OK;
+}
+
+int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* launches) {
+  if (!b || nsteps < 0) return fail(FM_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(b->device));
+  const int n = (int)b->probs.size();
+  std::vector<int32_t> add(n);
+  int64_t per_kernel = 0;
+  for (int i = 0; i < n; ++i) {
+    const int per = b->solver == FM_SOLVER_VMS ? b->probs[i]->params.tot_dual_steps + 1 : 1;
+    add[i] = nsteps * std::max(1, per);
+    per_kernel = std::max<int64_t>(per_kernel, add[i]);
+  }
+  double prof[2] = {0.0, 0.0};
+  int r = run_iterations(b, add, b->stream, prof);
+  if (r) return r;
+  for (int i = 0; i < n; ++i) b->probs[i]->steps_done += nsteps;
+  if (kernel_ms) {
+    kernel_ms[0] = prof[0];
+    kernel_ms[1] = prof[1];
+  }
+  if (launches) {
+    launches[0] = per_kernel;
+    launches[1] = per_kernel;
+  }
   return FM_OK;
 }
 
@@ -583,7 +693,7 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
   CK(cudaStreamSynchronize(b->stream));
   const int pi = p->index;
   const int64_t nb = b->L.node_begin[pi], eb = b->L.elem_begin[pi];
-  const int64_t N = p->N, E = p->E;
+  const int64_t N = p->N, E = p->E, EC = b->L.elem_count[pi];
   const std::vector<int32_t>& nn = b->L.node_new[pi];
   const std::vector<int32_t>& eo = b->L.elem_old[pi];
   std::vector<double> tmp(N);
@@ -604,11 +714,19 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
       for (int64_t i = 0; i < N; ++i) pres[i] = tmp[nn[i] - nb];
     }
     if (elem3 || sdus) {
-      std::vector<double> h((size_t)E * 12), col(E);
+      std::vector<double> h((size_t)E * 12), col(EC);
+      std::vector<float> colf(b->D.sdus32 ? EC : 0);
       for (int q = 0; q < 12; ++q) {
-        CK(cudaMemcpy(col.data(), b->D.sdus + (int64_t)q * b->L.n_elems + eb, sizeof(double) * E,
-                      cudaMemcpyDeviceToHost));
-        for (int64_t k = 0; k < E; ++k) h[(size_t)eo[k] * 12 + q] = col[k];
+        if (b->D.sdus32) {
+          CK(cudaMemcpy(colf.data(), b->D.sdus32 + (int64_t)q * b->L.n_elems + eb, sizeof(float) * EC,
+                        cudaMemcpyDeviceToHost));
+          for (int64_t k = 0; k < EC; ++k) col[k] = colf[k];
+        } else {
+          CK(cudaMemcpy(col.data(), b->D.sdus + (int64_t)q * b->L.n_elems + eb, sizeof(double) * EC,
+                        cudaMemcpyDeviceToHost));
+        }
+        for (int64_t k = 0; k < EC; ++k)
+          if (eo[k] >= 0) h[(size_t)eo[k] * 12 + q] = col[k];
       }
       if (sdus) memcpy(sdus, h.data(), sizeof(double) * E * 12);
       if (elem3)
@@ -625,15 +743,17 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
       cudaError_t e = launch_supg_pressure(b->D, b->tn_max, b->npe, b->d_scratch, b->stream);
       if (e != cudaSuccess) return fail(FM_ERR_CUDA, cudaGetErrorString(e));
       CK(cudaStreamSynchronize(b->stream));
-      std::vector<double> col(E);
-      CK(cudaMemcpy(col.data(), b->d_scratch + eb, sizeof(double) * E, cudaMemcpyDeviceToHost));
-      for (int64_t k = 0; k < E; ++k) pres[eo[k]] = col[k];
+      std::vector<double> col(EC);
+      CK(cudaMemcpy(col.data(), b->d_scratch + eb, sizeof(double) * EC, cudaMemcpyDeviceToHost));
+      for (int64_t k = 0; k < EC; ++k)
+        if (eo[k] >= 0) pres[eo[k]] = col[k];
     }
     if (elem3) {
-      std::vector<double> c1(E), c2(E);
-      CK(cudaMemcpy(c1.data(), b->D.el_lam + eb, sizeof(double) * E, cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(c2.data(), b->D.el_reg + eb, sizeof(double) * E, cudaMemcpyDeviceToHost));
-      for (int64_t k = 0; k < E; ++k) {
+      std::vector<double> c1(EC), c2(EC);
+      CK(cudaMemcpy(c1.data(), b->D.el_lam + eb, sizeof(double) * EC, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(c2.data(), b->D.el_reg + eb, sizeof(double) * EC, cudaMemcpyDeviceToHost));
+      for (int64_t k = 0; k < EC; ++k) {
+        if (eo[k] < 0) continue;
         elem3[(int64_t)eo[k] * 2 + 0] = c1[k];
         elem3[(int64_t)eo[k] * 2 + 1] = c2[k];
       }

@@ -190,4 +190,177 @@ __device__ __forceinline__ void vms_residual(const TetGeom& geo, const T U[4][3]
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed precision (FM_MIXED).  Gauss-point work in FP32; kept in FP64: the
+// element volume (it weights the FP64 nodal accumulation), the Jacobian
+// inverse of badly shaped elements (aspect ratio above FM_MIXED_ASPECT_LIMIT,
+// flagged on the host), the pressure-gradient term, the nodal accumulation,
+// the lumped-mass division and the state.  Nodal velocities enter FP32 as
+// differences to the element's first node (formed in FP64), so the velocity
+// gradient does not lose digits to cancellation.
+// ---------------------------------------------------------------------------
+struct TetGeomF {
+  float DN[3][4];
+  double V;
+};
+
+__device__ __forceinline__ void tet_geometry_mixed(const double X[4][3], bool precise, TetGeomF& g) {
+  double j[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) j[i][k] = X[k + 1][i] - X[0][i];
+  const double c00 = j[1][1] * j[2][2] - j[2][1] * j[1][2];
+  const double c01 = j[2][0] * j[1][2] - j[1][0] * j[2][2];
+  const double c02 = j[1][0] * j[2][1] - j[2][0] * j[1][1];
+  const double det = j[0][0] * c00 + j[0][1] * c01 + j[0][2] * c02;
+  g.V = det / 6.0;
+  float inv[3][3];
+  if (precise) {
+    const double id = 1.0 / det;
+    const double c10 = j[2][1] * j[0][2] - j[0][1] * j[2][2];
+    const double c11 = j[0][0] * j[2][2] - j[2][0] * j[0][2];
+    const double c12 = j[2][0] * j[0][1] - j[0][0] * j[2][1];
+    const double c20 = j[0][1] * j[1][2] - j[1][1] * j[0][2];
+    const double c21 = j[1][0] * j[0][2] - j[0][0] * j[1][2];
+    const double c22 = j[0][0] * j[1][1] - j[1][0] * j[0][1];
+    inv[0][0] = (float)(c00 * id); inv[0][1] = (float)(c10 * id); inv[0][2] = (float)(c20 * id);
+    inv[1][0] = (float)(c01 * id); inv[1][1] = (float)(c11 * id); inv[1][2] = (float)(c21 * id);
+    inv[2][0] = (float)(c02 * id); inv[2][1] = (float)(c12 * id); inv[2][2] = (float)(c22 * id);
+  } else {
+    float f[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) f[i][k] = (float)j[i][k];
+    const float d00 = f[1][1] * f[2][2] - f[2][1] * f[1][2];
+    const float d01 = f[2][0] * f[1][2] - f[1][0] * f[2][2];
+    const float d02 = f[1][0] * f[2][1] - f[2][0] * f[1][1];
+    const float d10 = f[2][1] * f[0][2] - f[0][1] * f[2][2];
+    const float d11 = f[0][0] * f[2][2] - f[2][0] * f[0][2];
+    const float d12 = f[2][0] * f[0][1] - f[0][0] * f[2][1];
+    const float d20 = f[0][1] * f[1][2] - f[1][1] * f[0][2];
+    const float d21 = f[1][0] * f[0][2] - f[0][0] * f[1][2];
+    const float d22 = f[0][0] * f[1][1] - f[1][0] * f[0][1];
+    const float id = 1.0f / (float)det;
+    inv[0][0] = d00 * id; inv[0][1] = d10 * id; inv[0][2] = d20 * id;
+    inv[1][0] = d01 * id; inv[1][1] = d11 * id; inv[1][2] = d21 * id;
+    inv[2][0] = d02 * id; inv[2][1] = d12 * id; inv[2][2] = d22 * id;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    g.DN[i][0] = -inv[0][i] - inv[1][i] - inv[2][i];
+    g.DN[i][1] = inv[0][i];
+    g.DN[i][2] = inv[1][i];
+    g.DN[i][3] = inv[2][i];
+  }
+}
+
+// Subscale update, FP32.  U0: velocity of node 0; Ud[a] = U[a] - U0 (Ud[0] = 0);
+// pqd[a] = pq[a] - pq[0].
+__device__ __forceinline__ void vms_subscale_update_mixed(const TetGeomF& geo, const float U0[3], const float Ud[4][3],
+                                                          const float pqd[4], float sdu[4][3], float inv_dt, float c1nu,
+                                                          float c2, float ih) {
+  const float A = (float)FM_VA, Bt = (float)FM_VB, AB = (float)(FM_VA - FM_VB);
+  const float S = A + 3.0f * Bt;
+  float G[3][3], gp[3], Ds[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) G[i][j] = geo.DN[j][1] * Ud[1][i] + geo.DN[j][2] * Ud[2][i] + geo.DN[j][3] * Ud[3][i];
+    gp[i] = geo.DN[i][1] * pqd[1] + geo.DN[i][2] * pqd[2] + geo.DN[i][3] * pqd[3];
+    Ds[i] = Ud[1][i] + Ud[2][i] + Ud[3][i];
+  }
+  float r[4][3];
+  float maxa2 = 0.0f;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    float hah[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) hah[i] = S * U0[i] + Bt * Ds[i] + AB * Ud[g][i] + sdu[g][i];
+    const float a2 = hah[0] * hah[0] + hah[1] * hah[1] + hah[2] * hah[2];
+    maxa2 = fmaxf(a2, maxa2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2] + gp[i];
+  }
+  const float invS = 1.0f / S;
+  const float tau1 = 1.0f / (inv_dt + c1nu * ih * ih + c2 * sqrtf(maxa2) * ih);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);
+    float Pa[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) Pa[a] = (Bt * R + AB * r[a][i]) * invS;
+    const float Ps = (Pa[0] + Pa[1]) + (Pa[2] + Pa[3]);
+#pragma unroll
+    for (int g = 0; g < 4; ++g) sdu[g][i] = ((sdu[g][i] * inv_dt - r[g][i]) + (Bt * Ps + AB * Pa[g])) * tau1;
+  }
+}
+
+// Element residual, FP32 Gauss-point work with FP64 output.  P: nodal
+// pressures (FP64, the pressure-gradient term is formed in FP64); Dacc[a] =
+// U[a] - Uprev[a] (only with HAS_PREV).
+template <bool HAS_PREV>
+__device__ __forceinline__ void vms_residual_mixed(const TetGeomF& geo, const float U0[3], const float Ud[4][3],
+                                                   const double P[4], const float Dacc[4][3], const float sdu[4][3],
+                                                   float nu4, float inv_eps, float inv_dt, double lRes[4][4]) {
+  const float A = (float)FM_VA, Bt = (float)FM_VB, AB = (float)(FM_VA - FM_VB);
+  const float S = A + 3.0f * Bt;
+  float G[3][3], Ds[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) G[i][j] = geo.DN[j][1] * Ud[1][i] + geo.DN[j][2] * Ud[2][i] + geo.DN[j][3] * Ud[3][i];
+    Ds[i] = Ud[1][i] + Ud[2][i] + Ud[3][i];
+  }
+  const float tr = (G[0][0] + G[1][1]) + G[2][2];
+  float X[4][3], M2[3][3], Ssdu[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    Ssdu[i] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) M2[i][k] = 0.0f;
+  }
+  float Dsum[3];
+  if (HAS_PREV) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Dsum[i] = (Dacc[0][i] + Dacc[1][i]) + (Dacc[2][i] + Dacc[3][i]);
+  }
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    float hah[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) hah[i] = S * U0[i] + Bt * Ds[i] + AB * Ud[g][i] + sdu[g][i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      X[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2];
+      if (HAS_PREV) X[g][i] += (Bt * Dsum[i] + AB * Dacc[g][i]) * inv_dt;
+      Ssdu[i] += sdu[g][i];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) M2[i][k] += sdu[g][i] * hah[k];
+    }
+  }
+  float Kp[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Kp[i][k] = nu4 * G[i][k] - M2[i][k];
+  const double w = geo.V * 0.25;
+  const double Hs = (double)S * ((P[0] + P[1]) + (P[2] + P[3]));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float Xs = (X[0][i] + X[1][i]) + (X[2][i] + X[3][i]);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const float v = Bt * Xs + AB * X[a][i] + Kp[i][0] * geo.DN[0][a] + Kp[i][1] * geo.DN[1][a] + Kp[i][2] * geo.DN[2][a];
+      lRes[a][i] = w * ((double)v - Hs * (double)geo.DN[i][a]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const float v = tr * S - (Ssdu[0] * geo.DN[0][a] + Ssdu[1] * geo.DN[1][a] + Ssdu[2] * geo.DN[2][a]);
+    lRes[a][3] = w * (double)(inv_eps * v);
+  }
+}
+
 }  // namespace fm

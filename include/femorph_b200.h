@@ -49,6 +49,9 @@ enum {
 enum { FM_TET4 = 4, FM_HEXA8 = 8 };
 enum { FM_SOLVER_VMS = 0, FM_SOLVER_SUPG = 1 };
 enum { FM_FP64 = 0, FM_MIXED = 1 };
+/* FM_MIXED: tets whose aspect ratio h_max / (2 sqrt(6) r_in) exceeds this
+ * limit keep their Jacobian inverse in FP64 (regular tet 1.0, Kuhn tet 1.7). */
+#define FM_MIXED_ASPECT_LIMIT 3.0
 /* NODEDOF global fixed dofs (femSUPGExplicitFluidSolver.cpp:1527-1561) */
 enum { FM_FIX_NONE = 0, FM_FIX_X = 1, FM_FIX_Y = 2, FM_FIX_Z = 4 };
 
@@ -172,6 +175,12 @@ FM_API int fm_problem_get_mass(fm_problem* p, double* mass);
  * milliseconds and the number of kernel launches (CUDA events on the batch
  * stream; valid after fm_batch_sync). */
 FM_API int fm_batch_last_timing(fm_batch* b, double* ms, int64_t* launches);
+
+/* Advances the batch by nsteps like fm_batch_step, bracketing every kernel
+ * launch with CUDA events on the batch stream, and returns the summed device
+ * time of the element (tile) kernel in kernel_ms[0] and of the interface
+ * kernel in kernel_ms[1], with their launch counts.  Synchronous. */
+FM_API int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* launches);
 
 /* Bytes of device memory a batch of these problems needs (admission). */
 FM_API int fm_batch_estimate_bytes(fm_problem* const* problems, int32_t n, const fm_tuning* tuning, int64_t* bytes);

@@ -32,3 +32,14 @@ g++ $CXXFLAGS -DFM_EXPORT_SYM="\"$EXPORT_SYM\"" -DFM_SETVEL_SYM="\"$SETVEL_SYM\"
   "$HERE/refdrv.cpp" "$OBJ"/*.o -o "$OUT/fm_refdrv" \
   -Wl,--wrap="$EXPORT_SYM" -Wl,--wrap="$SETVEL_SYM"
 echo "built $OUT/fm_refdrv"
+# Drop-in check binary: the same driver linked with femorph_b200's femSolver
+# adapters (femorph_b200/adapter) and libfemorph_b200.so.
+LIBDIR=$HERE/../femorph_b200
+if [ -f "$LIBDIR/libfemorph_b200.so" ]; then
+  g++ $CXXFLAGS -DFM_WITH_GPU_ADAPTER -I"$LIBDIR/adapter" -I"$HERE/../include" \
+    -DFM_EXPORT_SYM="\"$EXPORT_SYM\"" -DFM_SETVEL_SYM="\"$SETVEL_SYM\"" \
+    "$HERE/refdrv.cpp" "$LIBDIR/adapter/femExplicitFluidSolverGPU.cpp" "$OBJ"/*.o -o "$OUT/fm_gpudrv" \
+    -L"$LIBDIR" -lfemorph_b200 -Wl,-rpath,'$ORIGIN/../../femorph_b200' \
+    -Wl,--wrap="$EXPORT_SYM" -Wl,--wrap="$SETVEL_SYM"
+  echo "built $OUT/fm_gpudrv"
+fi

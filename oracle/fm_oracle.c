@@ -867,6 +867,15 @@ int fmo_get(void* h, double* state, double* elem, double* sdus, double* time_out
   return c->err;
 }
 
+/* VMS: the state before the last BC application (sol_prev after
+   update_solution), N x 4. */
+int fmo_get_prebc(void* h, double* state) {
+  fmo_ctx* c = (fmo_ctx*)h;
+  if (c->solver != 0) return FMO_ERR_INVALID;
+  memcpy(state, c->sol_prev, sizeof(double) * c->N * 4);
+  return 0;
+}
+
 void fmo_destroy(void* h) {
   fmo_ctx* c = (fmo_ctx*)h;
   if (!c) return;

@@ -30,6 +30,12 @@
 #include "femModel.h"
 #include "femSUPGExplicitFluidSolver.h"
 #include "femVMSExplicitFluidSolver.h"
+#ifdef FM_WITH_GPU_ADAPTER
+// Drop-in check: the same driver with femorph_b200's femSolver adapters
+// ("vms-gpu", "supg-gpu"), i.e. the reference's reader and VTK exporter
+// around the B200 solver.
+#include "femExplicitFluidSolverGPU.h"
+#endif
 
 void real_export(femModel*, std::string, bool) __asm__("__real_" FM_EXPORT_SYM);
 void real_setvel(femModel*, double, femDoubleMat&) __asm__("__real_" FM_SETVEL_SYM);
@@ -150,6 +156,14 @@ int main(int argc, char** argv) {
     } else if (solver == "supg") {
       femSUPGExplicitFluidSolver* s = new femSUPGExplicitFluidSolver();
       s->solve(model);
+#ifdef FM_WITH_GPU_ADAPTER
+    } else if (solver == "vms-gpu" || solver == "vms-gpu-mixed") {
+      femVMSExplicitFluidSolverGPU* s = new femVMSExplicitFluidSolverGPU(0, solver == "vms-gpu-mixed");
+      s->solve(model);
+    } else if (solver == "supg-gpu") {
+      femSUPGExplicitFluidSolverGPU* s = new femSUPGExplicitFluidSolverGPU(0, false);
+      s->solve(model);
+#endif
     } else {
       fprintf(stderr, "unknown solver %s\n", solver.c_str());
       return 2;

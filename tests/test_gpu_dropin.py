@@ -1,0 +1,85 @@
+"""Drop-in check: the reference's own driver path (femModel::ReadFromFEMTextFile
+-> solver.solve(model) -> femModel::ExportToVTKLegacy) with the reference
+solver classes (oracle/_ref/fm_refdrv) and with femorph_b200's femSolver
+adapters (oracle/_ref/fm_gpudrv, the same objects plus
+femorph_b200/adapter), compared step by step on the full-precision dumps of
+every exported result."""
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from femorph_b200 import mesh
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+GPUDRV = os.path.join(os.path.dirname(ref.REFDRV), "fm_gpudrv")
+
+
+def _run(binary, dat, solver, wd):
+    os.makedirs(wd, exist_ok=True)
+    r = subprocess.run([binary, dat, solver, "--dump", wd], cwd=wd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:] + r.stdout[-2000:]
+    out = {}
+    for fn in os.listdir(wd):
+        if fn.endswith(".vtk.f64"):
+            step = int(fn.split("_")[-1].split(".")[0])
+            out[step] = ref.read_dump(os.path.join(wd, fn))
+    return out
+
+
+def _rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+@pytest.fixture
+def workdir():
+    d = tempfile.mkdtemp(prefix="fm_dropin_")
+    yield d
+    shutil.rmtree(d, ignore_errors=True)
+
+
+def _need():
+    if not (ref.available() and os.path.exists(GPUDRV)):
+        pytest.skip("oracle/_ref binaries not built")
+
+
+def test_dropin_vms(workdir):
+    _need()
+    p = mesh.cavity(5, seed=2, steps=6)
+    p.init_state = None
+    p.save_every = 2
+    dat = os.path.join(workdir, "model.dat")
+    mesh.write_dat(p, dat)
+    A = _run(ref.REFDRV, dat, "vms", os.path.join(workdir, "ref"))
+    G = _run(GPUDRV, dat, "vms-gpu", os.path.join(workdir, "gpu"))
+    assert sorted(A) == sorted(G) == [0, 3, 5]
+    for s in A:
+        for lab in ("velocity", "pressure"):
+            assert _rel(G[s][lab], A[s][lab]) <= 1e-12, (s, lab)
+        if s > 0:
+            # centroid average of the Gauss-point subscales: zero up to rounding
+            # by construction of the orthogonal subscale, so checked absolutely
+            assert np.abs(G[s]["subgrid_u"] - A[s]["subgrid_u"]).max() <= 1e-16
+
+
+def test_dropin_supg_hexa(workdir):
+    _need()
+    p = mesh.channel(6, 3, 3, seed=1, steps=5)
+    p.init_state = None
+    p.save_every = 1
+    dat = os.path.join(workdir, "model.dat")
+    mesh.write_dat(p, dat)
+    A = _run(ref.REFDRV, dat, "supg", os.path.join(workdir, "ref"))
+    G = _run(GPUDRV, dat, "supg-gpu", os.path.join(workdir, "gpu"))
+    assert sorted(A) == sorted(G)
+    for s in A:
+        assert _rel(G[s]["velocity"], A[s]["velocity"]) <= 1e-12, s
+        assert _rel(G[s]["pressure"], A[s]["pressure"]) <= 1e-11, s
+        if s > 0:
+            assert _rel(G[s]["lambda"], A[s]["lambda"]) <= 1e-11, s
+            assert np.array_equal(G[s]["regime"], A[s]["regime"]), s

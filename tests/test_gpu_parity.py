@@ -24,26 +24,38 @@ def rel(a, b):
 
 
 def run_pair(p, steps, check_every=1, **tuning):
+    """Steps the GPU solve and the oracle side by side; yields per checked step
+    (step, rel L2 velocity, rel L2 pressure, subscale/lambda error).
+
+    VMS subscales: the GPU keeps the subscales the last residual pass read,
+    i.e. those after the subscale update of the previous step, which the
+    oracle returns one step earlier; their relative L2 difference is reported.
+    (The centroid average the reference writes as subgrid_u is a sum of the
+    four Gauss-point subscales, which the orthogonal projection makes vanish
+    up to rounding, so it is only checked in absolute terms.)"""
     g = api.GpuProblem(p)
     b = api.Batch([g], **tuning)
     o = oracle_b.OracleSolve(p)
-    worst = 0.0
+    prev_sd = np.zeros((p.n_elems, 12))
     for s in range(1, steps + 1):
         b.step(1)
         o.step(1)
         if s % check_every == 0 or s == steps:
             b.sync()
-            u, pr, el, _ = g.state()
-            st, oel, _, _ = o.state()
+            u, pr, el, sd = g.state()
+            st, oel, osd, _ = o.state()
             eu = rel(u, st[:, :3])
             if p.solver == mesh.VMS:
                 ep = rel(pr, st[:, 3])
-                es = rel(el, oel)
+                es = rel(sd, prev_sd)
+                scale = max(np.abs(prev_sd).max(), 1e-300)
+                assert np.abs(el - oel).max() <= 1e-13 * scale + 1e-300, s
             else:
                 ep = rel(pr, oel[:, 0])
                 es = rel(el[:, 0], oel[:, 1])
-            worst = max(worst, eu, ep)
             yield s, eu, ep, es
+        if p.solver == mesh.VMS:
+            prev_sd = o.state()[2].reshape(-1).reshape(12, p.n_elems).T.copy()
     b.close()
     g.close()
 
@@ -141,6 +153,41 @@ def test_supg_tet_cavity():
     for s, eu, ep, es in run_pair(p, 6):
         assert eu <= TOL_STEP, (s, eu)
         assert ep <= 1e-11, (s, ep)
+
+
+def test_vms_mixed_precision_200_steps():
+    """Mixed form (FP32 Gauss-point work and subscales, FP64 accumulation and
+    state) against the FP64 oracle after 200 steps of config 1: <= 1e-6."""
+    p = mesh.cavity(16, seed=0, steps=200)
+    g = api.GpuProblem(p, api.FM_MIXED)
+    b = api.Batch([g])
+    b.step(200)
+    b.sync()
+    u, pr, _, _ = g.state()
+    o = oracle_b.OracleSolve(p)
+    o.step(200)
+    st, _, _, _ = o.state()
+    eu, ep = rel(u, st[:, :3]), rel(pr, st[:, 3])
+    print(f"mixed vs FP64 after 200 steps: u {eu:.3e} p {ep:.3e}")
+    assert eu <= 1e-6 and ep <= 1e-6, (eu, ep)
+
+
+def test_vms_mixed_badly_shaped_elements():
+    """Strong jitter makes slivers: those elements take the FP64 Jacobian
+    inverse; the mixed result stays within 1e-6 of FP64 after 20 steps."""
+    from femorph_b200.mesh import kuhn_cavity_mesh
+    p = mesh.cavity(6, seed=3, steps=20)
+    X, conn, _ = kuhn_cavity_mesh(6, seed=3, jitter=0.3)  # ~4% of tets above aspect ratio 3
+    p.coords, p.conn = X, conn
+    g = api.GpuProblem(p, api.FM_MIXED)
+    b = api.Batch([g])
+    b.step(20)
+    b.sync()
+    o = oracle_b.OracleSolve(p)
+    o.step(20)
+    st, _, _, _ = o.state()
+    u, pr, _, _ = g.state()
+    assert rel(u, st[:, :3]) <= 1e-6 and rel(pr, st[:, 3]) <= 1e-6
 
 
 def test_divergence_reported_not_hung():
