@@ -113,7 +113,8 @@ def run_ours(args, rank, world, local_rank, dist):
     p = make_problem(args.n, seed=rank)
     E, N = p.n_elems, p.n_nodes
     g = api.GpuProblem(p, prec)
-    b = api.Batch([g], device=local_rank)
+    tune = dict(tile_elems=args.tile_elems, tile_nodes=args.tile_nodes, threads=args.threads)
+    b = api.Batch([g], device=local_rank, **tune)
     b.step(args.warmup)
     b.sync()
     if dist:
@@ -138,7 +139,7 @@ def run_ours(args, rank, world, local_rank, dist):
     if rank == 0:
         t0 = time.perf_counter()
         g2 = api.GpuProblem(p, prec)
-        b2 = api.Batch([g2], device=local_rank)
+        b2 = api.Batch([g2], device=local_rank, **tune)
         b2.step(args.steps)
         b2.sync()
         u, pr, _, _ = g2.state()
@@ -219,6 +220,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--ref-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile-elems", type=int, default=0)
+    ap.add_argument("--tile-nodes", type=int, default=0)
+    ap.add_argument("--threads", type=int, default=0)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

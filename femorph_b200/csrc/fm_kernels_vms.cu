@@ -145,7 +145,8 @@ __host__ __device__ constexpr size_t vms_stage_bytes() {
 }
 
 template <int THREADS, bool MIXED>
-__global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn_max) {
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (MIXED ? 2 : 1))
+    vms_tile_kernel(DevBatch B, int tn_max) {
   using S = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) double sm[];
   double* s_x = sm;
@@ -234,12 +235,13 @@ __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn
       fence_proxy_async_smem();  // buffer (k+1)&1 was last read before the previous barrier
       issue(k + 1);
     }
-    if (!mbar_wait_bounded(&bars[k & 1], (uint32_t)((k >> 1) & 1))) s_abort = 1;
-    __syncthreads();
-    if (s_abort) break;
+    // each thread waits for the chunk itself (the mbarrier phase makes the
+    // bulk-copied bytes visible to it); a timed-out wait skips the chunk and
+    // is agreed on at the end-of-chunk barrier
+    const bool arrived = mbar_wait_bounded(&bars[k & 1], (uint32_t)((k >> 1) & 1));
     const int base = k * THREADS;
     const int le = base + tid;
-    const bool active = le < tm.n_elem;
+    const bool active = arrived && le < tm.n_elem;
     double lres[4][4];
     int ln[4];
     if (active) {
@@ -265,8 +267,13 @@ __global__ void __launch_bounds__(THREADS, 2) vms_tile_kernel(DevBatch B, int tn
       }
       __syncthreads();
     }
-    __syncthreads();
+    // end of chunk: stage buffer k&1 is free again; any timed-out wait aborts
+    if (__syncthreads_or(!arrived)) {
+      if (tid == 0) s_abort = 1;
+      break;
+    }
   }
+  __syncthreads();
   if (s_abort) {
     // a copy never completed: wait (bounded) for the copies this CTA issued,
     // report, and leave the tile's nodes untouched
@@ -312,14 +319,16 @@ __global__ void vms_iface_kernel(DevBatch B) {
   finish_iteration(B);
 }
 
-size_t vms_smem_bytes(int tn_max) {
-  // node arrays + stage (sized for the largest variant: 256 threads, FP64) + colours
-  return (size_t)tn_max * 14 * sizeof(double) + vms_stage_bytes<256, false>() + 130 * sizeof(int32_t);
+size_t vms_smem_bytes(int tn_max, int threads, bool mixed) {
+  // node arrays + double-buffered chunk stage of this variant + colour offsets
+  size_t stage = threads == 256 ? (mixed ? vms_stage_bytes<256, true>() : vms_stage_bytes<256, false>())
+                                : (mixed ? vms_stage_bytes<128, true>() : vms_stage_bytes<128, false>());
+  return (size_t)tn_max * 14 * sizeof(double) + stage + 130 * sizeof(int32_t);
 }
 
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, bool mixed,
                                  cudaStream_t s, cudaEvent_t* ev) {
-  const size_t smem = vms_smem_bytes(tn_max);
+  const size_t smem = vms_smem_bytes(tn_max, threads, mixed);
   if (ev) cudaEventRecord(ev[0], s);
   if (mixed) {
     if (threads == 256)
@@ -338,12 +347,12 @@ cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int
   return cudaGetLastError();
 }
 
-cudaError_t vms_configure(size_t smem) {
+cudaError_t vms_configure(int tn_max) {
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256, false>, a, (int)smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, false>, a, (int)smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<256, true>, a, (int)smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, true>, a, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256, false>, a, (int)vms_smem_bytes(tn_max, 256, false));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, false>, a, (int)vms_smem_bytes(tn_max, 128, false));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<256, true>, a, (int)vms_smem_bytes(tn_max, 256, true));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, true>, a, (int)vms_smem_bytes(tn_max, 128, true));
   return e;
 }
 

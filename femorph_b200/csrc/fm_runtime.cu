@@ -13,8 +13,8 @@
 
 namespace fm {
 const char* last_error();
-size_t vms_smem_bytes(int tn_max);
-cudaError_t vms_configure(size_t smem);
+size_t vms_smem_bytes(int tn_max, int threads, bool mixed);
+cudaError_t vms_configure(int tn_max);
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, bool mixed,
                                  cudaStream_t s, cudaEvent_t* ev);
 
@@ -278,12 +278,13 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
   }
   Layout& L = b->L;
   for (auto& tm : L.tiles) b->tn_max = std::max(b->tn_max, tm.n_node);
-  size_t smem = solver == FM_SOLVER_VMS ? vms_smem_bytes(b->tn_max) : supg_smem_bytes(b->tn_max, npe);
+  size_t smem = solver == FM_SOLVER_VMS ? vms_smem_bytes(b->tn_max, b->threads, prec == FM_MIXED)
+                                        : supg_smem_bytes(b->tn_max, npe);
   if (smem > 227 * 1024) {
     delete b;
     return fail(FM_ERR_INVALID, "tile too large for shared memory; lower tile_nodes");
   }
-  cudaError_t ce = solver == FM_SOLVER_VMS ? vms_configure(smem) : supg_configure(smem, npe);
+  cudaError_t ce = solver == FM_SOLVER_VMS ? vms_configure(b->tn_max) : supg_configure(smem, npe);
   if (ce != cudaSuccess) {
     delete b;
     return fail(FM_ERR_CUDA, std::string("kernel attribute: ") + cudaGetErrorString(ce));

@@ -47,9 +47,12 @@ def run_pair(p, steps, check_every=1, **tuning):
             eu = rel(u, st[:, :3])
             if p.solver == mesh.VMS:
                 ep = rel(pr, st[:, 3])
-                es = rel(sd, prev_sd)
-                scale = max(np.abs(prev_sd).max(), 1e-300)
-                assert np.abs(el - oel).max() <= 1e-13 * scale + 1e-300, s
+                if p.tot_dual_steps == 0:
+                    es = rel(sd, prev_sd)
+                    scale = max(np.abs(prev_sd).max(), 1e-300)
+                    assert np.abs(el - oel).max() <= 1e-13 * scale + 1e-300, s
+                else:
+                    es = 0.0  # stored subscales are mid-step with dual iterations
             else:
                 ep = rel(pr, oel[:, 0])
                 es = rel(el[:, 0], oel[:, 1])
