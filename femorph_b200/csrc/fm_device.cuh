@@ -31,6 +31,8 @@ struct DevBatch {
   int32_t n_tiles;
   const int32_t* tile_nodes;
   const int32_t* tile_cols;
+  const uint16_t* tile_inc;       // per tile: node -> (element*npe + corner) entries, element order
+  const uint16_t* tile_off;       // per tile: n_node+1 offsets into tile_inc
   // interface
   double *part0, *part1, *part2, *part3;
   const int32_t* iface_node;

@@ -405,6 +405,25 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         const int32_t* c = &p->conn[oe * npe];
         for (int a = 0; a < npe; ++a) L.conn_local.push_back((uint16_t)local[c[a]]);
       }
+      // node -> incident (element, corner) lists in element order
+      {
+        if ((int64_t)ne * npe > 65535)
+          return fail(FM_ERR_INVALID, "tile_elems too large for 16-bit incidence entries");
+        std::vector<int32_t> cnt(tm.n_node + 1, 0);
+        const uint16_t* lc = &L.conn_local[(size_t)(elem_base + e_out) * npe];
+        for (int64_t i = 0; i < ne * npe; ++i) cnt[lc[i] + 1]++;
+        for (int k2 = 0; k2 < tm.n_node; ++k2) cnt[k2 + 1] += cnt[k2];
+        while (L.tile_inc.size() % 8) L.tile_inc.push_back(0);
+        tm.inc_begin = (int32_t)L.tile_inc.size();
+        tm.off_begin = (int32_t)L.tile_off.size();
+        for (int k2 = 0; k2 <= tm.n_node; ++k2) L.tile_off.push_back((uint16_t)cnt[k2]);
+        L.tile_inc.resize(L.tile_inc.size() + (size_t)ne * npe);
+        uint16_t* inc = &L.tile_inc[tm.inc_begin];
+        std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+        for (int64_t i = 0; i < ne; ++i)
+          for (int a = 0; a < npe; ++a) inc[pos[lc[i * npe + a]]++] = (uint16_t)(i * npe + a);
+        L.max_tile_elems = std::max<int32_t>(L.max_tile_elems, (int32_t)ne);
+      }
       e_out += ne;
       for (int32_t v : inter) local[v] = -1;
       for (int32_t v : ifc) local[v] = -1;
@@ -422,8 +441,10 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     L.elem_count.push_back(e_out);
     elem_base += e_out;
   }
-  // trailing padding: chunk copies round their length up to 16 bytes
+  // trailing padding: chunk copies round their length up to 16 bytes, and the
+  // incidence lists are copied in 16-byte pieces
   elem_base += ELEM_ALIGN;
+  L.tile_inc.resize((L.tile_inc.size() + 7) / 8 * 8 + 8, 0);
   L.conn_local.resize((size_t)elem_base * (probs[0]->etype), 0);
   L.iface_slot_beg.push_back((int32_t)L.iface_slots.size());
   L.n_nodes = node_base;

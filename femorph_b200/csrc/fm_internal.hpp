@@ -52,7 +52,10 @@ struct TileMeta {
   int32_t n_int;                // first n_int local nodes are interior
   int32_t slot_base;            // partial slot of local node n_int
   int32_t col_begin, n_col;     // colour offsets in tile_cols[col_begin .. +n_col]
-  int32_t problem, pad;
+  int32_t problem;
+  int32_t inc_begin;            // node->element incidence entries in tile_inc (multiple of 8)
+  int32_t off_begin;            // per-node offsets (n_node+1) into those entries, in tile_off
+  int32_t pad;
 };
 
 struct HostProblem;
@@ -92,6 +95,11 @@ struct Layout {
   int64_t n_nodes = 0, n_elems = 0;
   std::vector<TileMeta> tiles;
   std::vector<int32_t> tile_nodes, tile_cols;
+  // Per tile, for every local node, the (element-in-tile * npe + corner)
+  // entries of its incident elements in element order: the fixed order in
+  // which the node-owner threads add element contributions.
+  std::vector<uint16_t> tile_inc, tile_off;
+  int32_t max_tile_elems = 0;
   std::vector<uint16_t> conn_local;   // n_elems x npe
   std::vector<int32_t> iface_node, iface_slot_beg, iface_slots, iface_prob;
   int64_t n_slots = 0;
@@ -105,6 +113,9 @@ struct Layout {
 
 // Tiles start at multiples of this many element slots.
 constexpr int ELEM_ALIGN = 32;
+// VMS tiles: at most this many nodes (each CTA thread owns up to
+// FM_MAX_TILE_NODES / threads of them during accumulation).
+#define FM_MAX_TILE_NODES 512
 
 int build_layout(fm_problem* const* probs, int n, int tile_elems, int tile_nodes, Layout& L);
 }  // namespace fm

@@ -60,16 +60,22 @@ template <bool MIXED, typename S>
 __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P, int64_t e, const int ln[4],
                                             const double* s_x, const double* s_y, const double* s_z,
                                             const double* s_u, const double* s_v, const double* s_w,
-                                            const double* s_p, const double* s_qu, const double* s_qv,
-                                            const double* s_qw, const S sd_in[12], const double pq[4], bool pending,
-                                            bool first_dual, double inv_dt, double c1nu, double nu4,
-                                            double lres[4][4]) {
+                                            const double* s_p, const int32_t* s_bcg, const S sd_in[12],
+                                            const double pq[4], bool pending, bool first_dual, double inv_dt,
+                                            double c1nu, double nu4, double lres[4][4]) {
   const int64_t E = B.E;
   double X[4][3], U[4][3], Pn[4], Q[4][3];
+  // Q: velocity before the last BC application; it differs from the staged
+  // (after-BC) velocity only at BC nodes, whose values are read from memory
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     X[a][0] = s_x[ln[a]]; X[a][1] = s_y[ln[a]]; X[a][2] = s_z[ln[a]];
-    Q[a][0] = s_qu[ln[a]]; Q[a][1] = s_qv[ln[a]]; Q[a][2] = s_qw[ln[a]];
+    const int g = s_bcg[ln[a]];
+    if (g >= 0) {
+      Q[a][0] = B.pu[g]; Q[a][1] = B.pv[g]; Q[a][2] = B.pw[g];
+    } else {
+      Q[a][0] = s_u[ln[a]]; Q[a][1] = s_v[ln[a]]; Q[a][2] = s_w[ln[a]];
+    }
   }
   if constexpr (MIXED) {
     TetGeomF geo;
@@ -136,36 +142,49 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
   }
 }
 
-// Shared memory of one tile CTA: node arrays (14 x tn_max doubles), the
-// double-buffered chunk stage (2 x (12 subscale rows + 1 connectivity row) x
-// THREADS slots), colour offsets.
+// Shared memory of one tile CTA, in this order:
+//  node arrays: 11 doubles x tn_pad (x y z u v w p + four accumulators),
+//    tn_pad = tn_max rounded up to even so every later region is 16-byte aligned;
+//  chunk stage: two buffers, each 12 subscale rows + 1 connectivity row of
+//    THREADS slots (bulk-copy targets).  FP64: each buffer is sized to 16 rows
+//    of THREADS doubles because a thread overwrites its own column with its 16
+//    residual entries once it has read its inputs; mixed: a separate
+//    16 x THREADS double region holds the residual entries;
+//  per-node BC flag (int32 x tn_pad), incidence offsets (uint16 x tn_pad+2),
+//  incidence entries (uint16 x inc_max).
 template <int THREADS, bool MIXED>
 __host__ __device__ constexpr size_t vms_stage_bytes() {
-  return 2 * ((size_t)12 * THREADS * (MIXED ? sizeof(float) : sizeof(double)) + (size_t)THREADS * 8);
+  return MIXED ? 2 * ((size_t)12 * THREADS * sizeof(float) + (size_t)THREADS * 8) + (size_t)16 * THREADS * 8
+               : 2 * (size_t)16 * THREADS * 8;
+}
+template <int THREADS, bool MIXED>
+__host__ __device__ constexpr size_t vms_stage_buffer_bytes() {
+  return MIXED ? (size_t)12 * THREADS * sizeof(float) + (size_t)THREADS * 8 : (size_t)16 * THREADS * 8;
 }
 
 template <int THREADS, bool MIXED>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (MIXED ? 2 : 1))
-    vms_tile_kernel(DevBatch B, int tn_max) {
+    vms_tile_kernel(DevBatch B, int tn_max, int inc_max) {
   using S = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) double sm[];
+  const int tn_pad = (tn_max + 1) & ~1;
   double* s_x = sm;
-  double* s_y = s_x + tn_max;
-  double* s_z = s_y + tn_max;
-  double* s_u = s_z + tn_max;
-  double* s_v = s_u + tn_max;
-  double* s_w = s_v + tn_max;
-  double* s_p = s_w + tn_max;
-  double* s_qu = s_p + tn_max;   // velocity before the last BCs
-  double* s_qv = s_qu + tn_max;
-  double* s_qw = s_qv + tn_max;
-  double* s_a0 = s_qw + tn_max;  // residual accumulators
-  double* s_a1 = s_a0 + tn_max;
-  double* s_a2 = s_a1 + tn_max;
-  double* s_a3 = s_a2 + tn_max;
-  S* stage_s = reinterpret_cast<S*>(s_a3 + tn_max);                 // [2][12][THREADS]
-  uint2* stage_c = reinterpret_cast<uint2*>(stage_s + 2 * 12 * THREADS);  // [2][THREADS]
-  int32_t* s_col = reinterpret_cast<int32_t*>(stage_c + 2 * THREADS);     // colour offsets (<= 129)
+  double* s_y = s_x + tn_pad;
+  double* s_z = s_y + tn_pad;
+  double* s_u = s_z + tn_pad;
+  double* s_v = s_u + tn_pad;
+  double* s_w = s_v + tn_pad;
+  double* s_p = s_w + tn_pad;
+  double* s_a0 = s_p + tn_pad;  // residual accumulators (each node owned by one thread)
+  double* s_a1 = s_a0 + tn_pad;
+  double* s_a2 = s_a1 + tn_pad;
+  double* s_a3 = s_a2 + tn_pad;
+  char* stage = reinterpret_cast<char*>(s_a3 + tn_pad);
+  constexpr size_t BUF = vms_stage_buffer_bytes<THREADS, MIXED>();
+  double* s_lres_mixed = reinterpret_cast<double*>(stage + 2 * BUF);  // mixed only
+  uint16_t* s_inc = reinterpret_cast<uint16_t*>(stage + vms_stage_bytes<THREADS, MIXED>());  // inc_max (multiple of 8)
+  int32_t* s_bcg = reinterpret_cast<int32_t*>(s_inc + inc_max);  // global id of BC nodes, else -1
+  uint16_t* s_off = reinterpret_cast<uint16_t*>(s_bcg + tn_pad);
   __shared__ uint64_t bars[2];
   __shared__ int s_abort;
 
@@ -192,10 +211,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     const uint32_t rs = MIXED ? ((nch + 3) & ~3) : ((nch + 1) & ~1);  // 16-byte multiples
     const uint32_t bytes_s = rs * (uint32_t)sizeof(S);
     const uint32_t bytes_c = (uint32_t)((nch + 1) & ~1) * 8u;
+    S* bs = reinterpret_cast<S*>(stage + b * BUF);
     mbar_arrive_expect_tx(&bars[b], 12u * bytes_s + bytes_c);
 #pragma unroll 1
-    for (int q = 0; q < 12; ++q) bulk_load(stage_s + (b * 12 + q) * THREADS, sdus_g + (int64_t)q * E + e0, bytes_s, &bars[b]);
-    bulk_load(stage_c + b * THREADS, conn_g + e0, bytes_c, &bars[b]);
+    for (int q = 0; q < 12; ++q) bulk_load(bs + q * THREADS, sdus_g + (int64_t)q * E + e0, bytes_s, &bars[b]);
+    bulk_load(bs + 12 * THREADS, conn_g + e0, bytes_c, &bars[b]);
   };
 
   if (tid == 0) {
@@ -209,14 +229,16 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
     const double u = B.su[g], v = B.sv[g], w = B.sw[g];
     s_u[ln] = u; s_v[ln] = v; s_w[ln] = w; s_p[ln] = B.sp[g];
-    if (B.node_bc[g] >= 0) {
-      s_qu[ln] = B.pu[g]; s_qv[ln] = B.pv[g]; s_qw[ln] = B.pw[g];
-    } else {
-      s_qu[ln] = u; s_qv[ln] = v; s_qw[ln] = w;
-    }
+    s_bcg[ln] = B.node_bc[g] >= 0 ? g : -1;
     s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0; s_a3[ln] = 0.0;
   }
-  for (int c = tid; c <= tm.n_col; c += THREADS) s_col[c] = B.tile_cols[tm.col_begin + c];
+  for (int i = tid; i <= tm.n_node; i += THREADS) s_off[i] = B.tile_off[tm.off_begin + i];
+  {
+    const int ninc = tm.n_elem * 4;
+    const uint4* src = reinterpret_cast<const uint4*>(B.tile_inc + tm.inc_begin);  // 16-byte aligned
+    uint4* dst = reinterpret_cast<uint4*>(s_inc);
+    for (int i = tid; i < (ninc + 7) / 8; i += THREADS) dst[i] = src[i];
+  }
   double pq[4];
   {
     const double* q = B.q1p + pidx * 8 + ((st.iter - 1) & 1) * 4;
@@ -228,7 +250,16 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   __syncthreads();
   if (tid == 0 && nchunks > 0) issue(0);
 
-  int c_lo = 0;
+  // nodes owned by this thread for the accumulation: tid, tid+THREADS, ...;
+  // cur/end walk each one's incidence list in element order
+  constexpr int MAXOWN = FM_MAX_TILE_NODES / THREADS;  // the host caps tile_nodes
+  int cur[MAXOWN], endi[MAXOWN];
+#pragma unroll
+  for (int j = 0; j < MAXOWN; ++j) {
+    const int ln = tid + j * THREADS;
+    cur[j] = ln < tm.n_node ? s_off[ln] : 0;
+    endi[j] = ln < tm.n_node ? s_off[ln + 1] : 0;
+  }
   int k = 0;
   for (; k < nchunks; ++k) {
     if (tid == 0 && k + 1 < nchunks) {
@@ -242,30 +273,43 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     const int base = k * THREADS;
     const int le = base + tid;
     const bool active = arrived && le < tm.n_elem;
-    double lres[4][4];
-    int ln[4];
+    char* buf = stage + (k & 1) * BUF;
+    double* R = MIXED ? s_lres_mixed : reinterpret_cast<double*>(buf);  // [16][THREADS] residual entries
     if (active) {
-      const uint2 cw = stage_c[(k & 1) * THREADS + tid];
+      const S* bs = reinterpret_cast<const S*>(buf);
+      const uint2 cw = reinterpret_cast<const uint2*>(bs + 12 * THREADS)[tid];
+      int ln[4];
       ln[0] = cw.x & 0xffff; ln[1] = cw.x >> 16; ln[2] = cw.y & 0xffff; ln[3] = cw.y >> 16;
       S sd_in[12];
 #pragma unroll
-      for (int q = 0; q < 12; ++q) sd_in[q] = stage_s[((k & 1) * 12 + q) * THREADS + tid];
-      vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, s_x, s_y, s_z, s_u, s_v, s_w, s_p, s_qu, s_qv, s_qw,
-                            sd_in, pq, pending, first_dual, inv_dt, c1nu, nu4, lres);
-    }
-    // colour rounds over this chunk: elements of one colour share no node
-    while (c_lo < tm.n_col && s_col[c_lo + 1] <= base) ++c_lo;
-    for (int c = c_lo; c < tm.n_col && s_col[c] < base + THREADS; ++c) {
-      if (active && le >= s_col[c] && le < s_col[c + 1]) {
+      for (int q = 0; q < 12; ++q) sd_in[q] = bs[q * THREADS + tid];
+      double lres[4][4];
+      vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, s_x, s_y, s_z, s_u, s_v, s_w, s_p, s_bcg, sd_in, pq,
+                            pending, first_dual, inv_dt, c1nu, nu4, lres);
+      // FP64: this thread's column held only its own inputs, read above
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          s_a0[ln[a]] += lres[a][0];
-          s_a1[ln[a]] += lres[a][1];
-          s_a2[ln[a]] += lres[a][2];
-          s_a3[ln[a]] += lres[a][3];
+      for (int r = 0; r < 16; ++r) R[r * THREADS + tid] = lres[r >> 2][r & 3];
+    }
+    __syncthreads();
+    // owners add this chunk's contributions to their nodes, in element order
+#pragma unroll
+    for (int j = 0; j < MAXOWN; ++j) {
+      const int ln = tid + j * THREADS;
+      if (ln < tm.n_node) {
+        double a0 = s_a0[ln], a1 = s_a1[ln], a2 = s_a2[ln], a3 = s_a3[ln];
+        while (cur[j] < endi[j]) {
+          const int ent = s_inc[cur[j]];
+          const int col = (ent >> 2) - base;
+          if (col >= THREADS) break;
+          const int r = (ent & 3) * 4;
+          a0 += R[(r + 0) * THREADS + col];
+          a1 += R[(r + 1) * THREADS + col];
+          a2 += R[(r + 2) * THREADS + col];
+          a3 += R[(r + 3) * THREADS + col];
+          ++cur[j];
         }
+        s_a0[ln] = a0; s_a1[ln] = a1; s_a2[ln] = a2; s_a3[ln] = a3;
       }
-      __syncthreads();
     }
     // end of chunk: stage buffer k&1 is free again; any timed-out wait aborts
     if (__syncthreads_or(!arrived)) {
@@ -319,27 +363,28 @@ __global__ void vms_iface_kernel(DevBatch B) {
   finish_iteration(B);
 }
 
-size_t vms_smem_bytes(int tn_max, int threads, bool mixed) {
-  // node arrays + double-buffered chunk stage of this variant + colour offsets
-  size_t stage = threads == 256 ? (mixed ? vms_stage_bytes<256, true>() : vms_stage_bytes<256, false>())
-                                : (mixed ? vms_stage_bytes<128, true>() : vms_stage_bytes<128, false>());
-  return (size_t)tn_max * 14 * sizeof(double) + stage + 130 * sizeof(int32_t);
+size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed) {
+  const size_t tn_pad = (size_t)((tn_max + 1) & ~1);
+  const size_t stage = threads == 256 ? (mixed ? vms_stage_bytes<256, true>() : vms_stage_bytes<256, false>())
+                                      : (mixed ? vms_stage_bytes<128, true>() : vms_stage_bytes<128, false>());
+  return tn_pad * 11 * sizeof(double) + stage + (size_t)inc_max * sizeof(uint16_t) + tn_pad * sizeof(int32_t) +
+         (tn_pad + 2) * sizeof(uint16_t);
 }
 
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, bool mixed,
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
                                  cudaStream_t s, cudaEvent_t* ev) {
-  const size_t smem = vms_smem_bytes(tn_max, threads, mixed);
+  const size_t smem = vms_smem_bytes(tn_max, inc_max, threads, mixed);
   if (ev) cudaEventRecord(ev[0], s);
   if (mixed) {
     if (threads == 256)
-      vms_tile_kernel<256, true><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+      vms_tile_kernel<256, true><<<B.n_tiles, 256, smem, s>>>(B, tn_max, inc_max);
     else
-      vms_tile_kernel<128, true><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+      vms_tile_kernel<128, true><<<B.n_tiles, 128, smem, s>>>(B, tn_max, inc_max);
   } else {
     if (threads == 256)
-      vms_tile_kernel<256, false><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+      vms_tile_kernel<256, false><<<B.n_tiles, 256, smem, s>>>(B, tn_max, inc_max);
     else
-      vms_tile_kernel<128, false><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+      vms_tile_kernel<128, false><<<B.n_tiles, 128, smem, s>>>(B, tn_max, inc_max);
   }
   if (ev) cudaEventRecord(ev[1], s);
   vms_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
@@ -347,12 +392,15 @@ cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int
   return cudaGetLastError();
 }
 
-cudaError_t vms_configure(int tn_max) {
+cudaError_t vms_configure(int tn_max, int inc_max) {
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256, false>, a, (int)vms_smem_bytes(tn_max, 256, false));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, false>, a, (int)vms_smem_bytes(tn_max, 128, false));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<256, true>, a, (int)vms_smem_bytes(tn_max, 256, true));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(vms_tile_kernel<128, true>, a, (int)vms_smem_bytes(tn_max, 128, true));
+  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256, false>, a, (int)vms_smem_bytes(tn_max, inc_max, 256, false));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vms_tile_kernel<128, false>, a, (int)vms_smem_bytes(tn_max, inc_max, 128, false));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vms_tile_kernel<256, true>, a, (int)vms_smem_bytes(tn_max, inc_max, 256, true));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vms_tile_kernel<128, true>, a, (int)vms_smem_bytes(tn_max, inc_max, 128, true));
   return e;
 }
 

@@ -13,9 +13,9 @@
 
 namespace fm {
 const char* last_error();
-size_t vms_smem_bytes(int tn_max, int threads, bool mixed);
-cudaError_t vms_configure(int tn_max);
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int threads, int iface_blocks, bool mixed,
+size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed);
+cudaError_t vms_configure(int tn_max, int inc_max);
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
                                  cudaStream_t s, cudaEvent_t* ev);
 
 // Aspect ratio h_max / (2 sqrt(6) r_in) of a tet (1 for the regular tet,
@@ -72,7 +72,7 @@ struct fm_batch {
   Layout L;
   DevBatch D;
   std::vector<void*> allocs;
-  int tn_max = 0, threads = 128, iface_blocks = 1, graph_steps = 0;
+  int tn_max = 0, inc_max = 0, threads = 128, iface_blocks = 1, graph_steps = 0;
   int solver = 0, npe = 4, precision = 0;
   std::vector<int32_t> iters;   // host copy of each problem's completed iterations
   int32_t* h_targets = nullptr;    // pinned staging of the target array
@@ -225,6 +225,7 @@ static void default_tuning(int solver, int npe, fm_tuning& t) {
   if (t.tile_elems <= 0) t.tile_elems = (npe == 8) ? 384 : 1024;
   if (t.tile_nodes <= 0) t.tile_nodes = (npe == 8) ? 640 : 512;
   if (t.tile_nodes > 4096) t.tile_nodes = 4096;
+  if (solver == FM_SOLVER_VMS && t.tile_nodes > FM_MAX_TILE_NODES) t.tile_nodes = FM_MAX_TILE_NODES;
   if (t.graph_steps < 0) t.graph_steps = 0;
   (void)solver;
 }
@@ -278,13 +279,14 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
   }
   Layout& L = b->L;
   for (auto& tm : L.tiles) b->tn_max = std::max(b->tn_max, tm.n_node);
-  size_t smem = solver == FM_SOLVER_VMS ? vms_smem_bytes(b->tn_max, b->threads, prec == FM_MIXED)
+  b->inc_max = (L.max_tile_elems * npe + 7) / 8 * 8;
+  size_t smem = solver == FM_SOLVER_VMS ? vms_smem_bytes(b->tn_max, b->inc_max, b->threads, prec == FM_MIXED)
                                         : supg_smem_bytes(b->tn_max, npe);
   if (smem > 227 * 1024) {
     delete b;
     return fail(FM_ERR_INVALID, "tile too large for shared memory; lower tile_nodes");
   }
-  cudaError_t ce = solver == FM_SOLVER_VMS ? vms_configure(b->tn_max) : supg_configure(smem, npe);
+  cudaError_t ce = solver == FM_SOLVER_VMS ? vms_configure(b->tn_max, b->inc_max) : supg_configure(smem, npe);
   if (ce != cudaSuccess) {
     delete b;
     return fail(FM_ERR_CUDA, std::string("kernel attribute: ") + cudaGetErrorString(ce));
@@ -486,6 +488,11 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
   UP(dtc, L.tile_cols);
   D.tile_nodes = dtn;
   D.tile_cols = dtc;
+  uint16_t *dinc, *doff;
+  UP(dinc, L.tile_inc);
+  UP(doff, L.tile_off);
+  D.tile_inc = dinc;
+  D.tile_off = doff;
   for (double** pp2 : {&D.part0, &D.part1, &D.part2, &D.part3}) {
     r = dalloc(b, (void**)pp2, (size_t)std::max<int64_t>(L.n_slots, 1) * sizeof(double));
     if (r) { release(b); delete b; return r; }
@@ -574,7 +581,7 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
     cudaError_t e;
     cudaEvent_t* ev = prof ? &evs[(size_t)it * 3] : nullptr;
     if (b->solver == FM_SOLVER_VMS) {
-      e = launch_vms_iteration(b->D, b->tn_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s, ev);
+      e = launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s, ev);
     } else {
       e = launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, s, ev);
     }
