@@ -556,6 +556,15 @@ int fm_batch_destroy(fm_batch* b) {
   return FM_OK;
 }
 
+// One iteration (dual iteration for VMS, step for SUPG): tile kernel +
+// interface kernel.
+static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
+  if (b->solver == FM_SOLVER_VMS)
+    return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s,
+                                ev);
+  return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, s, ev);
+}
+
 // Sets per-problem targets (iterations) and launches enough iterations.
 // With prof != nullptr every kernel is bracketed by CUDA events and the
 // per-kernel device times are summed into prof[0] (element/tile kernel) and
@@ -577,14 +586,34 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
     evs.resize((size_t)maxit * 3);
     for (auto& e : evs) CK(cudaEventCreate(&e));
   }
-  for (int it = 0; it < maxit; ++it) {
-    cudaError_t e;
-    cudaEvent_t* ev = prof ? &evs[(size_t)it * 3] : nullptr;
-    if (b->solver == FM_SOLVER_VMS) {
-      e = launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s, ev);
-    } else {
-      e = launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, s, ev);
+  int it = 0;
+  // whole blocks of graph_steps iterations replay one captured CUDA graph
+  // (the per-problem targets live in device memory, so the same graph serves
+  // every block and every ragged step pattern)
+  if (!prof && b->graph_steps > 0 && maxit >= b->graph_steps) {
+    if (!b->graph) {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = cudaSuccess;
+      for (int i = 0; i < b->graph_steps && e == cudaSuccess; ++i) e = launch_one(b, s, nullptr);
+      cudaError_t e2 = cudaStreamEndCapture(s, &g);
+      if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(FM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+      }
+      e = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      b->graph_iters = b->graph_steps;
     }
+    for (; it + b->graph_iters <= maxit; it += b->graph_iters) {
+      CK(cudaGraphLaunch(b->graph, s));
+      launches += 2 * (int64_t)b->graph_iters;
+    }
+  }
+  for (; it < maxit; ++it) {
+    cudaEvent_t* ev = prof ? &evs[(size_t)it * 3] : nullptr;
+    cudaError_t e = launch_one(b, s, ev);
     if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     launches += 2;
   }
