@@ -132,9 +132,11 @@ def run_ours(args, rank, world, local_rank, dist):
     kprof, klaunch = b.profile(min(args.steps, 50))
     b.sync()
     lay = b.layout()
+    state = g.state()[:2]
     b.close()
     g.close()
-    res = dict(E=E, N=N, ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch, layout=lay)
+    res = dict(E=E, N=N, ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch, layout=lay,
+               state=state, steps_total=args.warmup + args.steps + min(args.steps, 50))
     # end to end through the C ABI: host buffers in, state out
     if rank == 0:
         t0 = time.perf_counter()
@@ -150,6 +152,94 @@ def run_ours(args, rank, world, local_rank, dist):
         res["h2d"] = p.coords.nbytes + p.conn.nbytes + p.init_state.nbytes
         res["d2h"] = u.nbytes + pr.nbytes
     return res
+
+
+def batched_problems(count: int = 256, seed: int = 0, n_lo: int = 8, n_hi: int = 48):
+    """BASELINE config 4: `count` independent cavities, each with its own seed;
+    n ~ U{n_lo..n_hi}, viscosity log-uniform in [1e-3, 1e-1] (rho = 1), lid
+    speed uniform in [0.5, 2]."""
+    from femorph_b200 import mesh
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_lo, n_hi + 1, count)
+    nus = np.exp(rng.uniform(np.log(1e-3), np.log(1e-1), count))
+    lids = rng.uniform(0.5, 2.0, count)
+    return [mesh.cavity(int(n), seed=seed * 100003 + i, mu=float(nu), lid=float(lid), steps=200)
+            for i, (n, nu, lid) in enumerate(zip(ns, nus, lids))]
+
+
+def run_batched(args, rank, world, local_rank, dist):
+    """Config 4 on each rank: the rank's share of the problems in one batch
+    (one launch pair per step for all of them), 50-step CUDA graphs, launch
+    shape from the autotuner.  Also runs the FP64 form on the same problems
+    and reports the mixed-vs-FP64 relative L2 after the timed steps."""
+    from femorph_b200 import api, shard
+    probs = batched_problems(args.batch_count, seed=args.seed)
+    costs = [p.n_elems for p in probs]
+    owned = shard.mine(costs, world, rank)
+    probs = [probs[i] for i in owned]
+    E = sum(p.n_elems for p in probs)
+    res = {}
+    states = {}
+    for prec_name, prec in (("mixed", api.FM_MIXED), ("fp64", api.FM_FP64)):
+        gs = [api.GpuProblem(p, prec) for p in probs]
+        cache = os.path.join(ROOT, "femorph_b200", "autotune_cache.txt")
+        tune = api.autotune(gs[:16], device=local_rank, steps=5, cache_path=cache)
+        b = api.Batch(gs, device=local_rank, graph_steps=50, **tune)
+        b.step(args.warmup)
+        b.sync()
+        if dist:
+            dist.barrier()
+        with ClockSampler(local_rank) as clk:
+            b.step(args.steps)
+            b.sync()
+        ms, launches = b.last_timing()
+        ms = shard.reduce_max(ms, dist, f"cuda:{local_rank}")
+        kprof, klaunch = b.profile(min(args.steps, 50))
+        states[prec_name] = [g.state()[:2] for g in gs]
+        res[prec_name] = dict(ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch,
+                              tune=tune, layout=b.layout())
+        b.close()
+        for g in gs:
+            g.close()
+    err_u = max(np.linalg.norm(a[0] - b_[0]) / max(np.linalg.norm(b_[0]), 1e-300)
+                for a, b_ in zip(states["mixed"], states["fp64"]))
+    err_p = max(np.linalg.norm(a[1] - b_[1]) / max(np.linalg.norm(b_[1]), 1e-300)
+                for a, b_ in zip(states["mixed"], states["fp64"]))
+    res["E"] = E
+    res["E_total"] = shard.reduce_sum(E, dist, f"cuda:{local_rank}")
+    res["err"] = (err_u, err_p)
+    res["N"] = sum(p.n_nodes for p in probs)
+    return res
+
+
+def batched_line(args, world, rb):
+    peak, peak_kind = hbm_peak()
+    out = {}
+    for pn in ("mixed", "fp64"):
+        r = rb[pn]
+        kl = max(1, r["klaunch"])
+        tile_ms = r["kprof"]["tile"] / kl
+        ab = algorithmic_bytes(rb["E"], rb["N"], pn)
+        out[pn] = {"value": rb["E_total"] * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
+                   "tuning": r["tune"], "gpu_launches": r["launches"], "clocks": r["clocks"],
+                   "roofline": {"bound": "hbm", "achieved": ab / (tile_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                                "frac": ab / (tile_ms * 1e-3) / 1e9 / peak, "traffic": None,
+                                "peak_source": peak_kind, "kernel": "vms_tile_kernel",
+                                "algorithmic_bytes_per_launch": ab, "avg_launch_ms": tile_ms}}
+    m = out["mixed"]
+    return {"metric": "VMS element-steps/s, batched cavities (mixed; FP64 beside)", "value": m["value"],
+            "unit": "element-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{args.batch_count} independent VMS cavities per GPU job, n~U{{8..48}}, "
+                                   f"nu log-U[1e-3,1e-1], lid U[0.5,2], one launch pair per step for all, "
+                                   f"50-step CUDA graphs, autotuned tiles", "elements": rb["E_total"],
+                       "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"problems sharded over {world} GPU(s) by LPT on element count"},
+            "roofline": m["roofline"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
+            "fp64": out["fp64"], "mixed_over_fp64": m["value"] / out["fp64"]["value"],
+            "mixed_vs_fp64_rel_l2": {"u_max_over_problems": rb["err"][0], "p_max_over_problems": rb["err"][1],
+                                     "after_steps": args.warmup + args.steps + min(args.steps, 50)}}
 
 
 def cpu_baseline(n: int, steps: int = 1):
@@ -217,7 +307,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=96)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--config", default="cavity", choices=["cavity", "batched"])
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--ref-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tile-elems", type=int, default=0)
@@ -243,31 +336,60 @@ def main():
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = td
-    r = run_ours(args, rank, world, local_rank, dist)
+    if args.config == "batched":
+        rb = run_batched(args, rank, world, local_rank, dist)
+        if rank == 0:
+            print(json.dumps(batched_line(args, world, rb)), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    precs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    runs = {}
+    for pn in precs:
+        a2 = argparse.Namespace(**vars(args))
+        a2.precision = pn
+        runs[pn] = run_ours(a2, rank, world, local_rank, dist)
     if rank == 0:
-        E, N = r["E"], r["N"]
-        sec = r["ms"] / 1e3
-        value = world * E * args.steps / sec
         peak, peak_kind = hbm_peak()
-        ab = algorithmic_bytes(E, N, args.precision)
-        klaunch = max(1, r["klaunch"])
-        tile_ms = r["kprof"]["tile"] / klaunch
-        achieved = ab / (tile_ms * 1e-3) / 1e9
-        p = make_problem(args.n, seed=0) if False else None
+
+        def summary(pn, r):
+            E, N = r["E"], r["N"]
+            ab = algorithmic_bytes(E, N, pn)
+            klaunch = max(1, r["klaunch"])
+            tile_ms = r["kprof"]["tile"] / klaunch
+            achieved = ab / (tile_ms * 1e-3) / 1e9
+            return {"value": world * E * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
+                    "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                 "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                                 "kernel": "vms_tile_kernel", "algorithmic_bytes_per_launch": ab,
+                                 "avg_launch_ms": tile_ms, "iface_kernel_avg_ms": r["kprof"]["iface"] / klaunch}}
+
+        head = precs[0]
+        r = runs[head]
+        E, N = r["E"], r["N"]
+        s = summary(head, r)
         line = {
-            "metric": METRIC, "value": value, "unit": "element-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+            "metric": METRIC, "value": s["value"], "unit": "element-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": s["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
             "config": {"workload": f"VMS tet4 lid-driven cavity {args.n}^3 cells x 6 Kuhn tets ({E} tets, {N} nodes), "
-                                   f"invEps=400, nu=0.01, dt from CFL 0.2 on lid+sqrt(invEps), {args.precision}",
+                                   f"invEps=400, nu=0.01, dt from CFL 0.2 on lid+sqrt(invEps), {head} form",
                        "elements": E, "nodes": N, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"{world} independent cavity solve(s), one per GPU"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "kernel": "vms_tile_kernel", "algorithmic_bytes_per_launch": ab,
-                         "avg_launch_ms": tile_ms, "iface_kernel_avg_ms": r["kprof"]["iface"] / klaunch},
+            "roofline": s["roofline"],
             "gpu_launches": r["launches"], "clocks": r["clocks"], "layout": r["layout"],
         }
+        if "fp64" in runs and head != "fp64":
+            sd = summary("fp64", runs["fp64"])
+            (um, pm), (ud, pd) = runs[head]["state"], runs["fp64"]["state"]
+            line["fp64"] = sd
+            line["mixed_over_fp64"] = s["value"] / sd["value"]
+            line["mixed_vs_fp64_rel_l2"] = {
+                "u": float(np.linalg.norm(um - ud) / np.linalg.norm(ud)),
+                "p": float(np.linalg.norm(pm - pd) / max(np.linalg.norm(pd), 1e-300)),
+                "after_steps": r["steps_total"],
+                "reference": "the FP64 GPU path (itself <= 1e-10 of the oracle after 200 steps of config 1)"}
         if "e2e_s" in r:
             line["e2e"] = {"value": E * args.steps / r["e2e_s"], "unit": "element-steps/s",
                            "h2d_bytes_per_step": r["h2d"] / args.steps, "d2h_bytes_per_step": r["d2h"] / args.steps,

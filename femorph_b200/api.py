@@ -26,7 +26,7 @@ SYMBOLS = [
     "fm_problem_read_dat", "fm_problem_info", "fm_batch_create", "fm_batch_destroy", "fm_batch_step",
     "fm_batch_sync", "fm_batch_step_ragged", "fm_problem_get_state", "fm_problem_write_vtk",
     "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
-    "fm_batch_profile",
+    "fm_batch_profile", "fm_autotune",
 ]
 
 
@@ -89,6 +89,7 @@ def lib():
         L.fm_batch_estimate_bytes.argtypes = [P, C.c_int32, P, P]
         L.fm_batch_layout.argtypes = [P, P, P, P, P]
         L.fm_batch_profile.argtypes = [P, C.c_int32, P, P]
+        L.fm_autotune.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, P]
         _lib = L
     return _lib
 
@@ -220,6 +221,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def autotune(problems, device: int = 0, steps: int = 10, cache_path: str | None = None) -> dict:
+    """Runs the library's autotuner on GpuProblems (not in a batch); returns
+    the best launch shape as Batch keyword arguments."""
+    arr = (C.c_void_p * len(problems))(*[q.h.value for q in problems])
+    t = FmTuning()
+    check(lib().fm_autotune(arr, len(problems), device, steps, cache_path.encode() if cache_path else None,
+                            C.byref(t)))
+    return dict(tile_elems=t.tile_elems, tile_nodes=t.tile_nodes, threads=t.threads)
 
 
 def solve(p: "_mesh.Problem", steps: int | None = None, precision: int = FM_FP64, **tuning):

@@ -89,6 +89,68 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// ---- reciprocal, inverse cube root and square root by Newton-Raphson ----
+// Seeds from the PTX approximate FP32 instructions (rcp/lg2/ex2/rsqrt
+// .approx, relative error below 2^-21), then Newton steps in FP64, each of
+// which squares the relative error: two steps leave it below 2^-84, i.e. the
+// results are within about one ulp of the correctly rounded values.
+__device__ __forceinline__ float ptx_rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ptx_lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ptx_ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ptx_rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+// 1/x; the seed path needs |x| inside the FP32 normal range, other values
+// take the IEEE division.
+__device__ __forceinline__ double rcp_nr(double x) {
+  const double ax = fabs(x);
+  if (!(ax > 1e-37 && ax < 1e37)) return 1.0 / x;
+  double y = (double)ptx_rcp_approx((float)x);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+// x^(-1/3) for x > 0: Newton on f(y) = y^-3 - x, y <- y + y (1 - x y^3) / 3.
+__device__ __forceinline__ double rcbrt_nr(double x) {
+  if (!(x > 1e-37 && x < 1e37)) return rcbrt(x);
+  double y = (double)ptx_ex2_approx(ptx_lg2_approx((float)x) * (-1.0f / 3.0f));
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double e = fma(-x, y * y * y, 1.0);
+    y = fma(y * (1.0 / 3.0), e, y);
+  }
+  return y;
+}
+__device__ __forceinline__ float rcbrt_nr(float x) {
+  float y = ptx_ex2_approx(ptx_lg2_approx(x) * (-1.0f / 3.0f));
+  const float e = fmaf(-x, y * y * y, 1.0f);
+  return fmaf(y * (1.0f / 3.0f), e, y);
+}
+// sqrt(x) for x >= 0 via 1/sqrt: Newton y <- y (3 - x y^2) / 2, then x y.
+__device__ __forceinline__ double sqrt_nr(double x) {
+  if (!(x > 0.0)) return 0.0;
+  if (!(x > 1e-37 && x < 1e37)) return sqrt(x);
+  double y = (double)ptx_rsqrt_approx((float)x);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) y = y * fma(-0.5 * x, y * y, 1.5);
+  return x * y;
+}
+
 // femUtils.cpp:830-871 (interpTableData) with femUtils.cpp:818-828
 // (interpVelocity).  Returns false when the time lies before the table.
 __device__ __forceinline__ bool interp_table(double t, const double* tab, int n, double v[3]) {

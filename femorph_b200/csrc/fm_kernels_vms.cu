@@ -58,29 +58,32 @@ __device__ __forceinline__ void vms_node_update(const DevBatch& B, const DevProb
 // type (double, or float in the mixed form).
 template <bool MIXED, typename S>
 __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P, int64_t e, const int ln[4],
-                                            const double* s_x, const double* s_y, const double* s_z,
-                                            const double* s_u, const double* s_v, const double* s_w,
-                                            const double* s_p, const int32_t* s_bcg, const S sd_in[12],
+                                            bool precise, const double2* s_rec, const S sd_in[12],
                                             const double pq[4], bool pending, bool first_dual, double inv_dt,
                                             double c1nu, double nu4, double lres[4][4]) {
   const int64_t E = B.E;
   double X[4][3], U[4][3], Pn[4], Q[4][3];
-  // Q: velocity before the last BC application; it differs from the staged
-  // (after-BC) velocity only at BC nodes, whose values are read from memory
+  // node record: (x, y) (z, u) (v, w) (p, BC tag); Q is the velocity before
+  // the last BC application, which differs from U only at BC nodes (tag >= 0:
+  // the node's global id), read from memory there
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    X[a][0] = s_x[ln[a]]; X[a][1] = s_y[ln[a]]; X[a][2] = s_z[ln[a]];
-    const int g = s_bcg[ln[a]];
+    const double2 r0 = s_rec[ln[a] * 4 + 0], r1 = s_rec[ln[a] * 4 + 1], r2 = s_rec[ln[a] * 4 + 2],
+                  r3 = s_rec[ln[a] * 4 + 3];
+    X[a][0] = r0.x; X[a][1] = r0.y; X[a][2] = r1.x;
+    U[a][0] = r1.y; U[a][1] = r2.x; U[a][2] = r2.y;
+    Pn[a] = r3.x;
+    const long long g = __double_as_longlong(r3.y);
     if (g >= 0) {
       Q[a][0] = B.pu[g]; Q[a][1] = B.pv[g]; Q[a][2] = B.pw[g];
     } else {
-      Q[a][0] = s_u[ln[a]]; Q[a][1] = s_v[ln[a]]; Q[a][2] = s_w[ln[a]];
+      Q[a][0] = U[a][0]; Q[a][1] = U[a][1]; Q[a][2] = U[a][2];
     }
   }
   if constexpr (MIXED) {
     TetGeomF geo;
-    tet_geometry_mixed(X, B.precise[e] != 0, geo);
-    const float ih = rcbrtf((float)(6.0 * geo.V));
+    tet_geometry_mixed(X, precise, geo);
+    const float ih = rcbrt_nr((float)(6.0 * geo.V));
     float sdu[4][3];
 #pragma unroll
     for (int q = 0; q < 12; ++q) sdu[q / 3][q % 3] = sd_in[q];
@@ -100,10 +103,6 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
     }
     float U0[3], Ud[4][3];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      U[a][0] = s_u[ln[a]]; U[a][1] = s_v[ln[a]]; U[a][2] = s_w[ln[a]]; Pn[a] = s_p[ln[a]];
-    }
-#pragma unroll
     for (int i = 0; i < 3; ++i) {
       U0[i] = (float)U[0][i];
 #pragma unroll
@@ -120,9 +119,10 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
       vms_residual_mixed<true>(geo, U0, Ud, Pn, Dacc, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, lres);
     }
   } else {
+    (void)precise;
     TetGeom geo;
     tet_geometry(X, geo);
-    const double ih = rcbrt(6.0 * geo.V);
+    const double ih = rcbrt_nr(6.0 * geo.V);
     double sdu[4][3];
 #pragma unroll
     for (int q = 0; q < 12; ++q) sdu[q / 3][q % 3] = sd_in[q];
@@ -130,10 +130,6 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
       vms_subscale_update<double>(geo, Q, pq, sdu, inv_dt, c1nu, P.c2, ih);
 #pragma unroll
       for (int q = 0; q < 12; ++q) __stcs(B.sdus + (int64_t)q * E + e, sdu[q / 3][q % 3]);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      U[a][0] = s_u[ln[a]]; U[a][1] = s_v[ln[a]]; U[a][2] = s_w[ln[a]]; Pn[a] = s_p[ln[a]];
     }
     if (first_dual)
       vms_residual<double, false>(geo, U, Pn, U, sdu, nu4, P.inv_eps, inv_dt, lres);
@@ -168,14 +164,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   using S = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) double sm[];
   const int tn_pad = (tn_max + 1) & ~1;
-  double* s_x = sm;
-  double* s_y = s_x + tn_pad;
-  double* s_z = s_y + tn_pad;
-  double* s_u = s_z + tn_pad;
-  double* s_v = s_u + tn_pad;
-  double* s_w = s_v + tn_pad;
-  double* s_p = s_w + tn_pad;
-  double* s_a0 = s_p + tn_pad;  // residual accumulators (each node owned by one thread)
+  double2* s_rec = reinterpret_cast<double2*>(sm);  // per node: (x,y) (z,u) (v,w) (p,BC tag)
+  double* s_a0 = sm + 8 * tn_pad;  // residual accumulators (each node owned by one thread)
   double* s_a1 = s_a0 + tn_pad;
   double* s_a2 = s_a1 + tn_pad;
   double* s_a3 = s_a2 + tn_pad;
@@ -183,8 +173,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   constexpr size_t BUF = vms_stage_buffer_bytes<THREADS, MIXED>();
   double* s_lres_mixed = reinterpret_cast<double*>(stage + 2 * BUF);  // mixed only
   uint16_t* s_inc = reinterpret_cast<uint16_t*>(stage + vms_stage_bytes<THREADS, MIXED>());  // inc_max (multiple of 8)
-  int32_t* s_bcg = reinterpret_cast<int32_t*>(s_inc + inc_max);  // global id of BC nodes, else -1
-  uint16_t* s_off = reinterpret_cast<uint16_t*>(s_bcg + tn_pad);
+  uint16_t* s_off = s_inc + inc_max;
   __shared__ uint64_t bars[2];
   __shared__ int s_abort;
 
@@ -226,10 +215,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   }
   for (int ln = tid; ln < tm.n_node; ln += THREADS) {
     const int g = B.tile_nodes[tm.node_begin + ln];
-    s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
-    const double u = B.su[g], v = B.sv[g], w = B.sw[g];
-    s_u[ln] = u; s_v[ln] = v; s_w[ln] = w; s_p[ln] = B.sp[g];
-    s_bcg[ln] = B.node_bc[g] >= 0 ? g : -1;
+    const long long tag = B.node_bc[g] >= 0 ? (long long)g : -1ll;
+    s_rec[ln * 4 + 0] = make_double2(B.x[g], B.y[g]);
+    s_rec[ln * 4 + 1] = make_double2(B.z[g], B.su[g]);
+    s_rec[ln * 4 + 2] = make_double2(B.sv[g], B.sw[g]);
+    s_rec[ln * 4 + 3] = make_double2(B.sp[g], __longlong_as_double(tag));
     s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0; s_a3[ln] = 0.0;
   }
   for (int i = tid; i <= tm.n_node; i += THREADS) s_off[i] = B.tile_off[tm.off_begin + i];
@@ -279,13 +269,16 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
       const S* bs = reinterpret_cast<const S*>(buf);
       const uint2 cw = reinterpret_cast<const uint2*>(bs + 12 * THREADS)[tid];
       int ln[4];
-      ln[0] = cw.x & 0xffff; ln[1] = cw.x >> 16; ln[2] = cw.y & 0xffff; ln[3] = cw.y >> 16;
+      // bit 15 of the first id flags (mixed form) an element whose Jacobian
+      // inverse stays in FP64
+      const bool precise = (cw.x & 0x8000u) != 0;
+      ln[0] = cw.x & 0x7fff; ln[1] = cw.x >> 16; ln[2] = cw.y & 0xffff; ln[3] = cw.y >> 16;
       S sd_in[12];
 #pragma unroll
       for (int q = 0; q < 12; ++q) sd_in[q] = bs[q * THREADS + tid];
       double lres[4][4];
-      vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, s_x, s_y, s_z, s_u, s_v, s_w, s_p, s_bcg, sd_in, pq,
-                            pending, first_dual, inv_dt, c1nu, nu4, lres);
+      vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, precise, s_rec, sd_in, pq, pending, first_dual, inv_dt,
+                            c1nu, nu4, lres);
       // FP64: this thread's column held only its own inputs, read above
 #pragma unroll
       for (int r = 0; r < 16; ++r) R[r * THREADS + tid] = lres[r >> 2][r & 3];
@@ -332,7 +325,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     const double acc[4] = {s_a0[ln2], s_a1[ln2], s_a2[ln2], s_a3[ln2]};
     if (ln2 < tm.n_int) {
       const int g = B.tile_nodes[tm.node_begin + ln2];
-      const double post[4] = {s_u[ln2], s_v[ln2], s_w[ln2], s_p[ln2]};
+      const double2 r1 = s_rec[ln2 * 4 + 1], r2 = s_rec[ln2 * 4 + 2], r3 = s_rec[ln2 * 4 + 3];
+      const double post[4] = {r1.y, r2.x, r2.y, r3.x};
       vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
     } else {
       const int s = tm.slot_base + (ln2 - tm.n_int);
@@ -367,8 +361,7 @@ size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed) {
   const size_t tn_pad = (size_t)((tn_max + 1) & ~1);
   const size_t stage = threads == 256 ? (mixed ? vms_stage_bytes<256, true>() : vms_stage_bytes<256, false>())
                                       : (mixed ? vms_stage_bytes<128, true>() : vms_stage_bytes<128, false>());
-  return tn_pad * 11 * sizeof(double) + stage + (size_t)inc_max * sizeof(uint16_t) + tn_pad * sizeof(int32_t) +
-         (tn_pad + 2) * sizeof(uint16_t);
+  return tn_pad * 12 * sizeof(double) + stage + (size_t)inc_max * sizeof(uint16_t) + (tn_pad + 2) * sizeof(uint16_t);
 }
 
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,

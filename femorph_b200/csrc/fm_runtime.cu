@@ -450,21 +450,17 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
     r = dalloc(b, (void**)&D.sdus32, (size_t)NE * 12 * sizeof(float));
     if (r) { release(b); delete b; return r; }
     CK(cudaMemset(D.sdus32, 0, (size_t)NE * 12 * sizeof(float)));
-    // elements whose Jacobian inverse stays in FP64 (aspect ratio above the limit)
-    std::vector<unsigned char> hprec(NE, 0);
+    // elements whose Jacobian inverse stays in FP64 (aspect ratio above the
+    // limit): flagged in bit 15 of their first tile-local node id
     for (int pi = 0; pi < n; ++pi) {
       fm_problem* p = probs[pi];
       for (int64_t k = 0; k < L.elem_count[pi]; ++k) {
         const int32_t oe = L.elem_old[pi][k];
-        if (oe >= 0)
-          hprec[L.elem_begin[pi] + k] =
-              tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT;
+        if (oe >= 0 && tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT)
+          L.conn_local[(size_t)(L.elem_begin[pi] + k) * 4] |= 0x8000;
       }
     }
-    unsigned char* dprec;
-    r = upload(b, &dprec, hprec);
-    if (r) { release(b); delete b; return r; }
-    D.precise = dprec;
+    CK(cudaMemcpy(dconn, L.conn_local.data(), L.conn_local.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
   } else if (solver == FM_SOLVER_VMS || any_ab2) {
     const int nhist = solver == FM_SOLVER_VMS ? 12 : 3 * npe;
     r = dalloc(b, (void**)&D.sdus, (size_t)NE * nhist * sizeof(double));

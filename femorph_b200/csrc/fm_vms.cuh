@@ -40,7 +40,7 @@ __device__ __forceinline__ void tet_geometry(const double X[4][3], TetGeom& g) {
   double c21 = __dsub_rn(__dmul_rn(j[1][0], j[0][2]), __dmul_rn(j[0][0], j[1][2]));
   double c22 = __dsub_rn(__dmul_rn(j[0][0], j[1][1]), __dmul_rn(j[1][0], j[0][1]));
   double det = __dadd_rn(__dadd_rn(__dmul_rn(j[0][0], c00), __dmul_rn(j[0][1], c01)), __dmul_rn(j[0][2], c02));
-  double id = 1.0 / det;
+  double id = rcp_nr(det);
   // invJac[i][k] = cof[k][i] / det ; DN[i][0] = -(inv[0][i]) - inv[1][i] - inv[2][i]
   double inv[3][3];
   inv[0][0] = __dmul_rn(c00, id); inv[0][1] = __dmul_rn(c10, id); inv[0][2] = __dmul_rn(c20, id);
@@ -53,7 +53,7 @@ __device__ __forceinline__ void tet_geometry(const double X[4][3], TetGeom& g) {
     g.DN[i][2] = inv[1][i];
     g.DN[i][3] = inv[2][i];
   }
-  g.V = det / 6.0;
+  g.V = det * (1.0 / 6.0);
 }
 
 // Pending subscale update of the previous dual iteration:
@@ -95,8 +95,8 @@ __device__ __forceinline__ void vms_subscale_update(const TetGeom& geo, const T 
   // Element-local L2 projection of r onto P1: P_a = sum_g lN[g][a] r_g / sum_g lN[g][a],
   // evaluated back at the Gauss points.
   const T invS = (T)1 / (A + (T)3 * Bt);
-  T tau_u_inv = c1nu * ih * ih + c2 * sqrt(maxa2) * ih;
-  T tau1 = (T)1 / (inv_dt + tau_u_inv);
+  T tau_u_inv = c1nu * ih * ih + c2 * sqrt_nr(maxa2) * ih;
+  T tau1 = rcp_nr(inv_dt + tau_u_inv);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     T R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);
@@ -214,10 +214,10 @@ __device__ __forceinline__ void tet_geometry_mixed(const double X[4][3], bool pr
   const double c01 = j[2][0] * j[1][2] - j[1][0] * j[2][2];
   const double c02 = j[1][0] * j[2][1] - j[2][0] * j[1][1];
   const double det = j[0][0] * c00 + j[0][1] * c01 + j[0][2] * c02;
-  g.V = det / 6.0;
+  g.V = det * (1.0 / 6.0);
   float inv[3][3];
   if (precise) {
-    const double id = 1.0 / det;
+    const double id = rcp_nr(det);
     const double c10 = j[2][1] * j[0][2] - j[0][1] * j[2][2];
     const double c11 = j[0][0] * j[2][2] - j[2][0] * j[0][2];
     const double c12 = j[2][0] * j[0][1] - j[0][0] * j[2][1];
@@ -242,7 +242,7 @@ __device__ __forceinline__ void tet_geometry_mixed(const double X[4][3], bool pr
     const float d20 = f[0][1] * f[1][2] - f[1][1] * f[0][2];
     const float d21 = f[1][0] * f[0][2] - f[0][0] * f[1][2];
     const float d22 = f[0][0] * f[1][1] - f[1][0] * f[0][1];
-    const float id = 1.0f / (float)det;
+    const float id = ptx_rcp_approx((float)det);
     inv[0][0] = d00 * id; inv[0][1] = d10 * id; inv[0][2] = d20 * id;
     inv[1][0] = d01 * id; inv[1][1] = d11 * id; inv[1][2] = d21 * id;
     inv[2][0] = d02 * id; inv[2][1] = d12 * id; inv[2][2] = d22 * id;
@@ -284,7 +284,7 @@ __device__ __forceinline__ void vms_subscale_update_mixed(const TetGeomF& geo, c
     for (int i = 0; i < 3; ++i) r[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2] + gp[i];
   }
   const float invS = 1.0f / S;
-  const float tau1 = 1.0f / (inv_dt + c1nu * ih * ih + c2 * sqrtf(maxa2) * ih);
+  const float tau1 = ptx_rcp_approx(inv_dt + c1nu * ih * ih + c2 * (maxa2 > 0.0f ? maxa2 * ptx_rsqrt_approx(maxa2) : 0.0f) * ih);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const float R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);

@@ -182,6 +182,16 @@ FM_API int fm_batch_last_timing(fm_batch* b, double* ms, int64_t* launches);
  * kernel in kernel_ms[1], with their launch counts.  Synchronous. */
 FM_API int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* launches);
 
+/* Autotuner: times the tile/interface kernels of these problems (as one
+ * batch, `steps` steps per candidate, per-kernel CUDA events) over the
+ * candidate launch shapes (tile elements x threads per CTA) and writes the
+ * fastest to *best.  With cache_path non-NULL the result is looked up first
+ * and stored afterwards, keyed by GPU name, solver, element type, precision
+ * and the batch's element count (rounded to a power of two).  The problems
+ * must not be in a batch; their host data is not modified. */
+FM_API int fm_autotune(fm_problem* const* problems, int32_t n, int32_t device, int32_t steps, const char* cache_path,
+                       fm_tuning* best);
+
 /* Bytes of device memory a batch of these problems needs (admission). */
 FM_API int fm_batch_estimate_bytes(fm_problem* const* problems, int32_t n, const fm_tuning* tuning, int64_t* bytes);
 
