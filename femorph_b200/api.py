@@ -26,7 +26,8 @@ SYMBOLS = [
     "fm_problem_read_dat", "fm_problem_info", "fm_batch_create", "fm_batch_destroy", "fm_batch_step",
     "fm_batch_sync", "fm_batch_step_ragged", "fm_problem_get_state", "fm_problem_write_vtk",
     "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
-    "fm_batch_profile", "fm_autotune",
+    "fm_batch_profile", "fm_autotune", "fm_batch_create_empty", "fm_batch_add", "fm_batch_remove",
+    "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
 ]
 
 
@@ -51,6 +52,12 @@ class FmParams(C.Structure):
 class FmTuning(C.Structure):
     _fields_ = [("tile_elems", C.c_int32), ("tile_nodes", C.c_int32), ("threads", C.c_int32),
                 ("graph_steps", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class FmCapacity(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("elem_type", C.c_int32), ("precision", C.c_int32),
+                ("max_problems", C.c_int32), ("max_elems", C.c_int64), ("max_nodes", C.c_int64),
+                ("max_table_rows", C.c_int64), ("reserved", C.c_int64 * 4)]
 
 
 class FmError(RuntimeError):
@@ -90,6 +97,13 @@ def lib():
         L.fm_batch_layout.argtypes = [P, P, P, P, P]
         L.fm_batch_profile.argtypes = [P, C.c_int32, P, P]
         L.fm_autotune.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, P]
+        L.fm_batch_create_empty.argtypes = [P, P, C.c_int32, P]
+        L.fm_batch_add.argtypes = [P, P]
+        L.fm_batch_remove.argtypes = [P, P]
+        L.fm_problem_prepare.argtypes = [P, P]
+        L.fm_batch_resident.argtypes = [P, P, P, P]
+        L.fm_batch_step_problems.argtypes = [P, P, P, C.c_int32, P]
+        L.fm_problem_status.argtypes = [P]
         _lib = L
     return _lib
 
@@ -159,6 +173,15 @@ class GpuProblem:
     def write_vtk(self, path: str) -> None:
         check(lib().fm_problem_write_vtk(self.h, path.encode()))
 
+    def prepare(self, tile_elems=0, tile_nodes=0, threads=0) -> None:
+        """Builds the tile layout now (host only, thread-safe per problem)."""
+        t = FmTuning(tile_elems, tile_nodes, threads, 0)
+        check(lib().fm_problem_prepare(self.h, C.byref(t)))
+
+    def status(self) -> int:
+        """Device status code of this problem in its batch (FM_OK when healthy)."""
+        return lib().fm_problem_status(self.h)
+
     def close(self):
         if getattr(self, "h", None):
             lib().fm_problem_destroy(self.h)
@@ -215,6 +238,65 @@ class Batch:
         if getattr(self, "h", None):
             lib().fm_batch_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pool:
+    """Batch with fixed device pools that problems join and leave between
+    launches (continuous batching)."""
+
+    def __init__(self, solver, elem_type, max_problems, max_elems, max_nodes, precision=FM_FP64,
+                 max_table_rows=0, tile_elems=0, tile_nodes=0, threads=0, graph_steps=0, device=0):
+        cap = FmCapacity(solver, elem_type, precision, max_problems, max_elems, max_nodes, max_table_rows)
+        t = FmTuning(tile_elems, tile_nodes, threads, graph_steps)
+        h = C.c_void_p()
+        check(lib().fm_batch_create_empty(C.byref(cap), C.byref(t), device, C.byref(h)))
+        self.h = h
+        self.members = []
+
+    def add(self, q: GpuProblem) -> bool:
+        """Places q; False when the pools have no room for it."""
+        r = lib().fm_batch_add(self.h, q.h)
+        if r == FM_ERR_OOM:
+            return False
+        check(r)
+        self.members.append(q)
+        return True
+
+    def remove(self, q: GpuProblem) -> None:
+        check(lib().fm_batch_remove(self.h, q.h))
+        self.members.remove(q)
+
+    def step(self, problems, steps, stream=None) -> None:
+        """Advances each listed problem by its entry of `steps` (others idle)."""
+        arr = (C.c_void_p * len(problems))(*[q.h.value for q in problems])
+        a = np.ascontiguousarray(steps, np.int32)
+        check(lib().fm_batch_step_problems(self.h, arr, _p(a), len(problems), stream))
+
+    def sync(self) -> None:
+        check(lib().fm_batch_sync(self.h))
+
+    def last_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        check(lib().fm_batch_last_timing(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def resident(self):
+        a, b, c = C.c_int32(), C.c_int64(), C.c_int64()
+        check(lib().fm_batch_resident(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return dict(problems=a.value, elems=b.value, largest_free_elems=c.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fm_batch_destroy(self.h)
+            self.h = None
+            self.members = []
 
     def __del__(self):
         try:

@@ -36,9 +36,10 @@ struct DevBatch {
   // interface
   double *part0, *part1, *part2, *part3;
   const int32_t* iface_node;
-  const int32_t* iface_slot_beg;
+  const int32_t* iface_slot_beg;  // first partial-slot entry of each interface node
+  const int32_t* iface_slot_cnt;  // number of entries
   const int32_t* iface_slots;
-  const int32_t* iface_prob;
+  const int32_t* iface_prob;      // problem slot, -1 for a free entry
   int32_t n_iface;
   // problems
   const DevProb* probs;
@@ -47,7 +48,6 @@ struct DevBatch {
   double* q1p;                    // [prob][2][4] pre-BC pressures of nodes 0..3
   int32_t n_probs;
   unsigned int* done;             // block counter of the interface pass
-  const unsigned char* precise;   // mixed: per element flag, FP64 Jacobian inverse
 };
 
 // ---- bulk asynchronous copies global -> shared (cp.async.bulk, sm_90+) ----

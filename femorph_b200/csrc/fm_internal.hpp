@@ -1,6 +1,7 @@
 // Internal host/device data structures of femorph_b200.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -60,6 +61,7 @@ struct TileMeta {
 
 struct HostProblem;
 
+struct Layout;
 }  // namespace fm
 
 struct fm_problem {
@@ -78,6 +80,9 @@ struct fm_problem {
   std::vector<double> tab_rows;    // rows x 4
   // Lumped mass (problem numbering): VMS N, SUPG N*3
   std::vector<double> mass;
+  // Prepared tile layout (fm_problem_prepare) and the tile sizes it was built for
+  std::shared_ptr<fm::Layout> layout;
+  int32_t layout_te = 0, layout_tn = 0;
   // Batch membership
   fm_batch* batch = nullptr;
   int32_t index = -1;

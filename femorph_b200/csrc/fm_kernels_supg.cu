@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int t
 
   const TileMeta tm = B.tiles[blockIdx.x];
   const int pidx = tm.problem;
+  if (pidx < 0) return;  // free tile slot
   const DevProbState st = B.pstate[pidx];
   if (st.iter >= B.target[pidx]) return;
   const DevProb& P = B.probs[pidx];
@@ -143,12 +144,14 @@ __global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int t
 __global__ void supg_iface_kernel(DevBatch B) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
     const int pidx = B.iface_prob[i];
+    if (pidx < 0) continue;  // free interface entry
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx]) continue;
     const DevProb& P = B.probs[pidx];
     const int g = B.iface_node[i];
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int kk = B.iface_slot_beg[i]; kk < B.iface_slot_beg[i + 1]; ++kk) {
+    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
+    for (int kk = k0; kk < k1; ++kk) {
       const int s = B.iface_slots[kk];
       acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s];
     }
@@ -174,6 +177,7 @@ __global__ void supg_pressure_kernel(DevBatch B, int tn_max, double* pres) {
   double* s_v = s_u + tn_max;
   double* s_w = s_v + tn_max;
   const TileMeta tm = B.tiles[blockIdx.x];
+  if (tm.problem < 0) return;  // free tile slot
   for (int ln = threadIdx.x; ln < tm.n_node; ln += blockDim.x) {
     const int g = B.tile_nodes[tm.node_begin + ln];
     s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
@@ -208,20 +212,34 @@ size_t supg_smem_bytes(int tn_max, int npe) {
   return (size_t)tn_max * 9 * sizeof(double) + 130 * sizeof(int32_t);
 }
 
+// Sets kernel k's dynamic shared-memory limit to the device's opt-in
+// maximum less the kernel's static shared memory.
+template <typename K>
+static cudaError_t raise_dyn_smem(K k, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, k);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+// Raises the kernels' dynamic shared-memory limit to the device's opt-in
+// maximum (the attribute is per kernel and process-wide, so a batch with
+// small tiles must not lower it below what another batch launches with; the
+// shared-memory carve-out still follows each launch's actual size).
 cudaError_t supg_configure(size_t smem, int npe) {
-  cudaError_t e;
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  (void)smem;  // checked against the limit by the caller
   if (npe == 4) {
-    e = cudaFuncSetAttribute(supg_tile_kernel<4, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(supg_tile_kernel<4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(supg_pressure_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = raise_dyn_smem(supg_tile_kernel<4, 128>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 256>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<4>, optin);
   } else {
-    e = cudaFuncSetAttribute(supg_tile_kernel<8, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(supg_tile_kernel<8, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(supg_pressure_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = raise_dyn_smem(supg_tile_kernel<8, 128>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<8>, optin);
   }
   return e;
 }

@@ -53,6 +53,14 @@ __device__ __forceinline__ void vms_node_update(const DevBatch& B, const DevProb
   B.su[g] = s[0]; B.sv[g] = s[1]; B.sw[g] = s[2]; B.sp[g] = s[3];
 }
 
+// Node records in shared memory: four 16-byte pieces per node, (x, y)
+// (z, u) (v, w) (p, BC tag), piece k of node ln stored at position
+// k ^ ((ln >> 1) & 3).  With 64-byte records the unswizzled piece k of every
+// node falls in one of only two 4-bank groups, so a warp's 16-byte loads of
+// 32 different nodes serialise up to 16-fold; the swizzle spreads them over
+// all eight groups.
+__device__ __forceinline__ int rec_index(int ln, int k) { return ln * 4 + (k ^ ((ln >> 1) & 3)); }
+
 // Per-element VMS work for one chunk slot: pending subscale update (written
 // back to global memory) and the element residual lres.  S: subscale storage
 // type (double, or float in the mixed form).
@@ -68,8 +76,8 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
   // the node's global id), read from memory there
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
-    const double2 r0 = s_rec[ln[a] * 4 + 0], r1 = s_rec[ln[a] * 4 + 1], r2 = s_rec[ln[a] * 4 + 2],
-                  r3 = s_rec[ln[a] * 4 + 3];
+    const double2 r0 = s_rec[rec_index(ln[a], 0)], r1 = s_rec[rec_index(ln[a], 1)],
+                  r2 = s_rec[rec_index(ln[a], 2)], r3 = s_rec[rec_index(ln[a], 3)];
     X[a][0] = r0.x; X[a][1] = r0.y; X[a][2] = r1.x;
     U[a][0] = r1.y; U[a][1] = r2.x; U[a][2] = r2.y;
     Pn[a] = r3.x;
@@ -139,15 +147,15 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
 }
 
 // Shared memory of one tile CTA, in this order:
-//  node arrays: 11 doubles x tn_pad (x y z u v w p + four accumulators),
-//    tn_pad = tn_max rounded up to even so every later region is 16-byte aligned;
+//  node records: 8 doubles x tn_pad (rec_index layout), then four residual
+//    accumulators of tn_pad doubles; tn_pad = tn_max rounded up to even so
+//    every later region is 16-byte aligned;
 //  chunk stage: two buffers, each 12 subscale rows + 1 connectivity row of
 //    THREADS slots (bulk-copy targets).  FP64: each buffer is sized to 16 rows
 //    of THREADS doubles because a thread overwrites its own column with its 16
 //    residual entries once it has read its inputs; mixed: a separate
 //    16 x THREADS double region holds the residual entries;
-//  per-node BC flag (int32 x tn_pad), incidence offsets (uint16 x tn_pad+2),
-//  incidence entries (uint16 x inc_max).
+//  incidence entries (uint16 x inc_max), incidence offsets (uint16 x tn_pad+2).
 template <int THREADS, bool MIXED>
 __host__ __device__ constexpr size_t vms_stage_bytes() {
   return MIXED ? 2 * ((size_t)12 * THREADS * sizeof(float) + (size_t)THREADS * 8) + (size_t)16 * THREADS * 8
@@ -179,6 +187,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
 
   const TileMeta tm = B.tiles[blockIdx.x];
   const int pidx = tm.problem;
+  if (pidx < 0) return;  // free tile slot
   const DevProbState st = B.pstate[pidx];
   if (st.iter >= B.target[pidx]) return;
   const DevProb& P = B.probs[pidx];
@@ -216,10 +225,10 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   for (int ln = tid; ln < tm.n_node; ln += THREADS) {
     const int g = B.tile_nodes[tm.node_begin + ln];
     const long long tag = B.node_bc[g] >= 0 ? (long long)g : -1ll;
-    s_rec[ln * 4 + 0] = make_double2(B.x[g], B.y[g]);
-    s_rec[ln * 4 + 1] = make_double2(B.z[g], B.su[g]);
-    s_rec[ln * 4 + 2] = make_double2(B.sv[g], B.sw[g]);
-    s_rec[ln * 4 + 3] = make_double2(B.sp[g], __longlong_as_double(tag));
+    s_rec[rec_index(ln, 0)] = make_double2(B.x[g], B.y[g]);
+    s_rec[rec_index(ln, 1)] = make_double2(B.z[g], B.su[g]);
+    s_rec[rec_index(ln, 2)] = make_double2(B.sv[g], B.sw[g]);
+    s_rec[rec_index(ln, 3)] = make_double2(B.sp[g], __longlong_as_double(tag));
     s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0; s_a3[ln] = 0.0;
   }
   for (int i = tid; i <= tm.n_node; i += THREADS) s_off[i] = B.tile_off[tm.off_begin + i];
@@ -325,7 +334,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     const double acc[4] = {s_a0[ln2], s_a1[ln2], s_a2[ln2], s_a3[ln2]};
     if (ln2 < tm.n_int) {
       const int g = B.tile_nodes[tm.node_begin + ln2];
-      const double2 r1 = s_rec[ln2 * 4 + 1], r2 = s_rec[ln2 * 4 + 2], r3 = s_rec[ln2 * 4 + 3];
+      const double2 r1 = s_rec[rec_index(ln2, 1)], r2 = s_rec[rec_index(ln2, 2)], r3 = s_rec[rec_index(ln2, 3)];
       const double post[4] = {r1.y, r2.x, r2.y, r3.x};
       vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
     } else {
@@ -339,13 +348,15 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
 __global__ void vms_iface_kernel(DevBatch B) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
     const int pidx = B.iface_prob[i];
+    if (pidx < 0) continue;  // free interface entry
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx]) continue;
     const DevProb& P = B.probs[pidx];
     const bool first_dual = (st.iter % (P.ndual + 1)) == 0;
     const int g = B.iface_node[i];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = B.iface_slot_beg[i]; k < B.iface_slot_beg[i + 1]; ++k) {
+    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
+    for (int k = k0; k < k1; ++k) {
       const int s = B.iface_slots[k];
       acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s]; acc[3] += B.part3[s];
     }
@@ -385,15 +396,31 @@ cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int
   return cudaGetLastError();
 }
 
+// Sets kernel k's dynamic shared-memory limit to the device's opt-in
+// maximum less the kernel's static shared memory.
+template <typename K>
+static cudaError_t raise_dyn_smem(K k, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, k);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+// Raises the tile kernels' dynamic shared-memory limit to the device's
+// opt-in maximum (the attribute is per kernel and process-wide, so a batch
+// with small tiles must not lower it below what another batch launches with;
+// the shared-memory carve-out still follows each launch's actual size).
 cudaError_t vms_configure(int tn_max, int inc_max) {
-  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute(vms_tile_kernel<256, false>, a, (int)vms_smem_bytes(tn_max, inc_max, 256, false));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vms_tile_kernel<128, false>, a, (int)vms_smem_bytes(tn_max, inc_max, 128, false));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vms_tile_kernel<256, true>, a, (int)vms_smem_bytes(tn_max, inc_max, 256, true));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vms_tile_kernel<128, true>, a, (int)vms_smem_bytes(tn_max, inc_max, 128, true));
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  (void)tn_max;  // sizes are checked against the limit by the caller
+  (void)inc_max;
+  e = raise_dyn_smem(vms_tile_kernel<256, false>, optin);
+  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<128, false>, optin);
+  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<256, true>, optin);
+  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<128, true>, optin);
   return e;
 }
 

@@ -1,10 +1,22 @@
 // Device runtime and C ABI of femorph_b200.
+//
+// A batch owns device pools (nodes, element slots, tiles, interface entries,
+// partial-sum slots, BC records, problem slots).  A problem is prepared on
+// the host (its own tile layout, fm_problem_prepare) and placed into free
+// ranges of the pools with its indices relocated (fm_batch_add); removing it
+// marks its tiles and interface entries inactive and frees its ranges.  The
+// kernels run over the pools' high-water marks and skip inactive entries, so
+// problems can join and leave between launches (continuous batching) while
+// every resident problem keeps its state on the device.  fm_batch_create
+// sizes the pools exactly for a fixed set of problems.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -17,6 +29,11 @@ size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed);
 cudaError_t vms_configure(int tn_max, int inc_max);
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
                                  cudaStream_t s, cudaEvent_t* ev);
+size_t supg_smem_bytes(int tn_max, int npe);
+cudaError_t supg_configure(size_t smem, int npe);
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, cudaStream_t s,
+                             cudaEvent_t* ev);
+cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
 
 // Aspect ratio h_max / (2 sqrt(6) r_in) of a tet (1 for the regular tet,
 // about 1.7 for a Kuhn tet); r_in = 3V / (sum of face areas).
@@ -56,11 +73,68 @@ static double tet_aspect_ratio(const double* X, const int32_t* c) {
   const double r_in = 3.0 * (vol6 / 6.0) / area;
   return hmax / (2.0 * std::sqrt(6.0) * r_in);
 }
-size_t supg_smem_bytes(int tn_max, int npe);
-cudaError_t supg_configure(size_t smem, int npe);
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, cudaStream_t s,
-                             cudaEvent_t* ev);
-cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
+
+// First-fit range allocator over [0, cap) with coalescing free list.
+struct Pool {
+  int64_t cap = 0, hwm = 0;
+  std::map<int64_t, int64_t> free;  // offset -> length
+  void init(int64_t c) {
+    cap = c;
+    hwm = 0;
+    free.clear();
+    if (c > 0) free[0] = c;
+  }
+  bool alloc(int64_t len, int64_t align, int64_t* off) {
+    if (len <= 0) {
+      *off = 0;
+      return true;
+    }
+    for (auto it = free.begin(); it != free.end(); ++it) {
+      const int64_t o = it->first, l = it->second;
+      const int64_t a = (o + align - 1) / align * align;
+      if (a + len <= o + l) {
+        free.erase(it);
+        if (a > o) free[o] = a - o;
+        if (a + len < o + l) free[a + len] = o + l - (a + len);
+        *off = a;
+        hwm = std::max(hwm, a + len);
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(int64_t off, int64_t len) {
+    if (len <= 0) return;
+    auto it = free.emplace(off, len).first;
+    auto nx = std::next(it);
+    if (nx != free.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free.erase(nx);
+    }
+    if (it != free.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free.erase(it);
+      }
+    }
+    // the high-water mark drops when the top of the pool is free again
+    auto last = free.empty() ? free.end() : std::prev(free.end());
+    if (last != free.end() && last->first + last->second == cap) hwm = std::min(hwm, last->first);
+  }
+};
+
+enum PoolId { P_NODE, P_ELEM, P_TILE, P_TNODE, P_TCOL, P_TINC, P_TOFF, P_SLOT, P_IFACE, P_ISLOT, P_REC, P_TAB, P_ROW, P_PROB,
+              P_COUNT };
+
+struct Placement {
+  fm_problem* p = nullptr;
+  int64_t off[P_COUNT] = {0};
+  int64_t len[P_COUNT] = {0};
+  int32_t tn_max = 0, inc_max = 0;
+  std::shared_ptr<Layout> L;  // the problem's layout (node and element numbering)
+};
+
 }  // namespace fm
 
 using namespace fm;
@@ -68,22 +142,24 @@ using namespace fm;
 struct fm_batch {
   int device = 0;
   cudaStream_t stream = nullptr;
-  std::vector<fm_problem*> probs;
-  Layout L;
-  DevBatch D;
+  int solver = 0, npe = 4, precision = 0;
+  fm_tuning tune{};
+  Pool pools[P_COUNT];
+  std::vector<Placement> slots;     // by problem slot (P_PROB offset)
+  DevBatch D{};
   std::vector<void*> allocs;
   int tn_max = 0, inc_max = 0, threads = 128, iface_blocks = 1, graph_steps = 0;
-  int solver = 0, npe = 4, precision = 0;
-  std::vector<int32_t> iters;   // host copy of each problem's completed iterations
-  int32_t* h_targets = nullptr;    // pinned staging of the target array
-  int32_t* d_targets = nullptr;
-  cudaEvent_t ev_tgt = nullptr;    // targets copied (staging reusable)
+  int configured_tn = 0, configured_inc = 0;
+  bool has_history = false;
+  std::vector<int32_t> iters;       // host copy of each slot's completed iterations
+  int32_t* h_targets = nullptr;     // pinned staging of the target array
+  cudaEvent_t ev_tgt = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int64_t last_launches = 0;
   bool timed = false;
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
-  double* d_scratch = nullptr;  // element-sized scratch for output passes
+  double* d_scratch = nullptr;
 };
 
 #define CK(x)                                                                                     \
@@ -104,16 +180,9 @@ static int dalloc(fm_batch* b, void** p, size_t bytes) {
   return FM_OK;
 }
 
-template <class T>
-static int upload(fm_batch* b, T** dst, const std::vector<T>& src) {
-  int r = dalloc(b, (void**)dst, src.size() * sizeof(T));
-  if (r) return r;
-  if (!src.empty()) CK(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
-  return FM_OK;
-}
-
-static void release(fm_batch* b) {
+static void release_all(fm_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
   for (void* p : b->allocs) cudaFree(p);
   b->allocs.clear();
   if (b->h_targets) cudaFreeHost(b->h_targets);
@@ -121,6 +190,389 @@ static void release(fm_batch* b) {
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+template <class T>
+static int put(T* dev_base, int64_t off, const T* src, int64_t n, cudaStream_t s) {
+  if (n <= 0) return FM_OK;
+  CK(cudaMemcpyAsync(dev_base + off, src, sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, s));
+  return FM_OK;
+}
+
+static void default_tuning(int solver, int npe, fm_tuning& t) {
+  if (t.threads != 128 && t.threads != 256) t.threads = 128;
+  if (t.tile_elems <= 0) t.tile_elems = (npe == 8) ? 384 : 1024;
+  if (t.tile_nodes <= 0) t.tile_nodes = (npe == 8) ? 640 : 512;
+  if (t.tile_nodes > 4096) t.tile_nodes = 4096;
+  if (solver == FM_SOLVER_VMS && t.tile_nodes > FM_MAX_TILE_NODES) t.tile_nodes = FM_MAX_TILE_NODES;
+  if (t.graph_steps < 0) t.graph_steps = 0;
+}
+
+// Builds (or reuses) the problem's own tile layout for the given tile sizes.
+// Touches only this problem, so different problems may be prepared on
+// different host threads while a batch runs.
+static int prepare(fm_problem* p, int te, int tn, std::shared_ptr<Layout>* out) {
+  if (p->layout && p->layout_te == te && p->layout_tn == tn) {
+    *out = p->layout;
+    return FM_OK;
+  }
+  std::shared_ptr<Layout> L = std::make_shared<Layout>();
+  fm_problem* arr[1] = {p};
+  int r = build_layout(arr, 1, te, tn, *L);
+  if (r) return r;
+  p->layout = L;
+  p->layout_te = te;
+  p->layout_tn = tn;
+  *out = L;
+  return FM_OK;
+}
+
+// Sizes of one prepared problem in each pool.
+static void pool_sizes(const fm_problem* p, const Layout& L, int64_t len[P_COUNT]) {
+  len[P_NODE] = p->N;
+  len[P_ELEM] = L.n_elems;  // includes the trailing over-read padding
+  len[P_TILE] = (int64_t)L.tiles.size();
+  len[P_TNODE] = (int64_t)L.tile_nodes.size();
+  len[P_TCOL] = (int64_t)L.tile_cols.size();
+  len[P_TINC] = (int64_t)L.tile_inc.size();
+  len[P_TOFF] = (int64_t)L.tile_off.size();
+  len[P_SLOT] = L.n_slots;
+  len[P_IFACE] = (int64_t)L.iface_node.size();
+  len[P_ISLOT] = (int64_t)L.iface_slots.size();
+  len[P_REC] = (int64_t)p->recs.size();
+  len[P_TAB] = (int64_t)p->tab_off.size();
+  len[P_ROW] = (int64_t)p->tab_rows.size() / 4;
+  len[P_PROB] = 1;
+}
+static const int64_t kAlign[P_COUNT] = {1, ELEM_ALIGN, 1, 1, 1, 8, 1, 1, 1, 1, 1, 1, 1, 1};
+
+// Allocates the device arrays for the given pool capacities.
+static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
+  for (int k = 0; k < P_COUNT; ++k) b->pools[k].init(cap[k]);
+  DevBatch& D = b->D;
+  memset(&D, 0, sizeof(D));
+  // element rows (subscales, connectivity) are bulk-copied from row q at
+  // q * NE + (multiple of 32): NE must be a multiple of 32 too, so every row
+  // start stays 16-byte aligned for FP32 and FP64 rows alike
+  const int64_t NN = std::max<int64_t>(cap[P_NODE], 1);
+  const int64_t NE = (std::max<int64_t>(cap[P_ELEM], 1) + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
+  int r = 0;
+  auto A = [&](void** p, size_t bytes) {
+    if (!r) r = dalloc(b, p, bytes);
+  };
+  double *x, *y, *z, *su, *sv, *sw, *sp, *pu, *pv, *pw, *pp, *ms;
+  for (double** q : {&x, &y, &z, &su, &sv, &sw, &sp, &pu, &pv, &pw, &pp, &ms}) A((void**)q, NN * sizeof(double));
+  int32_t* nbc;
+  A((void**)&nbc, NN * sizeof(int32_t));
+  uint16_t* conn;
+  A((void**)&conn, (size_t)NE * b->npe * sizeof(uint16_t));
+  if (b->solver == FM_SOLVER_VMS && b->precision == FM_MIXED) {
+    A((void**)&D.sdus32, (size_t)NE * 12 * sizeof(float));
+  } else if (b->solver == FM_SOLVER_VMS || b->has_history) {
+    A((void**)&D.sdus, (size_t)NE * (b->solver == FM_SOLVER_VMS ? 12 : 3 * b->npe) * sizeof(double));
+  }
+  if (b->solver == FM_SOLVER_SUPG) {
+    A((void**)&D.el_lam, NE * sizeof(double));
+    A((void**)&D.el_reg, NE * sizeof(double));
+    A((void**)&b->d_scratch, NE * sizeof(double));
+  }
+  TileMeta* tiles;
+  A((void**)&tiles, std::max<int64_t>(cap[P_TILE], 1) * sizeof(TileMeta));
+  int32_t *tnodes, *tcols;
+  A((void**)&tnodes, std::max<int64_t>(cap[P_TNODE], 1) * sizeof(int32_t));
+  A((void**)&tcols, std::max<int64_t>(cap[P_TCOL], 1) * sizeof(int32_t));
+  uint16_t *tinc, *toff;
+  A((void**)&tinc, std::max<int64_t>(cap[P_TINC], 8) * sizeof(uint16_t));
+  A((void**)&toff, std::max<int64_t>(cap[P_TOFF], 1) * sizeof(uint16_t));
+  for (double** q : {&D.part0, &D.part1, &D.part2, &D.part3})
+    A((void**)q, std::max<int64_t>(cap[P_SLOT], 1) * sizeof(double));
+  int32_t *inode, *isb, *isc, *iprob, *islots;
+  for (int32_t** q : {&inode, &isb, &isc, &iprob}) A((void**)q, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
+  A((void**)&islots, std::max<int64_t>(cap[P_ISLOT], 1) * sizeof(int32_t));
+  BCRec* recs;
+  A((void**)&recs, std::max<int64_t>(cap[P_REC], 1) * sizeof(BCRec));
+  int32_t *toffs, *tlens;
+  A((void**)&toffs, std::max<int64_t>(cap[P_TAB], 1) * sizeof(int32_t));
+  A((void**)&tlens, std::max<int64_t>(cap[P_TAB], 1) * sizeof(int32_t));
+  double* rows;
+  A((void**)&rows, std::max<int64_t>(cap[P_ROW], 1) * 4 * sizeof(double));
+  DevProb* dp;
+  DevProbState* ds;
+  int32_t* tg;
+  double* q1;
+  const int64_t NP = std::max<int64_t>(cap[P_PROB], 1);
+  A((void**)&dp, NP * sizeof(DevProb));
+  A((void**)&ds, NP * sizeof(DevProbState));
+  A((void**)&tg, NP * sizeof(int32_t));
+  A((void**)&q1, NP * 8 * sizeof(double));
+  uint32_t* done;
+  A((void**)&done, sizeof(uint32_t));
+  if (r) return r;
+  D.x = x; D.y = y; D.z = z; D.su = su; D.sv = sv; D.sw = sw; D.sp = sp;
+  D.pu = pu; D.pv = pv; D.pw = pw; D.pp = pp; D.mass = ms; D.node_bc = nbc;
+  D.conn = conn; D.E = NE;
+  D.tiles = tiles; D.tile_nodes = tnodes; D.tile_cols = tcols; D.tile_inc = tinc; D.tile_off = toff;
+  D.iface_node = inode; D.iface_slot_beg = isb; D.iface_slot_cnt = isc; D.iface_prob = iprob; D.iface_slots = islots;
+  D.recs = recs; D.tab_off = toffs; D.tab_len = tlens; D.tab_rows = rows;
+  D.probs = dp; D.pstate = ds; D.target = tg; D.q1p = q1; D.done = done;
+  // every slot starts inactive
+  CK(cudaMemset(tiles, 0xff, std::max<int64_t>(cap[P_TILE], 1) * sizeof(TileMeta)));
+  CK(cudaMemset(iprob, 0xff, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t)));
+  CK(cudaMemset(ds, 0, NP * sizeof(DevProbState)));
+  CK(cudaMemset(tg, 0, NP * sizeof(int32_t)));
+  CK(cudaMemset(q1, 0, NP * 8 * sizeof(double)));
+  CK(cudaMemset(done, 0, sizeof(uint32_t)));
+  b->iters.assign(NP, 0);
+  b->slots.assign(NP, Placement());
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&b->ev0));
+  CK(cudaEventCreate(&b->ev1));
+  CK(cudaEventCreateWithFlags(&b->ev_tgt, cudaEventDisableTiming));
+  CK(cudaMallocHost((void**)&b->h_targets, sizeof(int32_t) * NP));
+  return FM_OK;
+}
+
+// Makes the kernels' shared-memory limits cover the current tile maxima.
+static int configure(fm_batch* b) {
+  if (b->tn_max <= b->configured_tn && b->inc_max <= b->configured_inc) return FM_OK;
+  const int tn = std::max(b->tn_max, b->configured_tn), inc = std::max(b->inc_max, b->configured_inc);
+  size_t smem = b->solver == FM_SOLVER_VMS ? vms_smem_bytes(tn, inc, b->threads, b->precision == FM_MIXED)
+                                           : supg_smem_bytes(tn, b->npe);
+  // 227 KB opt-in limit per block, less room for the kernels' static shared memory
+  if (smem + 1024 > 227 * 1024) return fail(FM_ERR_INVALID, "tile too large for shared memory; lower tile_nodes");
+  cudaError_t ce = b->solver == FM_SOLVER_VMS ? vms_configure(tn, inc) : supg_configure(smem, b->npe);
+  if (ce != cudaSuccess) return fail(FM_ERR_CUDA, std::string("kernel attribute: ") + cudaGetErrorString(ce));
+  b->configured_tn = tn;
+  b->configured_inc = inc;
+  return FM_OK;
+}
+
+static void refresh_extent(fm_batch* b) {
+  DevBatch& D = b->D;
+  D.n_tiles = (int32_t)b->pools[P_TILE].hwm;
+  D.n_iface = (int32_t)b->pools[P_IFACE].hwm;
+  D.n_probs = (int32_t)b->pools[P_PROB].hwm;
+  b->iface_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((D.n_iface + 255) / 256, 148 * 8));
+  int tn = 0, inc = 0;
+  for (const Placement& pl : b->slots)
+    if (pl.p) {
+      tn = std::max(tn, pl.tn_max);
+      inc = std::max(inc, pl.inc_max);
+    }
+  b->tn_max = tn;
+  b->inc_max = inc;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+}
+
+// Places a prepared problem into the pools; FM_ERR_OOM if some pool has no
+// room (nothing is changed then).
+static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) {
+  const Layout& L = *Lp;
+  Placement pl;
+  pl.p = p;
+  pl.L = Lp;
+  pool_sizes(p, L, pl.len);
+  int k = 0;
+  for (; k < P_COUNT; ++k)
+    if (!b->pools[k].alloc(pl.len[k], kAlign[k], &pl.off[k])) break;
+  if (k < P_COUNT) {
+    for (int j = 0; j < k; ++j) b->pools[j].release(pl.off[j], pl.len[j]);
+    return fail(FM_ERR_OOM, "batch capacity exhausted");
+  }
+  const int ps = (int)pl.off[P_PROB];
+  const int64_t noff = pl.off[P_NODE], eoff = pl.off[P_ELEM], soff = pl.off[P_SLOT];
+  cudaStream_t s = b->stream;
+  DevBatch& D = b->D;
+  const int npe = b->npe;
+  int r = 0;
+  // node data: coordinates, initial state after the time-0 BCs, mass, BC records
+  const std::vector<int32_t>& nn = L.node_new[0];
+  const int64_t N = p->N;
+  std::vector<double> hx(N), hy(N), hz(N), hu(N), hv(N), hw(N), hp(N), hm(N);
+  std::vector<int32_t> hbc(N, -1);
+  std::vector<double> s0(N * 4, 0.0);
+  if (!p->init.empty()) s0 = p->init;
+  for (int64_t i = 0; i < N; ++i) {
+    const int64_t g = L.node_new[0][i];
+    hx[g] = p->coords[i * 3 + 0];
+    hy[g] = p->coords[i * 3 + 1];
+    hz[g] = p->coords[i * 3 + 2];
+    double st[4] = {s0[i * 4 + 0], s0[i * 4 + 1], s0[i * 4 + 2], s0[i * 4 + 3]};
+    if (b->solver == FM_SOLVER_SUPG) st[3] = 0.0;
+    if (p->node_rec[i] >= 0) {
+      const BCRec& rr = p->recs[p->node_rec[i]];
+      hbc[g] = (int32_t)pl.off[P_REC] + p->node_rec[i];
+      if (rr.tab >= 0) {
+        const double* tab = p->tab_rows.data() + (int64_t)p->tab_off[rr.tab] * 4;
+        const int nrow = p->tab_len[rr.tab];
+        double v[3];
+        if (0.0 >= tab[(nrow - 1) * 4 + 3]) {
+          for (int c = 0; c < 3; ++c) v[c] = tab[(nrow - 1) * 4 + c];
+        } else {
+          int cnt = 1;
+          bool found = false;
+          while (!found && cnt < nrow) {
+            found = (0.0 >= tab[(cnt - 1) * 4 + 3]) && (0.0 < tab[cnt * 4 + 3]);
+            if (!found) cnt++;
+          }
+          if (!found) {
+            for (int j = 0; j < P_COUNT; ++j) b->pools[j].release(pl.off[j], pl.len[j]);
+            return fail(FM_ERR_TABLE, "Could not find time in femUtils::interpTableData.");
+          }
+          const double t1 = tab[(cnt - 1) * 4 + 3], t2 = tab[cnt * 4 + 3];
+          for (int c = 0; c < 3; ++c)
+            v[c] = tab[(cnt - 1) * 4 + c] + ((tab[cnt * 4 + c] - tab[(cnt - 1) * 4 + c]) / (t2 - t1)) * (0.0 - t1);
+        }
+        if (rr.mask & BC_VX) st[0] = v[0];
+        if (rr.mask & BC_VY) st[1] = v[1];
+        if (rr.mask & BC_VZ) st[2] = v[2];
+      }
+      if (rr.mask & BC_PRES) st[3] = rr.p;
+      if (rr.mask & BC_DIR) {
+        st[0] = rr.d[0];
+        st[1] = rr.d[1];
+        st[2] = rr.d[2];
+      }
+    }
+    hu[g] = st[0];
+    hv[g] = st[1];
+    hw[g] = st[2];
+    hp[g] = st[3];
+    hm[g] = p->mass[i];
+  }
+  r = r ? r : put(const_cast<double*>(D.x), noff, hx.data(), N, s);
+  r = r ? r : put(const_cast<double*>(D.y), noff, hy.data(), N, s);
+  r = r ? r : put(const_cast<double*>(D.z), noff, hz.data(), N, s);
+  for (double* a : {D.su, D.pu}) r = r ? r : put(a, noff, hu.data(), N, s);
+  for (double* a : {D.sv, D.pv}) r = r ? r : put(a, noff, hv.data(), N, s);
+  for (double* a : {D.sw, D.pw}) r = r ? r : put(a, noff, hw.data(), N, s);
+  for (double* a : {D.sp, D.pp}) r = r ? r : put(a, noff, hp.data(), N, s);
+  r = r ? r : put(const_cast<double*>(D.mass), noff, hm.data(), N, s);
+  r = r ? r : put(const_cast<int32_t*>(D.node_bc), noff, hbc.data(), N, s);
+  {
+    std::vector<BCRec> recs(p->recs);
+    for (BCRec& q : recs)
+      if (q.tab >= 0) q.tab += (int32_t)pl.off[P_TAB];
+    std::vector<int32_t> toffs(p->tab_off);
+    for (int32_t& q : toffs) q += (int32_t)pl.off[P_ROW];
+    r = r ? r : put(const_cast<BCRec*>(D.recs), pl.off[P_REC], recs.data(), (int64_t)recs.size(), s);
+    r = r ? r : put(const_cast<int32_t*>(D.tab_off), pl.off[P_TAB], toffs.data(), (int64_t)toffs.size(), s);
+    r = r ? r : put(const_cast<int32_t*>(D.tab_len), pl.off[P_TAB], p->tab_len.data(), (int64_t)p->tab_len.size(), s);
+    r = r ? r : put(const_cast<double*>(D.tab_rows), pl.off[P_ROW] * 4, p->tab_rows.data(), (int64_t)p->tab_rows.size(), s);
+  }
+  // element data: connectivity (mixed: FP64-inverse flag in bit 15), zero history
+  {
+    std::vector<uint16_t> conn(L.conn_local);
+    if (b->solver == FM_SOLVER_VMS && b->precision == FM_MIXED)
+      for (int64_t k2 = 0; k2 < L.elem_count[0]; ++k2) {
+        const int32_t oe = L.elem_old[0][k2];
+        if (oe >= 0 && tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT)
+          conn[(size_t)k2 * 4] |= 0x8000;
+      }
+    r = r ? r : put(const_cast<uint16_t*>(D.conn), eoff * npe, conn.data(), (int64_t)conn.size(), s);
+    const int64_t ne = pl.len[P_ELEM];
+    if (D.sdus32)
+      for (int q = 0; q < 12; ++q) CK(cudaMemsetAsync(D.sdus32 + (int64_t)q * D.E + eoff, 0, ne * sizeof(float), s));
+    if (D.sdus) {
+      const int nh = b->solver == FM_SOLVER_VMS ? 12 : 3 * npe;
+      for (int q = 0; q < nh; ++q) CK(cudaMemsetAsync(D.sdus + (int64_t)q * D.E + eoff, 0, ne * sizeof(double), s));
+    }
+    if (D.el_lam) {
+      CK(cudaMemsetAsync(D.el_lam + eoff, 0, ne * sizeof(double), s));
+      CK(cudaMemsetAsync(D.el_reg + eoff, 0, ne * sizeof(double), s));
+    }
+  }
+  // tiles and their lists, relocated
+  {
+    std::vector<TileMeta> tiles(L.tiles);
+    for (TileMeta& tm : tiles) {
+      tm.elem_begin += (int32_t)eoff;
+      tm.node_begin += (int32_t)pl.off[P_TNODE];
+      tm.slot_base += (int32_t)soff;
+      tm.col_begin += (int32_t)pl.off[P_TCOL];
+      tm.inc_begin += (int32_t)pl.off[P_TINC];
+      tm.off_begin += (int32_t)pl.off[P_TOFF];
+      tm.problem = ps;
+      pl.tn_max = std::max(pl.tn_max, tm.n_node);
+    }
+    pl.inc_max = (L.max_tile_elems * npe + 7) / 8 * 8;
+    std::vector<int32_t> tnodes(L.tile_nodes);
+    for (int32_t& q : tnodes) q += (int32_t)noff;
+    r = r ? r : put(const_cast<TileMeta*>(D.tiles), pl.off[P_TILE], tiles.data(), (int64_t)tiles.size(), s);
+    r = r ? r : put(const_cast<int32_t*>(D.tile_nodes), pl.off[P_TNODE], tnodes.data(), (int64_t)tnodes.size(), s);
+    r = r ? r : put(const_cast<int32_t*>(D.tile_cols), pl.off[P_TCOL], L.tile_cols.data(), (int64_t)L.tile_cols.size(), s);
+    r = r ? r : put(const_cast<uint16_t*>(D.tile_inc), pl.off[P_TINC], L.tile_inc.data(), (int64_t)L.tile_inc.size(), s);
+    r = r ? r : put(const_cast<uint16_t*>(D.tile_off), pl.off[P_TOFF], L.tile_off.data(), (int64_t)L.tile_off.size(), s);
+  }
+  // interface entries
+  {
+    const int64_t ni = (int64_t)L.iface_node.size();
+    std::vector<int32_t> inode(ni), isb(ni), isc(ni), iprob(ni, ps), islots(L.iface_slots);
+    for (int64_t i = 0; i < ni; ++i) {
+      inode[i] = L.iface_node[i] + (int32_t)noff;
+      isb[i] = L.iface_slot_beg[i] + (int32_t)pl.off[P_ISLOT];
+      isc[i] = L.iface_slot_beg[i + 1] - L.iface_slot_beg[i];
+    }
+    for (int32_t& q : islots) q += (int32_t)soff;
+    r = r ? r : put(const_cast<int32_t*>(D.iface_node), pl.off[P_IFACE], inode.data(), ni, s);
+    r = r ? r : put(const_cast<int32_t*>(D.iface_slot_beg), pl.off[P_IFACE], isb.data(), ni, s);
+    r = r ? r : put(const_cast<int32_t*>(D.iface_slot_cnt), pl.off[P_IFACE], isc.data(), ni, s);
+    r = r ? r : put(const_cast<int32_t*>(D.iface_slots), pl.off[P_ISLOT], islots.data(), (int64_t)islots.size(), s);
+    r = r ? r : put(const_cast<int32_t*>(D.iface_prob), pl.off[P_IFACE], iprob.data(), ni, s);
+  }
+  // problem constants and progress
+  {
+    DevProb d;
+    memset(&d, 0, sizeof(d));
+    const fm_params& pr = p->params;
+    d.rho = pr.props[0];
+    d.mu = pr.props[1];
+    d.nu = pr.props[1] / pr.props[0];
+    d.inv_eps = pr.props[2];
+    d.alpha = pr.props[2];
+    d.c1 = pr.props[3];
+    d.c_i = pr.props[3];
+    d.c2 = pr.props[4];
+    d.dt = pr.time_step;
+    d.ds = pr.dual_step;
+    d.exit_cond = pr.exit_condition;
+    d.ndual = b->solver == FM_SOLVER_VMS ? std::max(0, pr.tot_dual_steps) : 0;
+    d.solver = b->solver;
+    d.precision = b->precision;
+    d.npe = npe;
+    for (int q = 0; q < 6; ++q)
+      if (pr.ex_opts[q]) d.ex_mask |= (1 << q);
+    d.glob_fixed = pr.glob_fixed;
+    for (int q = 0; q < 4; ++q) d.q1[q] = (q < p->N) ? (int32_t)(noff + nn[q]) : -1;
+    d.node_begin = noff;
+    d.n_nodes = p->N;
+    d.elem_begin = eoff;
+    d.n_elems = p->E;
+    DevProbState st;
+    memset(&st, 0, sizeof(st));
+    st.time = 0.0 + pr.time_step;
+    const double z8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int32_t zero = 0;
+    r = r ? r : put(const_cast<DevProb*>(D.probs), ps, &d, 1, s);
+    r = r ? r : put(D.pstate, ps, &st, 1, s);
+    r = r ? r : put(const_cast<int32_t*>(D.target), ps, &zero, 1, s);
+    r = r ? r : put(D.q1p, (int64_t)ps * 8, z8, 8, s);
+  }
+  CK(cudaStreamSynchronize(s));  // host staging vectors go out of scope
+  if (r) {
+    for (int j = 0; j < P_COUNT; ++j) b->pools[j].release(pl.off[j], pl.len[j]);
+    return r;
+  }
+  b->iters[ps] = 0;
+  p->batch = b;
+  p->index = ps;
+  p->steps_done = 0;
+  b->slots[ps] = std::move(pl);
+  refresh_extent(b);
+  return configure(b);
 }
 
 extern "C" {
@@ -141,7 +593,7 @@ const char* fm_strerror(int code) {
 }
 
 const char* fm_last_error_message(void) { return last_error(); }
-int fm_version(void) { return 100; }
+int fm_version(void) { return 101; }
 
 int fm_problem_create(const fm_mesh* m, const fm_bc* bc, const fm_params* prm, const double* init, fm_problem** out) {
   if (!m || !prm || !out) return fail(FM_ERR_INVALID, "null argument");
@@ -154,6 +606,8 @@ int fm_problem_create(const fm_mesh* m, const fm_bc* bc, const fm_params* prm, c
   if (prm->solver == FM_SOLVER_SUPG && m->elem_type == FM_TET4 && prm->ex_opts[1])
     return fail(FM_ERR_INVALID, "B-bar (EXOPTS 2nd field) is hexa8-only; the reference reads out of bounds on tet4");
   if (prm->precision != FM_FP64 && prm->precision != FM_MIXED) return fail(FM_ERR_INVALID, "bad precision");
+  if (prm->solver == FM_SOLVER_SUPG && prm->precision == FM_MIXED)
+    return fail(FM_ERR_INVALID, "the mixed form is implemented for the VMS solver");
   if (!(prm->time_step > 0)) return fail(FM_ERR_INVALID, "time_step must be positive");
   if (prm->props[0] == 0.0) return fail(FM_ERR_INVALID, "density must be non-zero");
   fm_problem* p = new fm_problem();
@@ -195,6 +649,8 @@ int fm_problem_create(const fm_mesh* m, const fm_bc* bc, const fm_params* prm, c
 }
 
 int fm_problem_destroy(fm_problem* p) {
+  if (!p) return FM_OK;
+  if (p->batch) fm_batch_remove(p->batch, p);
   delete p;
   return FM_OK;
 }
@@ -220,14 +676,14 @@ int fm_problem_get_mass(fm_problem* p, double* mass) {
   return FM_OK;
 }
 
-static void default_tuning(int solver, int npe, fm_tuning& t) {
-  if (t.threads != 128 && t.threads != 256) t.threads = 128;
-  if (t.tile_elems <= 0) t.tile_elems = (npe == 8) ? 384 : 1024;
-  if (t.tile_nodes <= 0) t.tile_nodes = (npe == 8) ? 640 : 512;
-  if (t.tile_nodes > 4096) t.tile_nodes = 4096;
-  if (solver == FM_SOLVER_VMS && t.tile_nodes > FM_MAX_TILE_NODES) t.tile_nodes = FM_MAX_TILE_NODES;
-  if (t.graph_steps < 0) t.graph_steps = 0;
-  (void)solver;
+int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning) {
+  if (!p) return fail(FM_ERR_INVALID, "null problem");
+  fm_tuning t;
+  memset(&t, 0, sizeof(t));
+  if (tuning) t = *tuning;
+  default_tuning(p->params.solver, p->etype, t);
+  std::shared_ptr<Layout> L;
+  return prepare(p, t.tile_elems, t.tile_nodes, &L);
 }
 
 int fm_batch_estimate_bytes(fm_problem* const* probs, int32_t n, const fm_tuning* tuning, int64_t* bytes) {
@@ -239,303 +695,160 @@ int fm_batch_estimate_bytes(fm_problem* const* probs, int32_t n, const fm_tuning
     E += probs[i]->E;
   }
   (void)tuning;
-  // nodes: coords 24 + state 32 + pre 32 + mass 8 + bc 4; elements: conn + 12 or 24 doubles;
-  // tiles/interface: bounded by ~24 B per element.
-  int64_t per_e = (int64_t)npe * 2 + (probs[0]->params.solver == FM_SOLVER_VMS ? 96 : 192 + 16) + 24;
-  *bytes = N * 100 + E * per_e + (64 << 20);
+  const bool vms = probs[0]->params.solver == FM_SOLVER_VMS;
+  const bool mixed = probs[0]->params.precision == FM_MIXED;
+  // nodes: 12 FP64 arrays + BC index; elements: connectivity + history;
+  // tiles, incidence lists and interface partials: ~40 B per element
+  const int64_t per_e = (int64_t)npe * 2 + (vms ? (mixed ? 48 : 96) : (3 * npe * 8 + 24)) + 40;
+  *bytes = N * 100 + E * per_e + (16 << 20);
+  return FM_OK;
+}
+
+static int check_same(fm_problem* const* probs, int n, int* solver, int* npe, int* prec) {
+  *solver = probs[0]->params.solver;
+  *npe = probs[0]->etype;
+  *prec = probs[0]->params.precision;
+  for (int i = 0; i < n; ++i) {
+    if (!probs[i]) return fail(FM_ERR_INVALID, "null problem");
+    if (probs[i]->batch) return fail(FM_ERR_INVALID, "problem already belongs to a batch");
+    if (probs[i]->params.solver != *solver || probs[i]->etype != *npe || probs[i]->params.precision != *prec)
+      return fail(FM_ERR_INVALID, "all problems of a batch must share solver, element type and precision");
+  }
+  return FM_OK;
+}
+
+static int new_batch(int solver, int npe, int prec, const fm_tuning* tuning, int32_t device, fm_batch** out) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FM_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(FM_ERR_INVALID, "bad device ordinal");
+  CK(cudaSetDevice(device));
+  fm_batch* b = new fm_batch();
+  memset(&b->tune, 0, sizeof(b->tune));
+  if (tuning) b->tune = *tuning;
+  default_tuning(solver, npe, b->tune);
+  b->device = device;
+  b->solver = solver;
+  b->npe = npe;
+  b->precision = prec;
+  b->threads = b->tune.threads;
+  b->graph_steps = b->tune.graph_steps;
+  *out = b;
   return FM_OK;
 }
 
 int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning, int32_t device, fm_batch** out) {
   if (!probs || n <= 0 || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
-  const int solver = probs[0]->params.solver, npe = probs[0]->etype, prec = probs[0]->params.precision;
+  int solver, npe, prec;
+  int r = check_same(probs, n, &solver, &npe, &prec);
+  if (r) return r;
+  fm_batch* b = nullptr;
+  r = new_batch(solver, npe, prec, tuning, device, &b);
+  if (r) return r;
+  // exact pool sizes from the prepared layouts
+  int64_t cap[P_COUNT] = {0};
+  std::vector<std::shared_ptr<Layout>> preps(n);
   for (int i = 0; i < n; ++i) {
-    if (!probs[i]) return fail(FM_ERR_INVALID, "null problem");
-    if (probs[i]->batch) return fail(FM_ERR_INVALID, "problem already belongs to a batch");
-    if (probs[i]->params.solver != solver || probs[i]->etype != npe || probs[i]->params.precision != prec)
-      return fail(FM_ERR_INVALID, "all problems of a batch must share solver, element type and precision");
+    r = prepare(probs[i], b->tune.tile_elems, b->tune.tile_nodes, &preps[i]);
+    if (r) {
+      delete b;
+      return r;
+    }
+    int64_t len[P_COUNT];
+    pool_sizes(probs[i], *preps[i], len);
+    for (int k = 0; k < P_COUNT; ++k) cap[k] += len[k] + (kAlign[k] > 1 ? kAlign[k] : 0);
+    b->has_history |= (solver == FM_SOLVER_SUPG && probs[i]->params.ex_opts[0] == 0);
   }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FM_ERR_NODEVICE, "no CUDA device");
-  if (device < 0 || device >= ndev) return fail(FM_ERR_INVALID, "bad device ordinal");
-  CK(cudaSetDevice(device));
-  fm_tuning t;
-  memset(&t, 0, sizeof(t));
-  if (tuning) t = *tuning;
-  default_tuning(solver, npe, t);
-  fm_batch* b = new fm_batch();
-  b->device = device;
-  b->solver = solver;
-  b->npe = npe;
-  b->precision = prec;
-  b->threads = t.threads;
-  b->graph_steps = t.graph_steps;
-  b->probs.assign(probs, probs + n);
-  int r = build_layout(probs, n, t.tile_elems, t.tile_nodes, b->L);
+  r = allocate(b, cap);
+  for (int i = 0; i < n && !r; ++i) r = place(b, probs[i], preps[i]);
   if (r) {
+    for (int i = 0; i < n; ++i)
+      if (probs[i]->batch == b) {
+        probs[i]->batch = nullptr;
+        probs[i]->index = -1;
+      }
+    release_all(b);
     delete b;
     return r;
   }
-  Layout& L = b->L;
-  for (auto& tm : L.tiles) b->tn_max = std::max(b->tn_max, tm.n_node);
-  b->inc_max = (L.max_tile_elems * npe + 7) / 8 * 8;
-  size_t smem = solver == FM_SOLVER_VMS ? vms_smem_bytes(b->tn_max, b->inc_max, b->threads, prec == FM_MIXED)
-                                        : supg_smem_bytes(b->tn_max, npe);
-  if (smem > 227 * 1024) {
+  *out = b;
+  return FM_OK;
+}
+
+int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning, int32_t device, fm_batch** out) {
+  if (!cap || !out) return fail(FM_ERR_INVALID, "null argument");
+  if (cap->elem_type != FM_TET4 && cap->elem_type != FM_HEXA8) return fail(FM_ERR_INVALID, "bad element type");
+  if (cap->max_elems <= 0 || cap->max_nodes <= 0 || cap->max_problems <= 0) return fail(FM_ERR_INVALID, "bad capacity");
+  *out = nullptr;
+  fm_batch* b = nullptr;
+  int r = new_batch(cap->solver, cap->elem_type, cap->precision, tuning, device, &b);
+  if (r) return r;
+  b->has_history = cap->solver == FM_SOLVER_SUPG;
+  const int64_t E = cap->max_elems, N = cap->max_nodes, P = cap->max_problems, npe = cap->elem_type;
+  const int64_t te = b->tune.tile_elems;
+  int64_t c[P_COUNT];
+  c[P_NODE] = N;
+  // tiles hold about tile_elems elements (fewer where tile_nodes binds first);
+  // each tile start is padded to a multiple of 32 element slots
+  c[P_TILE] = E / std::max<int64_t>(1, te / 4) + 2 * P;
+  c[P_ELEM] = E + 2 * P * ELEM_ALIGN;
+  c[P_TNODE] = N + npe * E / 2;
+  c[P_TCOL] = c[P_TILE] * 130;
+  c[P_TINC] = npe * E + 16 * c[P_TILE] + 16 * P;
+  c[P_TOFF] = c[P_TNODE] + c[P_TILE];
+  // interface partial slots: tile-boundary node copies (a few per cent of the
+  // nodes for compact tiles); a problem that needs more gets FM_ERR_OOM
+  c[P_SLOT] = N + npe * E / 8;
+  c[P_IFACE] = N;
+  c[P_ISLOT] = N + npe * E / 8;
+  c[P_REC] = N;
+  c[P_TAB] = N;
+  c[P_ROW] = cap->max_table_rows > 0 ? cap->max_table_rows : N;
+  c[P_PROB] = P;
+  c[P_ELEM] += c[P_TILE] * ELEM_ALIGN;
+  r = allocate(b, c);
+  if (r) {
+    release_all(b);
     delete b;
-    return fail(FM_ERR_INVALID, "tile too large for shared memory; lower tile_nodes");
-  }
-  cudaError_t ce = solver == FM_SOLVER_VMS ? vms_configure(b->tn_max, b->inc_max) : supg_configure(smem, npe);
-  if (ce != cudaSuccess) {
-    delete b;
-    return fail(FM_ERR_CUDA, std::string("kernel attribute: ") + cudaGetErrorString(ce));
-  }
-  const int64_t NN = L.n_nodes, NE = L.n_elems;
-  // ---- host arrays in batch numbering ----
-  std::vector<double> hx(NN), hy(NN), hz(NN), hu(NN), hv(NN), hw(NN), hp(NN), hm(NN);
-  std::vector<int32_t> hbc(NN, -1);
-  std::vector<BCRec> recs;
-  std::vector<int32_t> toff, tlen;
-  std::vector<double> trows;
-  std::vector<DevProb> dprob(n);
-  std::vector<DevProbState> dstate(n);
-  for (int pi = 0; pi < n; ++pi) {
-    fm_problem* p = probs[pi];
-    const std::vector<int32_t>& nn = L.node_new[pi];
-    const int32_t rbase = (int32_t)recs.size(), tbase = (int32_t)toff.size(), rowbase = (int32_t)(trows.size() / 4);
-    for (const BCRec& rr : p->recs) {
-      BCRec q = rr;
-      if (q.tab >= 0) q.tab += tbase;
-      recs.push_back(q);
-    }
-    for (size_t k = 0; k < p->tab_off.size(); ++k) {
-      toff.push_back(p->tab_off[k] + rowbase);
-      tlen.push_back(p->tab_len[k]);
-    }
-    trows.insert(trows.end(), p->tab_rows.begin(), p->tab_rows.end());
-    // initial state: init then BCs at time 0 (solve() prologue)
-    std::vector<double> s0(p->N * 4, 0.0);
-    if (!p->init.empty()) s0 = p->init;
-    for (int64_t i = 0; i < p->N; ++i) {
-      const int64_t g = nn[i];
-      hx[g] = p->coords[i * 3 + 0];
-      hy[g] = p->coords[i * 3 + 1];
-      hz[g] = p->coords[i * 3 + 2];
-      double s[4] = {s0[i * 4 + 0], s0[i * 4 + 1], s0[i * 4 + 2], s0[i * 4 + 3]};
-      if (solver == FM_SOLVER_SUPG) s[3] = 0.0;
-      if (p->node_rec[i] >= 0) {
-        const BCRec& rr = p->recs[p->node_rec[i]];
-        hbc[g] = rbase + p->node_rec[i];
-        if (rr.tab >= 0) {
-          // time 0 through the same table rule the device uses
-          const double* tab = p->tab_rows.data() + (int64_t)p->tab_off[rr.tab] * 4;
-          int nrow = p->tab_len[rr.tab];
-          double v[3];
-          bool ok = true;
-          if (0.0 >= tab[(nrow - 1) * 4 + 3]) {
-            for (int c = 0; c < 3; ++c) v[c] = tab[(nrow - 1) * 4 + c];
-          } else {
-            int cnt = 1;
-            bool found = false;
-            while (!found && cnt < nrow) {
-              found = (0.0 >= tab[(cnt - 1) * 4 + 3]) && (0.0 < tab[cnt * 4 + 3]);
-              if (!found) cnt++;
-            }
-            ok = found;
-            if (found) {
-              double t1 = tab[(cnt - 1) * 4 + 3], t2 = tab[cnt * 4 + 3];
-              for (int c = 0; c < 3; ++c)
-                v[c] = tab[(cnt - 1) * 4 + c] + ((tab[cnt * 4 + c] - tab[(cnt - 1) * 4 + c]) / (t2 - t1)) * (0.0 - t1);
-            }
-          }
-          if (!ok) {
-            delete b;
-            return fail(FM_ERR_TABLE, "Could not find time in femUtils::interpTableData.");
-          }
-          if (rr.mask & BC_VX) s[0] = v[0];
-          if (rr.mask & BC_VY) s[1] = v[1];
-          if (rr.mask & BC_VZ) s[2] = v[2];
-        }
-        if (rr.mask & BC_PRES) s[3] = rr.p;
-        if (rr.mask & BC_DIR) {
-          s[0] = rr.d[0];
-          s[1] = rr.d[1];
-          s[2] = rr.d[2];
-        }
-      }
-      hu[g] = s[0];
-      hv[g] = s[1];
-      hw[g] = s[2];
-      hp[g] = s[3];
-      hm[g] = p->mass[i];
-    }
-    DevProb& d = dprob[pi];
-    memset(&d, 0, sizeof(d));
-    const fm_params& pr = p->params;
-    d.rho = pr.props[0];
-    d.mu = pr.props[1];
-    d.nu = pr.props[1] / pr.props[0];
-    d.inv_eps = pr.props[2];
-    d.alpha = pr.props[2];
-    d.c1 = pr.props[3];
-    d.c_i = pr.props[3];
-    d.c2 = pr.props[4];
-    d.dt = pr.time_step;
-    d.ds = pr.dual_step;
-    d.exit_cond = pr.exit_condition;
-    d.ndual = solver == FM_SOLVER_VMS ? std::max(0, pr.tot_dual_steps) : 0;
-    d.solver = solver;
-    d.precision = prec;
-    d.npe = npe;
-    d.ex_mask = 0;
-    for (int k = 0; k < 6; ++k)
-      if (pr.ex_opts[k]) d.ex_mask |= (1 << k);
-    d.glob_fixed = pr.glob_fixed;
-    for (int k = 0; k < 4; ++k) d.q1[k] = (k < p->N) ? nn[k] : -1;
-    d.node_begin = L.node_begin[pi];
-    d.n_nodes = p->N;
-    d.elem_begin = L.elem_begin[pi];
-    d.n_elems = p->E;
-    DevProbState& s = dstate[pi];
-    memset(&s, 0, sizeof(s));
-    s.iter = 0;
-    s.status = FM_OK;
-    s.time = 0.0 + pr.time_step;
-  }
-  // q1 pressures at "iteration -1": pre-BC initial = post-BC initial except pinned nodes;
-  // never read before iteration 1 writes them.
-  std::vector<double> hq1(n * 8, 0.0);
-  DevBatch& D = b->D;
-  memset(&D, 0, sizeof(D));
-#define UP(dst, src)                              \
-  do {                                            \
-    r = upload(b, &dst, src);                     \
-    if (r) {                                      \
-      release(b);                                 \
-      delete b;                                   \
-      return r;                                   \
-    }                                             \
-  } while (0)
-  double *x, *y, *z, *su, *sv, *sw, *sp, *pu, *pv, *pw, *pp, *ms;
-  UP(x, hx); UP(y, hy); UP(z, hz);
-  UP(su, hu); UP(sv, hv); UP(sw, hw); UP(sp, hp);
-  UP(pu, hu); UP(pv, hv); UP(pw, hw); UP(pp, hp);
-  UP(ms, hm);
-  D.x = x; D.y = y; D.z = z; D.su = su; D.sv = sv; D.sw = sw; D.sp = sp;
-  D.pu = pu; D.pv = pv; D.pw = pw; D.pp = pp; D.mass = ms;
-  int32_t* nbc;
-  UP(nbc, hbc);
-  D.node_bc = nbc;
-  BCRec* drecs;
-  UP(drecs, recs);
-  D.recs = drecs;
-  int32_t *dtoff, *dtlen;
-  UP(dtoff, toff);
-  UP(dtlen, tlen);
-  D.tab_off = dtoff;
-  D.tab_len = dtlen;
-  double* dtrows;
-  UP(dtrows, trows);
-  D.tab_rows = dtrows;
-  uint16_t* dconn;
-  UP(dconn, L.conn_local);
-  D.conn = dconn;
-  D.E = NE;
-  // Per-element history: VMS subscales (12 per element, FP64 or FP32 in the
-  // mixed form); SUPG the previous step's element forces for AB2 (3*npe).
-  bool any_ab2 = false;
-  for (int pi = 0; pi < n; ++pi) any_ab2 |= (probs[pi]->params.ex_opts[0] == 0);
-  if (solver == FM_SOLVER_VMS && prec == FM_MIXED) {
-    r = dalloc(b, (void**)&D.sdus32, (size_t)NE * 12 * sizeof(float));
-    if (r) { release(b); delete b; return r; }
-    CK(cudaMemset(D.sdus32, 0, (size_t)NE * 12 * sizeof(float)));
-    // elements whose Jacobian inverse stays in FP64 (aspect ratio above the
-    // limit): flagged in bit 15 of their first tile-local node id
-    for (int pi = 0; pi < n; ++pi) {
-      fm_problem* p = probs[pi];
-      for (int64_t k = 0; k < L.elem_count[pi]; ++k) {
-        const int32_t oe = L.elem_old[pi][k];
-        if (oe >= 0 && tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT)
-          L.conn_local[(size_t)(L.elem_begin[pi] + k) * 4] |= 0x8000;
-      }
-    }
-    CK(cudaMemcpy(dconn, L.conn_local.data(), L.conn_local.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-  } else if (solver == FM_SOLVER_VMS || any_ab2) {
-    const int nhist = solver == FM_SOLVER_VMS ? 12 : 3 * npe;
-    r = dalloc(b, (void**)&D.sdus, (size_t)NE * nhist * sizeof(double));
-    if (r) { release(b); delete b; return r; }
-    CK(cudaMemset(D.sdus, 0, (size_t)NE * nhist * sizeof(double)));
-  }
-  if (solver == FM_SOLVER_SUPG) {
-    r = dalloc(b, (void**)&D.el_lam, (size_t)NE * sizeof(double));
-    if (!r) r = dalloc(b, (void**)&D.el_reg, (size_t)NE * sizeof(double));
-    if (!r) r = dalloc(b, (void**)&b->d_scratch, (size_t)NE * sizeof(double));
-    if (r) { release(b); delete b; return r; }
-    CK(cudaMemset(D.el_lam, 0, (size_t)NE * sizeof(double)));
-    CK(cudaMemset(D.el_reg, 0, (size_t)NE * sizeof(double)));
-  }
-  TileMeta* dtiles;
-  UP(dtiles, L.tiles);
-  D.tiles = dtiles;
-  D.n_tiles = (int32_t)L.tiles.size();
-  int32_t *dtn, *dtc;
-  UP(dtn, L.tile_nodes);
-  UP(dtc, L.tile_cols);
-  D.tile_nodes = dtn;
-  D.tile_cols = dtc;
-  uint16_t *dinc, *doff;
-  UP(dinc, L.tile_inc);
-  UP(doff, L.tile_off);
-  D.tile_inc = dinc;
-  D.tile_off = doff;
-  for (double** pp2 : {&D.part0, &D.part1, &D.part2, &D.part3}) {
-    r = dalloc(b, (void**)pp2, (size_t)std::max<int64_t>(L.n_slots, 1) * sizeof(double));
-    if (r) { release(b); delete b; return r; }
-  }
-  int32_t *din, *dsb, *dsl, *dip;
-  UP(din, L.iface_node);
-  UP(dsb, L.iface_slot_beg);
-  UP(dsl, L.iface_slots);
-  UP(dip, L.iface_prob);
-  D.iface_node = din;
-  D.iface_slot_beg = dsb;
-  D.iface_slots = dsl;
-  D.iface_prob = dip;
-  D.n_iface = (int32_t)L.iface_node.size();
-  DevProb* dp;
-  UP(dp, dprob);
-  D.probs = dp;
-  DevProbState* ds;
-  UP(ds, dstate);
-  D.pstate = ds;
-  double* dq1;
-  UP(dq1, hq1);
-  D.q1p = dq1;
-  D.n_probs = n;
-  std::vector<int32_t> zt(n, 0);
-  int32_t* dtg;
-  UP(dtg, zt);
-  D.target = dtg;
-  b->d_targets = dtg;
-  std::vector<uint32_t> zero1(1, 0);
-  uint32_t* ddone;
-  UP(ddone, zero1);
-  D.done = ddone;
-#undef UP
-  b->iface_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((D.n_iface + 255) / 256, 148 * 8));
-  b->iters.assign(n, 0);
-  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  CK(cudaEventCreate(&b->ev0));
-  CK(cudaEventCreate(&b->ev1));
-  CK(cudaEventCreateWithFlags(&b->ev_tgt, cudaEventDisableTiming));
-  CK(cudaMallocHost((void**)&b->h_targets, sizeof(int32_t) * n));
-  for (int i = 0; i < n; ++i) {
-    probs[i]->batch = b;
-    probs[i]->index = i;
-    probs[i]->steps_done = 0;
+    return r;
   }
   *out = b;
+  return FM_OK;
+}
+
+int fm_batch_add(fm_batch* b, fm_problem* p) {
+  if (!b || !p) return fail(FM_ERR_INVALID, "null argument");
+  if (p->batch) return fail(FM_ERR_INVALID, "problem already belongs to a batch");
+  if (p->params.solver != b->solver || p->etype != b->npe || p->params.precision != b->precision)
+    return fail(FM_ERR_INVALID, "problem does not match the batch's solver, element type and precision");
+  if (b->solver == FM_SOLVER_SUPG && p->params.ex_opts[0] == 0 && !b->has_history)
+    return fail(FM_ERR_INVALID, "batch was created without AB2 history");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  std::shared_ptr<Layout> L;
+  int r = prepare(p, b->tune.tile_elems, b->tune.tile_nodes, &L);
+  if (r) return r;
+  return place(b, p, L);
+}
+
+int fm_batch_remove(fm_batch* b, fm_problem* p) {
+  if (!b || !p || p->batch != b) return fail(FM_ERR_INVALID, "problem is not in this batch");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const int ps = p->index;
+  Placement& pl = b->slots[ps];
+  DevBatch& D = b->D;
+  // mark the problem's tiles and interface entries inactive, park its slot
+  CK(cudaMemset(const_cast<TileMeta*>(D.tiles) + pl.off[P_TILE], 0xff, pl.len[P_TILE] * sizeof(TileMeta)));
+  CK(cudaMemset(const_cast<int32_t*>(D.iface_prob) + pl.off[P_IFACE], 0xff, pl.len[P_IFACE] * sizeof(int32_t)));
+  CK(cudaMemset(const_cast<int32_t*>(D.target) + ps, 0, sizeof(int32_t)));
+  CK(cudaMemset(D.pstate + ps, 0, sizeof(DevProbState)));
+  for (int k = 0; k < P_COUNT; ++k) b->pools[k].release(pl.off[k], pl.len[k]);
+  b->iters[ps] = 0;
+  pl = Placement();
+  p->batch = nullptr;
+  p->index = -1;
+  refresh_extent(b);
   return FM_OK;
 }
 
@@ -543,14 +856,17 @@ int fm_batch_destroy(fm_batch* b) {
   if (!b) return FM_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  for (fm_problem* p : b->probs) {
-    p->batch = nullptr;
-    p->index = -1;
-  }
-  release(b);
+  for (Placement& pl : b->slots)
+    if (pl.p) {
+      pl.p->batch = nullptr;
+      pl.p->index = -1;
+    }
+  release_all(b);
   delete b;
   return FM_OK;
 }
+
+}  // extern "C"
 
 // One iteration (dual iteration for VMS, step for SUPG): tile kernel +
 // interface kernel.
@@ -561,19 +877,19 @@ static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
   return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, s, ev);
 }
 
-// Sets per-problem targets (iterations) and launches enough iterations.
-// With prof != nullptr every kernel is bracketed by CUDA events and the
-// per-kernel device times are summed into prof[0] (element/tile kernel) and
-// prof[1] (interface kernel), in milliseconds.
+// Sets per-slot targets (iterations) and launches enough iterations.  With
+// prof != nullptr every kernel is bracketed by CUDA events and the per-kernel
+// device times are summed into prof[0] (tile kernel) and prof[1] (interface
+// kernel), in milliseconds.
 static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cudaStream_t s, double* prof = nullptr) {
-  const int n = (int)b->probs.size();
+  const int n = (int)b->pools[P_PROB].hwm;
   int32_t maxit = 0;
   for (int i = 0; i < n; ++i) maxit = std::max(maxit, add_iters[i]);
-  if (maxit == 0) return FM_OK;
-  // new targets (the host tracks every problem's iteration count exactly)
+  if (maxit == 0 || b->D.n_tiles == 0) return FM_OK;
+  // new targets (the host tracks every slot's iteration count exactly)
   CK(cudaEventSynchronize(b->ev_tgt));  // staging buffer free again
   for (int i = 0; i < n; ++i) b->h_targets[i] = b->iters[i] + add_iters[i];
-  CK(cudaMemcpyAsync(b->d_targets, b->h_targets, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(const_cast<int32_t*>(b->D.target), b->h_targets, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(b->ev_tgt, s));
   CK(cudaEventRecord(b->ev0, s));
   int64_t launches = 0;
@@ -584,8 +900,9 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
   }
   int it = 0;
   // whole blocks of graph_steps iterations replay one captured CUDA graph
-  // (the per-problem targets live in device memory, so the same graph serves
-  // every block and every ragged step pattern)
+  // (the per-slot targets live in device memory, so the same graph serves
+  // every block and every ragged step pattern; it is re-captured when the
+  // batch's extent changes)
   if (!prof && b->graph_steps > 0 && maxit >= b->graph_steps) {
     if (!b->graph) {
       cudaGraph_t g = nullptr;
@@ -617,10 +934,10 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
   if (prof) {
     CK(cudaEventSynchronize(b->ev1));
     prof[0] = prof[1] = 0.0;
-    for (int it = 0; it < maxit; ++it) {
+    for (int i = 0; i < maxit; ++i) {
       float a = 0.f, c = 0.f;
-      CK(cudaEventElapsedTime(&a, evs[it * 3], evs[it * 3 + 1]));
-      CK(cudaEventElapsedTime(&c, evs[it * 3 + 1], evs[it * 3 + 2]));
+      CK(cudaEventElapsedTime(&a, evs[i * 3], evs[i * 3 + 1]));
+      CK(cudaEventElapsedTime(&c, evs[i * 3 + 1], evs[i * 3 + 2]));
       prof[0] += a;
       prof[1] += c;
     }
@@ -632,38 +949,79 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
   return FM_OK;
 }
 
+static void iters_for(fm_batch* b, const int32_t* nsteps_per_slot, std::vector<int32_t>& add) {
+  const int n = (int)b->pools[P_PROB].hwm;
+  add.assign(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const Placement& pl = b->slots[i];
+    if (!pl.p) continue;
+    const int per = b->solver == FM_SOLVER_VMS ? std::max(0, pl.p->params.tot_dual_steps) + 1 : 1;
+    add[i] = nsteps_per_slot[i] * per;
+  }
+}
+
+extern "C" {
+
 int fm_batch_step_ragged(fm_batch* b, const int32_t* nsteps, void* stream) {
   if (!b || !nsteps) return fail(FM_ERR_INVALID, "null argument");
   CK(cudaSetDevice(b->device));
   cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
-  const int n = (int)b->probs.size();
-  std::vector<int32_t> add(n);
-  for (int i = 0; i < n; ++i) {
-    if (nsteps[i] < 0) return fail(FM_ERR_INVALID, "negative step count");
-    const int per = b->solver == FM_SOLVER_VMS ? b->probs[i]->params.tot_dual_steps + 1 : 1;
-    add[i] = nsteps[i] * std::max(1, per);
-  }
+  // nsteps is indexed by the problems' order of addition to the batch: map
+  // to slots through each problem's index
+  const int n = (int)b->pools[P_PROB].hwm;
+  std::vector<int32_t> per_slot(n, 0);
+  int k = 0;
+  for (int i = 0; i < n; ++i)
+    if (b->slots[i].p) {
+      if (nsteps[k] < 0) return fail(FM_ERR_INVALID, "negative step count");
+      per_slot[i] = nsteps[k++];
+    }
+  std::vector<int32_t> add;
+  iters_for(b, per_slot.data(), add);
   int r = run_iterations(b, add, s);
   if (r) return r;
-  for (int i = 0; i < n; ++i) b->probs[i]->steps_done += nsteps[i];
+  for (int i = 0; i < n; ++i)
+    if (b->slots[i].p) b->slots[i].p->steps_done += per_slot[i];
   return FM_OK;
+}
+
+int fm_batch_step_problems(fm_batch* b, fm_problem* const* probs, const int32_t* nsteps, int32_t count, void* stream) {
+  if (!b || (count > 0 && (!probs || !nsteps))) return fail(FM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(b->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+  const int n = (int)b->pools[P_PROB].hwm;
+  std::vector<int32_t> per_slot(n, 0);
+  for (int i = 0; i < count; ++i) {
+    if (!probs[i] || probs[i]->batch != b || nsteps[i] < 0) return fail(FM_ERR_INVALID, "bad problem or step count");
+    per_slot[probs[i]->index] = nsteps[i];
+  }
+  std::vector<int32_t> add;
+  iters_for(b, per_slot.data(), add);
+  int r = run_iterations(b, add, s);
+  if (r) return r;
+  for (int i = 0; i < count; ++i) probs[i]->steps_done += nsteps[i];
+  return FM_OK;
+}
+
+int fm_batch_step(fm_batch* b, int32_t nsteps, void* stream) {
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  std::vector<int32_t> v(b->pools[P_PROB].hwm + 1, nsteps);
+  return fm_batch_step_ragged(b, v.data(), stream);
 }
 
 int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* launches) {
   if (!b || nsteps < 0) return fail(FM_ERR_INVALID, "bad argument");
   CK(cudaSetDevice(b->device));
-  const int n = (int)b->probs.size();
-  std::vector<int32_t> add(n);
+  const int n = (int)b->pools[P_PROB].hwm;
+  std::vector<int32_t> per_slot(n, nsteps), add;
+  iters_for(b, per_slot.data(), add);
   int64_t per_kernel = 0;
-  for (int i = 0; i < n; ++i) {
-    const int per = b->solver == FM_SOLVER_VMS ? b->probs[i]->params.tot_dual_steps + 1 : 1;
-    add[i] = nsteps * std::max(1, per);
-    per_kernel = std::max<int64_t>(per_kernel, add[i]);
-  }
+  for (int32_t a : add) per_kernel = std::max<int64_t>(per_kernel, a);
   double prof[2] = {0.0, 0.0};
   int r = run_iterations(b, add, b->stream, prof);
   if (r) return r;
-  for (int i = 0; i < n; ++i) b->probs[i]->steps_done += nsteps;
+  for (int i = 0; i < n; ++i)
+    if (b->slots[i].p) b->slots[i].p->steps_done += nsteps;
   if (kernel_ms) {
     kernel_ms[0] = prof[0];
     kernel_ms[1] = prof[1];
@@ -675,23 +1033,27 @@ int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* la
   return FM_OK;
 }
 
-int fm_batch_step(fm_batch* b, int32_t nsteps, void* stream) {
-  if (!b) return fail(FM_ERR_INVALID, "null batch");
-  std::vector<int32_t> v(b->probs.size(), nsteps);
-  return fm_batch_step_ragged(b, v.data(), stream);
-}
-
 int fm_batch_sync(fm_batch* b) {
   if (!b) return fail(FM_ERR_INVALID, "null batch");
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
   CK(cudaDeviceSynchronize());
-  const int n = (int)b->probs.size();
-  std::vector<DevProbState> st(n);
-  CK(cudaMemcpy(st.data(), b->D.pstate, sizeof(DevProbState) * n, cudaMemcpyDeviceToHost));
+  const int n = (int)b->pools[P_PROB].hwm;
+  std::vector<DevProbState> st(std::max(n, 1));
+  if (n > 0) CK(cudaMemcpy(st.data(), b->D.pstate, sizeof(DevProbState) * n, cudaMemcpyDeviceToHost));
   for (int i = 0; i < n; ++i)
-    if (st[i].status != FM_OK) return fail(st[i].status, fm_strerror(st[i].status));
+    if (b->slots[i].p && st[i].status != FM_OK) return fail(st[i].status, fm_strerror(st[i].status));
   return FM_OK;
+}
+
+int fm_problem_status(fm_problem* p) {
+  if (!p || !p->batch) return fail(FM_ERR_INVALID, "problem is not in a batch");
+  fm_batch* b = p->batch;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  DevProbState st;
+  CK(cudaMemcpy(&st, b->D.pstate + p->index, sizeof(st), cudaMemcpyDeviceToHost));
+  return st.status;
 }
 
 int fm_batch_last_timing(fm_batch* b, double* ms, int64_t* launches) {
@@ -711,10 +1073,38 @@ int fm_batch_last_timing(fm_batch* b, double* ms, int64_t* launches) {
 
 int fm_batch_layout(fm_batch* b, int64_t* nt, int64_t* ni, int32_t* mc, int64_t* ns) {
   if (!b) return fail(FM_ERR_INVALID, "null batch");
-  if (nt) *nt = (int64_t)b->L.tiles.size();
-  if (ni) *ni = (int64_t)b->L.iface_node.size();
-  if (mc) *mc = b->L.max_colors;
-  if (ns) *ns = b->L.n_slots;
+  int64_t t = 0, i = 0, s = 0;
+  int32_t c = 0;
+  for (const Placement& pl : b->slots)
+    if (pl.p) {
+      t += pl.len[P_TILE];
+      i += pl.len[P_IFACE];
+      s += pl.len[P_SLOT];
+      c = std::max(c, pl.L->max_colors);
+    }
+  if (nt) *nt = t;
+  if (ni) *ni = i;
+  if (mc) *mc = c;
+  if (ns) *ns = s;
+  return FM_OK;
+}
+
+int fm_batch_resident(fm_batch* b, int32_t* problems, int64_t* elems, int64_t* free_elems) {
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  int32_t np = 0;
+  int64_t ne = 0;
+  for (const Placement& pl : b->slots)
+    if (pl.p) {
+      ++np;
+      ne += pl.p->E;
+    }
+  if (problems) *problems = np;
+  if (elems) *elems = ne;
+  if (free_elems) {
+    int64_t f = 0;
+    for (auto& kv : b->pools[P_ELEM].free) f = std::max(f, kv.second);
+    *free_elems = f;
+  }
   return FM_OK;
 }
 
@@ -724,17 +1114,18 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
   if (!b) return fail(FM_ERR_INVALID, "problem is not in a batch");
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
-  const int pi = p->index;
-  const int64_t nb = b->L.node_begin[pi], eb = b->L.elem_begin[pi];
-  const int64_t N = p->N, E = p->E, EC = b->L.elem_count[pi];
-  const std::vector<int32_t>& nn = b->L.node_new[pi];
-  const std::vector<int32_t>& eo = b->L.elem_old[pi];
+  const Placement& pl = b->slots[p->index];
+  const int64_t nb = pl.off[P_NODE], eb = pl.off[P_ELEM];
+  const int64_t N = p->N, E = p->E;
+  const std::vector<int32_t>& nn = pl.L->node_new[0];
+  const std::vector<int32_t>& eo = pl.L->elem_old[0];
+  const int64_t EC = (int64_t)eo.size();
   std::vector<double> tmp(N);
   double* cols[4] = {b->D.su, b->D.sv, b->D.sw, b->D.sp};
   if (u) {
     for (int c = 0; c < 3; ++c) {
       CK(cudaMemcpy(tmp.data(), cols[c] + nb, sizeof(double) * N, cudaMemcpyDeviceToHost));
-      for (int64_t i = 0; i < N; ++i) u[i * 3 + c] = tmp[nn[i] - nb];
+      for (int64_t i = 0; i < N; ++i) u[i * 3 + c] = tmp[nn[i]];
     }
     if (b->solver == FM_SOLVER_SUPG && p->params.glob_fixed)
       for (int64_t i = 0; i < N; ++i)
@@ -744,18 +1135,18 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
   if (b->solver == FM_SOLVER_VMS) {
     if (pres) {
       CK(cudaMemcpy(tmp.data(), cols[3] + nb, sizeof(double) * N, cudaMemcpyDeviceToHost));
-      for (int64_t i = 0; i < N; ++i) pres[i] = tmp[nn[i] - nb];
+      for (int64_t i = 0; i < N; ++i) pres[i] = tmp[nn[i]];
     }
     if (elem3 || sdus) {
       std::vector<double> h((size_t)E * 12), col(EC);
       std::vector<float> colf(b->D.sdus32 ? EC : 0);
       for (int q = 0; q < 12; ++q) {
         if (b->D.sdus32) {
-          CK(cudaMemcpy(colf.data(), b->D.sdus32 + (int64_t)q * b->L.n_elems + eb, sizeof(float) * EC,
+          CK(cudaMemcpy(colf.data(), b->D.sdus32 + (int64_t)q * b->D.E + eb, sizeof(float) * EC,
                         cudaMemcpyDeviceToHost));
           for (int64_t k = 0; k < EC; ++k) col[k] = colf[k];
         } else {
-          CK(cudaMemcpy(col.data(), b->D.sdus + (int64_t)q * b->L.n_elems + eb, sizeof(double) * EC,
+          CK(cudaMemcpy(col.data(), b->D.sdus + (int64_t)q * b->D.E + eb, sizeof(double) * EC,
                         cudaMemcpyDeviceToHost));
         }
         for (int64_t k = 0; k < EC; ++k)

@@ -108,6 +108,19 @@ typedef struct fm_tuning {
   int32_t reserved[4];
 } fm_tuning;
 
+/* Pool capacities of a batch created empty (fm_batch_create_empty).  The
+ * batch's problems all share solver, element type and precision. */
+typedef struct fm_capacity {
+  int32_t solver;          /* FM_SOLVER_* */
+  int32_t elem_type;       /* FM_TET4 / FM_HEXA8 */
+  int32_t precision;       /* FM_FP64 / FM_MIXED */
+  int32_t max_problems;    /* resident problems at the same time */
+  int64_t max_elems;       /* resident elements, all problems together */
+  int64_t max_nodes;       /* resident nodes, all problems together */
+  int64_t max_table_rows;  /* NODEVEL table rows, all problems (0: max_nodes) */
+  int64_t reserved[4];
+} fm_capacity;
+
 typedef struct fm_problem fm_problem;
 typedef struct fm_batch fm_batch;
 
@@ -140,6 +153,26 @@ FM_API int fm_batch_create(fm_problem* const* problems, int32_t n, const fm_tuni
                     fm_batch** out);
 FM_API int fm_batch_destroy(fm_batch* b);
 
+/* Continuous batching.  fm_batch_create_empty allocates device pools of the
+ * given capacities once; fm_batch_add places a problem into free ranges of
+ * them (its state starts at the time-0 BCs, as in fm_batch_create) and
+ * returns FM_ERR_OOM when some pool has no room, leaving the batch as it was;
+ * fm_batch_remove frees a problem's ranges (its results are lost: read them
+ * first).  Both wait for the batch's stream.  A problem's stepping and
+ * results do not depend on which other problems share its batch.
+ * fm_problem_prepare builds the problem's tile layout ahead of
+ * fm_batch_add/fm_batch_create (host only; different problems may be
+ * prepared on different threads).  None of these has a counterpart in the
+ * reference, which solves one model per process (femSolver::solve). */
+FM_API int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning, int32_t device, fm_batch** out);
+FM_API int fm_batch_add(fm_batch* b, fm_problem* p);
+FM_API int fm_batch_remove(fm_batch* b, fm_problem* p);
+FM_API int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning);
+
+/* Resident problems, their elements and the largest free run of element
+ * slots (admission control). */
+FM_API int fm_batch_resident(fm_batch* b, int32_t* problems, int64_t* elems, int64_t* largest_free_elems);
+
 /* Advances every problem of the batch by nsteps time steps (VMS: each with
  * tot_dual_steps+1 dual iterations) on the given cudaStream_t (NULL: the
  * batch's own stream).  Asynchronous; fm_batch_sync waits and reports the
@@ -147,9 +180,19 @@ FM_API int fm_batch_destroy(fm_batch* b);
 FM_API int fm_batch_step(fm_batch* b, int32_t nsteps, void* stream);
 FM_API int fm_batch_sync(fm_batch* b);
 
-/* Per-problem step targets for ragged batches: problem i advances by
- * nsteps[i] (0 = idle) in the next fm_batch_step_ragged call. */
+/* Per-problem step targets for ragged batches: the i-th resident problem
+ * (in the order of the fm_batch_create array; problems added later follow
+ * in slot order) advances by nsteps[i] (0 = idle). */
 FM_API int fm_batch_step_ragged(fm_batch* b, const int32_t* nsteps, void* stream);
+
+/* Advances only the listed problems (each by its nsteps entry); the rest of
+ * the batch idles. */
+FM_API int fm_batch_step_problems(fm_batch* b, fm_problem* const* problems, const int32_t* nsteps, int32_t count,
+                                  void* stream);
+
+/* Device status of one problem of a batch (FM_OK, FM_ERR_DIVERGED,
+ * FM_ERR_TABLE, FM_ERR_TIMEOUT); waits for the batch's stream. */
+FM_API int fm_problem_status(fm_problem* p);
 
 /* Copies a problem's current state to host memory, in the problem's own
  * node/element numbering.
