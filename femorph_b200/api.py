@@ -28,6 +28,7 @@ SYMBOLS = [
     "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
     "fm_batch_profile", "fm_autotune", "fm_batch_create_empty", "fm_batch_add", "fm_batch_remove",
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
+    "fm_vms_solve_static",
 ]
 
 
@@ -104,6 +105,7 @@ def lib():
         L.fm_batch_resident.argtypes = [P, P, P, P]
         L.fm_batch_step_problems.argtypes = [P, P, P, C.c_int32, P]
         L.fm_problem_status.argtypes = [P]
+        L.fm_vms_solve_static.argtypes = [P, C.c_int32, C.c_int32, P, P, P]
         _lib = L
     return _lib
 

@@ -52,6 +52,8 @@ enum { FM_FP64 = 0, FM_MIXED = 1 };
 /* FM_MIXED: tets whose aspect ratio h_max / (2 sqrt(6) r_in) exceeds this
  * limit keep their Jacobian inverse in FP64 (regular tet 1.0, Kuhn tet 1.7). */
 #define FM_MIXED_ASPECT_LIMIT 3.0
+/* Size of the fixed device array behind fm_vms_solve_static (32 MiB). */
+#define FM_STATIC_SCRATCH_BYTES (32u << 20)
 /* NODEDOF global fixed dofs (femSUPGExplicitFluidSolver.cpp:1527-1561) */
 enum { FM_FIX_NONE = 0, FM_FIX_X = 1, FM_FIX_Y = 2, FM_FIX_Z = 4 };
 
@@ -172,6 +174,31 @@ FM_API int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning);
 /* Resident problems, their elements and the largest free run of element
  * slots (admission control). */
 FM_API int fm_batch_resident(fm_batch* b, int32_t* problems, int64_t* elems, int64_t* largest_free_elems);
+
+/* VMS solve that allocates no device memory, for callers that cannot call
+ * cudaMalloc: a process whose device memory another allocator already holds
+ * (a framework's caching allocator), or a latency-bound path on which
+ * cudaMalloc/cudaFree, which synchronise the whole device, are not
+ * acceptable.  It has no counterpart in the reference.
+ *
+ * Runs nsteps time steps of problem p (VMS, tet4, FP64; fm_problem_prepare
+ * must have built its tile layout) from its initial state with the same
+ * kernels as fm_batch_step, and writes the final velocity (n_nodes x 3) and
+ * pressure (n_nodes) to the host arrays u and pres (either may be NULL),
+ * in the problem's node numbering.  All device data - the problem's copy
+ * and the kernels' scratch - lives in one fixed array of
+ * FM_STATIC_SCRATCH_BYTES per GPU, held from the time the library's device
+ * code is loaded on that GPU (at the latest the first call) until the
+ * process exits.  Problems that need more (above roughly 200,000
+ * tetrahedra) are rejected with FM_ERR_INVALID.  The first call on a device
+ * looks up the array's device address and sets the kernels' shared-memory
+ * limit; make that first call before any stream capture on the device.
+ * Every call shares the array: calls that overlap on the GPU (from
+ * different host threads or streams) race and must be serialised by the
+ * caller.  Each call clears what has to start at zero.  stream: a
+ * cudaStream_t (NULL: the default stream); the call returns after the
+ * stream has finished its work. */
+FM_API int fm_vms_solve_static(fm_problem* p, int32_t nsteps, int32_t device, double* u, double* pres, void* stream);
 
 /* Advances every problem of the batch by nsteps time steps (VMS: each with
  * tot_dual_steps+1 dual iterations) on the given cudaStream_t (NULL: the
