@@ -14,7 +14,9 @@ import numpy as np
 from . import mesh as _mesh
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfemorph_b200.so")
+# FEMORPH_B200_LIB selects another build of the library (e.g. a variant built
+# elsewhere); by default the in-tree build is loaded.
+LIB_PATH = os.environ.get("FEMORPH_B200_LIB") or os.path.join(HERE, "libfemorph_b200.so")
 
 FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_ERR_CUDA, FM_ERR_DIVERGED, FM_ERR_TIMEOUT, FM_ERR_TABLE, FM_ERR_IO, \
     FM_ERR_NODEVICE = range(9)

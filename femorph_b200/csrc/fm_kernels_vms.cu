@@ -70,24 +70,38 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
                                             const double pq[4], bool pending, bool first_dual, double inv_dt,
                                             double c1nu, double nu4, double lres[4][4]) {
   const int64_t E = B.E;
-  double X[4][3], U[4][3], Pn[4], Q[4][3];
-  // node record: (x, y) (z, u) (v, w) (p, BC tag); Q is the velocity before
-  // the last BC application, which differs from U only at BC nodes (tag >= 0:
-  // the node's global id), read from memory there
+  // Pass 1 reads the coordinates and Q, the velocity before the last BC
+  // application (it differs from the staged state only at BC nodes, tag >= 0
+  // = the node's global id, and is read from memory there).  FP64: pass 2
+  // re-reads the post-BC velocity U and pressure from shared memory, so the
+  // two velocity sets are never held in registers at the same time (the
+  // FP32 form, with fewer live registers, reads them in pass 1).
+  // Node record: (x, y) (z, u) (v, w) (p, BC tag).
+  double X[4][3], Q[4][3], U[4][3], Pn[4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     const double2 r0 = s_rec[rec_index(ln[a], 0)], r1 = s_rec[rec_index(ln[a], 1)],
                   r2 = s_rec[rec_index(ln[a], 2)], r3 = s_rec[rec_index(ln[a], 3)];
     X[a][0] = r0.x; X[a][1] = r0.y; X[a][2] = r1.x;
-    U[a][0] = r1.y; U[a][1] = r2.x; U[a][2] = r2.y;
-    Pn[a] = r3.x;
+    if constexpr (MIXED) {
+      U[a][0] = r1.y; U[a][1] = r2.x; U[a][2] = r2.y;
+      Pn[a] = r3.x;
+    }
     const long long g = __double_as_longlong(r3.y);
     if (g >= 0) {
       Q[a][0] = B.pu[g]; Q[a][1] = B.pv[g]; Q[a][2] = B.pw[g];
     } else {
-      Q[a][0] = U[a][0]; Q[a][1] = U[a][1]; Q[a][2] = U[a][2];
+      Q[a][0] = r1.y; Q[a][1] = r2.x; Q[a][2] = r2.y;
     }
   }
+  auto load_post = [&]() {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const double2 r1 = s_rec[rec_index(ln[a], 1)], r2 = s_rec[rec_index(ln[a], 2)], r3 = s_rec[rec_index(ln[a], 3)];
+      U[a][0] = r1.y; U[a][1] = r2.x; U[a][2] = r2.y;
+      Pn[a] = r3.x;
+    }
+  };
   if constexpr (MIXED) {
     TetGeomF geo;
     tet_geometry_mixed(X, precise, geo);
@@ -95,7 +109,9 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
     float sdu[4][3];
 #pragma unroll
     for (int q = 0; q < 12; ++q) sdu[q / 3][q % 3] = sd_in[q];
+    float G[3][3], Ds[3];
     if (pending) {
+      // velocities enter FP32 as differences to node 0, formed in FP64
       float Q0[3], Qd[4][3], pqd[4];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -105,7 +121,7 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
       }
 #pragma unroll
       for (int a = 0; a < 4; ++a) pqd[a] = (float)(pq[a] - pq[0]);
-      vms_subscale_update_mixed(geo, Q0, Qd, pqd, sdu, (float)inv_dt, (float)c1nu, (float)P.c2, ih);
+      vms_subscale_update_mixed(geo, Q0, Qd, pqd, sdu, (float)inv_dt, (float)c1nu, (float)P.c2, ih, G, Ds);
 #pragma unroll
       for (int q = 0; q < 12; ++q) __stcs(B.sdus32 + (int64_t)q * E + e, sdu[q / 3][q % 3]);
     }
@@ -117,14 +133,16 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
       for (int a = 0; a < 4; ++a) Ud[a][i] = (float)(U[a][i] - U[0][i]);
     }
     if (first_dual) {
-      vms_residual_mixed<false>(geo, U0, Ud, Pn, Ud, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, lres);
+      vms_residual_mixed<false>(geo, U0, Ud, Pn, Ud, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, G, Ds, false,
+                                lres);
     } else {
       float Dacc[4][3];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int i = 0; i < 3; ++i) Dacc[a][i] = (float)(U[a][i] - Q[a][i]);
-      vms_residual_mixed<true>(geo, U0, Ud, Pn, Dacc, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, lres);
+      vms_residual_mixed<true>(geo, U0, Ud, Pn, Dacc, sdu, (float)nu4, (float)P.inv_eps, (float)inv_dt, G, Ds, false,
+                               lres);
     }
   } else {
     (void)precise;
@@ -134,15 +152,17 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
     double sdu[4][3];
 #pragma unroll
     for (int q = 0; q < 12; ++q) sdu[q / 3][q % 3] = sd_in[q];
+    double G[3][3], Gs[3];
     if (pending) {
-      vms_subscale_update<double>(geo, Q, pq, sdu, inv_dt, c1nu, P.c2, ih);
+      vms_subscale_update<double>(geo, Q, pq, sdu, inv_dt, c1nu, P.c2, ih, G, Gs);
 #pragma unroll
       for (int q = 0; q < 12; ++q) __stcs(B.sdus + (int64_t)q * E + e, sdu[q / 3][q % 3]);
     }
+    load_post();
     if (first_dual)
-      vms_residual<double, false>(geo, U, Pn, U, sdu, nu4, P.inv_eps, inv_dt, lres);
+      vms_residual<double, false>(geo, U, Pn, U, sdu, nu4, P.inv_eps, inv_dt, G, Gs, false, lres);
     else
-      vms_residual<double, true>(geo, U, Pn, Q, sdu, nu4, P.inv_eps, inv_dt, lres);
+      vms_residual<double, true>(geo, U, Pn, Q, sdu, nu4, P.inv_eps, inv_dt, G, Gs, false, lres);
   }
 }
 

@@ -15,6 +15,12 @@ namespace fm {
 
 #define FM_VA 0.58541020
 #define FM_VB 0.13819660
+// Gauss-point projection coefficients (see vms_subscale_update):
+// S = ALPHA + 3 BETA, FM_PR = BETA (S + ALPHA - BETA) / S,
+// FM_PG1 = (ALPHA - BETA)^2 / S - 1.
+#define FM_VS (FM_VA + 3.0 * FM_VB)
+#define FM_PR (FM_VB * (FM_VS + (FM_VA - FM_VB)) / FM_VS)
+#define FM_PG1 ((FM_VA - FM_VB) * (FM_VA - FM_VB) / FM_VS - 1.0)
 
 // Element geometry: initial_assemble (src lines 21-91).  Products are
 // rounded individually (no FMA contraction) so DN and V are bit-identical to
@@ -64,11 +70,13 @@ __device__ __forceinline__ void tet_geometry(const double X[4][3], TetGeom& g) {
 //   pq  : pressures of the problem's nodes 0..3 (src line 489 reads
 //         sol_n[i][3] with the local index i)
 //   sdu : in = subscales at the 4 Gauss points, out = updated subscales
+//   G, Us (out): velocity gradient and nodal velocity sum of U, which the
+//         residual reuses when U equals the post-BC state (no BC node)
 template <typename T>
 __device__ __forceinline__ void vms_subscale_update(const TetGeom& geo, const T U[4][3], const T pq[4], T sdu[4][3],
-                                                    T inv_dt, T c1nu, T c2, T ih) {
-  const T A = (T)FM_VA, Bt = (T)FM_VB, AB = (T)(FM_VA - FM_VB);
-  T G[3][3], gp[3];
+                                                    T inv_dt, T c1nu, T c2, T ih, T G[3][3], T Us[3]) {
+  const T Bt = (T)FM_VB, AB = (T)(FM_VA - FM_VB);
+  T gp[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
 #pragma unroll
@@ -77,7 +85,6 @@ __device__ __forceinline__ void vms_subscale_update(const TetGeom& geo, const T 
                 (T)geo.DN[j][3] * U[3][i];
     gp[i] = (T)geo.DN[i][0] * pq[0] + (T)geo.DN[i][1] * pq[1] + (T)geo.DN[i][2] * pq[2] + (T)geo.DN[i][3] * pq[3];
   }
-  T Us[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) Us[i] = (U[0][i] + U[1][i]) + (U[2][i] + U[3][i]);
   T r[4][3];
@@ -92,23 +99,18 @@ __device__ __forceinline__ void vms_subscale_update(const TetGeom& geo, const T 
 #pragma unroll
     for (int i = 0; i < 3; ++i) r[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2] + gp[i];
   }
-  // Element-local L2 projection of r onto P1: P_a = sum_g lN[g][a] r_g / sum_g lN[g][a],
-  // evaluated back at the Gauss points.
-  const T invS = (T)1 / (A + (T)3 * Bt);
+  // Element-local L2 projection of r onto P1, P_a = sum_g lN[g][a] r_g / S
+  // (S = sum_g lN[g][a] = ALPHA + 3 BETA), evaluated back at the Gauss
+  // points: sum_a lN[g][a] P_a = BETA sum_a P_a + (ALPHA - BETA) P_g, and
+  // sum_a P_a = R = sum_g r_g, so the projection at g is FM_PR R + FM_PG r_g.
   T tau_u_inv = c1nu * ih * ih + c2 * sqrt_nr(maxa2) * ih;
   T tau1 = rcp_nr(inv_dt + tau_u_inv);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    T R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);
-    T Pa[4];
+    const T R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);
+    const T cR = (T)FM_PR * R;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) Pa[a] = (Bt * R + AB * r[a][i]) * invS;
-    T Ps = (Pa[0] + Pa[1]) + (Pa[2] + Pa[3]);
-#pragma unroll
-    for (int g = 0; g < 4; ++g) {
-      T proj = Bt * Ps + AB * Pa[g];
-      sdu[g][i] = ((sdu[g][i] * inv_dt - r[g][i]) + proj) * tau1;
-    }
+    for (int g = 0; g < 4; ++g) sdu[g][i] = (sdu[g][i] * inv_dt + ((T)FM_PG1 * r[g][i] + cR)) * tau1;
   }
 }
 
@@ -116,24 +118,29 @@ __device__ __forceinline__ void vms_subscale_update(const TetGeom& geo, const T 
 // dual state after BCs), u_prev = Up (previous dual state), forcing 0
 // (femNode::force is never set) and subgrid pressure 0 (include_sg_p =
 // false).  Writes the 16 nodal residual entries lRes[a][0..3].
+// G, Us: velocity gradient and nodal velocity sum of U when have_G (from the
+// subscale update), else computed here.
 template <typename T, bool HAS_PREV>
 __device__ __forceinline__ void vms_residual(const TetGeom& geo, const T U[4][3], const T P[4], const T Up[4][3],
-                                             const T sdu[4][3], T nu4, T inv_eps, T inv_dt, double lRes[4][4]) {
+                                             const T sdu[4][3], T nu4, T inv_eps, T inv_dt, T G[3][3], T Us[3],
+                                             bool have_G, double lRes[4][4]) {
   const T Bt = (T)FM_VB, AB = (T)(FM_VA - FM_VB);
   const T S = (T)FM_VA + (T)3 * Bt;
-  T G[3][3];
+  if (!have_G) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 3; ++i) {
 #pragma unroll
-    for (int j = 0; j < 3; ++j)
-      G[i][j] = (T)geo.DN[j][0] * U[0][i] + (T)geo.DN[j][1] * U[1][i] + (T)geo.DN[j][2] * U[2][i] +
-                (T)geo.DN[j][3] * U[3][i];
+      for (int j = 0; j < 3; ++j)
+        G[i][j] = (T)geo.DN[j][0] * U[0][i] + (T)geo.DN[j][1] * U[1][i] + (T)geo.DN[j][2] * U[2][i] +
+                  (T)geo.DN[j][3] * U[3][i];
+      Us[i] = (U[0][i] + U[1][i]) + (U[2][i] + U[3][i]);
+    }
+  }
   const T tr = (G[0][0] + G[1][1]) + G[2][2];
-  T Us[3], Ups[3];
+  T Ups[3];
+  if (HAS_PREV) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    Us[i] = (U[0][i] + U[1][i]) + (U[2][i] + U[3][i]);
-    if (HAS_PREV) Ups[i] = (Up[0][i] + Up[1][i]) + (Up[2][i] + Up[3][i]);
+    for (int i = 0; i < 3; ++i) Ups[i] = (Up[0][i] + Up[1][i]) + (Up[2][i] + Up[3][i]);
   }
   const T Psum = (P[0] + P[1]) + (P[2] + P[3]);
   // X_g = (a_g . grad) u (+ acceleration); M2[i][k] = sum_g sdu_g[i] a_g[k]
@@ -164,8 +171,9 @@ __device__ __forceinline__ void vms_residual(const TetGeom& geo, const T U[4][3]
 #pragma unroll
       for (int k = 0; k < 3; ++k) M2[i][k] += sdu[g][i] * hah[k];
     }
-    Hs += Bt * Psum + AB * P[g];
   }
+  // sum_g (BETA Psum + (ALPHA - BETA) P_g) = S Psum
+  Hs = S * Psum;
   // K'[i][k] = 4 nu G[i][k] - M2[i][k] - Hs delta_ik ; lRes[a][i] = V/4 (lumped terms + K'.DN)
   T Kp[3][3];
 #pragma unroll
@@ -258,12 +266,14 @@ __device__ __forceinline__ void tet_geometry_mixed(const double X[4][3], bool pr
 
 // Subscale update, FP32.  U0: velocity of node 0; Ud[a] = U[a] - U0 (Ud[0] = 0);
 // pqd[a] = pq[a] - pq[0].
+// G, Ds (out): gradient and difference sum of Ud, reused by the residual
+// when there is no BC node.
 __device__ __forceinline__ void vms_subscale_update_mixed(const TetGeomF& geo, const float U0[3], const float Ud[4][3],
                                                           const float pqd[4], float sdu[4][3], float inv_dt, float c1nu,
-                                                          float c2, float ih) {
+                                                          float c2, float ih, float G[3][3], float Ds[3]) {
   const float A = (float)FM_VA, Bt = (float)FM_VB, AB = (float)(FM_VA - FM_VB);
   const float S = A + 3.0f * Bt;
-  float G[3][3], gp[3], Ds[3];
+  float gp[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
 #pragma unroll
@@ -283,17 +293,13 @@ __device__ __forceinline__ void vms_subscale_update_mixed(const TetGeomF& geo, c
 #pragma unroll
     for (int i = 0; i < 3; ++i) r[g][i] = G[i][0] * hah[0] + G[i][1] * hah[1] + G[i][2] * hah[2] + gp[i];
   }
-  const float invS = 1.0f / S;
   const float tau1 = ptx_rcp_approx(inv_dt + c1nu * ih * ih + c2 * (maxa2 > 0.0f ? maxa2 * ptx_rsqrt_approx(maxa2) : 0.0f) * ih);
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const float R = (r[0][i] + r[1][i]) + (r[2][i] + r[3][i]);
-    float Pa[4];
+    const float cR = (float)FM_PR * R;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) Pa[a] = (Bt * R + AB * r[a][i]) * invS;
-    const float Ps = (Pa[0] + Pa[1]) + (Pa[2] + Pa[3]);
-#pragma unroll
-    for (int g = 0; g < 4; ++g) sdu[g][i] = ((sdu[g][i] * inv_dt - r[g][i]) + (Bt * Ps + AB * Pa[g])) * tau1;
+    for (int g = 0; g < 4; ++g) sdu[g][i] = (sdu[g][i] * inv_dt + ((float)FM_PG1 * r[g][i] + cR)) * tau1;
   }
 }
 
@@ -303,15 +309,17 @@ __device__ __forceinline__ void vms_subscale_update_mixed(const TetGeomF& geo, c
 template <bool HAS_PREV>
 __device__ __forceinline__ void vms_residual_mixed(const TetGeomF& geo, const float U0[3], const float Ud[4][3],
                                                    const double P[4], const float Dacc[4][3], const float sdu[4][3],
-                                                   float nu4, float inv_eps, float inv_dt, double lRes[4][4]) {
+                                                   float nu4, float inv_eps, float inv_dt, float G[3][3], float Ds[3],
+                                                   bool have_G, double lRes[4][4]) {
   const float A = (float)FM_VA, Bt = (float)FM_VB, AB = (float)(FM_VA - FM_VB);
   const float S = A + 3.0f * Bt;
-  float G[3][3], Ds[3];
+  if (!have_G) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 3; ++i) {
 #pragma unroll
-    for (int j = 0; j < 3; ++j) G[i][j] = geo.DN[j][1] * Ud[1][i] + geo.DN[j][2] * Ud[2][i] + geo.DN[j][3] * Ud[3][i];
-    Ds[i] = Ud[1][i] + Ud[2][i] + Ud[3][i];
+      for (int j = 0; j < 3; ++j) G[i][j] = geo.DN[j][1] * Ud[1][i] + geo.DN[j][2] * Ud[2][i] + geo.DN[j][3] * Ud[3][i];
+      Ds[i] = Ud[1][i] + Ud[2][i] + Ud[3][i];
+    }
   }
   const float tr = (G[0][0] + G[1][1]) + G[2][2];
   float X[4][3], M2[3][3], Ssdu[3];
