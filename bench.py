@@ -242,6 +242,65 @@ def batched_line(args, world, rb):
                                      "after_steps": args.warmup + args.steps + min(args.steps, 50)}}
 
 
+def _gen_request_problem(args):
+    from femorph_b200 import serve
+    return serve.make_problem(*args)
+
+
+def run_serve(args, local_rank):
+    """Config 5: Poisson stream of cavity solves (n ~ U{12..64}, steps ~
+    U{100..2000}, nu log-U[1e-3,1e-1], lid U[0.5,2], per-request seed) served
+    by femorph_b200.serve.Server under a stated HBM budget, at each arrival
+    rate, for each precision.  The meshes are generated before the timed runs
+    (client side, spawned processes) and reused across rates."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    from femorph_b200 import api, serve
+    params = serve.request_params(args.requests, seed=args.seed)
+    with cf.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn")) as ex:
+        problems = list(ex.map(_gen_request_problem, params))
+    rates = [float(x) for x in args.rates.split(",")]
+    budget = int(args.budget_gb * (1 << 30))
+    precs = [("mixed", api.FM_MIXED), ("fp64", api.FM_FP64)]
+    if args.precision != "both":
+        precs = [x for x in precs if x[0] == args.precision]
+    out = {}
+    for pn, prec in precs:
+        rows = []
+        for rate in rates:
+            reqs = serve.draw_requests(args.requests, rate, seed=args.seed, problems=problems)
+            srv = serve.Server(precision=prec, hbm_budget=budget, max_problems=256, block=50, device=local_rank,
+                               keep_results=False)
+            with ClockSampler(local_rank) as clk:
+                st = srv.run(reqs)
+            srv.close()
+            mean_work = sum(r.problem.n_elems * r.steps for r in reqs) / len(reqs)
+            st.update({"rate_req_per_s": rate, "offered_element_steps_per_s": rate * mean_work,
+                       "clocks": clk.summary(), "capacity": srv.capacity})
+            rows.append(st)
+        out[pn] = rows
+    return out
+
+
+def serve_line(args, res):
+    head = "mixed" if "mixed" in res else "fp64"
+    rows = res[head]
+    top = rows[-1]
+    return {"metric": "served VMS cavity stream: aggregate element-steps/s with p50/p99 latency",
+            "value": top["element_steps_per_s"], "unit": "element-steps/s", "n_gpus": 1, "steps": None,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": f"{args.requests} cavity requests per rate, Poisson arrivals, n~U{{12..64}}, "
+                                   f"steps~U{{100..2000}}, nu log-U[1e-3,1e-1], lid U[0.5,2], dt from CFL 0.05 "
+                                   f"on lid+sqrt(invEps); continuous batching, "
+                                   f"50-step rounds, HBM budget {args.budget_gb} GiB",
+                       "rates_req_per_s": args.rates, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": "one GPU, one pooled batch"},
+            "p50_latency_s": top["p50_latency_s"], "p99_latency_s": top["p99_latency_s"],
+            "serving": res, "clocks": top["clocks"]}
+
+
 def cpu_baseline(n: int, steps: int = 1):
     """Oracle B (plain-C restatement, single thread) on `steps` steps of the same mesh."""
     from oracle import oracle_b
@@ -308,7 +367,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=96)
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
-    ap.add_argument("--config", default="cavity", choices=["cavity", "batched"])
+    ap.add_argument("--config", default="cavity", choices=["cavity", "batched", "serve"])
+    ap.add_argument("--rates", default="10,30,100,1000", help="serve: arrival rates, requests/s")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
+    ap.add_argument("--budget-gb", type=float, default=16.0, help="serve: HBM budget of the pooled batch")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--ref-steps", type=int, default=2)
@@ -336,6 +398,13 @@ def main():
         torch.cuda.set_device(local_rank)
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = td
+    if args.config == "serve":
+        if rank == 0:
+            print(json.dumps(serve_line(args, run_serve(args, local_rank))), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.config == "batched":
         rb = run_batched(args, rank, world, local_rank, dist)
         if rank == 0:

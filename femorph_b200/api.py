@@ -30,7 +30,7 @@ SYMBOLS = [
     "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
     "fm_batch_profile", "fm_autotune", "fm_batch_create_empty", "fm_batch_add", "fm_batch_remove",
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
-    "fm_vms_solve_static",
+    "fm_vms_solve_static", "fm_batch_capacity_bytes",
 ]
 
 
@@ -107,6 +107,7 @@ def lib():
         L.fm_batch_resident.argtypes = [P, P, P, P]
         L.fm_batch_step_problems.argtypes = [P, P, P, C.c_int32, P]
         L.fm_problem_status.argtypes = [P]
+        L.fm_batch_capacity_bytes.argtypes = [P, P, P]
         L.fm_vms_solve_static.argtypes = [P, C.c_int32, C.c_int32, P, P, P]
         _lib = L
     return _lib
@@ -250,6 +251,16 @@ class Batch:
             pass
 
 
+def capacity_bytes(solver, elem_type, max_problems, max_elems, max_nodes, precision=FM_FP64, max_table_rows=0,
+                   tile_elems=0, tile_nodes=0, threads=0) -> int:
+    """Device bytes a Pool of these capacities allocates."""
+    cap = FmCapacity(solver, elem_type, precision, max_problems, max_elems, max_nodes, max_table_rows)
+    t = FmTuning(tile_elems, tile_nodes, threads, 0)
+    out = C.c_int64()
+    check(lib().fm_batch_capacity_bytes(C.byref(cap), C.byref(t), C.byref(out)))
+    return out.value
+
+
 class Pool:
     """Batch with fixed device pools that problems join and leave between
     launches (continuous batching)."""
@@ -284,6 +295,16 @@ class Pool:
 
     def sync(self) -> None:
         check(lib().fm_batch_sync(self.h))
+
+    def wait(self) -> bool:
+        """Waits for the pool's work; True when some resident problem reports
+        a device error (FM_ERR_DIVERGED, FM_ERR_TABLE, FM_ERR_TIMEOUT), which
+        GpuProblem.status() then tells apart; other errors raise."""
+        r = lib().fm_batch_sync(self.h)
+        if r in (FM_ERR_DIVERGED, FM_ERR_TABLE, FM_ERR_TIMEOUT):
+            return True
+        check(r)
+        return False
 
     def last_timing(self):
         ms = C.c_double()

@@ -388,6 +388,10 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
       }
       std::vector<int64_t> idx(ne);
       std::iota(idx.begin(), idx.end(), 0);
+      // elements sorted by colour: SUPG processes a tile one colour at a
+      // time; for VMS it spreads each chunk's contributions over all of the
+      // tile's nodes (one or two per node and chunk, which balances the
+      // node-owner accumulation; the space-filling order measured slower)
       std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
       tm.col_begin = (int32_t)L.tile_cols.size();
       tm.n_col = ncol;

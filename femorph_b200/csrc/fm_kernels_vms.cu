@@ -241,6 +241,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     mbar_init(&bars[1], 1);
     fence_mbar_init();
     s_abort = 0;
+    // the first chunk's copies overlap the node staging below (they target
+    // the stage buffers, which the staging does not touch)
+    if (nchunks > 0) issue(0);
   }
   for (int ln = tid; ln < tm.n_node; ln += THREADS) {
     const int g = B.tile_nodes[tm.node_begin + ln];
@@ -267,15 +270,18 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   const double c1nu = P.c1 * P.nu;
   const double nu4 = 4.0 * P.nu;
   __syncthreads();
-  if (tid == 0 && nchunks > 0) issue(0);
 
-  // nodes owned by this thread for the accumulation: tid, tid+THREADS, ...;
-  // cur/end walk each one's incidence list in element order
+  // nodes owned by this thread for the accumulation: consecutive local nodes
+  // (which tend to be active in the same chunk) go to different warps,
+  // node = j * THREADS + lane * warps + warp; cur/end walk each one's
+  // incidence list in element order
   constexpr int MAXOWN = FM_MAX_TILE_NODES / THREADS;  // the host caps tile_nodes
+  constexpr int WARPS = THREADS / 32;
+  auto owned_node = [](int t, int j) { return j * THREADS + t; };
   int cur[MAXOWN], endi[MAXOWN];
 #pragma unroll
   for (int j = 0; j < MAXOWN; ++j) {
-    const int ln = tid + j * THREADS;
+    const int ln = owned_node(tid, j);
     cur[j] = ln < tm.n_node ? s_off[ln] : 0;
     endi[j] = ln < tm.n_node ? s_off[ln + 1] : 0;
   }
@@ -316,20 +322,23 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     // owners add this chunk's contributions to their nodes, in element order
 #pragma unroll
     for (int j = 0; j < MAXOWN; ++j) {
-      const int ln = tid + j * THREADS;
+      const int ln = owned_node(tid, j);
       if (ln < tm.n_node) {
         double a0 = s_a0[ln], a1 = s_a1[ln], a2 = s_a2[ln], a3 = s_a3[ln];
-        while (cur[j] < endi[j]) {
-          const int ent = s_inc[cur[j]];
+        int c = cur[j];
+        const int ce = endi[j];
+        while (c < ce) {
+          const int ent = s_inc[c];
           const int col = (ent >> 2) - base;
           if (col >= THREADS) break;
-          const int r = (ent & 3) * 4;
-          a0 += R[(r + 0) * THREADS + col];
-          a1 += R[(r + 1) * THREADS + col];
-          a2 += R[(r + 2) * THREADS + col];
-          a3 += R[(r + 3) * THREADS + col];
-          ++cur[j];
+          const double* Rp = R + (ent & 3) * 4 * THREADS + col;  // rows 4*corner .. 4*corner+3
+          a0 += Rp[0];
+          a1 += Rp[THREADS];
+          a2 += Rp[2 * THREADS];
+          a3 += Rp[3 * THREADS];
+          ++c;
         }
+        cur[j] = c;
         s_a0[ln] = a0; s_a1[ln] = a1; s_a2[ln] = a2; s_a3[ln] = a3;
       }
     }

@@ -200,7 +200,8 @@ static int put(T* dev_base, int64_t off, const T* src, int64_t n, cudaStream_t s
 }
 
 static void default_tuning(int solver, int npe, fm_tuning& t) {
-  if (t.threads != 128 && t.threads != 256) t.threads = 128;
+  // 64-thread CTAs exist for the VMS kernels only
+  if (t.threads != 128 && t.threads != 256 && !(t.threads == 64 && solver == FM_SOLVER_VMS)) t.threads = 128;
   if (t.tile_elems <= 0) t.tile_elems = (npe == 8) ? 384 : 1024;
   if (t.tile_nodes <= 0) t.tile_nodes = (npe == 8) ? 640 : 512;
   if (t.tile_nodes > 4096) t.tile_nodes = 4096;
@@ -220,6 +221,15 @@ static int prepare(fm_problem* p, int te, int tn, std::shared_ptr<Layout>* out) 
   fm_problem* arr[1] = {p};
   int r = build_layout(arr, 1, te, tn, *L);
   if (r) return r;
+  if (p->params.solver == FM_SOLVER_VMS && p->params.precision == FM_MIXED) {
+    // mixed form: elements whose Jacobian inverse stays in FP64 (aspect ratio
+    // above the limit) are flagged in bit 15 of their first tile-local node id
+    for (int64_t k = 0; k < L->elem_count[0]; ++k) {
+      const int32_t oe = L->elem_old[0][k];
+      if (oe >= 0 && tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT)
+        L->conn_local[(size_t)k * 4] |= 0x8000;
+    }
+  }
   p->layout = L;
   p->layout_te = te;
   p->layout_tn = tn;
@@ -463,15 +473,9 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
     r = r ? r : put(const_cast<int32_t*>(D.tab_len), pl.off[P_TAB], p->tab_len.data(), (int64_t)p->tab_len.size(), s);
     r = r ? r : put(const_cast<double*>(D.tab_rows), pl.off[P_ROW] * 4, p->tab_rows.data(), (int64_t)p->tab_rows.size(), s);
   }
-  // element data: connectivity (mixed: FP64-inverse flag in bit 15), zero history
+  // element data: connectivity (mixed: FP64-inverse flags set by prepare()), zero history
   {
-    std::vector<uint16_t> conn(L.conn_local);
-    if (b->solver == FM_SOLVER_VMS && b->precision == FM_MIXED)
-      for (int64_t k2 = 0; k2 < L.elem_count[0]; ++k2) {
-        const int32_t oe = L.elem_old[0][k2];
-        if (oe >= 0 && tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT)
-          conn[(size_t)k2 * 4] |= 0x8000;
-      }
+    const std::vector<uint16_t>& conn = L.conn_local;
     r = r ? r : put(const_cast<uint16_t*>(D.conn), eoff * npe, conn.data(), (int64_t)conn.size(), s);
     const int64_t ne = pl.len[P_ELEM];
     if (D.sdus32)
@@ -573,6 +577,49 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
   b->slots[ps] = std::move(pl);
   refresh_extent(b);
   return configure(b);
+}
+
+// Pool capacities of fm_batch_create_empty for the given maxima.  Tiles hold
+// about tile_elems elements (at least half that unless tile_nodes binds
+// first); each tile start is padded to a multiple of 32 element slots;
+// tile-boundary nodes appear once per tile that touches them (about 1.4 N
+// for tet tiles of 1024 elements) and own one interface partial slot each;
+// BC records exist for boundary nodes only.  A problem that needs more than
+// what is left gets FM_ERR_OOM from fm_batch_add.
+static void capacity_pools(const fm_capacity* cap, int te, int64_t c[P_COUNT]) {
+  const int64_t E = cap->max_elems, N = cap->max_nodes, P = cap->max_problems, npe = cap->elem_type;
+  c[P_NODE] = N;
+  c[P_TILE] = E / std::max<int64_t>(1, te / 2) + 2 * P;
+  c[P_ELEM] = E + 2 * P * ELEM_ALIGN + c[P_TILE] * ELEM_ALIGN;
+  c[P_TNODE] = 2 * N + 16 * c[P_TILE];
+  c[P_TCOL] = c[P_TILE] * 130;
+  c[P_TINC] = npe * E + 16 * c[P_TILE] + 16 * P;
+  c[P_TOFF] = c[P_TNODE] + c[P_TILE];
+  c[P_SLOT] = 2 * N + 32 * c[P_TILE];
+  c[P_IFACE] = N;
+  c[P_ISLOT] = c[P_SLOT];
+  c[P_REC] = N / 2 + 64 * P;
+  c[P_TAB] = c[P_REC];
+  c[P_ROW] = cap->max_table_rows > 0 ? cap->max_table_rows : c[P_REC];
+  c[P_PROB] = P;
+}
+
+// Device bytes allocate() takes for these pool capacities.
+static int64_t pool_bytes(const int64_t cap[P_COUNT], int solver, int npe, int prec, bool history) {
+  const int64_t NN = std::max<int64_t>(cap[P_NODE], 1);
+  const int64_t NE = (std::max<int64_t>(cap[P_ELEM], 1) + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
+  auto at_least = [](int64_t v, int64_t m) { return std::max<int64_t>(v, m); };
+  int64_t b = NN * (12 * 8 + 4) + NE * npe * 2;
+  if (solver == FM_SOLVER_VMS && prec == FM_MIXED) b += NE * 12 * 4;
+  else if (solver == FM_SOLVER_VMS || history) b += NE * (solver == FM_SOLVER_VMS ? 12 : 3 * npe) * 8;
+  if (solver == FM_SOLVER_SUPG) b += NE * 3 * 8;
+  b += at_least(cap[P_TILE], 1) * (int64_t)sizeof(TileMeta) + at_least(cap[P_TNODE], 1) * 4 +
+       at_least(cap[P_TCOL], 1) * 4 + at_least(cap[P_TINC], 8) * 2 + at_least(cap[P_TOFF], 1) * 2;
+  b += at_least(cap[P_SLOT], 1) * 4 * 8 + at_least(cap[P_IFACE], 1) * 4 * 4 + at_least(cap[P_ISLOT], 1) * 4;
+  b += at_least(cap[P_REC], 1) * (int64_t)sizeof(BCRec) + at_least(cap[P_TAB], 1) * 2 * 4 + at_least(cap[P_ROW], 1) * 32;
+  const int64_t NP = at_least(cap[P_PROB], 1);
+  b += NP * ((int64_t)sizeof(DevProb) + (int64_t)sizeof(DevProbState) + 4 + 64);
+  return b;
 }
 
 extern "C" {
@@ -784,28 +831,8 @@ int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning, int32
   int r = new_batch(cap->solver, cap->elem_type, cap->precision, tuning, device, &b);
   if (r) return r;
   b->has_history = cap->solver == FM_SOLVER_SUPG;
-  const int64_t E = cap->max_elems, N = cap->max_nodes, P = cap->max_problems, npe = cap->elem_type;
-  const int64_t te = b->tune.tile_elems;
   int64_t c[P_COUNT];
-  c[P_NODE] = N;
-  // tiles hold about tile_elems elements (fewer where tile_nodes binds first);
-  // each tile start is padded to a multiple of 32 element slots
-  c[P_TILE] = E / std::max<int64_t>(1, te / 4) + 2 * P;
-  c[P_ELEM] = E + 2 * P * ELEM_ALIGN;
-  c[P_TNODE] = N + npe * E / 2;
-  c[P_TCOL] = c[P_TILE] * 130;
-  c[P_TINC] = npe * E + 16 * c[P_TILE] + 16 * P;
-  c[P_TOFF] = c[P_TNODE] + c[P_TILE];
-  // interface partial slots: tile-boundary node copies (a few per cent of the
-  // nodes for compact tiles); a problem that needs more gets FM_ERR_OOM
-  c[P_SLOT] = N + npe * E / 8;
-  c[P_IFACE] = N;
-  c[P_ISLOT] = N + npe * E / 8;
-  c[P_REC] = N;
-  c[P_TAB] = N;
-  c[P_ROW] = cap->max_table_rows > 0 ? cap->max_table_rows : N;
-  c[P_PROB] = P;
-  c[P_ELEM] += c[P_TILE] * ELEM_ALIGN;
+  capacity_pools(cap, b->tune.tile_elems, c);
   r = allocate(b, c);
   if (r) {
     release_all(b);
@@ -813,6 +840,19 @@ int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning, int32
     return r;
   }
   *out = b;
+  return FM_OK;
+}
+
+int fm_batch_capacity_bytes(const fm_capacity* cap, const fm_tuning* tuning, int64_t* bytes) {
+  if (!cap || !bytes) return fail(FM_ERR_INVALID, "null argument");
+  if (cap->elem_type != FM_TET4 && cap->elem_type != FM_HEXA8) return fail(FM_ERR_INVALID, "bad element type");
+  fm_tuning t;
+  memset(&t, 0, sizeof(t));
+  if (tuning) t = *tuning;
+  default_tuning(cap->solver, cap->elem_type, t);
+  int64_t c[P_COUNT];
+  capacity_pools(cap, t.tile_elems, c);
+  *bytes = pool_bytes(c, cap->solver, cap->elem_type, cap->precision, cap->solver == FM_SOLVER_SUPG);
   return FM_OK;
 }
 

@@ -170,6 +170,9 @@ FM_API int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning
 FM_API int fm_batch_add(fm_batch* b, fm_problem* p);
 FM_API int fm_batch_remove(fm_batch* b, fm_problem* p);
 FM_API int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning);
+/* Device bytes fm_batch_create_empty allocates for these capacities (HBM
+ * budgeting). */
+FM_API int fm_batch_capacity_bytes(const fm_capacity* cap, const fm_tuning* tuning, int64_t* bytes);
 
 /* Resident problems, their elements and the largest free run of element
  * slots (admission control). */

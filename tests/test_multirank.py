@@ -69,3 +69,12 @@ def test_two_ranks_gloo():
         assert t == 2.0  # max over ranks of (1 + rank)
         assert total == sum(costs)
         assert gathered == owned
+
+
+def test_served_stream_draws_are_reproducible():
+    from femorph_b200 import serve
+    a = serve.request_params(16, seed=9)
+    b = serve.request_params(16, seed=9)
+    assert a == b
+    ns = [x[0] for x in a]
+    assert min(ns) >= 12 and max(ns) <= 64
