@@ -35,6 +35,22 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic_per_element.json")
+
+
+def measured_traffic(kernel: str, precision: str, E: int):
+    """DRAM bytes (read + write) of one launch of `kernel`, from the ncu
+    capture summarised in profiles/: bytes per element measured on a smaller
+    mesh of the same family, scaled by the element count (traffic grows in
+    proportion).  None when no capture is recorded."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            d = json.load(f)
+        return d[kernel][precision]["bytes_per_element"] * E
+    except Exception:
+        return None
+
+
 def hbm_peak():
     try:
         with open(MEASURED_PEAKS) as f:
@@ -92,17 +108,40 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def algorithmic_bytes(E: int, N: int, precision: str) -> int:
-    """Compulsory HBM bytes of one VMS step: per element connectivity (4 x int32)
-    and the 12 Gauss-point subscales read and written; per node coordinates,
-    the 4-dof state read and written and the lumped mass.  Geometry (DN, V, h)
-    is recomputed from coordinates and not counted."""
-    sub = 48 if precision == "mixed" else 96
-    return E * (16 + 2 * sub) + N * (24 + 32 + 32 + 8)
+def algorithmic_bytes(E: int, N: int, precision: str, config: str = "cavity") -> int:
+    """Compulsory HBM bytes of one step.  VMS: per element connectivity (4 x
+    int32) and the 12 Gauss-point subscales read and written; per node
+    coordinates, the 4-dof state read and written and the lumped mass.  SUPG
+    (Euler, no history): per element connectivity (npe x int32); per node
+    coordinates, velocity read and written and the lumped mass.  Geometry is
+    recomputed from coordinates and not counted."""
+    if config == "cavity":
+        sub = 48 if precision == "mixed" else 96
+        return E * (16 + 2 * sub) + N * (24 + 32 + 32 + 8)
+    npe = 8 if config == "channel" else 4
+    return E * 4 * npe + N * (24 + 24 + 24 + 8)
 
 
-def make_problem(n: int, seed: int):
+# FP64 operations of one SUPG element-step (matrix-free K u over the Gauss
+# points, counting an FMA as two), estimated from the kernel's arithmetic.
+SUPG_FLOPS = {"channel": 9000, "supg": 2000}
+
+CONFIG_DEFAULT_N = {"cavity": 96, "supg": 96, "channel": 64}
+
+
+def make_problem(args, seed: int, n: int | None = None):
+    """The configured single-GPU workload: 'cavity' VMS Kuhn cavity n^3 x 6
+    tets; 'supg' the same mesh with the SUPG solver (Euler, K1-K4, no B-bar);
+    'channel' the hexa8 channel 4n x n x n (256 x 64 x 64 at n = 64), SUPG."""
     from femorph_b200 import mesh
+    n = n or args.n
+    if args.config == "supg":
+        # CFL 0.2 (dt = 0.2 h_min / lid) lets the explicit SUPG cavity grow
+        # without bound within a few dozen steps at 48^3 and above; 0.05 stays
+        # bounded by the lid speed for 300+ steps at 96^3
+        return mesh.cavity(n, seed=seed, steps=200, solver=mesh.SUPG, cfl=0.05)
+    if args.config == "channel":
+        return mesh.channel(4 * n, n, n, seed=seed, steps=500)
     return mesh.cavity(n, seed=seed, steps=200)
 
 
@@ -110,7 +149,7 @@ def run_ours(args, rank, world, local_rank, dist):
     from femorph_b200 import api, mesh
 
     prec = api.FM_MIXED if args.precision == "mixed" else api.FM_FP64
-    p = make_problem(args.n, seed=rank)
+    p = make_problem(args, seed=rank)
     E, N = p.n_elems, p.n_nodes
     g = api.GpuProblem(p, prec)
     tune = dict(tile_elems=args.tile_elems, tile_nodes=args.tile_nodes, threads=args.threads)
@@ -136,7 +175,7 @@ def run_ours(args, rank, world, local_rank, dist):
     b.close()
     g.close()
     res = dict(E=E, N=N, ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch, layout=lay,
-               state=state, steps_total=args.warmup + args.steps + min(args.steps, 50))
+               state=state, steps_total=args.warmup + args.steps + min(args.steps, 50), p=p)
     # end to end through the C ABI: host buffers in, state out
     if rank == 0:
         t0 = time.perf_counter()
@@ -301,17 +340,27 @@ def serve_line(args, res):
             "serving": res, "clocks": top["clocks"]}
 
 
-def cpu_baseline(n: int, steps: int = 1):
-    """Oracle B (plain-C restatement, single thread) on `steps` steps of the same mesh."""
+def cpu_sample_n(args) -> int:
+    """Mesh size of the bounded CPU sample: the full mesh for the tet
+    configs (a few seconds per step), a 64 x 16 x 16 channel for the hexa
+    one (the full 1 M hexa take minutes per step on one core)."""
+    return 16 if args.config == "channel" else args.n
+
+
+def cpu_baseline(args, steps: int = 1):
+    """Oracle B (plain-C restatement, single thread) on `steps` steps of the
+    workload (or of the bounded sample of cpu_sample_n)."""
     from oracle import oracle_b
-    p = make_problem(n, seed=0)
+    n = cpu_sample_n(args)
+    p = make_problem(args, seed=0, n=n)
     o = oracle_b.OracleSolve(p)
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
+    solver = "femVMSExplicitFluidSolver" if args.config == "cavity" else "femSUPGExplicitFluidSolver"
     return {"value": p.n_elems * steps / dt, "unit": "element-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{steps} time step(s) of the {n}^3 cavity ({p.n_elems} tets) with the single-threaded C "
-                      f"restatement of femVMSExplicitFluidSolver, setup excluded"}
+            "sample": f"{steps} time step(s) of {workload_name(args, n)} ({p.n_elems} elements) with the "
+                      f"single-threaded C restatement of {solver}, setup excluded"}
 
 
 def run_reference(args):
@@ -322,10 +371,10 @@ def run_reference(args):
     from femorph_b200 import mesh
     if not ref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/fm_refdrv was not built (reference sources absent)"}
-    n = args.n
+    n = cpu_sample_n(args)
     steps = max(1, min(args.steps, args.ref_steps))
     warm = max(1, min(args.warmup, 1))
-    p = make_problem(n, seed=0)
+    p = make_problem(args, seed=0, n=n)
     p.total_steps = steps + warm + 1
     p.save_every = 10 ** 9
     wd = tempfile.mkdtemp(prefix="fm_refbench_")
@@ -338,25 +387,51 @@ def run_reference(args):
     sec = float(np.sum(per))
     val = p.n_elems * len(per) / sec
     cores = 1
-    return {"impl": "reference", "metric": METRIC, "value": val, "unit": "element-steps/s", "n_gpus": args.gpus,
+    return {"impl": "reference", "metric": METRIC[args.config], "value": val, "unit": "element-steps/s",
+            "n_gpus": args.gpus,
             "steps": len(per), "warmup": warm, "ms_per_step": 1e3 * sec / len(per), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(n, p),
+            "config": workload_config(args),
             "cpu_baseline": {"value": val, "unit": "element-steps/s", "cores": cores, "kind": "reference",
-                             "sample": f"{len(per)} timed steps after {warm} warm-up of the {n}^3 cavity through "
-                                       f"femVMSExplicitFluidSolver::solve (reference sources, g++ -O2), "
-                                       f"parse/setup excluded; the reference is single-threaded"},
+                             "sample": f"{len(per)} timed steps after {warm} warm-up of {workload_name(args, n)} "
+                                       f"({p.n_elems} elements) through "
+                                       f"{'femVMSExplicitFluidSolver' if args.config == 'cavity' else 'femSUPGExplicitFluidSolver'}"
+                                       f"::solve (reference sources, g++ -O2), parse/setup excluded; the reference "
+                                       f"is single-threaded"},
             "e2e": {"value": val, "unit": "element-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-METRIC = "VMS element-steps/s (explicit step, 96^3 Kuhn-tet cavity)"
+METRIC = {"cavity": "VMS element-steps/s (explicit step, 96^3 Kuhn-tet cavity)",
+          "supg": "SUPG tet4 element-steps/s (explicit step, 96^3 Kuhn-tet cavity)",
+          "channel": "SUPG hexa8 element-steps/s (explicit step, 256x64x64 channel)"}
 
 
-def workload_config(n, p):
-    return {"workload": f"VMS tet4 lid-driven cavity {n}^3 cells x 6 Kuhn tets ({p.n_elems} tets, {p.n_nodes} nodes)"
-                        f", invEps=400, nu=0.01, CFL 0.2 on lid+sqrt(invEps)",
-            "elements": p.n_elems, "nodes": p.n_nodes, "l2": "inputs larger than L2 (no flush)",
-            "parallelism": "independent problem per GPU"}
+def workload_name(args, n):
+    if args.config == "channel":
+        return f"the hexa8 channel {4 * n}x{n}x{n}"
+    return f"the {n}^3 Kuhn-tet cavity"
+
+
+def workload_config(args, p=None, prec_name="fp64"):
+    """The configured workload at its full size (element and node counts of
+    `p`, else from the mesh generator's formulas)."""
+    n = args.n
+    if args.config == "channel":
+        E, N = (p.n_elems, p.n_nodes) if p is not None else (4 * n ** 3, (4 * n + 1) * (n + 1) ** 2)
+    else:
+        E, N = (p.n_elems, p.n_nodes) if p is not None else (6 * n ** 3, (n + 1) ** 3)
+    if args.config == "channel":
+        w = (f"SUPG hexa8 channel [0,4]x[0,1]^2, {4 * n}x{n}x{n} cells ({E} hexa, {N} nodes), "
+             f"jitter 0.05h, parabolic inlet peak 1, mu=0.005, CFL 0.2, EXOPTS 1 0 1 1 1 1, {prec_name} form")
+    else:
+        if args.config == "cavity":
+            kind, dtrule = "VMS", "invEps=400, nu=0.01, dt from CFL 0.2 on lid+sqrt(invEps)"
+        else:
+            kind, dtrule = "SUPG (EXOPTS 1 0 1 1 1 1)", "alpha=1, cI=4, nu=0.01, dt from CFL 0.05 on the lid speed"
+        w = (f"{kind} tet4 lid-driven cavity {n}^3 cells x 6 Kuhn tets ({E} tets, {N} nodes), "
+             f"{dtrule}, {prec_name} form")
+    return {"workload": w, "elements": E, "nodes": N, "l2": "inputs larger than L2 (no flush)",
+            "parallelism": "one independent problem per GPU"}
 
 
 def main():
@@ -365,9 +440,9 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=96)
+    ap.add_argument("--n", type=int, default=0, help="mesh size (default 96 for cavity/supg, 64 for channel)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
-    ap.add_argument("--config", default="cavity", choices=["cavity", "batched", "serve"])
+    ap.add_argument("--config", default="cavity", choices=["cavity", "supg", "channel", "batched", "serve"])
     ap.add_argument("--rates", default="10,30,100,1000", help="serve: arrival rates, requests/s")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
     ap.add_argument("--budget-gb", type=float, default=16.0, help="serve: HBM budget of the pooled batch")
@@ -379,6 +454,10 @@ def main():
     ap.add_argument("--tile-nodes", type=int, default=0)
     ap.add_argument("--threads", type=int, default=0)
     args = ap.parse_args()
+    if not args.n:
+        args.n = CONFIG_DEFAULT_N.get(args.config, 96)
+    if args.config in ("supg", "channel") and args.precision != "fp64":
+        args.precision = "fp64"   # the mixed form is implemented for the VMS solver
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -424,28 +503,33 @@ def main():
 
         def summary(pn, r):
             E, N = r["E"], r["N"]
-            ab = algorithmic_bytes(E, N, pn)
+            ab = algorithmic_bytes(E, N, pn, args.config)
             klaunch = max(1, r["klaunch"])
             tile_ms = r["kprof"]["tile"] / klaunch
             achieved = ab / (tile_ms * 1e-3) / 1e9
+            kernel = "vms_tile_kernel" if args.config == "cavity" else "supg_tile_kernel"
+            roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": measured_traffic(kernel, pn, E), "peak_source": peak_kind, "kernel": kernel,
+                    "algorithmic_bytes_per_launch": ab, "avg_launch_ms": tile_ms,
+                    "iface_kernel_avg_ms": r["kprof"]["iface"] / klaunch}
+            if args.config in SUPG_FLOPS:
+                # the SUPG element work is FP64-pipe bound: FLOP rate beside the bytes
+                roof["fp64_tflops"] = SUPG_FLOPS[args.config] * E / (tile_ms * 1e-3) / 1e12
+                roof["fp64_flops_per_element_step"] = SUPG_FLOPS[args.config]
             return {"value": world * E * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
-                    "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                                 "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                                 "kernel": "vms_tile_kernel", "algorithmic_bytes_per_launch": ab,
-                                 "avg_launch_ms": tile_ms, "iface_kernel_avg_ms": r["kprof"]["iface"] / klaunch}}
+                    "roofline": roof}
 
         head = precs[0]
         r = runs[head]
         E, N = r["E"], r["N"]
         s = summary(head, r)
         line = {
-            "metric": METRIC, "value": s["value"], "unit": "element-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": s["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
-            "config": {"workload": f"VMS tet4 lid-driven cavity {args.n}^3 cells x 6 Kuhn tets ({E} tets, {N} nodes), "
-                                   f"invEps=400, nu=0.01, dt from CFL 0.2 on lid+sqrt(invEps), {head} form",
-                       "elements": E, "nodes": N, "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"{world} independent cavity solve(s), one per GPU"},
+            "metric": METRIC[args.config], "value": s["value"], "unit": "element-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": s["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": dict(workload_config(args, r["p"], head),
+                           parallelism=f"{world} independent solve(s), one per GPU"),
             "roofline": s["roofline"],
             "gpu_launches": r["launches"], "clocks": r["clocks"], "layout": r["layout"],
         }
@@ -466,7 +550,7 @@ def main():
                                    "wall clock"}
         if world == 1 and not args.no_cpu:
             try:
-                line["cpu_baseline"] = cpu_baseline(args.n, 1)
+                line["cpu_baseline"] = cpu_baseline(args, 1)
             except Exception as e:  # the baseline is reported, not required
                 line["cpu_baseline"] = {"error": str(e)}
         print(json.dumps(line), flush=True)
