@@ -340,6 +340,20 @@ def serve_line(args, res):
             "serving": res, "clocks": top["clocks"]}
 
 
+def host_cpu() -> dict:
+    """Host CPU model and core count (the CPU baselines use one core)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "cores_total": os.cpu_count(), "cores_used": 1}
+
+
 def cpu_sample_n(args) -> int:
     """Mesh size of the bounded CPU sample: the full mesh for the tet
     configs (a few seconds per step), a 64 x 16 x 16 channel for the hexa
@@ -358,7 +372,7 @@ def cpu_baseline(args, steps: int = 1):
     o.step(steps)
     dt = time.perf_counter() - t0
     solver = "femVMSExplicitFluidSolver" if args.config == "cavity" else "femSUPGExplicitFluidSolver"
-    return {"value": p.n_elems * steps / dt, "unit": "element-steps/s", "cores": 1, "kind": "port",
+    return {"value": p.n_elems * steps / dt, "unit": "element-steps/s", "cores": 1, "kind": "port", "host": host_cpu(),
             "sample": f"{steps} time step(s) of {workload_name(args, n)} ({p.n_elems} elements) with the "
                       f"single-threaded C restatement of {solver}, setup excluded"}
 
@@ -393,6 +407,7 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args),
             "cpu_baseline": {"value": val, "unit": "element-steps/s", "cores": cores, "kind": "reference",
+                             "host": host_cpu(),
                              "sample": f"{len(per)} timed steps after {warm} warm-up of {workload_name(args, n)} "
                                        f"({p.n_elems} elements) through "
                                        f"{'femVMSExplicitFluidSolver' if args.config == 'cavity' else 'femSUPGExplicitFluidSolver'}"
@@ -448,7 +463,7 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=16.0, help="serve: HBM budget of the pooled batch")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--ref-steps", type=int, default=2)
+    ap.add_argument("--ref-steps", type=int, default=5, help="reference arm: timed steps (bounded sample)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tile-elems", type=int, default=0)
     ap.add_argument("--tile-nodes", type=int, default=0)
