@@ -471,8 +471,6 @@ def main():
     args = ap.parse_args()
     if not args.n:
         args.n = CONFIG_DEFAULT_N.get(args.config, 96)
-    if args.config in ("supg", "channel") and args.precision != "fp64":
-        args.precision = "fp64"   # the mixed form is implemented for the VMS solver
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

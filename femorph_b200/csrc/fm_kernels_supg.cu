@@ -45,8 +45,10 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
   if (status != FM_OK) B.pstate[pidx].status = status;
 }
 
-template <int NPE, int THREADS>
-__global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int tn_max) {
+// MIXED: Gauss-point work in FP32 (supg_element_mixed), at most ~168
+// registers a thread so that three 128-thread CTAs fit an SM.
+template <int NPE, int THREADS, bool MIXED>
+__global__ void __launch_bounds__(THREADS, MIXED && THREADS == 128 ? 3 : 1) supg_tile_kernel(DevBatch B, int tn_max) {
   extern __shared__ double sm[];
   double* s_x = sm;
   double* s_y = s_x + tn_max;
@@ -58,6 +60,8 @@ __global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int t
   double* s_a1 = s_a0 + tn_max;
   double* s_a2 = s_a1 + tn_max;
   int32_t* s_col = (int32_t*)(s_a2 + tn_max);
+  __shared__ ShapeTable<NPE, double> s_shape;
+  __shared__ ShapeTable<NPE, float> s_shape_f;
 
   const TileMeta tm = B.tiles[blockIdx.x];
   const int pidx = tm.problem;
@@ -77,6 +81,8 @@ __global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int t
     s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0;
   }
   for (int c = tid; c <= tm.n_col; c += THREADS) s_col[c] = B.tile_cols[tm.col_begin + c];
+  fill_shape_table<NPE, double>(&s_shape);
+  if (MIXED) fill_shape_table<NPE, float>(&s_shape_f);
   __syncthreads();
   const int64_t E = B.E;
   int c_lo = 0;
@@ -96,7 +102,23 @@ __global__ void __launch_bounds__(THREADS, 1) supg_tile_kernel(DevBatch B, int t
         ln[4 % NPE] = cw.z & 0xffff; ln[5 % NPE] = cw.z >> 16; ln[6 % NPE] = cw.w & 0xffff; ln[7 % NPE] = cw.w >> 16;
       }
       double lam, reg;
-      supg_element<NPE>(P, s_x, s_y, s_z, s_u, s_v, s_w, ln, k, lam, reg);
+      if constexpr (MIXED) {
+        // bit 15 of the first id flags an element whose Jacobian stays FP64
+        const bool precise = (ln[0] & 0x8000) != 0;
+        ln[0] &= 0x7fff;
+        float Xr[NPE][3], U0[3], Ud[NPE][3];
+        const double x0 = s_x[ln[0]], y0 = s_y[ln[0]], z0 = s_z[ln[0]];
+        const double u0 = s_u[ln[0]], v0 = s_v[ln[0]], w0 = s_w[ln[0]];
+        U0[0] = (float)u0; U0[1] = (float)v0; U0[2] = (float)w0;
+#pragma unroll
+        for (int a = 0; a < NPE; ++a) {
+          Xr[a][0] = (float)(s_x[ln[a]] - x0); Xr[a][1] = (float)(s_y[ln[a]] - y0); Xr[a][2] = (float)(s_z[ln[a]] - z0);
+          Ud[a][0] = (float)(s_u[ln[a]] - u0); Ud[a][1] = (float)(s_v[ln[a]] - v0); Ud[a][2] = (float)(s_w[ln[a]] - w0);
+        }
+        supg_element_mixed<NPE>(P, s_shape_f, s_shape, Xr, U0, Ud, precise, s_x, s_y, s_z, ln, k, lam, reg);
+      } else {
+        supg_element<NPE>(P, s_shape, s_x, s_y, s_z, s_u, s_v, s_w, ln, k, lam, reg);
+      }
       B.el_lam[e] = lam;
       B.el_reg[e] = reg;
       if (ab2) {
@@ -187,7 +209,7 @@ __global__ void supg_pressure_kernel(DevBatch B, int tn_max, double* pres) {
   for (int le = threadIdx.x; le < tm.n_elem; le += blockDim.x) {
     const int64_t e = tm.elem_begin + le;
     int ln[NPE];
-    for (int a = 0; a < NPE; ++a) ln[a] = B.conn[e * NPE + a];
+    for (int a = 0; a < NPE; ++a) ln[a] = B.conn[e * NPE + a] & 0x7fff;  // bit 15: mixed-form flag
     double num = 0.0, den = 0.0;
     for (int g = 0; g < GaussRule<NPE>::n; ++g) {
       double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
@@ -233,31 +255,39 @@ cudaError_t supg_configure(size_t smem, int npe) {
   if (e != cudaSuccess) return e;
   (void)smem;  // checked against the limit by the caller
   if (npe == 4) {
-    e = raise_dyn_smem(supg_tile_kernel<4, 128>, optin);
-    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 256>, optin);
+    e = raise_dyn_smem(supg_tile_kernel<4, 128, false>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 256, false>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 128, true>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 256, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<4>, optin);
   } else {
-    e = raise_dyn_smem(supg_tile_kernel<8, 128>, optin);
-    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256>, optin);
+    e = raise_dyn_smem(supg_tile_kernel<8, 128, false>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256, false>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 128, true>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<8>, optin);
   }
   return e;
 }
 
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, cudaStream_t s,
-                             cudaEvent_t* ev) {
+template <int NPE, bool MIXED>
+static void launch_supg_tile(const DevBatch& B, int tn_max, int threads, size_t smem, cudaStream_t s) {
+  if (threads == 256)
+    supg_tile_kernel<NPE, 256, MIXED><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+  else
+    supg_tile_kernel<NPE, 128, MIXED><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+}
+
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
+                             cudaStream_t s, cudaEvent_t* ev) {
   const size_t smem = supg_smem_bytes(tn_max, npe);
   if (ev) cudaEventRecord(ev[0], s);
   if (npe == 4) {
-    if (threads == 256)
-      supg_tile_kernel<4, 256><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
-    else
-      supg_tile_kernel<4, 128><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+    if (mixed) launch_supg_tile<4, true>(B, tn_max, threads, smem, s);
+    else launch_supg_tile<4, false>(B, tn_max, threads, smem, s);
   } else {
-    if (threads == 256)
-      supg_tile_kernel<8, 256><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
-    else
-      supg_tile_kernel<8, 128><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+    if (mixed) launch_supg_tile<8, true>(B, tn_max, threads, smem, s);
+    else launch_supg_tile<8, false>(B, tn_max, threads, smem, s);
   }
   if (ev) cudaEventRecord(ev[1], s);
   supg_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);

@@ -31,8 +31,8 @@ cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int
                                  cudaStream_t s, cudaEvent_t* ev);
 size_t supg_smem_bytes(int tn_max, int npe);
 cudaError_t supg_configure(size_t smem, int npe);
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, cudaStream_t s,
-                             cudaEvent_t* ev);
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
+                             cudaStream_t s, cudaEvent_t* ev);
 cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
 
 // Aspect ratio h_max / (2 sqrt(6) r_in) of a tet (1 for the regular tet,
@@ -72,6 +72,25 @@ static double tet_aspect_ratio(const double* X, const int32_t* c) {
   if (!(vol6 > 0.0)) return 1e300;
   const double r_in = 3.0 * (vol6 / 6.0) / area;
   return hmax / (2.0 * std::sqrt(6.0) * r_in);
+}
+
+// Aspect ratio of a hexa8 (corner order of femHexa8: bottom face 0-3, top
+// face 4-7): longest over shortest of its 12 edges (1 for a cube).
+static double hexa_aspect_ratio(const double* X, const int32_t* c) {
+  static const int ed[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  double lo = 1e300, hi = 0.0;
+  for (int k = 0; k < 12; ++k) {
+    double s = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double v = X[(int64_t)c[ed[k][0]] * 3 + d] - X[(int64_t)c[ed[k][1]] * 3 + d];
+      s += v * v;
+    }
+    lo = std::min(lo, s);
+    hi = std::max(hi, s);
+  }
+  if (!(lo > 0.0)) return 1e300;
+  return std::sqrt(hi / lo);
 }
 
 // First-fit range allocator over [0, cap) with coalescing free list.
@@ -221,13 +240,16 @@ static int prepare(fm_problem* p, int te, int tn, std::shared_ptr<Layout>* out) 
   fm_problem* arr[1] = {p};
   int r = build_layout(arr, 1, te, tn, *L);
   if (r) return r;
-  if (p->params.solver == FM_SOLVER_VMS && p->params.precision == FM_MIXED) {
+  if (p->params.precision == FM_MIXED) {
     // mixed form: elements whose Jacobian inverse stays in FP64 (aspect ratio
     // above the limit) are flagged in bit 15 of their first tile-local node id
+    const int npe = p->etype;
     for (int64_t k = 0; k < L->elem_count[0]; ++k) {
       const int32_t oe = L->elem_old[0][k];
-      if (oe >= 0 && tet_aspect_ratio(p->coords.data(), &p->conn[(int64_t)oe * 4]) > FM_MIXED_ASPECT_LIMIT)
-        L->conn_local[(size_t)k * 4] |= 0x8000;
+      if (oe < 0) continue;
+      const int32_t* c = &p->conn[(int64_t)oe * npe];
+      const double ar = npe == 4 ? tet_aspect_ratio(p->coords.data(), c) : hexa_aspect_ratio(p->coords.data(), c);
+      if (ar > FM_MIXED_ASPECT_LIMIT) L->conn_local[(size_t)k * npe] |= 0x8000;
     }
   }
   p->layout = L;
@@ -653,8 +675,6 @@ int fm_problem_create(const fm_mesh* m, const fm_bc* bc, const fm_params* prm, c
   if (prm->solver == FM_SOLVER_SUPG && m->elem_type == FM_TET4 && prm->ex_opts[1])
     return fail(FM_ERR_INVALID, "B-bar (EXOPTS 2nd field) is hexa8-only; the reference reads out of bounds on tet4");
   if (prm->precision != FM_FP64 && prm->precision != FM_MIXED) return fail(FM_ERR_INVALID, "bad precision");
-  if (prm->solver == FM_SOLVER_SUPG && prm->precision == FM_MIXED)
-    return fail(FM_ERR_INVALID, "the mixed form is implemented for the VMS solver");
   if (!(prm->time_step > 0)) return fail(FM_ERR_INVALID, "time_step must be positive");
   if (prm->props[0] == 0.0) return fail(FM_ERR_INVALID, "density must be non-zero");
   fm_problem* p = new fm_problem();
@@ -914,7 +934,7 @@ static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
   if (b->solver == FM_SOLVER_VMS)
     return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s,
                                 ev);
-  return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, s, ev);
+  return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, b->precision == FM_MIXED, s, ev);
 }
 
 // Sets per-slot targets (iterations) and launches enough iterations.  With

@@ -74,6 +74,30 @@ __device__ __forceinline__ void shape(const double q[3], double N[NPE], double d
   }
 }
 
+// Shape values and local derivatives at the Gauss points, tabulated once per
+// CTA in shared memory with the same expressions as shape<NPE> (identical
+// values); the Gauss-point loops read them at warp-uniform addresses.
+template <int NPE, typename T>
+struct ShapeTable {
+  T N[GaussRule<NPE>::n][NPE];
+  T dN[GaussRule<NPE>::n][NPE][3];
+};
+
+template <int NPE, typename T>
+__device__ __forceinline__ void fill_shape_table(ShapeTable<NPE, T>* t) {
+  for (int g = threadIdx.x; g < GaussRule<NPE>::n; g += blockDim.x) {
+    double q[3], Nf[NPE], dN[NPE][3];
+    GaussRule<NPE>::point(g, q);
+    shape<NPE>(q, Nf, dN);
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+      t->N[g][a] = (T)Nf[a];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) t->dN[g][a][c] = (T)dN[a][c];
+    }
+  }
+}
+
 // Jacobian J[a][b] = sum_n dN[n][a] x[n][b] (femElement.cpp:104-127), its
 // cofactor inverse (femUtils.cpp:716-770), global derivatives
 // gd[n][b] = sum_c inv[b][c] dN[n][c] (femElement.cpp:345-352) and the
@@ -114,9 +138,10 @@ __device__ __forceinline__ double jacobian(const double dN[NPE][3], const double
 // the local ids ln[].  Also returns the element's lambda (volume average) and
 // regime (average of the Gauss-point regimes) for output.
 template <int NPE>
-__device__ __forceinline__ void supg_element(const DevProb& P, const double* sx, const double* sy, const double* sz,
-                                             const double* su, const double* sv, const double* sw, const int ln[NPE],
-                                             double k[NPE][3], double& lam_el, double& reg_el) {
+__device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<NPE, double>& tab, const double* sx,
+                                             const double* sy, const double* sz, const double* su, const double* sv,
+                                             const double* sw, const int ln[NPE], double k[NPE][3], double& lam_el,
+                                             double& reg_el) {
   const double rho = P.rho, mu = P.mu, alpha = P.alpha, cI = P.c_i;
   const double nu = mu / rho;
   const bool bbar = (P.ex_mask & 2) != 0;
@@ -133,9 +158,11 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const double* sx,
     for (int a = 0; a < NPE; ++a) num[a][0] = num[a][1] = num[a][2] = 0.0;
 #pragma unroll 1
     for (int g = 0; g < GaussRule<NPE>::n; ++g) {
-      double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
-      GaussRule<NPE>::point(g, q);
-      shape<NPE>(q, Nf, dN);
+      double dN[NPE][3], inv[3][3];
+#pragma unroll
+      for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dN[a][c] = tab.dN[g][a][c];
       const double det = jacobian<NPE>(dN, sx, sy, sz, ln, inv);
       const double w = det * wq;
       den += w;
@@ -153,9 +180,20 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const double* sx,
   double vol = 0.0, lam_int = 0.0, reg = 0.0;
 #pragma unroll 1
   for (int g = 0; g < GaussRule<NPE>::n; ++g) {
-    double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
-    GaussRule<NPE>::point(g, q);
-    shape<NPE>(q, Nf, dN);
+    double Nf[NPE], dN[NPE][3], inv[3][3];
+    if (NPE == 4) {
+      // tet4: constant derivatives, N from the point (cheaper than the table)
+      double q[3];
+      GaussRule<NPE>::point(g, q);
+      shape<NPE>(q, Nf, dN);
+    } else {
+#pragma unroll
+      for (int a = 0; a < NPE; ++a) {
+        Nf[a] = tab.N[g][a];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dN[a][c] = tab.dN[g][a][c];
+      }
+    }
     const double det = jacobian<NPE>(dN, sx, sy, sz, ln, inv);
     double gd[NPE][3];
 #pragma unroll
@@ -289,6 +327,260 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const double* sx,
     for (int c = 0; c < 3; ++c) k[a][c] *= mdt;
   lam_el = lam_int / vol;
   reg_el = reg / (double)GaussRule<NPE>::n;
+}
+
+}  // namespace fm
+
+namespace fm {
+
+// ---------------------------------------------------------------------------
+// Mixed precision SUPG element (FM_MIXED): the Gauss-point work in FP32,
+// k = -dt K u_e converted to FP64 for the nodal accumulation, the AB2 history
+// and the update, which stay FP64.  Coordinates and velocities enter FP32 as
+// differences to the element's node 0, formed in FP64 (Xr, Ud; Xr[0] = Ud[0]
+// = 0), so the Jacobian and the velocity gradient lose no digits to
+// cancellation.  Elements flagged `precise` (aspect ratio above
+// FM_MIXED_ASPECT_LIMIT) form the Jacobian and its inverse in FP64 from the
+// staged FP64 coordinates.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float rcp_f(float x) {
+  const float y = ptx_rcp_approx(x);
+  return fmaf(y, fmaf(-x, y, 1.0f), y);  // one Newton step: full FP32 accuracy
+}
+__device__ __forceinline__ float rsqrt_f(float x) {
+  const float y = ptx_rsqrt_approx(x);
+  return y * fmaf(-0.5f * x, y * y, 1.5f);
+}
+
+template <int NPE>
+__device__ __forceinline__ void supg_element_mixed(const DevProb& P, const ShapeTable<NPE, float>& tab,
+                                                   const ShapeTable<NPE, double>& tabd, const float Xr[NPE][3],
+                                                   const float U0[3], const float Ud[NPE][3], bool precise,
+                                                   const double* sx, const double* sy, const double* sz,
+                                                   const int ln[NPE], double k[NPE][3], double& lam_el,
+                                                   double& reg_el) {
+  const float rho = (float)P.rho, mu = (float)P.mu, alpha = (float)P.alpha, cI = (float)P.c_i;
+  const float nu = (float)(P.mu / P.rho);
+  const bool bbar = (P.ex_mask & 2) != 0;
+  const bool iK1 = (P.ex_mask & 4) != 0, iK2 = (P.ex_mask & 8) != 0, iK3 = (P.ex_mask & 16) != 0,
+             iK4 = (P.ex_mask & 32) != 0;
+  const float wq = (float)GaussRule<NPE>::weight();
+  float kf[NPE][3];
+#pragma unroll
+  for (int a = 0; a < NPE; ++a) kf[a][0] = kf[a][1] = kf[a][2] = 0.0f;
+  // shape values / local derivatives at Gauss point g: tet4 in closed form
+  // (constant derivatives), hexa8 from the shared-memory table
+  auto dNv = [&](int g, int a, int c) -> float {
+    if (NPE == 4) return a == 3 ? -1.0f : (a == c ? 1.0f : 0.0f);
+    return tab.dN[g][a][c];
+  };
+  auto Nv = [&](int g, int a) -> float {
+    if (NPE == 4) {
+      double q[3];
+      GaussRule<NPE>::point(g, q);
+      return a < 3 ? (float)q[a] : (float)(1.0 - q[0] - q[1] - q[2]);
+    }
+    return tab.N[g][a];
+  };
+  // per Gauss point: inverse Jacobian and det, FP32 or (precise) FP64
+  auto geometry = [&](int g, float inv[3][3]) -> float {
+    if (precise) {
+      double dN[NPE][3], invd[3][3];
+#pragma unroll
+      for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dN[a][c] = tabd.dN[g][a][c];
+      const double det = jacobian<NPE>(dN, sx, sy, sz, ln, invd);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) inv[i][j] = (float)invd[i][j];
+      return (float)det;
+    }
+    float J[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        float s = 0.0f;
+#pragma unroll
+        for (int n = 1; n < NPE; ++n) s += dNv(g, n, a) * Xr[n][b];
+        J[a][b] = s;
+      }
+    const float c00 = J[1][1] * J[2][2] - J[2][1] * J[1][2], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+                c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const float det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    const float id = rcp_f(det);
+    inv[0][0] = c00 * id;
+    inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+    inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    inv[1][0] = c01 * id;
+    inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+    inv[1][2] = (J[1][0] * J[0][2] - J[0][0] * J[1][2]) * id;
+    inv[2][0] = c02 * id;
+    inv[2][1] = (J[2][0] * J[0][1] - J[0][0] * J[2][1]) * id;
+    inv[2][2] = (J[0][0] * J[1][1] - J[1][0] * J[0][1]) * id;
+    return det;
+  };
+  // volume-averaged derivatives for B-bar (eval_avg_shapeDeriv, src lines 660-707)
+  float sd0[NPE][3];
+  if (NPE == 8 && bbar) {
+    float num[NPE][3], den = 0.0f;
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) num[a][0] = num[a][1] = num[a][2] = 0.0f;
+#pragma unroll 1
+    for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+      float inv[3][3];
+      const float w = geometry(g, inv) * wq;
+      den += w;
+#pragma unroll
+      for (int a = 0; a < NPE; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          num[a][b] += (inv[b][0] * dNv(g, a, 0) + inv[b][1] * dNv(g, a, 1) + inv[b][2] * dNv(g, a, 2)) * w;
+    }
+    const float iden = rcp_f(den);
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) sd0[a][b] = num[a][b] * iden;
+  }
+  float vol = 0.0f, lam_int = 0.0f, reg = 0.0f;
+#pragma unroll 1
+  for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+    float inv[3][3];
+    const float det = geometry(g, inv);
+    float gd[NPE][3];
+#pragma unroll
+    for (int a = 0; a < NPE; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        gd[a][b] = inv[b][0] * dNv(g, a, 0) + inv[b][1] * dNv(g, a, 1) + inv[b][2] * dNv(g, a, 2);
+    float G[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
+    float u[3] = {U0[0], U0[1], U0[2]}, gr[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+#pragma unroll
+    for (int a = 1; a < NPE; ++a) {
+      const float Na = Nv(g, a);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[c] += Na * Ud[a][c];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gr[c][d] += gd[a][d] * Ud[a][c];
+      }
+    }
+    const float div = gr[0][0] + gr[1][1] + gr[2][2];
+    // eval_stabilization (dt term removed in the reference)
+    const float trG = G[0][0] + G[1][1] + G[2][2];
+    float t2 = 0.0f, t3 = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
+      t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
+    }
+    t3 = t3 * nu * nu * cI;
+    const float tau = rsqrt_f(t2 + t3);
+    const float nuC = rcp_f(trG * tau);
+    // eval_bulk_modulus: lambda = alpha * max(mu/rho, sqrt(u^T G^-1 u))
+    float lam, regime;
+    {
+      const float m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
+                  m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
+      const float dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+      const float idg = rcp_f(dG);
+      const float i00 = (m11 * m22 - m21 * m12) * idg, i01 = (m02 * m21 - m01 * m22) * idg,
+                  i02 = (m01 * m12 - m02 * m11) * idg, i10 = (m12 * m20 - m10 * m22) * idg,
+                  i11 = (m00 * m22 - m02 * m20) * idg, i12 = (m10 * m02 - m00 * m12) * idg,
+                  i20 = (m10 * m21 - m20 * m11) * idg, i21 = (m20 * m01 - m00 * m21) * idg,
+                  i22 = (m00 * m11 - m10 * m01) * idg;
+      const float q2 = (i00 * u[0] + i01 * u[1] + i02 * u[2]) * u[0] + (i10 * u[0] + i11 * u[1] + i12 * u[2]) * u[1] +
+                       (i20 * u[0] + i21 * u[1] + i22 * u[2]) * u[2];
+      const float l2 = q2 > 0.0f ? q2 * rsqrt_f(q2) : sqrtf(q2);  // sqrt; NaN for negative input as sqrt
+      const float l1 = nu;
+      lam = alpha * ((l1 < l2) ? l2 : l1);  // std::max(limit_1, limit_2)
+      regime = (l1 > l2) ? 1.0f : 2.0f;
+    }
+    const float w = det * wq;
+    vol += w;
+    lam_int += lam * w;
+    reg += regime;
+    float conv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) conv[c] = u[0] * gr[c][0] + u[1] * gr[c][1] + u[2] * gr[c][2];
+    float eps[6];
+    if (NPE == 8 && bbar) {
+      float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f;
+#pragma unroll
+      for (int a = 1; a < NPE; ++a) {
+        const float B1 = (1.0f / 3.0f) * (sd0[a][0] - gd[a][0]), B2 = gd[a][0] - B1;
+        const float B3 = (1.0f / 3.0f) * (sd0[a][1] - gd[a][1]), B4 = gd[a][1] - B3;
+        const float B5 = (1.0f / 3.0f) * (sd0[a][2] - gd[a][2]), B6 = gd[a][2] - B5;
+        e0 += B2 * Ud[a][0] + B3 * Ud[a][1] + B5 * Ud[a][2];
+        e1 += B1 * Ud[a][0] + B4 * Ud[a][1] + B5 * Ud[a][2];
+        e2 += B1 * Ud[a][0] + B3 * Ud[a][1] + B6 * Ud[a][2];
+      }
+      // the node-0 term: B-bar rows sum to zero over the nodes, so the
+      // differences to node 0 give the same strain
+      eps[0] = e0; eps[1] = e1; eps[2] = e2;
+    } else {
+      eps[0] = gr[0][0]; eps[1] = gr[1][1]; eps[2] = gr[2][2];
+    }
+    eps[3] = gr[0][1] + gr[1][0];
+    eps[4] = gr[1][2] + gr[2][1];
+    eps[5] = gr[0][2] + gr[2][0];
+    const float l2m = lam + 2.0f * mu;
+    const float sig[6] = {l2m * eps[0] + lam * eps[1] + lam * eps[2], lam * eps[0] + l2m * eps[1] + lam * eps[2],
+                          lam * eps[0] + lam * eps[1] + l2m * eps[2], mu * eps[3], mu * eps[4], mu * eps[5]};
+    const float c1w = rho * w, c3w = rho * tau * w, c4w = rho * nuC * div * w;
+#pragma unroll
+    for (int a = 0; a < NPE; ++a) {
+      const float Aa = u[0] * gd[a][0] + u[1] * gd[a][1] + u[2] * gd[a][2];
+      float f[3] = {0.0f, 0.0f, 0.0f};
+      if (iK1) {
+        const float Na = Nv(g, a);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] += c1w * Na * conv[c];
+      }
+      if (iK3) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] += c3w * Aa * conv[c];
+      }
+      if (iK4) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f[c] += c4w * gd[a][c];
+      }
+      if (iK2) {
+        float r0, r1, r2;
+        if (NPE == 8 && bbar) {
+          const float B1 = (1.0f / 3.0f) * (sd0[a][0] - gd[a][0]), B2 = gd[a][0] - B1;
+          const float B3 = (1.0f / 3.0f) * (sd0[a][1] - gd[a][1]), B4 = gd[a][1] - B3;
+          const float B5 = (1.0f / 3.0f) * (sd0[a][2] - gd[a][2]), B6 = gd[a][2] - B5;
+          r0 = B2 * sig[0] + B1 * sig[1] + B1 * sig[2];
+          r1 = B3 * sig[0] + B4 * sig[1] + B3 * sig[2];
+          r2 = B5 * sig[0] + B5 * sig[1] + B6 * sig[2];
+        } else {
+          r0 = gd[a][0] * sig[0];
+          r1 = gd[a][1] * sig[1];
+          r2 = gd[a][2] * sig[2];
+        }
+        f[0] += (r0 + gd[a][1] * sig[3] + gd[a][2] * sig[5]) * w;
+        f[1] += (r1 + gd[a][0] * sig[3] + gd[a][2] * sig[4]) * w;
+        f[2] += (r2 + gd[a][1] * sig[4] + gd[a][0] * sig[5]) * w;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) kf[a][c] += f[c];
+    }
+  }
+  const double mdt = -P.dt;
+#pragma unroll
+  for (int a = 0; a < NPE; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) k[a][c] = mdt * (double)kf[a][c];
+  lam_el = (double)lam_int / (double)vol;
+  reg_el = (double)reg / (double)GaussRule<NPE>::n;
 }
 
 }  // namespace fm

@@ -196,6 +196,48 @@ def test_vms_mixed_precision_200_steps():
     assert eu <= 1e-6 and ep <= 1e-6, (eu, ep)
 
 
+def _mixed_vs_oracle(p, steps):
+    g = api.GpuProblem(p, api.FM_MIXED)
+    b = api.Batch([g])
+    b.step(steps)
+    b.sync()
+    u, pr, el, _ = g.state()
+    o = oracle_b.OracleSolve(p)
+    o.step(steps)
+    st, oel, _, _ = o.state()
+    b.close()
+    g.close()
+    return rel(u, st[:, :3]), rel(pr, oel[:, 0])
+
+
+def test_supg_mixed_hexa_channel_200_steps():
+    """SUPG mixed form (FP32 Gauss-point work, FP64 accumulation, history and
+    state) on the hexa8 channel, Euler and AB2 + B-bar, against the FP64
+    oracle after 200 steps: velocity <= 1e-6 relative L2."""
+    for ex in ((1, 0, 1, 1, 1, 1), (0, 1, 1, 1, 1, 1)):
+        p = mesh.channel(12, 6, 6, seed=3, steps=200, ex_opts=ex, noise=1e-3)
+        eu, ep = _mixed_vs_oracle(p, 200)
+        print(f"SUPG hexa mixed {ex}: u {eu:.3e} element p {ep:.3e}")
+        assert eu <= 1e-6, (ex, eu, ep)
+        assert ep <= 1e-4, (ex, eu, ep)
+
+
+def test_supg_mixed_tet_cavity_200_steps():
+    p = mesh.cavity(10, seed=4, steps=200, solver=mesh.SUPG, cfl=0.05)
+    eu, ep = _mixed_vs_oracle(p, 200)
+    print(f"SUPG tet mixed: u {eu:.3e} element p {ep:.3e}")
+    assert eu <= 1e-6, (eu, ep)
+
+
+def test_supg_mixed_badly_shaped_hexa():
+    """Strongly stretched hexa (aspect ratio > 3) take the FP64 Jacobian."""
+    p = mesh.channel(24, 4, 4, seed=5, steps=50, noise=1e-3)
+    p.coords[:, 0] *= 8.0   # cells 4/3 x 1/4 x 1/4: aspect ratio 5.3
+    eu, ep = _mixed_vs_oracle(p, 50)
+    print(f"SUPG stretched hexa mixed: u {eu:.3e} element p {ep:.3e}")
+    assert eu <= 1e-6, (eu, ep)
+
+
 def test_vms_mixed_badly_shaped_elements():
     """Strong jitter makes slivers: those elements take the FP64 Jacobian
     inverse; the mixed result stays within 1e-6 of FP64 after 20 steps."""
