@@ -49,8 +49,11 @@ enum {
 enum { FM_TET4 = 4, FM_HEXA8 = 8 };
 enum { FM_SOLVER_VMS = 0, FM_SOLVER_SUPG = 1 };
 enum { FM_FP64 = 0, FM_MIXED = 1 };
-/* FM_MIXED: tets whose aspect ratio h_max / (2 sqrt(6) r_in) exceeds this
- * limit keep their Jacobian inverse in FP64 (regular tet 1.0, Kuhn tet 1.7). */
+/* FM_MIXED (VMS and SUPG): Gauss-point work in FP32, nodal accumulation,
+ * history, lumped-mass division and state in FP64.  Elements whose aspect
+ * ratio exceeds this limit keep their Jacobian inverse in FP64: tets by
+ * h_max / (2 sqrt(6) r_in) (regular tet 1.0, Kuhn tet 1.7), hexa8 by longest
+ * over shortest edge (cube 1.0). */
 #define FM_MIXED_ASPECT_LIMIT 3.0
 /* Size of the fixed device array behind fm_vms_solve_static (32 MiB). */
 #define FM_STATIC_SCRATCH_BYTES (32u << 20)
