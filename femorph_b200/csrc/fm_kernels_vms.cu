@@ -245,14 +245,29 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     // the stage buffers, which the staging does not touch)
     if (nchunks > 0) issue(0);
   }
-  for (int ln = tid; ln < tm.n_node; ln += THREADS) {
-    const int g = B.tile_nodes[tm.node_begin + ln];
-    const long long tag = B.node_bc[g] >= 0 ? (long long)g : -1ll;
-    s_rec[rec_index(ln, 0)] = make_double2(B.x[g], B.y[g]);
-    s_rec[rec_index(ln, 1)] = make_double2(B.z[g], B.su[g]);
-    s_rec[rec_index(ln, 2)] = make_double2(B.sv[g], B.sw[g]);
-    s_rec[rec_index(ln, 3)] = make_double2(B.sp[g], __longlong_as_double(tag));
-    s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0; s_a3[ln] = 0.0;
+  // node staging: all of this thread's node ids first, then their loads,
+  // so the gathers of its (up to FM_MAX_TILE_NODES / THREADS) nodes overlap
+  constexpr int MAXOWN = FM_MAX_TILE_NODES / THREADS;  // the host caps tile_nodes
+  {
+    int gid[MAXOWN];
+#pragma unroll
+    for (int j = 0; j < MAXOWN; ++j) {
+      const int ln = tid + j * THREADS;
+      gid[j] = ln < tm.n_node ? B.tile_nodes[tm.node_begin + ln] : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < MAXOWN; ++j) {
+      const int ln = tid + j * THREADS;
+      const int g = gid[j];
+      if (g >= 0) {
+        const long long tag = B.node_bc[g] >= 0 ? (long long)g : -1ll;
+        s_rec[rec_index(ln, 0)] = make_double2(B.x[g], B.y[g]);
+        s_rec[rec_index(ln, 1)] = make_double2(B.z[g], B.su[g]);
+        s_rec[rec_index(ln, 2)] = make_double2(B.sv[g], B.sw[g]);
+        s_rec[rec_index(ln, 3)] = make_double2(B.sp[g], __longlong_as_double(tag));
+        s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0; s_a3[ln] = 0.0;
+      }
+    }
   }
   for (int i = tid; i <= tm.n_node; i += THREADS) s_off[i] = B.tile_off[tm.off_begin + i];
   {
@@ -275,7 +290,6 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
   // (which tend to be active in the same chunk) go to different warps,
   // node = j * THREADS + lane * warps + warp; cur/end walk each one's
   // incidence list in element order
-  constexpr int MAXOWN = FM_MAX_TILE_NODES / THREADS;  // the host caps tile_nodes
   constexpr int WARPS = THREADS / 32;
   auto owned_node = [](int t, int j) { return j * THREADS + t; };
   int cur[MAXOWN], endi[MAXOWN];
@@ -359,7 +373,10 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
     return;
   }
   int32_t status = FM_OK;
-  for (int ln2 = tid; ln2 < tm.n_node; ln2 += THREADS) {
+#pragma unroll
+  for (int j = 0; j < MAXOWN; ++j) {
+    const int ln2 = tid + j * THREADS;
+    if (ln2 >= tm.n_node) break;
     const double acc[4] = {s_a0[ln2], s_a1[ln2], s_a2[ln2], s_a3[ln2]};
     if (ln2 < tm.n_int) {
       const int g = B.tile_nodes[tm.node_begin + ln2];
