@@ -102,3 +102,72 @@ def test_batch_without_device_fails_loudly():
     with pytest.raises(api.FmError) as ei:
         api.Batch([g])
     assert ei.value.code == api.FM_ERR_NODEVICE
+
+
+def _mesh_struct(p, n_nodes=None, n_elems=None):
+    keep = (np.ascontiguousarray(p.coords, np.float64), np.ascontiguousarray(p.conn, np.int32))
+    m = api.FmMesh(p.elem_type, p.n_nodes if n_nodes is None else n_nodes,
+                   p.n_elems if n_elems is None else n_elems, keep[0].ctypes.data, keep[1].ctypes.data)
+    return m, keep
+
+
+def test_edge_case_inputs_rejected():
+    """Empty meshes, non-positive time steps, zero density, element types and
+    tile sizes beyond the 16-bit tile-local indices are errors, not crashes."""
+    L = api.lib()
+    p = mesh.cavity(2, seed=0, steps=1)
+    prm = api.FmParams()
+    prm.solver, prm.precision, prm.time_step = p.solver, api.FM_FP64, p.time_step
+    for i in range(5):
+        prm.props[i] = float(p.props[i])
+    h = C.c_void_p()
+    for nn, ne in ((0, p.n_elems), (p.n_nodes, 0)):
+        m, keep = _mesh_struct(p, nn, ne)
+        assert L.fm_problem_create(C.byref(m), None, C.byref(prm), None, C.byref(h)) == api.FM_ERR_INVALID
+    m, keep = _mesh_struct(p)
+    m.elem_type = 6
+    assert L.fm_problem_create(C.byref(m), None, C.byref(prm), None, C.byref(h)) == api.FM_ERR_INVALID
+    m.elem_type = 4
+    prm.time_step = 0.0
+    assert L.fm_problem_create(C.byref(m), None, C.byref(prm), None, C.byref(h)) == api.FM_ERR_INVALID
+    prm.time_step = p.time_step
+    prm.props[0] = 0.0
+    assert L.fm_problem_create(C.byref(m), None, C.byref(prm), None, C.byref(h)) == api.FM_ERR_INVALID
+    prm.props[0] = 1.0
+    assert L.fm_problem_create(C.byref(m), None, C.byref(prm), None, C.byref(h)) == api.FM_OK
+    L.fm_problem_destroy(h)
+    # tiles of more than 16383 tets overflow the 16-bit incidence entries
+    # (reachable with the SUPG node cap of 4096 per tile)
+    g = api.GpuProblem(mesh.cavity(16, seed=1, steps=1, solver=mesh.SUPG))
+    with pytest.raises(api.FmError) as ei:
+        g.prepare(tile_elems=20000, tile_nodes=4096)
+    assert ei.value.code == api.FM_ERR_INVALID
+    g.prepare()   # the default layout builds on the host without a GPU
+    g.close()
+
+
+def test_batch_composition_checked_before_device():
+    """Problems of different solvers / precisions cannot share a batch."""
+    a = api.GpuProblem(mesh.cavity(2, seed=0, steps=1))
+    b = api.GpuProblem(mesh.cavity(2, seed=1, steps=1), api.FM_MIXED)
+    arr = (C.c_void_p * 2)(a.h.value, b.h.value)
+    h = C.c_void_p()
+    assert api.lib().fm_batch_create(arr, 2, None, 0, C.byref(h)) == api.FM_ERR_INVALID
+    a.close()
+    b.close()
+
+
+def test_capacity_bytes_grow_with_capacity_and_static_entry_validates():
+    small = api.capacity_bytes(mesh.VMS, 4, 4, 100_000, 20_000, api.FM_FP64)
+    big = api.capacity_bytes(mesh.VMS, 4, 4, 1_000_000, 200_000, api.FM_FP64)
+    mixed = api.capacity_bytes(mesh.VMS, 4, 4, 1_000_000, 200_000, api.FM_MIXED)
+    assert 0 < small < big and mixed < big
+    # the allocation-free entry point checks its inputs before any device work
+    L = api.lib()
+    s = api.GpuProblem(mesh.cavity(2, seed=0, steps=1, solver=mesh.SUPG))
+    s.prepare()
+    assert L.fm_vms_solve_static(s.h, 1, 0, None, None, None) == api.FM_ERR_INVALID
+    v = api.GpuProblem(mesh.cavity(2, seed=0, steps=1))
+    assert L.fm_vms_solve_static(v.h, 1, 0, None, None, None) == api.FM_ERR_INVALID   # not prepared
+    s.close()
+    v.close()
