@@ -171,7 +171,7 @@ def run_ours(args, rank, world, local_rank, dist):
     kprof, klaunch = b.profile(min(args.steps, 50))
     b.sync()
     lay = b.layout()
-    state = g.state()[:2]
+    state = g.state(elements=False)[:2]
     b.close()
     g.close()
     res = dict(E=E, N=N, ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch, layout=lay,
@@ -183,7 +183,7 @@ def run_ours(args, rank, world, local_rank, dist):
         b2 = api.Batch([g2], device=local_rank, **tune)
         b2.step(args.steps)
         b2.sync()
-        u, pr, _, _ = g2.state()
+        u, pr, _, _ = g2.state(elements=False)
         t1 = time.perf_counter()
         b2.close()
         g2.close()

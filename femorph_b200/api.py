@@ -159,15 +159,17 @@ class GpuProblem:
         self.h = h
         self.n_nodes, self.n_elems, self.solver = p.n_nodes, p.n_elems, p.solver
 
-    def state(self):
-        """(u (N,3), p (N,) VMS | (E,) SUPG, elem (E,3) VMS | (E,2) SUPG, sdus (E,12) VMS | None)."""
+    def state(self, elements: bool = True):
+        """(u (N,3), p (N,) VMS | (E,) SUPG, elem (E,3) VMS | (E,2) SUPG, sdus (E,12) VMS | None);
+        elements=False reads velocity and pressure only (elem, sdus None)."""
         N, E = self.n_nodes, self.n_elems
         u = np.zeros((N, 3))
         vms = self.solver == _mesh.VMS
         p = np.zeros(N if vms else E)
-        el = np.zeros((E, 3 if vms else 2))
-        sd = np.zeros((E, 12)) if vms else None
-        check(lib().fm_problem_get_state(self.h, _p(u), _p(p), _p(el), _p(sd) if sd is not None else None))
+        el = np.zeros((E, 3 if vms else 2)) if elements else None
+        sd = np.zeros((E, 12)) if (vms and elements) else None
+        check(lib().fm_problem_get_state(self.h, _p(u), _p(p), _p(el) if el is not None else None,
+                                         _p(sd) if sd is not None else None))
         return u, p, el, sd
 
     def mass(self):

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 #include "fm_internal.hpp"
 
@@ -196,6 +197,75 @@ void compute_mass(fm_problem* p) {
 
 // ---- tiled layout ----
 
+// Runs f(begin, end, worker) over [0, n) in contiguous blocks on up to
+// hardware_concurrency host threads (inline for small n).
+template <class F>
+static void parallel_blocks(int64_t n, F f) {
+  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  const int64_t nt = std::min<int64_t>(hw, std::max<int64_t>(1, n / 4096));
+  if (nt <= 1) {
+    f((int64_t)0, n, 0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int64_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt, (int)t); });
+  for (auto& x : th) x.join();
+}
+
+// Sorts element indices by (key, index) - the order a stable sort by key
+// gives.  Keys are below 2^63 (3 x 21-bit Morton interleave): the pairs are
+// distributed into 4096 buckets by their top 12 bits (per-worker histograms),
+// then the buckets are sorted in parallel.
+static void sort_by_key(const std::vector<uint64_t>& key, std::vector<int64_t>& order) {
+  const int64_t E = (int64_t)key.size();
+  constexpr int NB = 4096, SHIFT = 63 - 12;
+  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  const int64_t nw = std::min<int64_t>(hw, std::max<int64_t>(1, E / 65536));
+  std::vector<int64_t> hist((size_t)nw * NB, 0);
+  auto run = [&](auto&& f) {
+    std::vector<std::thread> th;
+    for (int64_t w = 0; w < nw; ++w) th.emplace_back([&, w] { f(w, E * w / nw, E * (w + 1) / nw); });
+    for (auto& x : th) x.join();
+  };
+  run([&](int64_t w, int64_t b, int64_t e) {
+    int64_t* h = &hist[(size_t)w * NB];
+    for (int64_t i = b; i < e; ++i) h[std::min<uint64_t>(key[i] >> SHIFT, NB - 1)]++;
+  });
+  // bucket-major, worker-minor offsets
+  std::vector<int64_t> start(NB + 1, 0);
+  {
+    int64_t acc = 0;
+    for (int k = 0; k < NB; ++k) {
+      start[k] = acc;
+      for (int64_t w = 0; w < nw; ++w) {
+        const int64_t c = hist[(size_t)w * NB + k];
+        hist[(size_t)w * NB + k] = acc;
+        acc += c;
+      }
+    }
+    start[NB] = acc;
+  }
+  std::vector<std::pair<uint64_t, int64_t>> kv(E);
+  run([&](int64_t w, int64_t b, int64_t e) {
+    int64_t* h = &hist[(size_t)w * NB];
+    for (int64_t i = b; i < e; ++i) kv[h[std::min<uint64_t>(key[i] >> SHIFT, NB - 1)]++] = {key[i], i};
+  });
+  {
+    std::vector<std::thread> th;
+    for (int64_t w = 0; w < nw; ++w)
+      th.emplace_back([&, w] {
+        for (int k = (int)(NB * w / nw); k < (int)(NB * (w + 1) / nw); ++k)
+          std::sort(kv.begin() + start[k], kv.begin() + start[k + 1]);
+      });
+    for (auto& x : th) x.join();
+  }
+  order.resize(E);
+  parallel_blocks(E, [&](int64_t b, int64_t e, int) {
+    for (int64_t i = b; i < e; ++i) order[i] = kv[i].second;
+  });
+}
+
 static inline uint64_t spread3(uint64_t v) {
   v &= 0x1fffff;
   v = (v | v << 32) & 0x1f00000000ffffULL;
@@ -240,21 +310,30 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
     if (!(span > 0)) span = 1.0;
     std::vector<uint64_t> code(E);
-    for (int64_t e = 0; e < E; ++e) {
-      double c[3] = {0, 0, 0};
-      for (int a = 0; a < npe; ++a)
-        for (int k = 0; k < 3; ++k) c[k] += p->coords[(int64_t)p->conn[e * npe + a] * 3 + k];
-      uint64_t q[3];
-      for (int k = 0; k < 3; ++k) {
-        double t = (c[k] / npe - lo[k]) / span;
-        t = std::min(std::max(t, 0.0), 1.0);
-        q[k] = (uint64_t)(t * 2097151.0);
+    parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
+      for (int64_t e = eb; e < ee; ++e) {
+        double c[3] = {0, 0, 0};
+        for (int a = 0; a < npe; ++a)
+          for (int k = 0; k < 3; ++k) c[k] += p->coords[(int64_t)p->conn[e * npe + a] * 3 + k];
+        uint64_t q[3];
+        for (int k = 0; k < 3; ++k) {
+          double t = (c[k] / npe - lo[k]) / span;
+          t = std::min(std::max(t, 0.0), 1.0);
+          q[k] = (uint64_t)(t * 2097151.0);
+        }
+        code[e] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
       }
-      code[e] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
-    }
-    std::vector<int64_t> order(E);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return code[a] < code[b]; });
+    });
+    std::vector<int64_t> order;
+    sort_by_key(code, order);
+    std::vector<uint64_t>().swap(code);
+    // connectivity in sorted order: the sequential passes below then read
+    // contiguous memory
+    std::vector<int32_t> cs((size_t)E * npe);
+    parallel_blocks(E, [&](int64_t b, int64_t e, int) {
+      for (int64_t oi = b; oi < e; ++oi)
+        for (int a = 0; a < npe; ++a) cs[(size_t)oi * npe + a] = p->conn[order[oi] * npe + a];
+    });
     // 2. greedy tiles
     std::vector<int64_t> tile_start;
     std::vector<int32_t> stamp(N, -1);
@@ -263,7 +342,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
       int32_t tid = 0;
       tile_start.push_back(0);
       for (int64_t oi = 0; oi < E; ++oi) {
-        const int32_t* c = &p->conn[order[oi] * npe];
+        const int32_t* c = &cs[(size_t)oi * npe];
         int fresh = 0;
         for (int a = 0; a < npe; ++a)
           if (stamp[c[a]] != tid) {
@@ -294,150 +373,237 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     std::vector<int32_t> ntiles(N, 0), first_tile(N, -1), last(N, -1);
     for (int t = 0; t < ntile; ++t)
       for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
-        const int32_t* c = &p->conn[order[oi] * npe];
+        const int32_t* c = &cs[(size_t)oi * npe];
         for (int a = 0; a < npe; ++a)
           if (last[c[a]] != t) {
             last[c[a]] = t;
             if (ntiles[c[a]]++ == 0) first_tile[c[a]] = t;
           }
       }
+    // node renumbering: interior nodes tile by tile, interface nodes after
+    // them, each group in order of first touch along the sorted elements
+    // (per-tile first-touch lists in parallel, then prefix offsets)
+    const int64_t hwt = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+    const int64_t nwk = std::min<int64_t>(hwt, std::max<int64_t>(1, ntile / 4));
+    std::vector<std::vector<int32_t>> first_int(ntile), first_ifc(ntile);
+    {
+      std::vector<std::thread> th;
+      for (int64_t w = 0; w < nwk; ++w)
+        th.emplace_back([&, w] {
+          std::vector<int32_t> stamp2(N, -1);
+          for (int t = (int)(ntile * w / nwk); t < (int)(ntile * (w + 1) / nwk); ++t)
+            for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+              const int32_t* c = &cs[(size_t)oi * npe];
+              for (int a = 0; a < npe; ++a) {
+                const int32_t v = c[a];
+                if (stamp2[v] == t) continue;
+                stamp2[v] = t;
+                if (ntiles[v] == 1) first_int[t].push_back(v);
+                else if (first_tile[v] == t) first_ifc[t].push_back(v);
+              }
+            }
+        });
+      for (auto& x : th) x.join();
+    }
     std::vector<int32_t>& nn = L.node_new[pi];
     nn.assign(N, -1);
     int64_t next = 0;
-    std::vector<int64_t> int_begin(ntile + 1, 0);
-    for (int t = 0; t < ntile; ++t) {
-      int_begin[t] = next;
-      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
-        const int32_t* c = &p->conn[order[oi] * npe];
-        for (int a = 0; a < npe; ++a)
-          if (ntiles[c[a]] == 1 && nn[c[a]] < 0) nn[c[a]] = (int32_t)(node_base + next++);
-      }
-    }
-    int_begin[ntile] = next;
+    for (int t = 0; t < ntile; ++t)
+      for (int32_t v : first_int[t]) nn[v] = (int32_t)(node_base + next++);
     const int64_t iface_begin = next;
     for (int t = 0; t < ntile; ++t)
-      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
-        const int32_t* c = &p->conn[order[oi] * npe];
-        for (int a = 0; a < npe; ++a)
-          if (ntiles[c[a]] > 1 && nn[c[a]] < 0) nn[c[a]] = (int32_t)(node_base + next++);
-      }
+      for (int32_t v : first_ifc[t]) nn[v] = (int32_t)(node_base + next++);
+    std::vector<std::vector<int32_t>>().swap(first_int);
+    std::vector<std::vector<int32_t>>().swap(first_ifc);
     for (int64_t i = 0; i < N; ++i)
       if (nn[i] < 0) nn[i] = (int32_t)(node_base + next++);  // isolated nodes
-    // 4./5. tiles: local nodes, colouring, local connectivity, slots
-    std::vector<int32_t>& eo = L.elem_old[pi];
-    eo.clear();
-    std::vector<int32_t> local(N, -1);
-    std::vector<std::vector<int32_t>> iface_lists(N - (iface_begin));
-    int64_t e_out = 0;
-    for (int t = 0; t < ntile; ++t) {
-      // every tile starts at a multiple of ELEM_ALIGN elements (padding slots
-      // in between are never processed), so each chunk of a tile's element
-      // arrays starts on a 16-byte (in fact 128-byte) boundary
-      e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
-      eo.resize(e_out, -1);
-      L.conn_local.resize((size_t)(elem_base + e_out) * npe, 0);
-      TileMeta tm;
-      memset(&tm, 0, sizeof(tm));
-      tm.problem = pi;
-      tm.elem_begin = (int32_t)(elem_base + e_out);
-      tm.n_elem = (int32_t)(tile_start[t + 1] - tile_start[t]);
-      tm.node_begin = (int32_t)L.tile_nodes.size();
-      // local nodes: interior (contiguous batch ids) then interface sorted by id
-      std::vector<int32_t> inter, ifc;
-      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
-        const int32_t* c = &p->conn[order[oi] * npe];
-        for (int a = 0; a < npe; ++a)
-          if (local[c[a]] != -2 - t) {
-            local[c[a]] = -2 - t;
-            (ntiles[c[a]] == 1 ? inter : ifc).push_back(c[a]);
-          }
-      }
-      std::sort(inter.begin(), inter.end(), [&](int32_t a, int32_t b) { return nn[a] < nn[b]; });
-      std::sort(ifc.begin(), ifc.end(), [&](int32_t a, int32_t b) { return nn[a] < nn[b]; });
-      tm.n_int = (int32_t)inter.size();
-      tm.n_node = (int32_t)(inter.size() + ifc.size());
-      tm.slot_base = (int32_t)slot_base;
-      std::vector<int32_t> lid;  // old node -> local id via map below
-      int32_t li = 0;
-      for (int32_t v : inter) { local[v] = li++; L.tile_nodes.push_back(nn[v]); }
-      for (int32_t v : ifc) {
-        iface_lists[nn[v] - node_base - iface_begin].push_back((int32_t)(slot_base + (li - tm.n_int)));
-        local[v] = li++;
-        L.tile_nodes.push_back(nn[v]);
-      }
-      slot_base += (int64_t)ifc.size();
-      // colouring (greedy, up to 128 colours)
-      const int64_t ne = tm.n_elem;
-      std::vector<uint64_t> used(2 * tm.n_node, 0);
-      std::vector<int32_t> col(ne);
+    // 4./5. tiles: local nodes, colouring, local connectivity, incidence
+    // lists - built for every tile in parallel (per-worker scratch), then
+    // placed in tile order
+    struct TileWork {
+      std::vector<int32_t> inter, ifc;  // old node ids in local order
+      std::vector<int32_t> eo;          // old element of each tile element (colour order)
+      std::vector<uint16_t> conn;       // ne x npe tile-local ids
+      std::vector<int32_t> colcnt;      // colour offsets (ncol + 1)
+      std::vector<uint16_t> off, inc;   // incidence offsets (n_node + 1) and entries (ne * npe)
       int ncol = 0;
-      for (int64_t i = 0; i < ne; ++i) {
-        const int32_t* c = &p->conn[order[tile_start[t] + i] * npe];
-        uint64_t m0 = 0, m1 = 0;
-        for (int a = 0; a < npe; ++a) {
-          m0 |= used[2 * local[c[a]]];
-          m1 |= used[2 * local[c[a]] + 1];
-        }
-        int k;
-        if (~m0) k = __builtin_ctzll(~m0);
-        else if (~m1) k = 64 + __builtin_ctzll(~m1);
-        else return fail(FM_ERR_INVALID, "element colouring needs more than 128 colours in one tile");
-        col[i] = k;
-        ncol = std::max(ncol, k + 1);
-        for (int a = 0; a < npe; ++a) used[2 * local[c[a]] + (k >> 6)] |= (1ULL << (k & 63));
-      }
-      std::vector<int64_t> idx(ne);
-      std::iota(idx.begin(), idx.end(), 0);
-      // elements sorted by colour: SUPG processes a tile one colour at a
-      // time; for VMS it spreads each chunk's contributions over all of the
-      // tile's nodes (one or two per node and chunk, which balances the
-      // node-owner accumulation; the space-filling order measured slower)
-      std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
-      tm.col_begin = (int32_t)L.tile_cols.size();
-      tm.n_col = ncol;
-      {
-        std::vector<int32_t> cnt(ncol + 1, 0);
-        for (int64_t i = 0; i < ne; ++i) cnt[col[i] + 1]++;
-        for (int k = 0; k < ncol; ++k) cnt[k + 1] += cnt[k];
-        for (int k = 0; k <= ncol; ++k) L.tile_cols.push_back(cnt[k]);
-      }
-      L.max_colors = std::max(L.max_colors, ncol);
-      eo.resize(e_out + ne, -1);
-      for (int64_t i = 0; i < ne; ++i) {
-        int64_t oe = order[tile_start[t] + idx[i]];
-        eo[e_out + i] = (int32_t)oe;
-        const int32_t* c = &p->conn[oe * npe];
-        for (int a = 0; a < npe; ++a) L.conn_local.push_back((uint16_t)local[c[a]]);
-      }
-      // node -> incident (element, corner) lists in element order
-      {
-        if ((int64_t)ne * npe > 65535)
-          return fail(FM_ERR_INVALID, "tile_elems too large for 16-bit incidence entries");
-        std::vector<int32_t> cnt(tm.n_node + 1, 0);
-        const uint16_t* lc = &L.conn_local[(size_t)(elem_base + e_out) * npe];
-        for (int64_t i = 0; i < ne * npe; ++i) cnt[lc[i] + 1]++;
-        for (int k2 = 0; k2 < tm.n_node; ++k2) cnt[k2 + 1] += cnt[k2];
-        while (L.tile_inc.size() % 8) L.tile_inc.push_back(0);
-        tm.inc_begin = (int32_t)L.tile_inc.size();
-        tm.off_begin = (int32_t)L.tile_off.size();
-        for (int k2 = 0; k2 <= tm.n_node; ++k2) L.tile_off.push_back((uint16_t)cnt[k2]);
-        L.tile_inc.resize(L.tile_inc.size() + (size_t)ne * npe);
-        uint16_t* inc = &L.tile_inc[tm.inc_begin];
-        std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
-        for (int64_t i = 0; i < ne; ++i)
-          for (int a = 0; a < npe; ++a) inc[pos[lc[i * npe + a]]++] = (uint16_t)(i * npe + a);
-        L.max_tile_elems = std::max<int32_t>(L.max_tile_elems, (int32_t)ne);
-      }
-      e_out += ne;
-      for (int32_t v : inter) local[v] = -1;
-      for (int32_t v : ifc) local[v] = -1;
-      L.tiles.push_back(tm);
+      int err = 0;                      // 1: > 128 colours, 2: 16-bit incidence overflow
+    };
+    std::vector<TileWork> tw(ntile);
+    {
+      const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+      const int64_t nw = std::min<int64_t>(hw, std::max<int64_t>(1, ntile / 4));
+      std::vector<std::thread> th;
+      for (int64_t w = 0; w < nw; ++w)
+        th.emplace_back([&, w] {
+          std::vector<int32_t> local(N, -1);
+          for (int t = (int)(ntile * w / nw); t < (int)(ntile * (w + 1) / nw); ++t) {
+            TileWork& W = tw[t];
+            for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+              const int32_t* c = &cs[(size_t)oi * npe];
+              for (int a = 0; a < npe; ++a)
+                if (local[c[a]] != -2 - t) {
+                  local[c[a]] = -2 - t;
+                  (ntiles[c[a]] == 1 ? W.inter : W.ifc).push_back(c[a]);
+                }
+            }
+            // interior nodes in their (contiguous) batch order, then interface nodes by id
+            std::sort(W.inter.begin(), W.inter.end(), [&](int32_t x, int32_t y) { return nn[x] < nn[y]; });
+            std::sort(W.ifc.begin(), W.ifc.end(), [&](int32_t x, int32_t y) { return nn[x] < nn[y]; });
+            int32_t li = 0;
+            for (int32_t v : W.inter) local[v] = li++;
+            for (int32_t v : W.ifc) local[v] = li++;
+            const int32_t n_node = li;
+            // colouring (greedy, up to 128 colours)
+            const int64_t ne = tile_start[t + 1] - tile_start[t];
+            std::vector<uint64_t> used(2 * (size_t)n_node, 0);
+            std::vector<int32_t> col(ne);
+            int ncol = 0;
+            for (int64_t i = 0; i < ne; ++i) {
+              const int32_t* c = &cs[(size_t)(tile_start[t] + i) * npe];
+              uint64_t m0 = 0, m1 = 0;
+              for (int a = 0; a < npe; ++a) {
+                m0 |= used[2 * local[c[a]]];
+                m1 |= used[2 * local[c[a]] + 1];
+              }
+              int k;
+              if (~m0) k = __builtin_ctzll(~m0);
+              else if (~m1) k = 64 + __builtin_ctzll(~m1);
+              else {
+                W.err = 1;
+                break;
+              }
+              col[i] = k;
+              ncol = std::max(ncol, k + 1);
+              for (int a = 0; a < npe; ++a) used[2 * local[c[a]] + (k >> 6)] |= (1ULL << (k & 63));
+            }
+            if (W.err) continue;
+            // elements sorted by colour: SUPG processes a tile one colour at a
+            // time; for VMS it spreads each chunk's contributions over all of
+            // the tile's nodes (one or two per node and chunk, which balances
+            // the node-owner accumulation; the space-filling order measured
+            // slower)
+            std::vector<int64_t> idx(ne);
+            std::iota(idx.begin(), idx.end(), 0);
+            std::stable_sort(idx.begin(), idx.end(), [&](int64_t x, int64_t y) { return col[x] < col[y]; });
+            W.ncol = ncol;
+            W.colcnt.assign(ncol + 1, 0);
+            for (int64_t i = 0; i < ne; ++i) W.colcnt[col[i] + 1]++;
+            for (int k = 0; k < ncol; ++k) W.colcnt[k + 1] += W.colcnt[k];
+            W.eo.resize(ne);
+            W.conn.resize((size_t)ne * npe);
+            for (int64_t i = 0; i < ne; ++i) {
+              const int64_t oe = order[tile_start[t] + idx[i]];
+              W.eo[i] = (int32_t)oe;
+              const int32_t* c = &p->conn[oe * npe];
+              for (int a = 0; a < npe; ++a) W.conn[(size_t)i * npe + a] = (uint16_t)local[c[a]];
+            }
+            // node -> incident (element, corner) lists in element order
+            if (ne * npe > 65535) {
+              W.err = 2;
+              continue;
+            }
+            std::vector<int32_t> cnt(n_node + 1, 0);
+            for (int64_t i = 0; i < ne * npe; ++i) cnt[W.conn[i] + 1]++;
+            for (int k2 = 0; k2 < n_node; ++k2) cnt[k2 + 1] += cnt[k2];
+            W.off.resize(n_node + 1);
+            for (int k2 = 0; k2 <= n_node; ++k2) W.off[k2] = (uint16_t)cnt[k2];
+            W.inc.resize((size_t)ne * npe);
+            std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+            for (int64_t i = 0; i < ne; ++i)
+              for (int a = 0; a < npe; ++a) W.inc[pos[W.conn[i * npe + a]]++] = (uint16_t)(i * npe + a);
+          }
+        });
+      for (auto& x : th) x.join();
     }
-    for (int64_t k = 0; k < (int64_t)iface_lists.size(); ++k) {
-      L.iface_node.push_back((int32_t)(node_base + iface_begin + k));
-      L.iface_slot_beg.push_back((int32_t)L.iface_slots.size());
-      for (int32_t s : iface_lists[k]) L.iface_slots.push_back(s);
-      L.iface_prob.push_back(pi);
+    for (int t = 0; t < ntile; ++t) {
+      if (tw[t].err == 1) return fail(FM_ERR_INVALID, "element colouring needs more than 128 colours in one tile");
+      if (tw[t].err == 2) return fail(FM_ERR_INVALID, "tile_elems too large for 16-bit incidence entries");
+    }
+    // placement: every tile starts at a multiple of ELEM_ALIGN element slots
+    // (padding slots in between are never processed, so each chunk of a
+    // tile's element arrays starts on a 16-byte, in fact 128-byte, boundary)
+    // and its incidence entries at a multiple of 8; offsets first, then the
+    // blocks are copied in parallel
+    std::vector<TileMeta> tms(ntile);
+    int64_t e_out = 0;
+    {
+      int64_t tn_off = (int64_t)L.tile_nodes.size(), col_off = (int64_t)L.tile_cols.size();
+      int64_t inc_off = (int64_t)L.tile_inc.size(), off_off = (int64_t)L.tile_off.size(), sb = slot_base;
+      for (int t = 0; t < ntile; ++t) {
+        const TileWork& W = tw[t];
+        TileMeta& tm = tms[t];
+        memset(&tm, 0, sizeof(tm));
+        e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
+        tm.problem = pi;
+        tm.elem_begin = (int32_t)(elem_base + e_out);
+        tm.n_elem = (int32_t)(tile_start[t + 1] - tile_start[t]);
+        tm.node_begin = (int32_t)tn_off;
+        tm.n_int = (int32_t)W.inter.size();
+        tm.n_node = (int32_t)(W.inter.size() + W.ifc.size());
+        tm.slot_base = (int32_t)sb;
+        tm.col_begin = (int32_t)col_off;
+        tm.n_col = W.ncol;
+        inc_off = (inc_off + 7) / 8 * 8;
+        tm.inc_begin = (int32_t)inc_off;
+        tm.off_begin = (int32_t)off_off;
+        e_out += tm.n_elem;
+        tn_off += tm.n_node;
+        sb += (int64_t)W.ifc.size();
+        col_off += (int64_t)W.colcnt.size();
+        inc_off += (int64_t)W.inc.size();
+        off_off += (int64_t)W.off.size();
+        L.max_colors = std::max(L.max_colors, W.ncol);
+        L.max_tile_elems = std::max<int32_t>(L.max_tile_elems, tm.n_elem);
+      }
+      L.tile_nodes.resize(tn_off);
+      L.tile_cols.resize(col_off);
+      L.tile_inc.resize(inc_off, 0);
+      L.tile_off.resize(off_off);
+      slot_base = sb;
+    }
+    e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
+    std::vector<int32_t>& eo = L.elem_old[pi];
+    eo.assign(e_out, -1);
+    L.conn_local.resize((size_t)(elem_base + e_out) * npe, 0);
+    parallel_blocks(ntile, [&](int64_t tb, int64_t te2, int) {
+      for (int64_t t = tb; t < te2; ++t) {
+        const TileWork& W = tw[t];
+        const TileMeta& tm = tms[t];
+        int32_t* tn = &L.tile_nodes[tm.node_begin];
+        for (int32_t v : W.inter) *tn++ = nn[v];
+        for (int32_t v : W.ifc) *tn++ = nn[v];
+        std::copy(W.colcnt.begin(), W.colcnt.end(), L.tile_cols.begin() + tm.col_begin);
+        std::copy(W.inc.begin(), W.inc.end(), L.tile_inc.begin() + tm.inc_begin);
+        std::copy(W.off.begin(), W.off.end(), L.tile_off.begin() + tm.off_begin);
+        std::copy(W.conn.begin(), W.conn.end(), L.conn_local.begin() + (size_t)tm.elem_begin * npe);
+        std::copy(W.eo.begin(), W.eo.end(), eo.begin() + (tm.elem_begin - elem_base));
+      }
+    });
+    L.tiles.insert(L.tiles.end(), tms.begin(), tms.end());
+    // interface nodes: one partial-sum slot per (tile, node), listed per node
+    // in tile order
+    {
+      const int64_t NI = N - iface_begin;
+      std::vector<int32_t> cnt(NI + 1, 0);
+      for (int t = 0; t < ntile; ++t)
+        for (int32_t v : tw[t].ifc) cnt[nn[v] - node_base - iface_begin + 1]++;
+      for (int64_t k = 0; k < NI; ++k) cnt[k + 1] += cnt[k];
+      const int64_t s0 = (int64_t)L.iface_slots.size();
+      L.iface_slots.resize(s0 + cnt[NI]);
+      std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+      for (int t = 0; t < ntile; ++t) {
+        int32_t k = 0;
+        for (int32_t v : tw[t].ifc) {
+          const int64_t j = nn[v] - node_base - iface_begin;
+          L.iface_slots[s0 + pos[j]++] = tms[t].slot_base + k++;
+        }
+      }
+      for (int64_t k = 0; k < NI; ++k) {
+        L.iface_node.push_back((int32_t)(node_base + iface_begin + k));
+        L.iface_slot_beg.push_back((int32_t)(s0 + cnt[k]));
+        L.iface_prob.push_back(pi);
+      }
     }
     node_base += N;
     e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;

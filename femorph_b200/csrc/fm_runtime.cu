@@ -18,6 +18,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fm_device.cuh"
@@ -218,11 +219,14 @@ static int put(T* dev_base, int64_t off, const T* src, int64_t n, cudaStream_t s
   return FM_OK;
 }
 
-static void default_tuning(int solver, int npe, fm_tuning& t) {
-  // 64-thread CTAs exist for the VMS kernels only
-  if (t.threads != 128 && t.threads != 256 && !(t.threads == 64 && solver == FM_SOLVER_VMS)) t.threads = 128;
-  if (t.tile_elems <= 0) t.tile_elems = (npe == 8) ? 384 : 1024;
-  if (t.tile_nodes <= 0) t.tile_nodes = (npe == 8) ? 640 : 512;
+// Default launch shape (measured on the 96^3 cavity and the hexa channel):
+// VMS FP64 1024-tet tiles (3 CTAs/SM, register bound), VMS mixed 512-tet
+// tiles (4 CTAs/SM fit the shared memory), SUPG hexa8 384 elements.
+static void default_tuning(int solver, int npe, int precision, fm_tuning& t) {
+  if (t.threads != 128 && t.threads != 256) t.threads = 128;
+  const bool vms_mixed = solver == FM_SOLVER_VMS && precision == FM_MIXED;
+  if (t.tile_elems <= 0) t.tile_elems = (npe == 8) ? 384 : (vms_mixed ? 512 : 1024);
+  if (t.tile_nodes <= 0) t.tile_nodes = (npe == 8) ? 640 : (vms_mixed ? 256 : 512);
   if (t.tile_nodes > 4096) t.tile_nodes = 4096;
   if (solver == FM_SOLVER_VMS && t.tile_nodes > FM_MAX_TILE_NODES) t.tile_nodes = FM_MAX_TILE_NODES;
   if (t.graph_steps < 0) t.graph_steps = 0;
@@ -244,13 +248,22 @@ static int prepare(fm_problem* p, int te, int tn, std::shared_ptr<Layout>* out) 
     // mixed form: elements whose Jacobian inverse stays in FP64 (aspect ratio
     // above the limit) are flagged in bit 15 of their first tile-local node id
     const int npe = p->etype;
-    for (int64_t k = 0; k < L->elem_count[0]; ++k) {
-      const int32_t oe = L->elem_old[0][k];
-      if (oe < 0) continue;
-      const int32_t* c = &p->conn[(int64_t)oe * npe];
-      const double ar = npe == 4 ? tet_aspect_ratio(p->coords.data(), c) : hexa_aspect_ratio(p->coords.data(), c);
-      if (ar > FM_MIXED_ASPECT_LIMIT) L->conn_local[(size_t)k * npe] |= 0x8000;
-    }
+    const int64_t EC = L->elem_count[0];
+    const int nw = (int)std::max<int64_t>(1, std::min<int64_t>({32, (int64_t)std::thread::hardware_concurrency(),
+                                                                  EC / 16384}));
+    std::vector<std::thread> th;
+    for (int w = 0; w < nw; ++w)
+      th.emplace_back([&, w] {
+        for (int64_t k = EC * w / nw; k < EC * (w + 1) / nw; ++k) {
+          const int32_t oe = L->elem_old[0][k];
+          if (oe < 0) continue;
+          const int32_t* c = &p->conn[(int64_t)oe * npe];
+          const double ar =
+              npe == 4 ? tet_aspect_ratio(p->coords.data(), c) : hexa_aspect_ratio(p->coords.data(), c);
+          if (ar > FM_MIXED_ASPECT_LIMIT) L->conn_local[(size_t)k * npe] |= 0x8000;
+        }
+      });
+    for (auto& x : th) x.join();
   }
   p->layout = L;
   p->layout_te = te;
@@ -748,7 +761,7 @@ int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning) {
   fm_tuning t;
   memset(&t, 0, sizeof(t));
   if (tuning) t = *tuning;
-  default_tuning(p->params.solver, p->etype, t);
+  default_tuning(p->params.solver, p->etype, p->params.precision, t);
   std::shared_ptr<Layout> L;
   return prepare(p, t.tile_elems, t.tile_nodes, &L);
 }
@@ -792,7 +805,7 @@ static int new_batch(int solver, int npe, int prec, const fm_tuning* tuning, int
   fm_batch* b = new fm_batch();
   memset(&b->tune, 0, sizeof(b->tune));
   if (tuning) b->tune = *tuning;
-  default_tuning(solver, npe, b->tune);
+  default_tuning(solver, npe, prec, b->tune);
   b->device = device;
   b->solver = solver;
   b->npe = npe;
@@ -869,7 +882,7 @@ int fm_batch_capacity_bytes(const fm_capacity* cap, const fm_tuning* tuning, int
   fm_tuning t;
   memset(&t, 0, sizeof(t));
   if (tuning) t = *tuning;
-  default_tuning(cap->solver, cap->elem_type, t);
+  default_tuning(cap->solver, cap->elem_type, cap->precision, t);
   int64_t c[P_COUNT];
   capacity_pools(cap, t.tile_elems, c);
   *bytes = pool_bytes(c, cap->solver, cap->elem_type, cap->precision, cap->solver == FM_SOLVER_SUPG);

@@ -138,7 +138,7 @@ class Server:
                 # lookup failed; the other problems are unaffected
                 r.status = status
                 if self.keep_results:
-                    u, p, _, _ = g.state()
+                    u, p, _, _ = g.state(elements=False)
                     r.result = (u, p)
                 self.pool.remove(g)
                 g.close()
