@@ -201,32 +201,21 @@ void femSUPGExplicitFluidSolverGPU::solve(femModel* model) {
   FILE* lf = fopen(model->log_file.c_str(), "w");
   if (lf) fclose(lf);
   const long steps = (long)model->totalSteps - 1;
-  const double nan = std::numeric_limits<double>::quiet_NaN();
   double t = 0.0;
+  double l_cfl_max = 0.0;  // the reference never resets it between steps (src line 996)
   for (long step = 1; step <= steps; ++step) {
     t += model->timeStep;
+    // Gauss-point log quantities of the state this step starts from, as the
+    // reference's element loop accumulates them (src lines 1066-1459), and
+    // the velocity extrema after the step (get_solution_extrema, src lines
+    // 604-655): both reduced on the device
+    double st[11], ex[7];
+    fm_check(fm_problem_supg_log_stats(s.p, st));
     fm_check(fm_batch_step(s.b, 1, nullptr));
     int rc = fm_batch_sync(s.b);
     if (rc != FM_OK && rc != FM_ERR_DIVERGED) fm_check(rc);
-    fm_check(fm_problem_get_state(s.p, u.data(), nullptr, lr.data(), nullptr));
-    // velocity extrema (get_solution_extrema, src lines 604-655) and the
-    // element-average lambda range; the Gauss-point tau/CFL/E/nu columns of
-    // the reference's log are not reduced on the device (written as nan).
-    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, maxmod = 0.0;
-    for (size_t i = 0; i < N; ++i) {
-      double m2 = 0.0;
-      for (int c = 0; c < 3; ++c) {
-        mn[c] = std::min(mn[c], u[i * 3 + c]);
-        mx[c] = std::max(mx[c], u[i * 3 + c]);
-        m2 += u[i * 3 + c] * u[i * 3 + c];
-      }
-      maxmod = std::max(maxmod, std::sqrt(m2));
-    }
-    double lmin = 1e300, lmax = -1e300;
-    for (size_t e = 0; e < E; ++e) {
-      lmin = std::min(lmin, lr[e * 2]);
-      lmax = std::max(lmax, lr[e * 2]);
-    }
+    fm_check(fm_problem_velocity_extrema(s.p, ex));
+    if (st[6] > l_cfl_max) l_cfl_max = st[6];
     FILE* f = fopen(model->log_file.c_str(), "a");
     if (f) {
       if (step == 1 || step % 10 == 0)
@@ -236,10 +225,11 @@ void femSUPGExplicitFluidSolverGPU::solve(femModel* model) {
       fprintf(f,
               "%5ld %10.3e %10.3e %10.3e %10.3e %10.3e %10.3e %10.3e %10.3e %10.3e %10.3e %10.3e %10.3f %10.3f %10.3f "
               "%10.3e %10.3e %10.3e %10.3e\n",
-              step, t, mn[0], mx[0], mn[1], mx[1], mn[2], mx[2], nan, nan, lmin, lmax, nan, nan, nan, nan, nan, nan, nan);
+              step, t, ex[0], ex[1], ex[2], ex[3], ex[4], ex[5], st[0], st[1], st[2], st[3], st[4], st[5], l_cfl_max,
+              st[7], st[8], st[9], st[10]);
       fclose(f);
     }
-    if (rc == FM_ERR_DIVERGED || maxmod > model->exit_condition) {
+    if (rc == FM_ERR_DIVERGED || ex[6] > model->exit_condition) {
       FILE* f2 = fopen(model->log_file.c_str(), "a");
       if (f2) {
         fprintf(f2, "ERROR: Maximum velocity module larger than admissible threshold.\n");

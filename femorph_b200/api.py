@@ -30,7 +30,7 @@ SYMBOLS = [
     "fm_problem_get_mass", "fm_batch_last_timing", "fm_batch_estimate_bytes", "fm_batch_layout",
     "fm_batch_profile", "fm_autotune", "fm_batch_create_empty", "fm_batch_add", "fm_batch_remove",
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
-    "fm_vms_solve_static", "fm_batch_capacity_bytes",
+    "fm_vms_solve_static", "fm_batch_capacity_bytes", "fm_problem_velocity_extrema", "fm_problem_supg_log_stats",
 ]
 
 
@@ -108,6 +108,8 @@ def lib():
         L.fm_batch_step_problems.argtypes = [P, P, P, C.c_int32, P]
         L.fm_problem_status.argtypes = [P]
         L.fm_batch_capacity_bytes.argtypes = [P, P, P]
+        L.fm_problem_velocity_extrema.argtypes = [P, P]
+        L.fm_problem_supg_log_stats.argtypes = [P, P]
         L.fm_vms_solve_static.argtypes = [P, C.c_int32, C.c_int32, P, P, P]
         _lib = L
     return _lib
@@ -184,6 +186,18 @@ class GpuProblem:
         """Builds the tile layout now (host only, thread-safe per problem)."""
         t = FmTuning(tile_elems, tile_nodes, threads, 0)
         check(lib().fm_problem_prepare(self.h, C.byref(t)))
+
+    def velocity_extrema(self):
+        """(min u, max u, min v, max v, min w, max w, max |u|), reduced on the device."""
+        out = np.zeros(7)
+        check(lib().fm_problem_velocity_extrema(self.h, _p(out)))
+        return out
+
+    def supg_log_stats(self):
+        """SUPG log quantities of the current state (see the C header)."""
+        out = np.zeros(11)
+        check(lib().fm_problem_supg_log_stats(self.h, _p(out)))
+        return out
 
     def status(self) -> int:
         """Device status code of this problem in its batch (FM_OK when healthy)."""

@@ -16,6 +16,9 @@
 
 namespace fm {
 
+template <int NPE>
+__global__ void supg_stats_kernel(DevBatch B, int tile0, int tn_max, double* out);
+
 __device__ __forceinline__ void mask_fixed(int gf, double& u, double& v, double& w) {
   if (gf & FM_FIX_X) u = 0.0;
   if (gf & FM_FIX_Y) v = 0.0;
@@ -260,12 +263,14 @@ cudaError_t supg_configure(size_t smem, int npe) {
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 128, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<4, 256, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<4>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_stats_kernel<4>, optin);
   } else {
     e = raise_dyn_smem(supg_tile_kernel<8, 128, false>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256, false>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 128, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<8>, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_stats_kernel<8>, optin);
   }
   return e;
 }
@@ -301,6 +306,191 @@ cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double*
     supg_pressure_kernel<4><<<B.n_tiles, 128, smem, s>>>(B, tn_max, pres);
   else
     supg_pressure_kernel<8><<<B.n_tiles, 128, smem, s>>>(B, tn_max, pres);
+  return cudaGetLastError();
+}
+
+}  // namespace fm
+
+namespace fm {
+
+// ---------------------------------------------------------------------------
+// Per-step log quantities of the SUPG solver (output only).
+//
+// supg_stats_kernel: one CTA per tile of one problem, on the state about to
+// be stepped (the one the reference's element loop sees): per Gauss point
+// tau_SUPG (eval_stabilization), lambda (eval_bulk_modulus), the element
+// length 2 sqrt(u^T G^-1 u) / |u| (get_el_lengths_from_G, src lines 756-790;
+// NaN for u = 0 as there) and the advective |u_x| dt / l, viscous
+// 2 nu dt / l^2 and lambda 2 lambda dt / l^2 CFL numbers; per element E and
+// nu of the volume-averaged lambda (src lines 1180-1245, 1430-1459).  A value
+// enters a minimum or maximum only by a strict comparison, as in the
+// reference, so NaNs never do.  Each CTA writes its 11 partial results:
+// min/max tau, min/max lambda, max viscous / advective / lambda CFL,
+// min/max E, min/max nu.
+//
+// velocity_extrema_kernel: min/max of each velocity component and max |u|
+// over one problem's nodes (get_solution_extrema, src lines 604-655), global
+// fixed dofs masked; each CTA writes 7 partial results.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void upd_min(double& m, double v) { if (v < m) m = v; }
+__device__ __forceinline__ void upd_max(double& m, double v) { if (v > m) m = v; }
+
+template <int NPE>
+__global__ void supg_stats_kernel(DevBatch B, int tile0, int tn_max, double* out) {
+  extern __shared__ double sm[];
+  double* s_x = sm;
+  double* s_y = s_x + tn_max;
+  double* s_z = s_y + tn_max;
+  double* s_u = s_z + tn_max;
+  double* s_v = s_u + tn_max;
+  double* s_w = s_v + tn_max;
+  __shared__ double s_red[11][32];
+  const TileMeta tm = B.tiles[tile0 + blockIdx.x];
+  const DevProb& P = B.probs[tm.problem];
+  for (int ln = threadIdx.x; ln < tm.n_node; ln += blockDim.x) {
+    const int g = B.tile_nodes[tm.node_begin + ln];
+    s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
+    double u = B.su[g], v = B.sv[g], w = B.sw[g];
+    if (P.glob_fixed & FM_FIX_X) u = 0.0;
+    if (P.glob_fixed & FM_FIX_Y) v = 0.0;
+    if (P.glob_fixed & FM_FIX_Z) w = 0.0;
+    s_u[ln] = u; s_v[ln] = v; s_w[ln] = w;
+  }
+  __syncthreads();
+  const double big = 1.7976931348623157e308;
+  double r[11] = {big, -big, big, -big, 0.0, 0.0, 0.0, big, -big, big, -big};
+  const double rho = P.rho, mu = P.mu, nu = mu / rho, alpha = P.alpha, cI = P.c_i, dt = P.dt;
+  for (int le = threadIdx.x; le < tm.n_elem; le += blockDim.x) {
+    const int64_t e = tm.elem_begin + le;
+    int ln[NPE];
+    for (int a = 0; a < NPE; ++a) ln[a] = B.conn[e * NPE + a] & 0x7fff;
+    double vol = 0.0, lam_int = 0.0;
+    for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+      double q[3], Nf[NPE], dN[NPE][3], inv[3][3];
+      GaussRule<NPE>::point(g, q);
+      shape<NPE>(q, Nf, dN);
+      const double det = jacobian<NPE>(dN, s_x, s_y, s_z, ln, inv);
+      double u[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < NPE; ++a) {
+        u[0] += Nf[a] * s_u[ln[a]];
+        u[1] += Nf[a] * s_v[ln[a]];
+        u[2] += Nf[a] * s_w[ln[a]];
+      }
+      double G[3][3];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
+      double t2 = 0.0, t3 = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
+        t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
+      }
+      const double tau = 1.0 / sqrt(t2 + t3 * nu * nu * cI);
+      const double m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
+                   m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
+      const double dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+      const double idg = 1.0 / dG;
+      const double iG[3][3] = {{(m11 * m22 - m21 * m12) * idg, (m02 * m21 - m01 * m22) * idg, (m01 * m12 - m02 * m11) * idg},
+                               {(m12 * m20 - m10 * m22) * idg, (m00 * m22 - m02 * m20) * idg, (m10 * m02 - m00 * m12) * idg},
+                               {(m10 * m21 - m20 * m11) * idg, (m20 * m01 - m00 * m21) * idg, (m00 * m11 - m10 * m01) * idg}};
+      const double l2 = sqrt((iG[0][0] * u[0] + iG[0][1] * u[1] + iG[0][2] * u[2]) * u[0] +
+                             (iG[1][0] * u[0] + iG[1][1] * u[1] + iG[1][2] * u[2]) * u[1] +
+                             (iG[2][0] * u[0] + iG[2][1] * u[1] + iG[2][2] * u[2]) * u[2]);
+      const double lam = alpha * ((nu < l2) ? l2 : nu);
+      const double un = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      const double o[3] = {u[0] / un, u[1] / un, u[2] / un};
+      double el = 0.0;
+      for (int a = 0; a < 3; ++a) el += (iG[a][0] * o[0] + iG[a][1] * o[1] + iG[a][2] * o[2]) * o[a];
+      el = 2.0 * sqrt(el);
+      const double w = det * GaussRule<NPE>::weight();
+      vol += w;
+      lam_int += lam * w;
+      upd_min(r[0], tau); upd_max(r[1], tau);
+      upd_min(r[2], lam); upd_max(r[3], lam);
+      upd_max(r[4], 2.0 * nu * (dt / (el * el)));
+      upd_max(r[5], fabs(u[0] * dt) / el);
+      upd_max(r[6], 2.0 * lam * (dt / (el * el)));
+    }
+    const double lam_el = lam_int / vol;
+    const double E = (mu * (3 * lam_el + 2 * mu)) / (lam_el + mu);
+    const double nue = lam_el / (2 * (lam_el + mu));
+    upd_min(r[7], E); upd_max(r[8], E);
+    upd_min(r[9], nue); upd_max(r[10], nue);
+  }
+  // block reduction (warp results through shared memory, then warp 0)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+  for (int k = 0; k < 11; ++k) {
+    const bool isMin = (k == 0 || k == 2 || k == 7 || k == 9);
+    double v = r[k];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o2 = __shfl_down_sync(0xffffffffu, v, off);
+      if (isMin) upd_min(v, o2); else upd_max(v, o2);
+    }
+    if (lane == 0) s_red[k][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 11) {
+    const int k = threadIdx.x;
+    const bool isMin = (k == 0 || k == 2 || k == 7 || k == 9);
+    double v = s_red[k][0];
+    for (int i = 1; i < nwarp; ++i) {
+      if (isMin) upd_min(v, s_red[k][i]); else upd_max(v, s_red[k][i]);
+    }
+    out[(int64_t)blockIdx.x * 11 + k] = v;
+  }
+}
+
+__global__ void velocity_extrema_kernel(DevBatch B, int64_t node_begin, int64_t n_nodes, int glob_fixed, double* out) {
+  __shared__ double s_red[7][32];
+  const double big = 1.7976931348623157e308;
+  double r[7] = {big, -big, big, -big, big, -big, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_nodes; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = node_begin + i;
+    double u[3] = {B.su[g], B.sv[g], B.sw[g]};
+    if (glob_fixed & FM_FIX_X) u[0] = 0.0;
+    if (glob_fixed & FM_FIX_Y) u[1] = 0.0;
+    if (glob_fixed & FM_FIX_Z) u[2] = 0.0;
+    upd_max(r[6], sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+    for (int c = 0; c < 3; ++c) {
+      upd_min(r[2 * c], u[c]);
+      upd_max(r[2 * c + 1], u[c]);
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = (blockDim.x + 31) >> 5;
+  for (int k = 0; k < 7; ++k) {
+    const bool isMin = (k == 0 || k == 2 || k == 4);
+    double v = r[k];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o2 = __shfl_down_sync(0xffffffffu, v, off);
+      if (isMin) upd_min(v, o2); else upd_max(v, o2);
+    }
+    if (lane == 0) s_red[k][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    const int k = threadIdx.x;
+    const bool isMin = (k == 0 || k == 2 || k == 4);
+    double v = s_red[k][0];
+    for (int i = 1; i < nwarp; ++i) {
+      if (isMin) upd_min(v, s_red[k][i]); else upd_max(v, s_red[k][i]);
+    }
+    out[(int64_t)blockIdx.x * 7 + k] = v;
+  }
+}
+
+cudaError_t launch_supg_stats(const DevBatch& B, int tile0, int ntiles, int tn_max, int npe, double* out,
+                              cudaStream_t s) {
+  const size_t smem = (size_t)tn_max * 6 * sizeof(double);
+  if (ntiles <= 0) return cudaSuccess;
+  if (npe == 4)
+    supg_stats_kernel<4><<<ntiles, 128, smem, s>>>(B, tile0, tn_max, out);
+  else
+    supg_stats_kernel<8><<<ntiles, 128, smem, s>>>(B, tile0, tn_max, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_velocity_extrema(const DevBatch& B, int64_t node_begin, int64_t n_nodes, int glob_fixed, int blocks,
+                                    double* out, cudaStream_t s) {
+  velocity_extrema_kernel<<<blocks, 256, 0, s>>>(B, node_begin, n_nodes, glob_fixed, out);
   return cudaGetLastError();
 }
 

@@ -35,6 +35,10 @@ cudaError_t supg_configure(size_t smem, int npe);
 cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
                              cudaStream_t s, cudaEvent_t* ev);
 cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
+cudaError_t launch_supg_stats(const DevBatch& B, int tile0, int ntiles, int tn_max, int npe, double* out,
+                              cudaStream_t s);
+cudaError_t launch_velocity_extrema(const DevBatch& B, int64_t node_begin, int64_t n_nodes, int glob_fixed, int blocks,
+                                    double* out, cudaStream_t s);
 
 // Aspect ratio h_max / (2 sqrt(6) r_in) of a tet (1 for the regular tet,
 // about 1.7 for a Kuhn tet); r_in = 3V / (sum of face areas).
@@ -180,6 +184,7 @@ struct fm_batch {
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
   double* d_scratch = nullptr;
+  double* d_stats = nullptr;   // per-CTA partial results of the log reductions
 };
 
 #define CK(x)                                                                                     \
@@ -352,6 +357,7 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
   A((void**)&q1, NP * 8 * sizeof(double));
   uint32_t* done;
   A((void**)&done, sizeof(uint32_t));
+  A((void**)&b->d_stats, std::max<int64_t>(cap[P_TILE], 256) * 11 * sizeof(double));
   if (r) return r;
   D.x = x; D.y = y; D.z = z; D.su = su; D.sv = sv; D.sw = sw; D.sp = sp;
   D.pu = pu; D.pv = pv; D.pw = pw; D.pp = pp; D.mass = ms; D.node_bc = nbc;
@@ -1127,6 +1133,52 @@ int fm_problem_status(fm_problem* p) {
   DevProbState st;
   CK(cudaMemcpy(&st, b->D.pstate + p->index, sizeof(st), cudaMemcpyDeviceToHost));
   return st.status;
+}
+
+int fm_problem_velocity_extrema(fm_problem* p, double* out) {
+  if (!p || !out) return fail(FM_ERR_INVALID, "null argument");
+  fm_batch* b = p->batch;
+  if (!b) return fail(FM_ERR_INVALID, "problem is not in a batch");
+  CK(cudaSetDevice(b->device));
+  const Placement& pl = b->slots[p->index];
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(256, (p->N + 255) / 256));
+  const int gf = b->solver == FM_SOLVER_SUPG ? p->params.glob_fixed : 0;
+  cudaError_t e = launch_velocity_extrema(b->D, pl.off[P_NODE], p->N, gf, blocks, b->d_stats, b->stream);
+  if (e != cudaSuccess) return fail(FM_ERR_CUDA, cudaGetErrorString(e));
+  std::vector<double> h((size_t)blocks * 7);
+  CK(cudaMemcpyAsync(h.data(), b->d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int k = 0; k < 7; ++k) out[k] = h[k];
+  for (int i = 1; i < blocks; ++i)
+    for (int k = 0; k < 7; ++k) {
+      const double v = h[(size_t)i * 7 + k];
+      const bool isMin = (k == 0 || k == 2 || k == 4);
+      if (isMin ? v < out[k] : v > out[k]) out[k] = v;
+    }
+  return FM_OK;
+}
+
+int fm_problem_supg_log_stats(fm_problem* p, double* out) {
+  if (!p || !out) return fail(FM_ERR_INVALID, "null argument");
+  fm_batch* b = p->batch;
+  if (!b) return fail(FM_ERR_INVALID, "problem is not in a batch");
+  if (b->solver != FM_SOLVER_SUPG) return fail(FM_ERR_INVALID, "log statistics are those of the SUPG solver");
+  CK(cudaSetDevice(b->device));
+  const Placement& pl = b->slots[p->index];
+  const int nt = (int)pl.len[P_TILE];
+  cudaError_t e = launch_supg_stats(b->D, (int)pl.off[P_TILE], nt, pl.tn_max, b->npe, b->d_stats, b->stream);
+  if (e != cudaSuccess) return fail(FM_ERR_CUDA, cudaGetErrorString(e));
+  std::vector<double> h((size_t)nt * 11);
+  CK(cudaMemcpyAsync(h.data(), b->d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int k = 0; k < 11; ++k) out[k] = h[k];
+  for (int i = 1; i < nt; ++i)
+    for (int k = 0; k < 11; ++k) {
+      const double v = h[(size_t)i * 11 + k];
+      const bool isMin = (k == 0 || k == 2 || k == 7 || k == 9);
+      if (isMin ? v < out[k] : v > out[k]) out[k] = v;
+    }
+  return FM_OK;
 }
 
 int fm_batch_last_timing(fm_batch* b, double* ms, int64_t* launches) {

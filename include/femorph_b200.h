@@ -223,6 +223,21 @@ FM_API int fm_batch_step_ragged(fm_batch* b, const int32_t* nsteps, void* stream
 FM_API int fm_batch_step_problems(fm_batch* b, fm_problem* const* problems, const int32_t* nsteps, int32_t count,
                                   void* stream);
 
+/* Velocity extrema of a problem's current state, reduced on the device
+ * (get_solution_extrema, femSUPGExplicitFluidSolver.cpp:604-655; SUPG
+ * global fixed dofs masked): out[0..5] min/max of u, v, w, out[6] max |u|. */
+FM_API int fm_problem_velocity_extrema(fm_problem* p, double* out);
+
+/* SUPG log quantities of the state about to be stepped, reduced on the
+ * device as the reference's element loop accumulates them
+ * (femSUPGExplicitFluidSolver.cpp:1066-1091, 1180-1245, 1430-1459, printed at
+ * :1594-1630): out[0..1] min/max tau_SUPG, out[2..3] min/max lambda at the
+ * Gauss points, out[4..6] max viscous, advective and lambda CFL, out[7..8]
+ * min/max E and out[9..10] min/max nu of the element-averaged lambda.  (The
+ * reference never resets its lambda CFL maximum between steps; a caller that
+ * prints its log keeps that running maximum.) */
+FM_API int fm_problem_supg_log_stats(fm_problem* p, double* out);
+
 /* Device status of one problem of a batch (FM_OK, FM_ERR_DIVERGED,
  * FM_ERR_TABLE, FM_ERR_TIMEOUT); waits for the batch's stream. */
 FM_API int fm_problem_status(fm_problem* p);

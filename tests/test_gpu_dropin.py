@@ -83,3 +83,21 @@ def test_dropin_supg_hexa(workdir):
         if s > 0:
             assert _rel(G[s]["lambda"], A[s]["lambda"]) <= 1e-11, s
             assert np.array_equal(G[s]["regime"], A[s]["regime"]), s
+    # the per-step log (velocity extrema, tau / lambda / CFL / E / nu ranges,
+    # reduced on the device) equals the reference's to its printed precision
+    la = _log_rows(os.path.join(workdir, "ref", "log.txt"))
+    lg = _log_rows(os.path.join(workdir, "gpu", "log.txt"))
+    assert len(la) == len(lg) == 5
+    for ra, rg in zip(la, lg):
+        assert ra[0] == rg[0]
+        for a, g in zip(ra[1:], rg[1:]):
+            assert (np.isnan(a) and np.isnan(g)) or abs(a - g) <= 2e-3 * abs(a) + 1e-300, (ra, rg)
+
+
+def _log_rows(path):
+    rows = []
+    for line in open(path):
+        tok = line.split()
+        if tok and tok[0].isdigit():
+            rows.append([int(tok[0])] + [float(x) for x in tok[1:]])
+    return rows

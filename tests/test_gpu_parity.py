@@ -280,3 +280,29 @@ def test_lumped_mass_kat_gpu_path():
     b.sync()
     m = g.mass().reshape(-1, 3)[k["check_nodes"]]
     assert np.max(np.abs(m - k["lumped_mass"]) / k["lumped_mass"]) < 2e-7
+
+
+def test_device_extrema_and_supg_log_stats():
+    """Velocity extrema and the SUPG log quantities reduced on the device
+    against the same reductions of the state read back to the host."""
+    p = mesh.channel(8, 4, 4, seed=6, steps=4, noise=1e-3)
+    g = api.GpuProblem(p)
+    b = api.Batch([g])
+    b.step(3)
+    b.sync()
+    u = g.state(elements=False)[0]
+    ex = g.velocity_extrema()
+    ref = [u[:, 0].min(), u[:, 0].max(), u[:, 1].min(), u[:, 1].max(), u[:, 2].min(), u[:, 2].max(),
+           np.sqrt((u * u).sum(1)).max()]
+    assert np.array_equal(ex, np.array(ref))
+    st = g.supg_log_stats()
+    assert np.all(np.isfinite(st)) and st[0] <= st[1] and st[2] <= st[3] and st[7] <= st[8] and st[9] <= st[10]
+    # E and nu of the element-averaged lambda bound those of the element lambdas read back
+    lam = g.state()[2][:, 0]
+    mu = p.props[1]
+    E = mu * (3 * lam + 2 * mu) / (lam + mu)
+    # the element lambda the step wrote comes from the state before the step;
+    # the statistics are of the current state, so compare ranges loosely
+    assert st[7] > 0 and st[8] < 1e3 * E.max()
+    b.close()
+    g.close()
