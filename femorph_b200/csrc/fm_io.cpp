@@ -1,10 +1,12 @@
 // .dat keyword reader and legacy-VTK writer with the reference's formats.
+#include <algorithm>
 #include <cctype>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fm_internal.hpp"
@@ -13,44 +15,159 @@ using namespace fm;
 
 namespace {
 
-std::string upper(std::string s) {
-  for (auto& c : s) c = (char)std::toupper((unsigned char)c);
-  return s;
-}
+// A token of a line: [b, e).  The file buffer is NUL-terminated, and every
+// token is followed by a separator, a line end or the terminator, so strtod
+// and strtol stop at the token's end as atof / atoi on the token would.
+struct Tok {
+  const char* b = nullptr;
+  const char* e = nullptr;
+};
 
-// boost::trim + boost::split(is_any_of(" ,"), token_compress_on) as used by
-// femModel::ReadFromFEMTextFile (femModel.cpp:3790-3794).
-void tokenize(const std::string& line, std::vector<std::string>& tok) {
-  tok.clear();
-  size_t b = 0, e = line.size();
-  while (b < e && std::isspace((unsigned char)line[b])) ++b;
-  while (e > b && std::isspace((unsigned char)line[e - 1])) --e;
-  std::string cur;
-  size_t i = b;
+// boost::trim + boost::split(is_any_of(" ,"), token_compress_on) on one line
+// (femModel::ReadFromFEMTextFile, femModel.cpp:3790-3794); returns the
+// number of tokens (at least 1; tokens beyond maxtok are counted, not kept).
+int split_line(const char* b, const char* e, Tok* tok, int maxtok) {
+  while (b < e && std::isspace((unsigned char)*b)) ++b;
+  while (e > b && std::isspace((unsigned char)e[-1])) --e;
+  int n = 0;
+  const char* cur = b;
+  const char* i = b;
   while (i < e) {
-    char c = line[i];
-    if (c == ' ' || c == ',') {
-      tok.push_back(cur);
-      cur.clear();
-      while (i < e && (line[i] == ' ' || line[i] == ',')) ++i;
+    if (*i == ' ' || *i == ',') {
+      if (n < maxtok) tok[n] = {cur, i};
+      ++n;
+      while (i < e && (*i == ' ' || *i == ',')) ++i;
+      cur = i;
     } else {
-      cur.push_back(c);
       ++i;
     }
   }
-  tok.push_back(cur);
+  if (n < maxtok) tok[n] = {cur, e};
+  return n + 1;
 }
 
-double tokd(const std::vector<std::string>& t, size_t i) { return i < t.size() ? atof(t[i].c_str()) : 0.0; }
-int toki(const std::vector<std::string>& t, size_t i) { return i < t.size() ? atoi(t[i].c_str()) : 0; }
+bool tok_is(const Tok& t, const char* kw) {  // case-insensitive equality
+  const size_t n = strlen(kw);
+  if ((size_t)(t.e - t.b) != n) return false;
+  for (size_t i = 0; i < n; ++i)
+    if (std::toupper((unsigned char)t.b[i]) != kw[i]) return false;
+  return true;
+}
+std::string tok_upper(const Tok& t) {
+  std::string s(t.b, t.e);
+  for (auto& c : s) c = (char)std::toupper((unsigned char)c);
+  return s;
+}
+double tdbl(const Tok* t, int n, int i) { return i < n ? strtod(t[i].b, nullptr) : 0.0; }
+int tint(const Tok* t, int n, int i) { return i < n ? (int)strtol(t[i].b, nullptr, 10) : 0; }
+
+// Everything one block of lines contributes, in line order.
+struct DatBlock {
+  std::vector<double> coords, vel_vals, dir_vals, pres_vals;
+  std::vector<int32_t> conn, vel_node, vel_dir, dir_node, pres_node;
+  int etype = 0;
+  int64_t etype_line = -1;              // first ELEMENT line of a handled type (block-local)
+  int64_t change_line = -1;             // first ELEMENT line whose type differs from etype
+  int64_t bad_line = -1;                // first ELEMENT line of an unhandled type
+  std::string bad_type;
+  std::vector<std::pair<int64_t, std::vector<std::string>>> scalars;  // (local line, upper-cased tokens)
+  int64_t lines = 0;
+};
+
+void parse_block(const char* b, const char* e, DatBlock& B) {
+  constexpr int MT = 16;
+  Tok t[MT];
+  const char* line = b;
+  while (line < e) {
+    const char* le = (const char*)memchr(line, '\n', (size_t)(e - line));
+    if (!le) le = e;
+    const int n = split_line(line, le, t, MT);
+    const int nt = n < MT ? n : MT;
+    const int64_t ln = B.lines++;
+    if (tok_is(t[0], "NODE")) {
+      B.coords.push_back(tdbl(t, nt, 2));
+      B.coords.push_back(tdbl(t, nt, 3));
+      B.coords.push_back(tdbl(t, nt, 4));
+    } else if (tok_is(t[0], "ELEMENT")) {
+      const int npe = (nt > 1 && tok_is(t[1], "TET4")) ? 4 : ((nt > 1 && tok_is(t[1], "HEXA8")) ? 8 : 0);
+      if (!npe) {
+        if (B.bad_line < 0) {
+          B.bad_line = ln;
+          B.bad_type = nt > 1 ? tok_upper(t[1]) : std::string();
+        }
+      } else {
+        if (!B.etype) {
+          B.etype = npe;
+          B.etype_line = ln;
+        } else if (B.etype != npe && B.change_line < 0) {
+          B.change_line = ln;
+        }
+        for (int a = 0; a < npe; ++a) B.conn.push_back(tint(t, nt, 4 + a) - 1);
+      }
+    } else if (tok_is(t[0], "NODEDIRBC")) {
+      B.dir_node.push_back(tint(t, nt, 1) - 1);
+      B.dir_vals.push_back(tdbl(t, nt, 2));
+      // one value: the reference stores a 1-entry row and setDirichletBC then
+      // reads past it; missing components are taken as 0 here.
+      B.dir_vals.push_back(n > 3 ? tdbl(t, nt, 3) : 0.0);
+      B.dir_vals.push_back(n > 3 ? tdbl(t, nt, 4) : 0.0);
+    } else if (tok_is(t[0], "NODEVEL")) {
+      B.vel_node.push_back(tint(t, nt, 1) - 1);
+      for (int c = 0; c < 4; ++c) B.vel_vals.push_back(tdbl(t, nt, 2 + c));
+      B.vel_dir.push_back(n > 6 ? (int32_t)tdbl(t, nt, 6) : 6);
+    } else if (tok_is(t[0], "NODEPRES")) {
+      B.pres_node.push_back(tint(t, nt, 1) - 1);
+      B.pres_vals.push_back(tdbl(t, nt, 2));
+    } else if (tok_is(t[0], "NODEDOF") || tok_is(t[0], "TIMESTEP") || tok_is(t[0], "DUALSTEP") ||
+               tok_is(t[0], "VMSPROPS") || tok_is(t[0], "EXOPTS") || tok_is(t[0], "EXITCOND") ||
+               tok_is(t[0], "SOLVER") || tok_is(t[0], "PRECISION")) {
+      std::vector<std::string> v;
+      for (int i = 0; i < nt; ++i) v.emplace_back(t[i].b, t[i].e);
+      v[0] = tok_upper(t[0]);
+      B.scalars.emplace_back(ln, std::move(v));
+    }
+    line = le + 1;
+  }
+}
 
 }  // namespace
 
+// Reads the whole file, cuts it at line ends into one block per host thread,
+// parses the blocks in parallel and joins them in file order (keyword rows
+// keep their order; for the single-valued keywords the last line wins, as in
+// the reference's sequential reader).
 extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t precision, fm_problem** out) {
   if (!path || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
-  std::ifstream in(path);
-  if (!in) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  FILE* fp = fopen(path, "rb");
+  if (!fp) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  fseek(fp, 0, SEEK_END);
+  const long size = ftell(fp);
+  fseek(fp, 0, SEEK_SET);
+  std::vector<char> buf((size_t)std::max(0L, size) + 1, '\0');
+  if (size > 0 && fread(buf.data(), 1, (size_t)size, fp) != (size_t)size) {
+    fclose(fp);
+    return fail(FM_ERR_IO, std::string("cannot read ") + path);
+  }
+  fclose(fp);
+  const char* base = buf.data();
+  const int64_t len = size;
+  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  const int64_t nb = std::min<int64_t>(hw, std::max<int64_t>(1, len / (1 << 20)));
+  std::vector<int64_t> cut(nb + 1, 0);
+  cut[nb] = len;
+  for (int64_t k = 1; k < nb; ++k) {
+    int64_t c = std::max(cut[k - 1], len * k / nb);
+    while (c < len && base[c - 1] != '\n') ++c;  // start of a line
+    cut[k] = c;
+  }
+  std::vector<DatBlock> blk(nb);
+  {
+    std::vector<std::thread> th;
+    for (int64_t k = 0; k < nb; ++k)
+      th.emplace_back([&, k] { parse_block(base + cut[k], base + cut[k + 1], blk[k]); });
+    for (auto& x : th) x.join();
+  }
   std::vector<double> coords, vel_vals, dir_vals, pres_vals;
   std::vector<int32_t> conn, vel_node, vel_dir, dir_node, pres_node;
   int etype = 0;
@@ -60,62 +177,62 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
   prm.precision = precision;
   bool have_dual = false;
   std::string glob = "NONE";
-  std::string line;
-  std::vector<std::string> t;
-  int64_t lineno = 0;
-  while (std::getline(in, line)) {
-    ++lineno;
-    tokenize(line, t);
-    const std::string k = upper(t[0]);
-    if (k == "NODE") {
-      coords.push_back(tokd(t, 2));
-      coords.push_back(tokd(t, 3));
-      coords.push_back(tokd(t, 4));
-    } else if (k == "ELEMENT") {
-      const std::string et = upper(t.size() > 1 ? t[1] : "");
-      int npe = et == "TET4" ? 4 : (et == "HEXA8" ? 8 : 0);
-      if (!npe) return fail(FM_ERR_INVALID, "line " + std::to_string(lineno) + ": element type " + et +
-                                                " is not handled by the explicit flow solvers");
-      if (etype && etype != npe) return fail(FM_ERR_INVALID, "mixed element types are not supported");
-      etype = npe;
-      for (int a = 0; a < npe; ++a) conn.push_back(toki(t, 4 + a) - 1);
-    } else if (k == "NODEDIRBC") {
-      dir_node.push_back(toki(t, 1) - 1);
-      dir_vals.push_back(tokd(t, 2));
-      // one value: the reference stores a 1-entry row and setDirichletBC then
-      // reads past it; missing components are taken as 0 here.
-      dir_vals.push_back(t.size() > 3 ? tokd(t, 3) : 0.0);
-      dir_vals.push_back(t.size() > 3 ? tokd(t, 4) : 0.0);
-    } else if (k == "NODEVEL") {
-      vel_node.push_back(toki(t, 1) - 1);
-      for (int c = 0; c < 4; ++c) vel_vals.push_back(tokd(t, 2 + c));
-      vel_dir.push_back(t.size() > 6 ? (int32_t)atof(t[6].c_str()) : 6);
-    } else if (k == "NODEPRES") {
-      pres_node.push_back(toki(t, 1) - 1);
-      pres_vals.push_back(tokd(t, 2));
-    } else if (k == "NODEDOF") {
-      if (t.size() > 2) glob = upper(t[2]);
-    } else if (k == "TIMESTEP") {
-      prm.time_step = tokd(t, 1);
-      prm.total_steps = toki(t, 2);
-      prm.save_every = toki(t, 3);
-    } else if (k == "DUALSTEP") {
-      prm.dual_step = tokd(t, 1);
-      prm.tot_dual_steps = toki(t, 2);
-      have_dual = true;
-    } else if (k == "VMSPROPS") {
-      for (int c = 0; c < 5; ++c) prm.props[c] = tokd(t, 1 + c);
-    } else if (k == "EXOPTS") {
-      for (int c = 0; c < 6; ++c) prm.ex_opts[c] = toki(t, 1 + c) != 0;
-    } else if (k == "EXITCOND") {
-      prm.exit_condition = tokd(t, 1);
-    } else if (k == "SOLVER") {
-      const std::string v = upper(t.size() > 1 ? t[1] : "");
-      prm.solver = v == "SUPG" ? FM_SOLVER_SUPG : FM_SOLVER_VMS;
-    } else if (k == "PRECISION") {
-      const std::string v = upper(t.size() > 1 ? t[1] : "");
-      prm.precision = v == "MIXED" ? FM_MIXED : FM_FP64;
+  int64_t line0 = 0;
+  auto cat = [](auto& dst, const auto& src) { dst.insert(dst.end(), src.begin(), src.end()); };
+  for (int64_t k = 0; k < nb; ++k) {
+    DatBlock& B = blk[k];
+    // the first element-type problem in file order, as the sequential reader meets it
+    const int64_t INF = INT64_MAX;
+    int64_t at_mix = B.change_line >= 0 ? B.change_line : INF;
+    if (B.etype && etype && B.etype != etype) at_mix = std::min(at_mix, B.etype_line);
+    const int64_t at_bad = B.bad_line >= 0 ? B.bad_line : INF;
+    if (at_bad < at_mix)
+      return fail(FM_ERR_INVALID, "line " + std::to_string(line0 + at_bad + 1) + ": element type " + B.bad_type +
+                                      " is not handled by the explicit flow solvers");
+    if (at_mix < INF) return fail(FM_ERR_INVALID, "mixed element types are not supported");
+    if (B.etype) etype = B.etype;
+    cat(coords, B.coords); cat(conn, B.conn);
+    cat(vel_node, B.vel_node); cat(vel_vals, B.vel_vals); cat(vel_dir, B.vel_dir);
+    cat(dir_node, B.dir_node); cat(dir_vals, B.dir_vals);
+    cat(pres_node, B.pres_node); cat(pres_vals, B.pres_vals);
+    for (auto& sc : B.scalars) {
+      const std::vector<std::string>& t = sc.second;
+      const int n = (int)t.size();
+      auto d = [&](int i) { return i < n ? atof(t[i].c_str()) : 0.0; };
+      auto in = [&](int i) { return i < n ? atoi(t[i].c_str()) : 0; };
+      const std::string& kw = t[0];
+      if (kw == "NODEDOF") {
+        if (n > 2) {
+          glob = t[2];
+          for (auto& c : glob) c = (char)std::toupper((unsigned char)c);
+        }
+      } else if (kw == "TIMESTEP") {
+        prm.time_step = d(1);
+        prm.total_steps = in(2);
+        prm.save_every = in(3);
+      } else if (kw == "DUALSTEP") {
+        prm.dual_step = d(1);
+        prm.tot_dual_steps = in(2);
+        have_dual = true;
+      } else if (kw == "VMSPROPS") {
+        for (int c = 0; c < 5; ++c) prm.props[c] = d(1 + c);
+      } else if (kw == "EXOPTS") {
+        for (int c = 0; c < 6; ++c) prm.ex_opts[c] = in(1 + c) != 0;
+      } else if (kw == "EXITCOND") {
+        prm.exit_condition = d(1);
+      } else if (kw == "SOLVER") {
+        std::string v = n > 1 ? t[1] : "";
+        for (auto& c : v) c = (char)std::toupper((unsigned char)c);
+        prm.solver = v == "SUPG" ? FM_SOLVER_SUPG : FM_SOLVER_VMS;
+      } else if (kw == "PRECISION") {
+        std::string v = n > 1 ? t[1] : "";
+        for (auto& c : v) c = (char)std::toupper((unsigned char)c);
+        prm.precision = v == "MIXED" ? FM_MIXED : FM_FP64;
+      }
     }
+    line0 += B.lines;
+    std::vector<double>().swap(B.coords);  // release as we go
+    std::vector<int32_t>().swap(B.conn);
   }
   if (glob == "NONE") prm.glob_fixed = FM_FIX_NONE;
   else if (glob == "X") prm.glob_fixed = FM_FIX_X;
@@ -155,6 +272,44 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
 // lambda, regime (element).  res_v/res_p are the reference's diagnostic
 // centroid averages of a partially assembled residual (they depend on the
 // element loop order and carry no state); they are written as zeros.
+namespace {
+
+// Writes rows 0..n-1, row i formatted by fmt(i, buf) (returns its length,
+// < 256), formatting blocks of rows on host threads and writing the blocks
+// in order: the bytes are those of the sequential fprintf loop.
+template <class F>
+void write_rows(FILE* f, int64_t n, F fmt) {
+  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  const int64_t nb = std::min<int64_t>(hw * 4, std::max<int64_t>(1, n / 65536));
+  std::vector<std::string> out(nb);
+  auto work = [&](int64_t k) {
+    std::string& o = out[k];
+    char buf[256];
+    for (int64_t i = n * k / nb; i < n * (k + 1) / nb; ++i) o.append(buf, (size_t)fmt(i, buf));
+  };
+  if (nb == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    const int64_t nt = std::min<int64_t>(hw, nb);
+    for (int64_t w = 0; w < nt; ++w)
+      th.emplace_back([&, w] {
+        for (int64_t k = w; k < nb; k += nt) work(k);
+      });
+    for (auto& x : th) x.join();
+  }
+  for (auto& o : out) fwrite(o.data(), 1, o.size(), f);
+}
+
+}  // namespace
+
+// femModel::ExportToVTKLegacy (femModel.cpp:1294-1530) for the explicit
+// solvers' result lists: VMS writes velocity + pressure (node) and res_v,
+// res_p, subgrid_u, subgrid_p (element); SUPG velocity (node) and pressure,
+// lambda, regime (element).  res_v/res_p are the reference's diagnostic
+// centroid averages of a partially assembled residual (they depend on the
+// element loop order and carry no state); they are written as zeros.  The
+// rows are formatted on the host threads (write_rows).
 extern "C" int fm_problem_write_vtk(fm_problem* p, const char* path) {
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
   const int64_t N = p->N, E = p->E;
@@ -168,57 +323,62 @@ extern "C" int fm_problem_write_vtk(fm_problem* p, const char* path) {
   }
   FILE* f = fopen(path, "w");
   if (!f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  const double* X = p->coords.data();
+  const int npe = p->etype;
+  const int32_t* cn = p->conn.data();
   fprintf(f, "# vtk DataFile Version 2.0\nModel Exported from feMorph\nASCII\nDATASET UNSTRUCTURED_GRID\n");
   fprintf(f, "POINTS %d float\n", (int)N);
-  for (int64_t i = 0; i < N; ++i) fprintf(f, "%e %e %e\n", p->coords[i * 3], p->coords[i * 3 + 1], p->coords[i * 3 + 2]);
-  const int npe = p->etype;
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e %e %e\n", X[i * 3], X[i * 3 + 1], X[i * 3 + 2]); });
   fprintf(f, "CELLS %d %d\n", (int)E, (int)(E * (npe + 1)));
-  for (int64_t e = 0; e < E; ++e) {
-    fprintf(f, "%d ", npe);
-    for (int a = 0; a < npe; ++a) fprintf(f, "%d ", p->conn[e * npe + a]);
-    fprintf(f, "\n");
-  }
+  write_rows(f, E, [&](int64_t e, char* b) {
+    int k = snprintf(b, 256, "%d ", npe);
+    for (int a = 0; a < npe; ++a) k += snprintf(b + k, 256 - k, "%d ", cn[e * npe + a]);
+    k += snprintf(b + k, 256 - k, "\n");
+    return k;
+  });
   fprintf(f, "CELL_TYPES %d\n", (int)E);
-  for (int64_t e = 0; e < E; ++e) fprintf(f, "%d\n", npe == 4 ? 10 : 12);
+  const int ctype = npe == 4 ? 10 : 12;
+  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%d\n", ctype); });
   fprintf(f, "POINT_DATA %d\n", (int)N);
   fprintf(f, "VECTORS DXYZ double\n");
-  for (int64_t i = 0; i < N; ++i) fprintf(f, "%e %e %e\n", 0.0, 0.0, 0.0);
+  write_rows(f, N, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e\n", 0.0, 0.0, 0.0); });
   fprintf(f, "VECTORS velocity double\n");
-  for (int64_t i = 0; i < N; ++i) fprintf(f, "%e %e %e \n", u[i * 3], u[i * 3 + 1], u[i * 3 + 2]);
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e %e %e \n", u[i * 3], u[i * 3 + 1], u[i * 3 + 2]); });
   if (vms) {
     fprintf(f, "SCALARS pressure double 1\nLOOKUP_TABLE default\n");
-    for (int64_t i = 0; i < N; ++i) fprintf(f, "%e \n", pres[i]);
+    write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e \n", pres[i]); });
   }
   std::vector<double> dirbc(N, 0.0);
   for (int32_t n : p->vel_node) dirbc[n] = 2.0;
   for (int32_t n : p->pres_node) dirbc[n] = 3.0;
   for (int32_t n : p->dir_node) dirbc[n] = 1.0;
   fprintf(f, "SCALARS dirBC double 1\nLOOKUP_TABLE default\n");
-  for (int64_t i = 0; i < N; ++i) fprintf(f, "%e\n", dirbc[i]);
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e\n", dirbc[i]); });
   fprintf(f, "SCALARS neuBC double\nLOOKUP_TABLE default\n");
-  for (int64_t i = 0; i < N; ++i) fprintf(f, "%e\n", 0.0);
+  write_rows(f, N, [&](int64_t, char* b) { return snprintf(b, 256, "%e\n", 0.0); });
   fprintf(f, "CELL_DATA %d\n", (int)E);
   fprintf(f, "VECTORS normal double\n");
-  for (int64_t e = 0; e < E; ++e) fprintf(f, "%e %e %e\n", 0.0, 0.0, 0.0);
+  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e\n", 0.0, 0.0, 0.0); });
   fprintf(f, "SCALARS source double 1\nLOOKUP_TABLE default\n");
-  for (int64_t e = 0; e < E; ++e) fprintf(f, "%e\n", 0.0);
+  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e\n", 0.0); });
   if (vms) {
     fprintf(f, "VECTORS res_v double\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e %e %e \n", 0.0, 0.0, 0.0);
+    write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e \n", 0.0, 0.0, 0.0); });
     fprintf(f, "SCALARS res_p double 1\nLOOKUP_TABLE default\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e \n", 0.0);
+    write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e \n", 0.0); });
     fprintf(f, "VECTORS subgrid_u double\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e %e %e \n", e3[e * 3], e3[e * 3 + 1], e3[e * 3 + 2]);
+    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e %e %e \n", e3[e * 3], e3[e * 3 + 1], e3[e * 3 + 2]); });
     fprintf(f, "SCALARS subgrid_p double 1\nLOOKUP_TABLE default\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e \n", 0.0);
+    write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e \n", 0.0); });
   } else {
     fprintf(f, "SCALARS pressure double 1\nLOOKUP_TABLE default\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e \n", pres[e]);
+    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", pres[e]); });
     fprintf(f, "SCALARS lambda double 1\nLOOKUP_TABLE default\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e \n", e3[e * 2]);
+    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", e3[e * 2]); });
     fprintf(f, "SCALARS regime double 1\nLOOKUP_TABLE default\n");
-    for (int64_t e = 0; e < E; ++e) fprintf(f, "%e \n", e3[e * 2 + 1]);
+    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", e3[e * 2 + 1]); });
   }
+  const bool ok = ferror(f) == 0;
   fclose(f);
-  return FM_OK;
+  return ok ? FM_OK : fail(FM_ERR_IO, std::string("cannot write ") + path);
 }

@@ -171,3 +171,15 @@ def test_capacity_bytes_grow_with_capacity_and_static_entry_validates():
     assert L.fm_vms_solve_static(v.h, 1, 0, None, None, None) == api.FM_ERR_INVALID   # not prepared
     s.close()
     v.close()
+
+
+def test_dat_reader_multi_block_file_equals_in_memory_problem(tmp_path):
+    p = mesh.cavity(40, seed=3, steps=2)      # ~40 MB: several parse blocks
+    path = str(tmp_path / "m.dat")
+    mesh.write_dat(p, path)
+    h = C.c_void_p()
+    api.check(api.lib().fm_problem_read_dat(path.encode(), 0, 0, C.byref(h)))
+    m = np.zeros(p.n_nodes)
+    api.check(api.lib().fm_problem_get_mass(h, m.ctypes.data))
+    assert np.array_equal(m, api.GpuProblem(p).mass())
+    api.lib().fm_problem_destroy(h)
