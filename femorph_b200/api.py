@@ -94,6 +94,7 @@ def lib():
         L.fm_batch_step_ragged.argtypes = [P, P, P]
         L.fm_problem_get_state.argtypes = [P, P, P, P, P]
         L.fm_problem_write_vtk.argtypes = [P, C.c_char_p]
+        L.fm_problem_write_vtk_binary.argtypes = [P, C.c_char_p]
         L.fm_problem_get_mass.argtypes = [P, P]
         L.fm_batch_last_timing.argtypes = [P, P, P]
         L.fm_batch_estimate_bytes.argtypes = [P, C.c_int32, P, P]
@@ -179,8 +180,9 @@ class GpuProblem:
         check(lib().fm_problem_get_mass(self.h, _p(m)))
         return m
 
-    def write_vtk(self, path: str) -> None:
-        check(lib().fm_problem_write_vtk(self.h, path.encode()))
+    def write_vtk(self, path: str, binary: bool = False) -> None:
+        f = lib().fm_problem_write_vtk_binary if binary else lib().fm_problem_write_vtk
+        check(f(self.h, path.encode()))
 
     def prepare(self, tile_elems=0, tile_nodes=0, threads=0) -> None:
         """Builds the tile layout now (host only, thread-safe per problem)."""

@@ -256,6 +256,10 @@ FM_API int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* 
 /* Writes the problem's current state as legacy ASCII VTK in the layout of
  * femModel::ExportToVTKLegacy (femModel.cpp:1294-1530). */
 FM_API int fm_problem_write_vtk(fm_problem* p, const char* path);
+/* The same sections in legacy BINARY VTK (big-endian float32 points, int32
+ * cells, float64 data); no counterpart in the reference, which writes ASCII
+ * only. */
+FM_API int fm_problem_write_vtk_binary(fm_problem* p, const char* path);
 
 /* Nodal lumped mass as the solver uses it, problem numbering: VMS n_nodes
  * (initial_assemble, femVMSExplicitFluidSolver.cpp:87-89), SUPG n_nodes x 3
