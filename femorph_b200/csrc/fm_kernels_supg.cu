@@ -48,10 +48,14 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
   if (status != FM_OK) B.pstate[pidx].status = status;
 }
 
-// MIXED: Gauss-point work in FP32 (supg_element_mixed), at most ~168
-// registers a thread so that three 128-thread CTAs fit an SM.
+// MIXED: Gauss-point work in FP32 (supg_element_mixed).  The mixed kernels
+// and the FP64 tet4 kernel are held to ~168 registers a thread so that three
+// 128-thread CTAs fit an SM (FP64 tet4: a small spill, 12% faster than two
+// CTAs at 241 registers); the FP64 hexa8 kernel keeps 255 (three CTAs spill
+// 1 KB a thread and run 30% slower).
 template <int NPE, int THREADS, bool MIXED>
-__global__ void __launch_bounds__(THREADS, MIXED && THREADS == 128 ? 3 : 1) supg_tile_kernel(DevBatch B, int tn_max) {
+__global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4) ? 3 : 1)
+    supg_tile_kernel(DevBatch B, int tn_max) {
   extern __shared__ double sm[];
   double* s_x = sm;
   double* s_y = s_x + tn_max;

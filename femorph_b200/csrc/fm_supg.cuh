@@ -102,18 +102,21 @@ __device__ __forceinline__ void fill_shape_table(ShapeTable<NPE, T>* t) {
 // cofactor inverse (femUtils.cpp:716-770), global derivatives
 // gd[n][b] = sum_c inv[b][c] dN[n][c] (femElement.cpp:345-352) and the
 // geometric matrix G[a][b] = sum_c inv[c][a] inv[c][b] (femElement.cpp:222-230).
-template <int NPE>
-__device__ __forceinline__ double jacobian(const double dN[NPE][3], const double* sx, const double* sy, const double* sz,
-                                           const int ln[NPE], double inv[3][3]) {
+// The local derivatives are read through dN(n, a): a register array, or a
+// shared-memory table read where used.
+template <int NPE, class DN>
+__device__ __forceinline__ double jacobian_at(DN dN, const double* sx, const double* sy, const double* sz, const int ln[NPE],
+                                              double inv[3][3]) {
   double J[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     double j0 = 0.0, j1 = 0.0, j2 = 0.0;
 #pragma unroll
     for (int n = 0; n < NPE; ++n) {
-      j0 += dN[n][a] * sx[ln[n]];
-      j1 += dN[n][a] * sy[ln[n]];
-      j2 += dN[n][a] * sz[ln[n]];
+      const double d = dN(n, a);
+      j0 += d * sx[ln[n]];
+      j1 += d * sy[ln[n]];
+      j2 += d * sz[ln[n]];
     }
     J[a][0] = j0; J[a][1] = j1; J[a][2] = j2;
   }
@@ -133,6 +136,12 @@ __device__ __forceinline__ double jacobian(const double dN[NPE][3], const double
   return det;
 }
 
+template <int NPE>
+__device__ __forceinline__ double jacobian(const double dN[NPE][3], const double* sx, const double* sy, const double* sz,
+                                           const int ln[NPE], double inv[3][3]) {
+  return jacobian_at<NPE>([&](int n, int a) { return dN[n][a]; }, sx, sy, sz, ln, inv);
+}
+
 // One element: k[a][c] = -dt (sum of the enabled K_i u_e)[a][c].  Coordinates
 // and velocities are read from the tile's shared-memory node arrays through
 // the local ids ln[].  Also returns the element's lambda (volume average) and
@@ -150,56 +159,64 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
   const double wq = GaussRule<NPE>::weight();
 #pragma unroll
   for (int a = 0; a < NPE; ++a) k[a][0] = k[a][1] = k[a][2] = 0.0;
-  // volume-averaged derivatives for B-bar (eval_avg_shapeDeriv, src lines 660-707)
-  double sd0[NPE][3];
+  // B-bar (eval_avg_shapeDeriv, src lines 660-707, and the B matrix rows
+  // 0-2, src lines 234-256).  With sd0[a][c] = sum_g w_g gd_g[a][c] / V the
+  // volume-averaged derivatives, B1 = (sd0[a][0] - gd[a][0]) / 3, B2 =
+  // gd[a][0] - B1 and likewise B3/B4, B5/B6 for y and z, the sums over the
+  // nodes are
+  //   strain:  eps_c = gr_cc - 2 d_c + (d_0 + d_1 + d_2),
+  //            d_c = (Dbar_c - gr_cc) / 3,  Dbar_c = sum_a sd0[a][c] u_c(a)
+  //   force:   r_c(a) w = gd[a][c] (w sig_c - q_c) + sd0[a][c] q_c,
+  //            q_c = w (sig_0 + sig_1 + sig_2 - 2 sig_c) / 3,
+  // so sd0 enters only through the element constants Dbar_c = sum_g w_g
+  // gr_g[c][c] / V (before the Gauss loop) and sd0[a][c] Q_c, Q_c = sum_g q_c
+  // (after it): the 24 averaged derivatives are never held in registers.
+  auto jac_inv = [&](int g, double inv[3][3]) -> double {
+    return jacobian_at<NPE>([&](int n, int c) { return tab.dN[g][n][c]; }, sx, sy, sz, ln, inv);
+  };
+  double Dbar[3] = {0.0, 0.0, 0.0}, Qb[3] = {0.0, 0.0, 0.0}, bden = 0.0;
   if (NPE == 8 && bbar) {
-    double num[NPE][3], den = 0.0;
-#pragma unroll
-    for (int a = 0; a < NPE; ++a) num[a][0] = num[a][1] = num[a][2] = 0.0;
+    double dsum[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
     for (int g = 0; g < GaussRule<NPE>::n; ++g) {
-      double dN[NPE][3], inv[3][3];
+      double inv[3][3];
+      const double w = jac_inv(g, inv) * wq;
+      bden += w;
+      double g0 = 0.0, g1 = 0.0, g2 = 0.0;
 #pragma unroll
-      for (int a = 0; a < NPE; ++a)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) dN[a][c] = tab.dN[g][a][c];
-      const double det = jacobian<NPE>(dN, sx, sy, sz, ln, inv);
-      const double w = det * wq;
-      den += w;
-#pragma unroll
-      for (int a = 0; a < NPE; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-          num[a][b] += (inv[b][0] * dN[a][0] + inv[b][1] * dN[a][1] + inv[b][2] * dN[a][2]) * w;
+      for (int a = 0; a < NPE; ++a) {
+        const double d0 = tab.dN[g][a][0], d1 = tab.dN[g][a][1], d2 = tab.dN[g][a][2];
+        g0 += (inv[0][0] * d0 + inv[0][1] * d1 + inv[0][2] * d2) * su[ln[a]];
+        g1 += (inv[1][0] * d0 + inv[1][1] * d1 + inv[1][2] * d2) * sv[ln[a]];
+        g2 += (inv[2][0] * d0 + inv[2][1] * d1 + inv[2][2] * d2) * sw[ln[a]];
+      }
+      dsum[0] += w * g0; dsum[1] += w * g1; dsum[2] += w * g2;
     }
 #pragma unroll
-    for (int a = 0; a < NPE; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) sd0[a][b] = num[a][b] / den;
+    for (int c = 0; c < 3; ++c) Dbar[c] = dsum[c] / bden;
   }
   double vol = 0.0, lam_int = 0.0, reg = 0.0;
 #pragma unroll 1
   for (int g = 0; g < GaussRule<NPE>::n; ++g) {
-    double Nf[NPE], dN[NPE][3], inv[3][3];
+    // shape values and local derivatives: tet4 in closed form (constant
+    // derivatives), hexa8 read from the shared-memory table where used; the
+    // global derivatives are formed where used too (no register arrays)
+    double Nq[NPE];
     if (NPE == 4) {
-      // tet4: constant derivatives, N from the point (cheaper than the table)
       double q[3];
       GaussRule<NPE>::point(g, q);
-      shape<NPE>(q, Nf, dN);
-    } else {
-#pragma unroll
-      for (int a = 0; a < NPE; ++a) {
-        Nf[a] = tab.N[g][a];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) dN[a][c] = tab.dN[g][a][c];
-      }
+      Nq[0] = q[0]; Nq[1] = q[1]; Nq[2] = q[2]; Nq[3 % NPE] = 1.0 - q[0] - q[1] - q[2];
     }
-    const double det = jacobian<NPE>(dN, sx, sy, sz, ln, inv);
-    double gd[NPE][3];
-#pragma unroll
-    for (int a = 0; a < NPE; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) gd[a][b] = inv[b][0] * dN[a][0] + inv[b][1] * dN[a][1] + inv[b][2] * dN[a][2];
+    auto Nv = [&](int a) -> double { return NPE == 4 ? Nq[a] : tab.N[g][a]; };
+    auto dNv = [&](int a, int c) -> double {
+      if (NPE == 4) return a == 3 ? -1.0 : (a == c ? 1.0 : 0.0);
+      return tab.dN[g][a][c];
+    };
+    double inv[3][3];
+    const double det = NPE == 8 ? jac_inv(g, inv) : jacobian_at<NPE>(dNv, sx, sy, sz, ln, inv);
+    auto gdv = [&](int a, int b) -> double {
+      return inv[b][0] * dNv(a, 0) + inv[b][1] * dNv(a, 1) + inv[b][2] * dNv(a, 2);
+    };
     double G[3][3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
@@ -210,11 +227,13 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
 #pragma unroll
     for (int a = 0; a < NPE; ++a) {
       const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
+      const double ga[3] = {gdv(a, 0), gdv(a, 1), gdv(a, 2)};
+      const double Na = Nv(a);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        u[c] += Nf[a] * ua[c];
+        u[c] += Na * ua[c];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) gr[c][d] += gd[a][d] * ua[c];
+        for (int d = 0; d < 3; ++d) gr[c][d] += ga[d] * ua[c];
       }
     }
     const double div = gr[0][0] + gr[1][1] + gr[2][2];
@@ -256,39 +275,43 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
     for (int c = 0; c < 3; ++c) conv[c] = u[0] * gr[c][0] + u[1] * gr[c][1] + u[2] * gr[c][2];
     // strain (B u) and stress (D B u)
     double eps[6];
-    double sdiv[3] = {0.0, 0.0, 0.0};  // B-bar volumetric parts
     if (NPE == 8 && bbar) {
-      // rows 0-2 of the B-bar matrix (src lines 234-256)
-      double e0 = 0.0, e1 = 0.0, e2 = 0.0;
-#pragma unroll
-      for (int a = 0; a < NPE; ++a) {
-        const double B1 = (1.0 / 3.0) * (sd0[a][0] - gd[a][0]), B2 = gd[a][0] - B1;
-        const double B3 = (1.0 / 3.0) * (sd0[a][1] - gd[a][1]), B4 = gd[a][1] - B3;
-        const double B5 = (1.0 / 3.0) * (sd0[a][2] - gd[a][2]), B6 = gd[a][2] - B5;
-        const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
-        e0 += B2 * ua[0] + B3 * ua[1] + B5 * ua[2];
-        e1 += B1 * ua[0] + B4 * ua[1] + B5 * ua[2];
-        e2 += B1 * ua[0] + B3 * ua[1] + B6 * ua[2];
-      }
-      eps[0] = e0; eps[1] = e1; eps[2] = e2;
+      const double d0 = (1.0 / 3.0) * (Dbar[0] - gr[0][0]), d1 = (1.0 / 3.0) * (Dbar[1] - gr[1][1]),
+                   d2 = (1.0 / 3.0) * (Dbar[2] - gr[2][2]);
+      eps[0] = gr[0][0] - d0 + d1 + d2;
+      eps[1] = d0 + gr[1][1] - d1 + d2;
+      eps[2] = d0 + d1 + gr[2][2] - d2;
     } else {
       eps[0] = gr[0][0]; eps[1] = gr[1][1]; eps[2] = gr[2][2];
     }
     eps[3] = gr[0][1] + gr[1][0];
     eps[4] = gr[1][2] + gr[2][1];
     eps[5] = gr[0][2] + gr[2][0];
-    (void)sdiv;
     const double l2m = lam + 2 * mu;
     const double sig[6] = {l2m * eps[0] + lam * eps[1] + lam * eps[2], lam * eps[0] + l2m * eps[1] + lam * eps[2],
                            lam * eps[0] + lam * eps[1] + l2m * eps[2], mu * eps[3], mu * eps[4], mu * eps[5]};
     const double c1w = rho * w, c3w = rho * tau * w, c4w = rho * nuC * div * w;
+    // normal-stress parts of K2: w sig_c multiplies gd[a][c]; with B-bar less
+    // q_c, whose sd0 part is added after the loop
+    double sd[3] = {sig[0] * w, sig[1] * w, sig[2] * w};
+    if (NPE == 8 && bbar && iK2) {
+      const double st = sig[0] + sig[1] + sig[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double q = (1.0 / 3.0) * w * (st - 2.0 * sig[c]);
+        Qb[c] += q;
+        sd[c] -= q;
+      }
+    }
 #pragma unroll
     for (int a = 0; a < NPE; ++a) {
-      const double Aa = u[0] * gd[a][0] + u[1] * gd[a][1] + u[2] * gd[a][2];
+      const double ga[3] = {gdv(a, 0), gdv(a, 1), gdv(a, 2)};
+      const double Aa = u[0] * ga[0] + u[1] * ga[1] + u[2] * ga[2];
       double f[3] = {0.0, 0.0, 0.0};
       if (iK1) {
+        const double Na = Nv(a);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] += c1w * Nf[a] * conv[c];
+        for (int c = 0; c < 3; ++c) f[c] += c1w * Na * conv[c];
       }
       if (iK3) {
 #pragma unroll
@@ -296,28 +319,33 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
       }
       if (iK4) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] += c4w * gd[a][c];
+        for (int c = 0; c < 3; ++c) f[c] += c4w * ga[c];
       }
       if (iK2) {
-        double r0, r1, r2;  // sum_r B[r][a,c] sigma_r for rows 0-2
-        if (NPE == 8 && bbar) {
-          const double B1 = (1.0 / 3.0) * (sd0[a][0] - gd[a][0]), B2 = gd[a][0] - B1;
-          const double B3 = (1.0 / 3.0) * (sd0[a][1] - gd[a][1]), B4 = gd[a][1] - B3;
-          const double B5 = (1.0 / 3.0) * (sd0[a][2] - gd[a][2]), B6 = gd[a][2] - B5;
-          r0 = B2 * sig[0] + B1 * sig[1] + B1 * sig[2];
-          r1 = B3 * sig[0] + B4 * sig[1] + B3 * sig[2];
-          r2 = B5 * sig[0] + B5 * sig[1] + B6 * sig[2];
-        } else {
-          r0 = gd[a][0] * sig[0];
-          r1 = gd[a][1] * sig[1];
-          r2 = gd[a][2] * sig[2];
-        }
-        f[0] += (r0 + gd[a][1] * sig[3] + gd[a][2] * sig[5]) * w;
-        f[1] += (r1 + gd[a][0] * sig[3] + gd[a][2] * sig[4]) * w;
-        f[2] += (r2 + gd[a][1] * sig[4] + gd[a][0] * sig[5]) * w;
+        f[0] += ga[0] * sd[0] + (ga[1] * sig[3] + ga[2] * sig[5]) * w;
+        f[1] += ga[1] * sd[1] + (ga[0] * sig[3] + ga[2] * sig[4]) * w;
+        f[2] += ga[2] * sd[2] + (ga[1] * sig[4] + ga[0] * sig[5]) * w;
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) k[a][c] += f[c];
+    }
+  }
+  if (NPE == 8 && bbar && iK2) {
+    // k[a][c] += sd0[a][c] Q_c, sd0 formed again Gauss point by Gauss point
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Qb[c] /= bden;
+#pragma unroll 1
+    for (int g = 0; g < GaussRule<NPE>::n; ++g) {
+      double inv[3][3];
+      const double w = jac_inv(g, inv) * wq;
+      const double s0 = w * Qb[0], s1 = w * Qb[1], s2 = w * Qb[2];
+#pragma unroll
+      for (int a = 0; a < NPE; ++a) {
+        const double d0 = tab.dN[g][a][0], d1 = tab.dN[g][a][1], d2 = tab.dN[g][a][2];
+        k[a][0] += (inv[0][0] * d0 + inv[0][1] * d1 + inv[0][2] * d2) * s0;
+        k[a][1] += (inv[1][0] * d0 + inv[1][1] * d1 + inv[1][2] * d2) * s1;
+        k[a][2] += (inv[2][0] * d0 + inv[2][1] * d1 + inv[2][2] * d2) * s2;
+      }
     }
   }
   const double mdt = -P.dt;
