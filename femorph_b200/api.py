@@ -31,6 +31,8 @@ SYMBOLS = [
     "fm_batch_profile", "fm_autotune", "fm_batch_create_empty", "fm_batch_add", "fm_batch_remove",
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
     "fm_vms_solve_static", "fm_batch_capacity_bytes", "fm_problem_velocity_extrema", "fm_problem_supg_log_stats",
+    "fm_partition_elements", "fm_problem_partition", "fm_problem_part_info", "fm_problem_part_map",
+    "fm_batch_exchange_buffers", "fm_batch_exchange_begin", "fm_batch_exchange_end", "fm_batch_iterations_per_step",
 ]
 
 
@@ -112,6 +114,14 @@ def lib():
         L.fm_problem_velocity_extrema.argtypes = [P, P]
         L.fm_problem_supg_log_stats.argtypes = [P, P]
         L.fm_vms_solve_static.argtypes = [P, C.c_int32, C.c_int32, P, P, P]
+        L.fm_partition_elements.argtypes = [P, C.c_int32, P]
+        L.fm_problem_partition.argtypes = [P, P, C.c_int32, C.c_int32, P]
+        L.fm_problem_part_info.argtypes = [P, P, P, P]
+        L.fm_problem_part_map.argtypes = [P, P, P, P]
+        L.fm_batch_exchange_buffers.argtypes = [P, P, P, P]
+        L.fm_batch_exchange_begin.argtypes = [P, P]
+        L.fm_batch_exchange_end.argtypes = [P, P]
+        L.fm_batch_iterations_per_step.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -161,6 +171,20 @@ class GpuProblem:
                                   else None, C.byref(h)))
         self.h = h
         self.n_nodes, self.n_elems, self.solver = p.n_nodes, p.n_elems, p.solver
+
+    def partition_elements(self, n_parts: int):
+        """Default element split: part index of every element (Morton bands)."""
+        out = np.zeros(self.n_elems, np.int32)
+        check(lib().fm_partition_elements(self.h, int(n_parts), _p(out)))
+        return out
+
+    def part(self, n_parts: int, part: int, elem_part=None) -> "GpuPart":
+        """The problem of one part of this mesh split into n_parts (elem_part:
+        the part of every element, default Morton bands)."""
+        ep = None if elem_part is None else np.ascontiguousarray(elem_part, np.int32)
+        h = C.c_void_p()
+        check(lib().fm_problem_partition(self.h, _p(ep), int(n_parts), int(part), C.byref(h)))
+        return GpuPart(h, self.solver, self.src)
 
     def state(self, elements: bool = True):
         """(u (N,3), p (N,) VMS | (E,) SUPG, elem (E,3) VMS | (E,2) SUPG, sdus (E,12) VMS | None);
@@ -217,6 +241,38 @@ class GpuProblem:
             pass
 
 
+class GpuPart(GpuProblem):
+    """One part of a partitioned mesh (GpuProblem.part).  State and masses
+    are in the part's local numbering; node_global / elem_global map them to
+    the whole mesh, xidx gives each local node's exchange index (-1: not
+    shared)."""
+
+    def __init__(self, h, solver, src):
+        L = lib()
+        self.h = h
+        self.src = src
+        self.solver = solver
+        nn, ne = C.c_int64(), C.c_int64()
+        check(L.fm_problem_info(h, C.byref(nn), C.byref(ne), None, None, None))
+        self.n_nodes, self.n_elems = nn.value, ne.value
+        part, nparts, xt = C.c_int32(), C.c_int32(), C.c_int64()
+        check(L.fm_problem_part_info(h, C.byref(part), C.byref(nparts), C.byref(xt)))
+        self.part_index, self.n_parts, self.x_total = part.value, nparts.value, xt.value
+        self.node_global = np.zeros(self.n_nodes, np.int32)
+        self.elem_global = np.zeros(self.n_elems, np.int32)
+        self.xidx = np.zeros(self.n_nodes, np.int32)
+        check(L.fm_problem_part_map(h, _p(self.node_global), _p(self.elem_global), _p(self.xidx)))
+
+
+class _DeviceArray:
+    """A device buffer of the library seen through __cuda_array_interface__
+    (torch.as_tensor wraps it without a copy)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 2, "strides": None}
+
+
 class Batch:
     """Device-resident batch of GpuProblems (all share solver and element type)."""
 
@@ -251,6 +307,24 @@ class Batch:
         ln = (C.c_int64 * 2)()
         check(lib().fm_batch_profile(self.h, int(n), ms, ln))
         return {"tile": ms[0], "iface": ms[1]}, ln[0]
+
+    def exchange_buffers(self):
+        """(send, recv, count) of a batch of partition parts: objects with
+        __cuda_array_interface__ over count doubles each."""
+        s, r, n = C.c_void_p(), C.c_void_p(), C.c_int64()
+        check(lib().fm_batch_exchange_buffers(self.h, C.byref(s), C.byref(r), C.byref(n)))
+        return _DeviceArray(s.value, n.value), _DeviceArray(r.value, n.value), n.value
+
+    def exchange_begin(self, stream=None) -> None:
+        check(lib().fm_batch_exchange_begin(self.h, stream))
+
+    def exchange_end(self, stream=None) -> None:
+        check(lib().fm_batch_exchange_end(self.h, stream))
+
+    def iterations_per_step(self) -> int:
+        n = C.c_int32()
+        check(lib().fm_batch_iterations_per_step(self.h, C.byref(n)))
+        return n.value
 
     def layout(self):
         a, b, c, d = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()

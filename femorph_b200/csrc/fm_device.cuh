@@ -48,7 +48,22 @@ struct DevBatch {
   double* q1p;                    // [prob][2][4] pre-BC pressures of nodes 0..3
   int32_t n_probs;
   unsigned int* done;             // block counter of the interface pass
+  // partition exchange (null / 0 in a batch without partition parts)
+  const int32_t* iface_xidx;      // exchange index of each interface entry (-1: none)
+  const int32_t* x_entries;       // the interface entries that have one
+  int32_t n_xentries;
+  int32_t x_n;                    // length of the partition's exchange list
+  int32_t x_slices;               // one slice per part in the batch
+  double* xsend;                  // [x_slices][x_n][4] partial sums of this batch's parts
+  const double* xrecv;            // the same, summed over all processes (xsend when all parts are here)
 };
+
+// Sum over the part slices of exchange entry xi (component c).
+__device__ __forceinline__ double exchange_sum(const DevBatch& B, int xi, int c) {
+  double a = 0.0;
+  for (int q = 0; q < B.x_slices; ++q) a += B.xrecv[((int64_t)q * B.x_n + xi) * 4 + c];
+  return a;
+}
 
 // ---- bulk asynchronous copies global -> shared (cp.async.bulk, sm_90+) ----
 // Plain (non-multicast) 1D bulk copies completing on a CTA-local mbarrier.

@@ -276,6 +276,37 @@ static inline uint64_t spread3(uint64_t v) {
   return v;
 }
 
+// Element indices sorted by the Morton code of the element centroid (21
+// bits per axis over the mesh's bounding cube), ties in element order.
+void morton_order(const fm_problem* p, std::vector<int64_t>& order) {
+  const int npe = p->etype;
+  const int64_t E = p->E, N = p->N;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t i = 0; i < N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], p->coords[i * 3 + k]);
+      hi[k] = std::max(hi[k], p->coords[i * 3 + k]);
+    }
+  double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+  if (!(span > 0)) span = 1.0;
+  std::vector<uint64_t> code(E);
+  parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
+    for (int64_t e = eb; e < ee; ++e) {
+      double c[3] = {0, 0, 0};
+      for (int a = 0; a < npe; ++a)
+        for (int k = 0; k < 3; ++k) c[k] += p->coords[(int64_t)p->conn[e * npe + a] * 3 + k];
+      uint64_t q[3];
+      for (int k = 0; k < 3; ++k) {
+        double t = (c[k] / npe - lo[k]) / span;
+        t = std::min(std::max(t, 0.0), 1.0);
+        q[k] = (uint64_t)(t * 2097151.0);
+      }
+      code[e] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+    }
+  });
+  sort_by_key(code, order);
+}
+
 // Builds the batch layout:
 //  1. elements of each problem sorted by the Morton code of their centroid;
 //  2. cut greedily into tiles of <= tile_elems elements and <= tile_nodes
@@ -289,6 +320,9 @@ static inline uint64_t spread3(uint64_t v) {
 //     which contributions reach every node;
 //  5. each (tile, interface node) pair gets a partial-sum slot; the slots of
 //     an interface node are listed in tile order.
+// Nodes of a partition part that are shared with other parts (p->xidx >= 0)
+// are interface nodes even when one tile touches them: their sums are
+// completed by the exchange between the parts.
 int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
   L = Layout();
   L.node_new.resize(n);
@@ -301,32 +335,8 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     L.node_begin.push_back(node_base);
     L.elem_begin.push_back(elem_base);
     // 1. Morton order
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int64_t i = 0; i < N; ++i)
-      for (int k = 0; k < 3; ++k) {
-        lo[k] = std::min(lo[k], p->coords[i * 3 + k]);
-        hi[k] = std::max(hi[k], p->coords[i * 3 + k]);
-      }
-    double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
-    if (!(span > 0)) span = 1.0;
-    std::vector<uint64_t> code(E);
-    parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
-      for (int64_t e = eb; e < ee; ++e) {
-        double c[3] = {0, 0, 0};
-        for (int a = 0; a < npe; ++a)
-          for (int k = 0; k < 3; ++k) c[k] += p->coords[(int64_t)p->conn[e * npe + a] * 3 + k];
-        uint64_t q[3];
-        for (int k = 0; k < 3; ++k) {
-          double t = (c[k] / npe - lo[k]) / span;
-          t = std::min(std::max(t, 0.0), 1.0);
-          q[k] = (uint64_t)(t * 2097151.0);
-        }
-        code[e] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
-      }
-    });
     std::vector<int64_t> order;
-    sort_by_key(code, order);
-    std::vector<uint64_t>().swap(code);
+    morton_order(p, order);
     // connectivity in sorted order: the sequential passes below then read
     // contiguous memory
     std::vector<int32_t> cs((size_t)E * npe);
@@ -369,7 +379,8 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
       tile_start.push_back(E);
     }
     const int ntile = (int)tile_start.size() - 1;
-    // 3. node tile counts and first tile
+    // 3. node tile counts and first tile (shared partition nodes count as
+    // touched by two tiles)
     std::vector<int32_t> ntiles(N, 0), first_tile(N, -1), last(N, -1);
     for (int t = 0; t < ntile; ++t)
       for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
@@ -380,6 +391,9 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
             if (ntiles[c[a]]++ == 0) first_tile[c[a]] = t;
           }
       }
+    if (!p->xidx.empty())
+      for (int64_t i = 0; i < N; ++i)
+        if (p->xidx[i] >= 0 && ntiles[i] == 1) ntiles[i] = 2;
     // node renumbering: interior nodes tile by tile, interface nodes after
     // them, each group in order of first touch along the sorted elements
     // (per-tile first-touch lists in parallel, then prefix offsets)
@@ -604,6 +618,13 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         L.iface_slot_beg.push_back((int32_t)(s0 + cnt[k]));
         L.iface_prob.push_back(pi);
       }
+      std::vector<int32_t> xi(NI, -1);
+      if (!p->xidx.empty())
+        for (int64_t i = 0; i < N; ++i) {
+          const int64_t j = nn[i] - node_base - iface_begin;
+          if (j >= 0) xi[j] = p->xidx[i];
+        }
+      L.iface_xidx.insert(L.iface_xidx.end(), xi.begin(), xi.end());
     }
     node_base += N;
     e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;

@@ -30,6 +30,8 @@ struct DevProb {
   int32_t ex_mask;     // SUPG: bit0 euler, bit1 B-bar, bit2..5 K1..K4
   int32_t glob_fixed;  // SUPG FM_FIX_* mask
   int32_t q1[4];       // VMS: batch ids of the problem's nodes 0..3 (-1 absent)
+  int32_t xslice;      // partition part: its slice of the exchange buffers (-1: not a part)
+  int32_t pad_x;
   int64_t node_begin, n_nodes, elem_begin, n_elems;
 };
 
@@ -83,6 +85,12 @@ struct fm_problem {
   // Prepared tile layout (fm_problem_prepare) and the tile sizes it was built for
   std::shared_ptr<fm::Layout> layout;
   int32_t layout_te = 0, layout_tn = 0;
+  // Partition part (fm_problem_partition): its index among n_parts, the
+  // global node / element of each local one, and per local node its index
+  // in the partition's exchange list (-1: the node is not shared)
+  int32_t part = -1, n_parts = 0;
+  int64_t x_total = 0;
+  std::vector<int32_t> node_global, elem_global, xidx;
   // Batch membership
   fm_batch* batch = nullptr;
   int32_t index = -1;
@@ -107,6 +115,7 @@ struct Layout {
   int32_t max_tile_elems = 0;
   std::vector<uint16_t> conn_local;   // n_elems x npe
   std::vector<int32_t> iface_node, iface_slot_beg, iface_slots, iface_prob;
+  std::vector<int32_t> iface_xidx;    // exchange index of each interface node (-1: none); partition parts only
   int64_t n_slots = 0;
   int32_t max_colors = 0;
   // per problem: batch node id of each problem node, problem element of each batch element
@@ -123,4 +132,5 @@ constexpr int ELEM_ALIGN = 32;
 #define FM_MAX_TILE_NODES 512
 
 int build_layout(fm_problem* const* probs, int n, int tile_elems, int tile_nodes, Layout& L);
+void morton_order(const fm_problem* p, std::vector<int64_t>& order);
 }  // namespace fm

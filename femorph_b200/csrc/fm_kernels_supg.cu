@@ -194,6 +194,58 @@ __global__ void supg_iface_kernel(DevBatch B) {
   finish_iteration(B);
 }
 
+// Partition parts: the interface pass in two halves around the exchange
+// (see vms_xpack_kernel / vms_xupdate_kernel).
+__global__ void supg_xpack_kernel(DevBatch B) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
+    const int pidx = B.iface_prob[i];
+    if (pidx < 0) continue;
+    const DevProbState st = B.pstate[pidx];
+    if (st.iter >= B.target[pidx]) continue;
+    const DevProb& P = B.probs[pidx];
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
+    for (int kk = k0; kk < k1; ++kk) {
+      const int s = B.iface_slots[kk];
+      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s];
+    }
+    const int xi = B.iface_xidx[i];
+    if (xi >= 0) {
+      double* d = B.xsend + ((int64_t)P.xslice * B.x_n + xi) * 4;
+      d[0] = acc[0]; d[1] = acc[1]; d[2] = acc[2]; d[3] = 0.0;
+      continue;
+    }
+    const int g = B.iface_node[i];
+    double old[3] = {B.su[g], B.sv[g], B.sw[g]};
+    mask_fixed(P.glob_fixed, old[0], old[1], old[2]);
+    int32_t status = FM_OK;
+    double max_u2 = 0.0;
+    supg_node_update(B, P, st.time, g, old, acc, &status, &max_u2);
+    check_exit(B, P, pidx, max_u2, status);
+  }
+}
+
+__global__ void supg_xupdate_kernel(DevBatch B) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < B.n_xentries; j += gridDim.x * blockDim.x) {
+    const int i = B.x_entries[j];
+    const int pidx = B.iface_prob[i];
+    if (pidx < 0) continue;
+    const DevProbState st = B.pstate[pidx];
+    if (st.iter >= B.target[pidx]) continue;
+    const DevProb& P = B.probs[pidx];
+    const int xi = B.iface_xidx[i];
+    const double acc[3] = {exchange_sum(B, xi, 0), exchange_sum(B, xi, 1), exchange_sum(B, xi, 2)};
+    const int g = B.iface_node[i];
+    double old[3] = {B.su[g], B.sv[g], B.sw[g]};
+    mask_fixed(P.glob_fixed, old[0], old[1], old[2]);
+    int32_t status = FM_OK;
+    double max_u2 = 0.0;
+    supg_node_update(B, P, st.time, g, old, acc, &status, &max_u2);
+    check_exit(B, P, pidx, max_u2, status);
+  }
+  finish_iteration(B);
+}
+
 // compute_pressure (src lines 446-501): p_e = -lambda_e * (int div u) / (int 1),
 // on the stored (pre-zeroing) state.  Output only.
 template <int NPE>
@@ -288,7 +340,7 @@ static void launch_supg_tile(const DevBatch& B, int tn_max, int threads, size_t 
 }
 
 cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
-                             cudaStream_t s, cudaEvent_t* ev) {
+                             bool xpack, cudaStream_t s, cudaEvent_t* ev) {
   const size_t smem = supg_smem_bytes(tn_max, npe);
   if (ev) cudaEventRecord(ev[0], s);
   if (npe == 4) {
@@ -299,8 +351,16 @@ cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int ifa
     else launch_supg_tile<8, false>(B, tn_max, threads, smem, s);
   }
   if (ev) cudaEventRecord(ev[1], s);
-  supg_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  if (xpack)
+    supg_xpack_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  else
+    supg_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[2], s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_supg_xupdate(const DevBatch& B, int blocks, cudaStream_t s) {
+  supg_xupdate_kernel<<<blocks, 256, 0, s>>>(B);
   return cudaGetLastError();
 }
 

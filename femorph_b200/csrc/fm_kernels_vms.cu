@@ -414,6 +414,59 @@ __global__ void vms_iface_kernel(DevBatch B) {
   finish_iteration(B);
 }
 
+// Partition parts, first half of the interface pass: interface nodes that
+// are not shared with other parts are updated as in vms_iface_kernel; the
+// shared ones put their sums into the part's slice of the exchange buffer.
+__global__ void vms_xpack_kernel(DevBatch B) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
+    const int pidx = B.iface_prob[i];
+    if (pidx < 0) continue;
+    const DevProbState st = B.pstate[pidx];
+    if (st.iter >= B.target[pidx]) continue;
+    const DevProb& P = B.probs[pidx];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
+    for (int k = k0; k < k1; ++k) {
+      const int s = B.iface_slots[k];
+      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s]; acc[3] += B.part3[s];
+    }
+    const int xi = B.iface_xidx[i];
+    if (xi >= 0) {
+      double* d = B.xsend + ((int64_t)P.xslice * B.x_n + xi) * 4;
+      d[0] = acc[0]; d[1] = acc[1]; d[2] = acc[2]; d[3] = acc[3];
+      continue;
+    }
+    const bool first_dual = (st.iter % (P.ndual + 1)) == 0;
+    const int g = B.iface_node[i];
+    const double post[4] = {B.su[g], B.sv[g], B.sw[g], B.sp[g]};
+    int32_t status = FM_OK;
+    vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
+    if (status != FM_OK) B.pstate[pidx].status = status;
+  }
+}
+
+// Second half: the shared nodes, from the sums over all parts; then the
+// iteration is complete.
+__global__ void vms_xupdate_kernel(DevBatch B) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < B.n_xentries; j += gridDim.x * blockDim.x) {
+    const int i = B.x_entries[j];
+    const int pidx = B.iface_prob[i];
+    if (pidx < 0) continue;
+    const DevProbState st = B.pstate[pidx];
+    if (st.iter >= B.target[pidx]) continue;
+    const DevProb& P = B.probs[pidx];
+    const int xi = B.iface_xidx[i];
+    const double acc[4] = {exchange_sum(B, xi, 0), exchange_sum(B, xi, 1), exchange_sum(B, xi, 2), exchange_sum(B, xi, 3)};
+    const bool first_dual = (st.iter % (P.ndual + 1)) == 0;
+    const int g = B.iface_node[i];
+    const double post[4] = {B.su[g], B.sv[g], B.sw[g], B.sp[g]};
+    int32_t status = FM_OK;
+    vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
+    if (status != FM_OK) B.pstate[pidx].status = status;
+  }
+  finish_iteration(B);
+}
+
 size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed) {
   const size_t tn_pad = (size_t)((tn_max + 1) & ~1);
   const size_t stage = threads == 256 ? (mixed ? vms_stage_bytes<256, true>() : vms_stage_bytes<256, false>())
@@ -421,8 +474,10 @@ size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed) {
   return tn_pad * 12 * sizeof(double) + stage + (size_t)inc_max * sizeof(uint16_t) + (tn_pad + 2) * sizeof(uint16_t);
 }
 
+// One dual iteration: tile kernel, then the interface pass (xpack: its first
+// half for a batch of partition parts; launch_vms_xupdate completes it).
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
-                                 cudaStream_t s, cudaEvent_t* ev) {
+                                 bool xpack, cudaStream_t s, cudaEvent_t* ev) {
   const size_t smem = vms_smem_bytes(tn_max, inc_max, threads, mixed);
   if (ev) cudaEventRecord(ev[0], s);
   if (mixed) {
@@ -437,8 +492,16 @@ cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int
       vms_tile_kernel<128, false><<<B.n_tiles, 128, smem, s>>>(B, tn_max, inc_max);
   }
   if (ev) cudaEventRecord(ev[1], s);
-  vms_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  if (xpack)
+    vms_xpack_kernel<<<iface_blocks, 256, 0, s>>>(B);
+  else
+    vms_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[2], s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vms_xupdate(const DevBatch& B, int blocks, cudaStream_t s) {
+  vms_xupdate_kernel<<<blocks, 256, 0, s>>>(B);
   return cudaGetLastError();
 }
 

@@ -29,11 +29,13 @@ const char* last_error();
 size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed);
 cudaError_t vms_configure(int tn_max, int inc_max);
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
-                                 cudaStream_t s, cudaEvent_t* ev);
+                                 bool xpack, cudaStream_t s, cudaEvent_t* ev);
+cudaError_t launch_vms_xupdate(const DevBatch& B, int blocks, cudaStream_t s);
 size_t supg_smem_bytes(int tn_max, int npe);
 cudaError_t supg_configure(size_t smem, int npe);
 cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
-                             cudaStream_t s, cudaEvent_t* ev);
+                             bool xpack, cudaStream_t s, cudaEvent_t* ev);
+cudaError_t launch_supg_xupdate(const DevBatch& B, int blocks, cudaStream_t s);
 cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
 cudaError_t launch_supg_stats(const DevBatch& B, int tile0, int ntiles, int tn_max, int npe, double* out,
                               cudaStream_t s);
@@ -185,6 +187,14 @@ struct fm_batch {
   int graph_iters = 0;
   double* d_scratch = nullptr;
   double* d_stats = nullptr;   // per-CTA partial results of the log reductions
+  // partition parts (fm_problem_partition): the batch holds x_slices parts
+  // of one partition; external when the others live in other processes,
+  // whose partial sums the caller adds between fm_batch_exchange_begin and
+  // fm_batch_exchange_end
+  bool exchange = false, x_external = false, x_open = false;
+  int32_t x_slices = 0, x_blocks = 1;
+  int64_t x_n = 0;
+  std::vector<int32_t> x_slice_of;  // by problem slot
 };
 
 #define CK(x)                                                                                     \
@@ -358,7 +368,23 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
   uint32_t* done;
   A((void**)&done, sizeof(uint32_t));
   A((void**)&b->d_stats, std::max<int64_t>(cap[P_TILE], 256) * 11 * sizeof(double));
+  int32_t* ixidx = nullptr;
+  const int64_t xcount = b->exchange ? (int64_t)b->x_slices * b->x_n * 4 : 0;
+  if (b->exchange) {
+    A((void**)&ixidx, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
+    A((void**)&D.xsend, std::max<int64_t>(xcount, 1) * sizeof(double));
+    if (b->x_external) A((void**)&D.xrecv, std::max<int64_t>(xcount, 1) * sizeof(double));
+  }
   if (r) return r;
+  if (b->exchange) {
+    D.iface_xidx = ixidx;
+    D.x_n = (int32_t)b->x_n;
+    D.x_slices = b->x_slices;
+    if (!b->x_external) D.xrecv = D.xsend;
+    CK(cudaMemset(ixidx, 0xff, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t)));
+    CK(cudaMemset(D.xsend, 0, std::max<int64_t>(xcount, 1) * sizeof(double)));
+    if (b->x_external) CK(cudaMemset(const_cast<double*>(D.xrecv), 0, std::max<int64_t>(xcount, 1) * sizeof(double)));
+  }
   D.x = x; D.y = y; D.z = z; D.su = su; D.sv = sv; D.sw = sw; D.sp = sp;
   D.pu = pu; D.pv = pv; D.pw = pw; D.pp = pp; D.mass = ms; D.node_bc = nbc;
   D.conn = conn; D.E = NE;
@@ -567,6 +593,7 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
     r = r ? r : put(const_cast<int32_t*>(D.iface_slot_cnt), pl.off[P_IFACE], isc.data(), ni, s);
     r = r ? r : put(const_cast<int32_t*>(D.iface_slots), pl.off[P_ISLOT], islots.data(), (int64_t)islots.size(), s);
     r = r ? r : put(const_cast<int32_t*>(D.iface_prob), pl.off[P_IFACE], iprob.data(), ni, s);
+    if (D.iface_xidx) r = r ? r : put(const_cast<int32_t*>(D.iface_xidx), pl.off[P_IFACE], L.iface_xidx.data(), ni, s);
   }
   // problem constants and progress
   {
@@ -592,6 +619,14 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
       if (pr.ex_opts[q]) d.ex_mask |= (1 << q);
     d.glob_fixed = pr.glob_fixed;
     for (int q = 0; q < 4; ++q) d.q1[q] = (q < p->N) ? (int32_t)(noff + nn[q]) : -1;
+    d.xslice = -1;
+    if (b->exchange && p->part >= 0) {
+      if ((int)b->x_slice_of.size() <= ps) b->x_slice_of.resize(ps + 1, -1);
+      int used = 0;
+      for (int32_t v : b->x_slice_of) used += (v >= 0);
+      b->x_slice_of[ps] = used;
+      d.xslice = used;
+    }
     d.node_begin = noff;
     d.n_nodes = p->N;
     d.elem_begin = eoff;
@@ -828,9 +863,29 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
   int solver, npe, prec;
   int r = check_same(probs, n, &solver, &npe, &prec);
   if (r) return r;
+  // partition parts: all of one partition (same part count and exchange
+  // list), each part once
+  int nparts = 0;
+  for (int i = 0; i < n; ++i) nparts += (probs[i]->part >= 0);
+  if (nparts > 0) {
+    if (nparts != n) return fail(FM_ERR_INVALID, "a batch of partition parts takes no other problems");
+    std::vector<char> seen(probs[0]->n_parts, 0);
+    for (int i = 0; i < n; ++i) {
+      if (probs[i]->n_parts != probs[0]->n_parts || probs[i]->x_total != probs[0]->x_total)
+        return fail(FM_ERR_INVALID, "partition parts of different partitions in one batch");
+      if (seen[probs[i]->part]++) return fail(FM_ERR_INVALID, "the same partition part twice in one batch");
+    }
+    if (probs[0]->x_total > INT32_MAX / 4) return fail(FM_ERR_INVALID, "partition exchange list too long");
+  }
   fm_batch* b = nullptr;
   r = new_batch(solver, npe, prec, tuning, device, &b);
   if (r) return r;
+  if (nparts > 0) {
+    b->exchange = true;
+    b->x_slices = n;
+    b->x_n = probs[0]->x_total;
+    b->x_external = n < probs[0]->n_parts;
+  }
   // exact pool sizes from the prepared layouts
   int64_t cap[P_COUNT] = {0};
   std::vector<std::shared_ptr<Layout>> preps(n);
@@ -847,6 +902,21 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
   }
   r = allocate(b, cap);
   for (int i = 0; i < n && !r; ++i) r = place(b, probs[i], preps[i]);
+  if (!r && b->exchange) {
+    // the interface entries of the shared nodes, for the second half of the pass
+    std::vector<int32_t> xe;
+    for (const Placement& pl : b->slots)
+      if (pl.p)
+        for (int64_t k = 0; k < pl.len[P_IFACE]; ++k)
+          if (pl.L->iface_xidx[k] >= 0) xe.push_back((int32_t)(pl.off[P_IFACE] + k));
+    int32_t* d = nullptr;
+    r = dalloc(b, (void**)&d, std::max<size_t>(xe.size(), 1) * sizeof(int32_t));
+    if (!r) r = put(d, 0, xe.data(), (int64_t)xe.size(), b->stream);
+    if (!r && cudaStreamSynchronize(b->stream) != cudaSuccess) r = fail(FM_ERR_CUDA, "exchange entry upload");
+    b->D.x_entries = d;
+    b->D.n_xentries = (int32_t)xe.size();
+    b->x_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)xe.size() + 255) / 256, 148 * 8));
+  }
   if (r) {
     for (int i = 0; i < n; ++i)
       if (probs[i]->batch == b) {
@@ -898,6 +968,8 @@ int fm_batch_capacity_bytes(const fm_capacity* cap, const fm_tuning* tuning, int
 int fm_batch_add(fm_batch* b, fm_problem* p) {
   if (!b || !p) return fail(FM_ERR_INVALID, "null argument");
   if (p->batch) return fail(FM_ERR_INVALID, "problem already belongs to a batch");
+  if (p->part >= 0 || b->exchange)
+    return fail(FM_ERR_INVALID, "partition parts are batched together by fm_batch_create, with no other problems");
   if (p->params.solver != b->solver || p->etype != b->npe || p->params.precision != b->precision)
     return fail(FM_ERR_INVALID, "problem does not match the batch's solver, element type and precision");
   if (b->solver == FM_SOLVER_SUPG && p->params.ex_opts[0] == 0 && !b->has_history)
@@ -912,6 +984,7 @@ int fm_batch_add(fm_batch* b, fm_problem* p) {
 
 int fm_batch_remove(fm_batch* b, fm_problem* p) {
   if (!b || !p || p->batch != b) return fail(FM_ERR_INVALID, "problem is not in this batch");
+  if (b->exchange) return fail(FM_ERR_INVALID, "partition parts stay in their batch until it is destroyed");
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
   const int ps = p->index;
@@ -949,11 +1022,26 @@ int fm_batch_destroy(fm_batch* b) {
 
 // One iteration (dual iteration for VMS, step for SUPG): tile kernel +
 // interface kernel.
-static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
+// A batch of partition parts runs the interface pass in two halves (shared
+// nodes packed, then updated from the sums over all parts); when every part
+// is in the batch the second half follows directly (ev[2] is then recorded
+// again after it).
+static cudaError_t launch_first(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
   if (b->solver == FM_SOLVER_VMS)
-    return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED, s,
-                                ev);
-  return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, b->precision == FM_MIXED, s, ev);
+    return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED,
+                                b->exchange, s, ev);
+  return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, b->precision == FM_MIXED, b->exchange,
+                          s, ev);
+}
+static cudaError_t launch_second(fm_batch* b, cudaStream_t s) {
+  return b->solver == FM_SOLVER_VMS ? launch_vms_xupdate(b->D, b->x_blocks, s) : launch_supg_xupdate(b->D, b->x_blocks, s);
+}
+static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
+  cudaError_t e = launch_first(b, s, ev);
+  if (e != cudaSuccess || !b->exchange) return e;
+  e = launch_second(b, s);
+  if (ev) cudaEventRecord(ev[2], s);
+  return e;
 }
 
 // Sets per-slot targets (iterations) and launches enough iterations.  With
@@ -961,9 +1049,17 @@ static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
 // device times are summed into prof[0] (tile kernel) and prof[1] (interface
 // kernel), in milliseconds.
 static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cudaStream_t s, double* prof = nullptr) {
+  if (b->x_external)
+    return fail(FM_ERR_INVALID,
+                "the batch holds partition parts whose other parts run elsewhere: advance it with "
+                "fm_batch_exchange_begin / fm_batch_exchange_end");
   const int n = (int)b->pools[P_PROB].hwm;
   int32_t maxit = 0;
   for (int i = 0; i < n; ++i) maxit = std::max(maxit, add_iters[i]);
+  if (b->exchange)
+    for (int i = 0; i < n; ++i)
+      if (b->slots[i].p && add_iters[i] != maxit)
+        return fail(FM_ERR_INVALID, "the parts of a partition advance together: give them the same step count");
   if (maxit == 0 || b->D.n_tiles == 0) return FM_OK;
   // new targets (the host tracks every slot's iteration count exactly)
   CK(cudaEventSynchronize(b->ev_tgt));  // staging buffer free again
@@ -1000,14 +1096,14 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
     }
     for (; it + b->graph_iters <= maxit; it += b->graph_iters) {
       CK(cudaGraphLaunch(b->graph, s));
-      launches += 2 * (int64_t)b->graph_iters;
+      launches += (b->exchange ? 3 : 2) * (int64_t)b->graph_iters;
     }
   }
   for (; it < maxit; ++it) {
     cudaEvent_t* ev = prof ? &evs[(size_t)it * 3] : nullptr;
     cudaError_t e = launch_one(b, s, ev);
     if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    launches += 2;
+    launches += b->exchange ? 3 : 2;
   }
   CK(cudaEventRecord(b->ev1, s));
   if (prof) {
@@ -1086,6 +1182,63 @@ int fm_batch_step(fm_batch* b, int32_t nsteps, void* stream) {
   if (!b) return fail(FM_ERR_INVALID, "null batch");
   std::vector<int32_t> v(b->pools[P_PROB].hwm + 1, nsteps);
   return fm_batch_step_ragged(b, v.data(), stream);
+}
+
+int fm_batch_exchange_buffers(fm_batch* b, double** send, double** recv, int64_t* count) {
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  if (!b->exchange) return fail(FM_ERR_INVALID, "the batch holds no partition parts");
+  if (send) *send = b->D.xsend;
+  if (recv) *recv = const_cast<double*>(b->D.xrecv);
+  if (count) *count = (int64_t)b->x_slices * b->x_n * 4;
+  return FM_OK;
+}
+
+int fm_batch_iterations_per_step(fm_batch* b, int32_t* per_step) {
+  if (!b || !per_step) return fail(FM_ERR_INVALID, "null argument");
+  *per_step = 1;
+  for (const Placement& pl : b->slots)
+    if (pl.p) {
+      if (b->solver == FM_SOLVER_VMS) *per_step = std::max(0, pl.p->params.tot_dual_steps) + 1;
+      break;
+    }
+  return FM_OK;
+}
+
+int fm_batch_exchange_begin(fm_batch* b, void* stream) {
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  if (!b->exchange) return fail(FM_ERR_INVALID, "the batch holds no partition parts");
+  if (b->x_open) return fail(FM_ERR_INVALID, "fm_batch_exchange_begin called twice without fm_batch_exchange_end");
+  CK(cudaSetDevice(b->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+  const int n = (int)b->pools[P_PROB].hwm;
+  // every part advances by one iteration
+  CK(cudaEventSynchronize(b->ev_tgt));
+  for (int i = 0; i < n; ++i) b->h_targets[i] = b->iters[i] + (b->slots[i].p ? 1 : 0);
+  CK(cudaMemcpyAsync(const_cast<int32_t*>(b->D.target), b->h_targets, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(b->ev_tgt, s));
+  cudaError_t e = launch_first(b, s, nullptr);
+  if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  b->x_open = true;
+  return FM_OK;
+}
+
+int fm_batch_exchange_end(fm_batch* b, void* stream) {
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  if (!b->x_open) return fail(FM_ERR_INVALID, "fm_batch_exchange_end called without fm_batch_exchange_begin");
+  CK(cudaSetDevice(b->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+  cudaError_t e = launch_second(b, s);
+  b->x_open = false;
+  if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  const int n = (int)b->pools[P_PROB].hwm;
+  for (int i = 0; i < n; ++i) {
+    fm_problem* p = b->slots[i].p;
+    if (!p) continue;
+    b->iters[i] += 1;
+    const int per = b->solver == FM_SOLVER_VMS ? std::max(0, p->params.tot_dual_steps) + 1 : 1;
+    if (b->iters[i] % per == 0) p->steps_done += 1;
+  }
+  return FM_OK;
 }
 
 int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* launches) {

@@ -223,6 +223,52 @@ FM_API int fm_batch_step_ragged(fm_batch* b, const int32_t* nsteps, void* stream
 FM_API int fm_batch_step_problems(fm_batch* b, fm_problem* const* problems, const int32_t* nsteps, int32_t count,
                                   void* stream);
 
+/* ---- one mesh split over several GPUs (partition parts) ----
+ * No reference counterpart: the reference solves one mesh in one process
+ * (femVMSExplicitFluidSolver::solve / femSUPGExplicitFluidSolver::solve loop
+ * over all elements, src/femVMSExplicitFluidSolver.cpp:1098-1208,
+ * src/femSUPGExplicitFluidSolver.cpp:1095-1514); these calls split exactly
+ * that loop.  A part owns some elements; nodes touched by several parts
+ * (and, for VMS, the problem's nodes 0..3, whose pressures every element
+ * reads) form the partition's exchange list.  Each dual iteration (VMS) or
+ * step (SUPG) has one exchange: the parts' partial sums at those nodes,
+ * 4 doubles a node, are added across parts, and every part updates its own
+ * copy from the same sum.  Masses and BCs are the whole mesh's. */
+
+/* Default split: n_parts bands of equal element count along the Morton
+ * order of the element centroids.  elem_part: n_elems entries, out. */
+FM_API int fm_partition_elements(const fm_problem* full, int32_t n_parts, int32_t* elem_part);
+/* The problem of one part (elem_part NULL: the default split).  Its nodes
+ * are the ones its elements touch (plus nodes 0..3 for VMS) in global
+ * order; fm_problem_get_state and the other per-problem calls work in that
+ * local numbering.  full stays valid and unchanged. */
+FM_API int fm_problem_partition(const fm_problem* full, const int32_t* elem_part, int32_t n_parts, int32_t part,
+                                fm_problem** out);
+/* part index, part count and exchange-list length (part -1: not a part). */
+FM_API int fm_problem_part_info(const fm_problem* p, int32_t* part, int32_t* n_parts, int64_t* x_total);
+/* Global node / element of each local one, and each local node's index in
+ * the exchange list (-1: not shared).  NULL arguments are skipped. */
+FM_API int fm_problem_part_map(const fm_problem* p, int32_t* node_global, int32_t* elem_global, int32_t* xidx);
+
+/* A batch created from partition parts (fm_batch_create, parts of one
+ * partition only) gives each part a slice of a packed exchange buffer:
+ * send and recv hold count = parts_in_batch x x_total x 4 doubles.  When
+ * the batch holds every part, fm_batch_step runs the exchange itself
+ * (recv == send).  Otherwise the other parts run in other processes (every
+ * process with the same number of parts in its batch) and each iteration
+ * is driven as
+ *   fm_batch_exchange_begin(b, stream);   tile kernel + partial sums -> send
+ *   <recv = sum over processes of send, enqueued on stream,
+ *    e.g. ncclAllReduce(send, recv, count, ncclDouble, ncclSum, comm, stream)>
+ *   fm_batch_exchange_end(b, stream);     shared nodes updated from recv
+ * with all three on one cudaStream_t (NULL means the batch's own stream,
+ * not the legacy default stream).  fm_batch_iterations_per_step gives the
+ * iterations of one time step (VMS: tot_dual_steps + 1, SUPG: 1). */
+FM_API int fm_batch_exchange_buffers(fm_batch* b, double** send, double** recv, int64_t* count);
+FM_API int fm_batch_exchange_begin(fm_batch* b, void* stream);
+FM_API int fm_batch_exchange_end(fm_batch* b, void* stream);
+FM_API int fm_batch_iterations_per_step(fm_batch* b, int32_t* per_step);
+
 /* Velocity extrema of a problem's current state, reduced on the device
  * (get_solution_extrema, femSUPGExplicitFluidSolver.cpp:604-655; SUPG
  * global fixed dofs masked): out[0..5] min/max of u, v, w, out[6] max |u|. */
