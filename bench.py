@@ -11,7 +11,9 @@ of femVMSExplicitFluidSolver over the whole mesh.  Inputs (5.3 M elements x
 96 B of subscales, ~0.5 GB) exceed the 126 MB L2, so no L2 flush is needed
 between steps.  With --gpus N each rank solves its own cavity (seed = rank):
 weak scaling, no data-path collective; value = element-steps/s summed over
-ranks with the time taken as the max over ranks.
+ranks with the time taken as the max over ranks.  --config partitioned
+splits ONE cavity over the N ranks instead (strong scaling, one all-reduce
+of the shared nodes' partial sums per dual iteration).
 
 Prints one JSON line (rank 0).
 """
@@ -340,6 +342,64 @@ def serve_line(args, res):
             "serving": res, "clocks": top["clocks"]}
 
 
+def run_partitioned(args, rank, world, local_rank, dist, prec_name):
+    """One 96^3 VMS cavity split into `world` parts (Morton bands), one part
+    per GPU; each dual iteration ends with one all-reduce of the shared
+    nodes' partial sums (femorph_b200.partition).  Strong scaling: the
+    whole mesh's element-steps per second, time = max over ranks of the
+    CUDA-event time of K steps on each part's stream."""
+    import torch
+    from femorph_b200 import api
+    from femorph_b200.partition import PartitionedSolve
+    a2 = argparse.Namespace(**vars(args))
+    a2.config = "cavity"
+    p = make_problem(a2, seed=0)
+    prec = api.FM_MIXED if prec_name == "mixed" else api.FM_FP64
+    ps = PartitionedSolve(p, prec, device=local_rank, tile_elems=args.tile_elems, tile_nodes=args.tile_nodes,
+                          threads=args.threads)
+    ps.step(args.warmup)
+    ps.sync()
+    if dist:
+        dist.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        t0.record(ps.stream)
+        ps.step(args.steps)
+        t1.record(ps.stream)
+        ps.sync()
+    ms = t0.elapsed_time(t1)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    res = dict(E=p.n_elems, N=p.n_nodes, part_elems=ps.part.n_elems, part_nodes=ps.part.n_nodes,
+               x_total=ps.part.x_total, count=ps.count, ms=ms, clocks=clk.summary(),
+               shared_local=int((ps.part.xidx >= 0).sum()))
+    ps.close()
+    return res
+
+
+def partitioned_line(args, world, runs):
+    head = "mixed" if "mixed" in runs else "fp64"
+    r = runs[head]
+    val = r["E"] * args.steps / (r["ms"] / 1e3)
+    line = {"metric": "VMS element-steps/s, one 96^3 Kuhn-tet cavity partitioned over the GPUs",
+            "value": val, "unit": "element-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": f"VMS tet4 lid-driven cavity {args.n}^3 cells x 6 Kuhn tets ({r['E']} tets, "
+                                   f"{r['N']} nodes), split into {world} Morton-band part(s), {head} form",
+                       "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"one mesh, {world} part(s), one part per GPU; one all-reduce of "
+                                      f"{r['count']} doubles (the shared nodes' partial sums) per dual iteration",
+                       "exchange_nodes": r["x_total"], "part_elements_rank0": r["part_elems"]},
+            "gpu_launches": 3 * args.steps, "clocks": r["clocks"]}
+    if "fp64" in runs and head != "fp64":
+        f = runs["fp64"]
+        line["fp64"] = {"value": f["E"] * args.steps / (f["ms"] / 1e3), "ms_per_step": f["ms"] / args.steps}
+    return line
+
+
 def host_cpu() -> dict:
     """Host CPU model and core count (the CPU baselines use one core)."""
     model = None
@@ -457,7 +517,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=0, help="mesh size (default 96 for cavity/supg, 64 for channel)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
-    ap.add_argument("--config", default="cavity", choices=["cavity", "supg", "channel", "batched", "serve"])
+    ap.add_argument("--config", default="cavity",
+                    choices=["cavity", "supg", "channel", "batched", "serve", "partitioned"])
     ap.add_argument("--rates", default="10,30,100,1000", help="serve: arrival rates, requests/s")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
     ap.add_argument("--budget-gb", type=float, default=16.0, help="serve: HBM budget of the pooled batch")
@@ -493,6 +554,15 @@ def main():
     if args.config == "serve":
         if rank == 0:
             print(json.dumps(serve_line(args, run_serve(args, local_rank))), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.config == "partitioned":
+        precs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+        runs = {pn: run_partitioned(args, rank, world, local_rank, dist, pn) for pn in precs}
+        if rank == 0:
+            print(json.dumps(partitioned_line(args, world, runs)), flush=True)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

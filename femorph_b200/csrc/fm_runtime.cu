@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -192,6 +193,7 @@ struct fm_batch {
   // whose partial sums the caller adds between fm_batch_exchange_begin and
   // fm_batch_exchange_end
   bool exchange = false, x_external = false, x_open = false;
+  bool x_free_targets = false;      // device targets left open by fm_batch_exchange_begin
   int32_t x_slices = 0, x_blocks = 1;
   int64_t x_n = 0;
   std::vector<int32_t> x_slice_of;  // by problem slot
@@ -1062,6 +1064,7 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
         return fail(FM_ERR_INVALID, "the parts of a partition advance together: give them the same step count");
   if (maxit == 0 || b->D.n_tiles == 0) return FM_OK;
   // new targets (the host tracks every slot's iteration count exactly)
+  b->x_free_targets = false;
   CK(cudaEventSynchronize(b->ev_tgt));  // staging buffer free again
   for (int i = 0; i < n; ++i) b->h_targets[i] = b->iters[i] + add_iters[i];
   CK(cudaMemcpyAsync(const_cast<int32_t*>(b->D.target), b->h_targets, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
@@ -1210,12 +1213,18 @@ int fm_batch_exchange_begin(fm_batch* b, void* stream) {
   if (b->x_open) return fail(FM_ERR_INVALID, "fm_batch_exchange_begin called twice without fm_batch_exchange_end");
   CK(cudaSetDevice(b->device));
   cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
-  const int n = (int)b->pools[P_PROB].hwm;
-  // every part advances by one iteration
-  CK(cudaEventSynchronize(b->ev_tgt));
-  for (int i = 0; i < n; ++i) b->h_targets[i] = b->iters[i] + (b->slots[i].p ? 1 : 0);
-  CK(cudaMemcpyAsync(const_cast<int32_t*>(b->D.target), b->h_targets, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-  CK(cudaEventRecord(b->ev_tgt, s));
+  // every part advances by one iteration per begin/end pair: the device
+  // targets are opened once (no per-iteration copy or host wait, so the
+  // host can run ahead of the GPU)
+  if (!b->x_free_targets) {
+    const int n = (int)b->pools[P_PROB].hwm;
+    CK(cudaEventSynchronize(b->ev_tgt));
+    for (int i = 0; i < n; ++i) b->h_targets[i] = b->slots[i].p ? INT32_MAX : 0;
+    CK(cudaMemcpyAsync(const_cast<int32_t*>(b->D.target), b->h_targets, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                       s));
+    CK(cudaEventRecord(b->ev_tgt, s));
+    b->x_free_targets = true;
+  }
   cudaError_t e = launch_first(b, s, nullptr);
   if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
   b->x_open = true;
