@@ -1,6 +1,7 @@
 // Host-side preparation: problem copies, boundary-condition resolution,
 // lumped masses and the tiled batch layout.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -96,21 +97,30 @@ int resolve_bcs(fm_problem* p) {
 // VMS: initial_assemble (femVMSExplicitFluidSolver.cpp:21-91):
 // nd_mass[n] += (detJ/6)/4 over elements in file order.
 static void vms_mass(fm_problem* p) {
-  p->mass.assign(p->N, 0.0);
+  // element shares in parallel, then added in element order
+  hvec<double> share(p->E);
   const double* X = p->coords.data();
+  parallel_blocks(p->E, [&](int64_t eb, int64_t ee, int) {
+    for (int64_t e = eb; e < ee; ++e) {
+      const int32_t* c = &p->conn[e * 4];
+      double x[4][3], j[3][3];
+      for (int i = 0; i < 4; ++i)
+        for (int k = 0; k < 3; ++k) x[i][k] = X[(int64_t)c[i] * 3 + k];
+      for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) j[i][k] = x[k + 1][i] - x[0][i];
+      double c00 = j[1][1] * j[2][2] - j[2][1] * j[1][2];
+      double c01 = j[2][0] * j[1][2] - j[1][0] * j[2][2];
+      double c02 = j[1][0] * j[2][1] - j[2][0] * j[1][1];
+      double det = j[0][0] * c00 + j[0][1] * c01 + j[0][2] * c02;
+      double V = det / 6.0;
+      share[e] = V / 4.0;
+    }
+  });
+  p->mass.assign(p->N, 0.0);
   for (int64_t e = 0; e < p->E; ++e) {
     const int32_t* c = &p->conn[e * 4];
-    double x[4][3], j[3][3];
-    for (int i = 0; i < 4; ++i)
-      for (int k = 0; k < 3; ++k) x[i][k] = X[(int64_t)c[i] * 3 + k];
-    for (int i = 0; i < 3; ++i)
-      for (int k = 0; k < 3; ++k) j[i][k] = x[k + 1][i] - x[0][i];
-    double c00 = j[1][1] * j[2][2] - j[2][1] * j[1][2];
-    double c01 = j[2][0] * j[1][2] - j[1][0] * j[2][2];
-    double c02 = j[1][0] * j[2][1] - j[2][0] * j[1][1];
-    double det = j[0][0] * c00 + j[0][1] * c01 + j[0][2] * c02;
-    double V = det / 6.0;
-    for (int i = 0; i < 4; ++i) p->mass[c[i]] += V / 4.0;
+    const double q = share[e];
+    for (int i = 0; i < 4; ++i) p->mass[c[i]] += q;
   }
 }
 
@@ -142,9 +152,11 @@ static void supg_mass(fm_problem* p) {
   static const double c1[8] = {-1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0, -1.0};
   static const double c2[8] = {-1.0, -1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0};
   static const double c3[8] = {-1.0, -1.0, -1.0, -1.0, 1.0, 1.0, 1.0, 1.0};
-  p->mass.assign(p->N, 0.0);
+  // element row sums in parallel, then added in element order
+  hvec<double> rows((size_t)p->E * npe);
   const double* X = p->coords.data();
-  for (int64_t e = 0; e < p->E; ++e) {
+  parallel_blocks(p->E, [&](int64_t eb, int64_t ee, int) {
+  for (int64_t e = eb; e < ee; ++e) {
     const int32_t* cn = &p->conn[e * npe];
     double xe[8][3];
     for (int a = 0; a < npe; ++a)
@@ -183,9 +195,13 @@ static void supg_mass(fm_problem* p) {
     for (int a = 0; a < npe; ++a) {
       double t = 0.0;
       for (int b = 0; b < npe; ++b) t += M[a][b];
-      p->mass[cn[a]] += t;
+      rows[(size_t)e * npe + a] = t;
     }
   }
+  }, 1024);
+  p->mass.assign(p->N, 0.0);
+  for (int64_t e = 0; e < p->E; ++e)
+    for (int a = 0; a < npe; ++a) p->mass[p->conn[e * npe + a]] += rows[(size_t)e * npe + a];
 }
 
 void compute_mass(fm_problem* p) {
@@ -197,27 +213,11 @@ void compute_mass(fm_problem* p) {
 
 // ---- tiled layout ----
 
-// Runs f(begin, end, worker) over [0, n) in contiguous blocks on up to
-// hardware_concurrency host threads (inline for small n).
-template <class F>
-static void parallel_blocks(int64_t n, F f) {
-  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
-  const int64_t nt = std::min<int64_t>(hw, std::max<int64_t>(1, n / 4096));
-  if (nt <= 1) {
-    f((int64_t)0, n, 0);
-    return;
-  }
-  std::vector<std::thread> th;
-  for (int64_t t = 0; t < nt; ++t)
-    th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt, (int)t); });
-  for (auto& x : th) x.join();
-}
-
 // Sorts element indices by (key, index) - the order a stable sort by key
 // gives.  Keys are below 2^63 (3 x 21-bit Morton interleave): the pairs are
 // distributed into 4096 buckets by their top 12 bits (per-worker histograms),
 // then the buckets are sorted in parallel.
-static void sort_by_key(const std::vector<uint64_t>& key, std::vector<int64_t>& order) {
+static void sort_by_key(const hvec<uint64_t>& key, hvec<int64_t>& order) {
   const int64_t E = (int64_t)key.size();
   constexpr int NB = 4096, SHIFT = 63 - 12;
   const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
@@ -246,7 +246,7 @@ static void sort_by_key(const std::vector<uint64_t>& key, std::vector<int64_t>& 
     }
     start[NB] = acc;
   }
-  std::vector<std::pair<uint64_t, int64_t>> kv(E);
+  hvec<std::pair<uint64_t, int64_t>> kv(E);
   run([&](int64_t w, int64_t b, int64_t e) {
     int64_t* h = &hist[(size_t)w * NB];
     for (int64_t i = b; i < e; ++i) kv[h[std::min<uint64_t>(key[i] >> SHIFT, NB - 1)]++] = {key[i], i};
@@ -266,6 +266,112 @@ static void sort_by_key(const std::vector<uint64_t>& key, std::vector<int64_t>& 
   });
 }
 
+// Set of node ids (open addressing, cleared in O(size)), for the distinct
+// nodes of one tile.
+struct NodeSet {
+  std::vector<int32_t> slot, used;
+  uint32_t mask = 0;
+  explicit NodeSet(int cap_nodes) {
+    uint32_t c = 64;
+    while (c < (uint32_t)cap_nodes * 4u) c <<= 1;
+    slot.assign(c, -1);
+    mask = c - 1;
+    used.reserve(cap_nodes + 16);
+  }
+  bool contains(int32_t v) const {
+    for (uint32_t h = ((uint32_t)v * 2654435761u) & mask;; h = (h + 1) & mask) {
+      if (slot[h] == v) return true;
+      if (slot[h] < 0) return false;
+    }
+  }
+  void insert(int32_t v) {
+    for (uint32_t h = ((uint32_t)v * 2654435761u) & mask;; h = (h + 1) & mask) {
+      if (slot[h] == v) return;
+      if (slot[h] < 0) {
+        slot[h] = v;
+        used.push_back((int32_t)h);
+        return;
+      }
+    }
+  }
+  void clear() {
+    for (int32_t h : used) slot[h] = -1;
+    used.clear();
+  }
+};
+
+// End of the greedy tile that starts at sorted position s: elements are
+// taken while the tile has at most TE of them and at most TN distinct nodes
+// (an element's repeated node counts once).  Depends on s only.
+static int64_t greedy_next(const int32_t* cs, int npe, int64_t E, int TE, int TN, int64_t s, NodeSet& set) {
+  int64_t n_el = 0, n_nodes = 0, oi = s;
+  for (; oi < E; ++oi) {
+    const int32_t* c = &cs[(size_t)oi * npe];
+    int fresh = 0;
+    for (int a = 0; a < npe; ++a) {
+      bool dup = false;
+      for (int b = 0; b < a; ++b) dup |= (c[b] == c[a]);
+      if (!dup && !set.contains(c[a])) ++fresh;
+    }
+    if (n_el > 0 && (n_el + 1 > TE || n_nodes + fresh > TN)) break;
+    for (int a = 0; a < npe; ++a) set.insert(c[a]);
+    n_nodes += fresh;
+    ++n_el;
+  }
+  set.clear();
+  return oi;
+}
+
+// Tile starts of the greedy cut over the whole sorted order, computed in
+// parallel: each worker follows the chain from a segment start (a multiple
+// of TE); the true chain is then joined segment by segment, following a
+// worker's chain from the first start the two share (the cut from a start
+// does not depend on how the start was reached) and recomputing only
+// between the true chain's entry into a segment and that meeting point.
+static void greedy_tiles(const int32_t* cs, int npe, int64_t E, int TE, int TN, std::vector<int64_t>& starts) {
+  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  int64_t P = std::min<int64_t>(hw, std::max<int64_t>(1, E / (64 * (int64_t)TE)));
+  std::vector<int64_t> b;
+  for (int64_t k = 0; k < P; ++k) {
+    const int64_t v = (E * k / P) / TE * TE;
+    if (b.empty() || v > b.back()) b.push_back(v);
+  }
+  P = (int64_t)b.size();
+  b.push_back(E);
+  std::vector<std::vector<int64_t>> chain(P);
+  std::vector<int64_t> exit_at(P);
+  {
+    std::vector<std::thread> th;
+    for (int64_t k = 0; k < P; ++k)
+      th.emplace_back([&, k] {
+        NodeSet set(TN);
+        int64_t cur = b[k];
+        while (cur < b[k + 1]) {
+          chain[k].push_back(cur);
+          cur = greedy_next(cs, npe, E, TE, TN, cur, set);
+        }
+        exit_at[k] = cur;
+      });
+    for (auto& x : th) x.join();
+  }
+  NodeSet set(TN);
+  starts.assign(chain[0].begin(), chain[0].end());
+  int64_t cur = exit_at[0];
+  for (int64_t k = 1; k < P; ++k) {
+    const std::vector<int64_t>& ck = chain[k];
+    while (cur < b[k + 1]) {
+      auto it = std::lower_bound(ck.begin(), ck.end(), cur);
+      if (it != ck.end() && *it == cur) {
+        starts.insert(starts.end(), it, ck.end());
+        cur = exit_at[k];
+        break;
+      }
+      starts.push_back(cur);
+      cur = greedy_next(cs, npe, E, TE, TN, cur, set);
+    }
+  }
+}
+
 static inline uint64_t spread3(uint64_t v) {
   v &= 0x1fffff;
   v = (v | v << 32) & 0x1f00000000ffffULL;
@@ -278,7 +384,7 @@ static inline uint64_t spread3(uint64_t v) {
 
 // Element indices sorted by the Morton code of the element centroid (21
 // bits per axis over the mesh's bounding cube), ties in element order.
-void morton_order(const fm_problem* p, std::vector<int64_t>& order) {
+void morton_order(const fm_problem* p, hvec<int64_t>& order) {
   const int npe = p->etype;
   const int64_t E = p->E, N = p->N;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -289,7 +395,7 @@ void morton_order(const fm_problem* p, std::vector<int64_t>& order) {
     }
   double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
   if (!(span > 0)) span = 1.0;
-  std::vector<uint64_t> code(E);
+  hvec<uint64_t> code(E);
   parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
     for (int64_t e = eb; e < ee; ++e) {
       double c[3] = {0, 0, 0};
@@ -335,62 +441,42 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     L.node_begin.push_back(node_base);
     L.elem_begin.push_back(elem_base);
     // 1. Morton order
-    std::vector<int64_t> order;
+    hvec<int64_t> order;
     morton_order(p, order);
     // connectivity in sorted order: the sequential passes below then read
     // contiguous memory
-    std::vector<int32_t> cs((size_t)E * npe);
+    hvec<int32_t> cs((size_t)E * npe);
     parallel_blocks(E, [&](int64_t b, int64_t e, int) {
       for (int64_t oi = b; oi < e; ++oi)
         for (int a = 0; a < npe; ++a) cs[(size_t)oi * npe + a] = p->conn[order[oi] * npe + a];
     });
     // 2. greedy tiles
     std::vector<int64_t> tile_start;
-    std::vector<int32_t> stamp(N, -1);
-    {
-      int64_t cur_nodes = 0, cur_elems = 0;
-      int32_t tid = 0;
-      tile_start.push_back(0);
-      for (int64_t oi = 0; oi < E; ++oi) {
-        const int32_t* c = &cs[(size_t)oi * npe];
-        int fresh = 0;
-        for (int a = 0; a < npe; ++a)
-          if (stamp[c[a]] != tid) {
-            bool dup = false;
-            for (int b = 0; b < a; ++b) dup |= (c[b] == c[a]);
-            if (!dup) ++fresh;
-          }
-        if (cur_elems > 0 && (cur_elems + 1 > TE || cur_nodes + fresh > TN)) {
-          ++tid;
-          tile_start.push_back(oi);
-          cur_nodes = 0;
-          cur_elems = 0;
-          fresh = 0;
-          for (int a = 0; a < npe; ++a) {
-            bool dup = false;
-            for (int b = 0; b < a; ++b) dup |= (c[b] == c[a]);
-            if (!dup) ++fresh;
-          }
-        }
-        for (int a = 0; a < npe; ++a) stamp[c[a]] = tid;
-        cur_nodes += fresh;
-        ++cur_elems;
-      }
-      tile_start.push_back(E);
-    }
+    greedy_tiles(cs.data(), npe, E, TE, TN, tile_start);
+    tile_start.push_back(E);
     const int ntile = (int)tile_start.size() - 1;
     // 3. node tile counts and first tile (shared partition nodes count as
-    // touched by two tiles)
-    std::vector<int32_t> ntiles(N, 0), first_tile(N, -1), last(N, -1);
-    for (int t = 0; t < ntile; ++t)
-      for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
-        const int32_t* c = &cs[(size_t)oi * npe];
-        for (int a = 0; a < npe; ++a)
-          if (last[c[a]] != t) {
-            last[c[a]] = t;
-            if (ntiles[c[a]]++ == 0) first_tile[c[a]] = t;
+    // touched by two tiles), tiles split over the host threads
+    std::vector<int32_t> ntiles(N, 0), first_tile(N, INT32_MAX);
+    parallel_blocks(ntile, [&](int64_t tb, int64_t te2, int) {
+      NodeSet set(TN);
+      for (int64_t t = tb; t < te2; ++t) {
+        for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
+          const int32_t* c = &cs[(size_t)oi * npe];
+          for (int a = 0; a < npe; ++a) set.insert(c[a]);
+        }
+        for (int32_t h : set.used) {
+          const int32_t v = set.slot[h];
+          __atomic_fetch_add(&ntiles[v], 1, __ATOMIC_RELAXED);
+          int32_t cur = __atomic_load_n(&first_tile[v], __ATOMIC_RELAXED);
+          while ((int32_t)t < cur &&
+                 !__atomic_compare_exchange_n(&first_tile[v], &cur, (int32_t)t, true, __ATOMIC_RELAXED,
+                                              __ATOMIC_RELAXED)) {
           }
+        }
+        set.clear();
       }
+    }, 64);
     if (!p->xidx.empty())
       for (int64_t i = 0; i < N; ++i)
         if (p->xidx[i] >= 0 && ntiles[i] == 1) ntiles[i] = 2;
@@ -540,10 +626,11 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     // and its incidence entries at a multiple of 8; offsets first, then the
     // blocks are copied in parallel
     std::vector<TileMeta> tms(ntile);
-    int64_t e_out = 0;
+    int64_t e_out = 0, inc_prev = 0;
     {
       int64_t tn_off = (int64_t)L.tile_nodes.size(), col_off = (int64_t)L.tile_cols.size();
       int64_t inc_off = (int64_t)L.tile_inc.size(), off_off = (int64_t)L.tile_off.size(), sb = slot_base;
+      inc_prev = inc_off;
       for (int t = 0; t < ntile; ++t) {
         const TileWork& W = tw[t];
         TileMeta& tm = tms[t];
@@ -570,16 +657,26 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         L.max_colors = std::max(L.max_colors, W.ncol);
         L.max_tile_elems = std::max<int32_t>(L.max_tile_elems, tm.n_elem);
       }
+      // final sizes at once (the last problem includes the trailing
+      // padding: chunk copies round their length up to 16 bytes, and the
+      // incidence lists are copied in 16-byte pieces); the new ranges are
+      // first written by the per-tile copies below
+      const bool last_prob = pi == n - 1;
       L.tile_nodes.resize(tn_off);
       L.tile_cols.resize(col_off);
-      L.tile_inc.resize(inc_off, 0);
+      L.tile_inc.resize(last_prob ? (inc_off + 7) / 8 * 8 + 8 : inc_off);
       L.tile_off.resize(off_off);
       slot_base = sb;
     }
     e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
-    std::vector<int32_t>& eo = L.elem_old[pi];
-    eo.assign(e_out, -1);
-    L.conn_local.resize((size_t)(elem_base + e_out) * npe, 0);
+    auto& eo = L.elem_old[pi];
+    eo.resize(e_out);
+    const int64_t conn_end = elem_base + e_out + (pi == n - 1 ? ELEM_ALIGN : 0);
+    L.conn_local.resize((size_t)conn_end * npe);
+    const int64_t inc_end = (int64_t)L.tile_inc.size();
+    if (ntile > 0)  // alignment gap after the previous problem's entries
+      std::fill(L.tile_inc.begin() + inc_prev, L.tile_inc.begin() + tms[0].inc_begin, 0);
+    // each tile fills its ranges and the padding up to the next tile
     parallel_blocks(ntile, [&](int64_t tb, int64_t te2, int) {
       for (int64_t t = tb; t < te2; ++t) {
         const TileWork& W = tw[t];
@@ -588,12 +685,23 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         for (int32_t v : W.inter) *tn++ = nn[v];
         for (int32_t v : W.ifc) *tn++ = nn[v];
         std::copy(W.colcnt.begin(), W.colcnt.end(), L.tile_cols.begin() + tm.col_begin);
-        std::copy(W.inc.begin(), W.inc.end(), L.tile_inc.begin() + tm.inc_begin);
         std::copy(W.off.begin(), W.off.end(), L.tile_off.begin() + tm.off_begin);
+        const int64_t inc_next = t + 1 < ntile ? tms[t + 1].inc_begin : inc_end;
+        std::copy(W.inc.begin(), W.inc.end(), L.tile_inc.begin() + tm.inc_begin);
+        std::fill(L.tile_inc.begin() + tm.inc_begin + (int64_t)W.inc.size(), L.tile_inc.begin() + inc_next, 0);
+        const int64_t el_next = t + 1 < ntile ? tms[t + 1].elem_begin : conn_end;
         std::copy(W.conn.begin(), W.conn.end(), L.conn_local.begin() + (size_t)tm.elem_begin * npe);
+        std::fill(L.conn_local.begin() + (size_t)(tm.elem_begin + tm.n_elem) * npe,
+                  L.conn_local.begin() + (size_t)el_next * npe, 0);
+        const int64_t eo_next = std::min<int64_t>(el_next, elem_base + e_out) - elem_base;
         std::copy(W.eo.begin(), W.eo.end(), eo.begin() + (tm.elem_begin - elem_base));
+        std::fill(eo.begin() + (tm.elem_begin - elem_base) + tm.n_elem, eo.begin() + eo_next, -1);
       }
     });
+    if (ntile == 0) {
+      std::fill(L.conn_local.begin() + (size_t)elem_base * npe, L.conn_local.end(), 0);
+      std::fill(eo.begin(), eo.end(), -1);
+    }
     L.tiles.insert(L.tiles.end(), tms.begin(), tms.end());
     // interface nodes: one partial-sum slot per (tile, node), listed per node
     // in tile order
@@ -632,11 +740,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     L.elem_count.push_back(e_out);
     elem_base += e_out;
   }
-  // trailing padding: chunk copies round their length up to 16 bytes, and the
-  // incidence lists are copied in 16-byte pieces
-  elem_base += ELEM_ALIGN;
-  L.tile_inc.resize((L.tile_inc.size() + 7) / 8 * 8 + 8, 0);
-  L.conn_local.resize((size_t)elem_base * (probs[0]->etype), 0);
+  elem_base += ELEM_ALIGN;  // trailing padding (sized with the last problem)
   L.iface_slot_beg.push_back((int32_t)L.iface_slots.size());
   L.n_nodes = node_base;
   L.n_elems = elem_base;

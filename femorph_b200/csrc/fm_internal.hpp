@@ -2,12 +2,59 @@
 #pragma once
 #include <cstdint>
 #include <memory>
+#include <new>
 #include <string>
+#include <thread>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/femorph_b200.h"
 
 namespace fm {
+
+// Allocator whose value-initialisation leaves trivial elements unset, so
+// large host arrays are first touched (and filled) by the host threads that
+// fill them instead of being zeroed by one thread first.
+template <class T>
+struct uninit_alloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = uninit_alloc<U>;
+  };
+  uninit_alloc() = default;
+  template <class U>
+  uninit_alloc(const uninit_alloc<U>&) {}
+  template <class U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new ((void*)p) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using hvec = std::vector<T, uninit_alloc<T>>;
+
+// Runs f(begin, end, worker) over [0, n) in contiguous blocks on up to 32
+// host threads, at least `grain` items a block (inline for small n).
+template <class F>
+inline void parallel_blocks(int64_t n, F f, int64_t grain = 4096) {
+  const int64_t hc = (int64_t)std::thread::hardware_concurrency();
+  const int64_t hw = hc < 1 ? 1 : (hc > 32 ? 32 : hc);
+  int64_t nt = n / (grain > 0 ? grain : 1);
+  nt = nt < 1 ? 1 : (nt > hw ? hw : nt);
+  if (nt <= 1) {
+    f((int64_t)0, n, 0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int64_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt, (int)t); });
+  for (auto& x : th) x.join();
+}
+
 
 // Resolved boundary condition of one node.  The reference applies, in this
 // order, setNodeVelocity (per NODEVEL node, table-interpolated components
@@ -69,8 +116,8 @@ struct Layout;
 struct fm_problem {
   int32_t etype = 4;
   int64_t N = 0, E = 0;
-  std::vector<double> coords;
-  std::vector<int32_t> conn;
+  fm::hvec<double> coords;
+  fm::hvec<int32_t> conn;
   fm_params params{};
   std::vector<int32_t> vel_node, vel_dir, dir_node, pres_node;
   std::vector<double> vel_vals, dir_vals, pres_vals;
@@ -107,20 +154,21 @@ void compute_mass(fm_problem* p);
 struct Layout {
   int64_t n_nodes = 0, n_elems = 0;
   std::vector<TileMeta> tiles;
-  std::vector<int32_t> tile_nodes, tile_cols;
+  hvec<int32_t> tile_nodes;
+  std::vector<int32_t> tile_cols;
   // Per tile, for every local node, the (element-in-tile * npe + corner)
   // entries of its incident elements in element order: the fixed order in
   // which the node-owner threads add element contributions.
-  std::vector<uint16_t> tile_inc, tile_off;
+  hvec<uint16_t> tile_inc, tile_off;
   int32_t max_tile_elems = 0;
-  std::vector<uint16_t> conn_local;   // n_elems x npe
+  hvec<uint16_t> conn_local;          // n_elems x npe
   std::vector<int32_t> iface_node, iface_slot_beg, iface_slots, iface_prob;
   std::vector<int32_t> iface_xidx;    // exchange index of each interface node (-1: none); partition parts only
   int64_t n_slots = 0;
   int32_t max_colors = 0;
   // per problem: batch node id of each problem node, problem element of each batch element
   std::vector<std::vector<int32_t>> node_new;   // [prob][old] -> batch id
-  std::vector<std::vector<int32_t>> elem_old;   // [prob][batch e - elem_begin] -> old element
+  std::vector<hvec<int32_t>> elem_old;   // [prob][batch e - elem_begin] -> old element
   std::vector<int64_t> node_begin, elem_begin;
   std::vector<int64_t> elem_count;   // per problem: padded element slots (elem_old has this size, -1 = padding)
 };
@@ -132,5 +180,5 @@ constexpr int ELEM_ALIGN = 32;
 #define FM_MAX_TILE_NODES 512
 
 int build_layout(fm_problem* const* probs, int n, int tile_elems, int tile_nodes, Layout& L);
-void morton_order(const fm_problem* p, std::vector<int64_t>& order);
+void morton_order(const fm_problem* p, hvec<int64_t>& order);
 }  // namespace fm

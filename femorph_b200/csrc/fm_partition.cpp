@@ -24,7 +24,7 @@
 using namespace fm;
 
 static int default_parts(const fm_problem* full, int32_t n_parts, std::vector<int32_t>& part) {
-  std::vector<int64_t> order;
+  hvec<int64_t> order;
   morton_order(full, order);
   const int64_t E = full->E;
   part.assign(E, 0);

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -544,7 +545,7 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
   }
   // element data: connectivity (mixed: FP64-inverse flags set by prepare()), zero history
   {
-    const std::vector<uint16_t>& conn = L.conn_local;
+    const auto& conn = L.conn_local;
     r = r ? r : put(const_cast<uint16_t*>(D.conn), eoff * npe, conn.data(), (int64_t)conn.size(), s);
     const int64_t ne = pl.len[P_ELEM];
     if (D.sdus32)
@@ -572,10 +573,16 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
       pl.tn_max = std::max(pl.tn_max, tm.n_node);
     }
     pl.inc_max = (L.max_tile_elems * npe + 7) / 8 * 8;
-    std::vector<int32_t> tnodes(L.tile_nodes);
-    for (int32_t& q : tnodes) q += (int32_t)noff;
     r = r ? r : put(const_cast<TileMeta*>(D.tiles), pl.off[P_TILE], tiles.data(), (int64_t)tiles.size(), s);
-    r = r ? r : put(const_cast<int32_t*>(D.tile_nodes), pl.off[P_TNODE], tnodes.data(), (int64_t)tnodes.size(), s);
+    if (noff == 0) {  // node ids need no relocation
+      r = r ? r : put(const_cast<int32_t*>(D.tile_nodes), pl.off[P_TNODE], L.tile_nodes.data(),
+                      (int64_t)L.tile_nodes.size(), s);
+    } else {
+      std::vector<int32_t> tnodes(L.tile_nodes.begin(), L.tile_nodes.end());
+      for (int32_t& q : tnodes) q += (int32_t)noff;
+      r = r ? r : put(const_cast<int32_t*>(D.tile_nodes), pl.off[P_TNODE], tnodes.data(), (int64_t)tnodes.size(), s);
+      CK(cudaStreamSynchronize(s));  // tnodes goes out of scope
+    }
     r = r ? r : put(const_cast<int32_t*>(D.tile_cols), pl.off[P_TCOL], L.tile_cols.data(), (int64_t)L.tile_cols.size(), s);
     r = r ? r : put(const_cast<uint16_t*>(D.tile_inc), pl.off[P_TINC], L.tile_inc.data(), (int64_t)L.tile_inc.size(), s);
     r = r ? r : put(const_cast<uint16_t*>(D.tile_off), pl.off[P_TOFF], L.tile_off.data(), (int64_t)L.tile_off.size(), s);
@@ -737,13 +744,26 @@ int fm_problem_create(const fm_mesh* m, const fm_bc* bc, const fm_params* prm, c
   p->etype = m->elem_type;
   p->N = m->n_nodes;
   p->E = m->n_elems;
-  p->coords.assign(m->coords, m->coords + m->n_nodes * 3);
-  p->conn.assign(m->conn, m->conn + m->n_elems * m->elem_type);
-  for (int32_t c : p->conn)
-    if (c < 0 || c >= p->N) {
-      delete p;
-      return fail(FM_ERR_INVALID, "connectivity out of range");
+  // copies and the connectivity check on the host threads
+  p->coords.resize(m->n_nodes * 3);
+  p->conn.resize(m->n_elems * m->elem_type);
+  parallel_blocks((int64_t)p->coords.size(), [&](int64_t b, int64_t e, int) {
+    std::copy(m->coords + b, m->coords + e, p->coords.begin() + b);
+  }, 1 << 16);
+  std::atomic<bool> bad{false};
+  parallel_blocks((int64_t)p->conn.size(), [&](int64_t b, int64_t e, int) {
+    bool any = false;
+    for (int64_t i = b; i < e; ++i) {
+      const int32_t c = m->conn[i];
+      p->conn[i] = c;
+      any |= (c < 0 || c >= p->N);
     }
+    if (any) bad = true;
+  }, 1 << 16);
+  if (bad) {
+    delete p;
+    return fail(FM_ERR_INVALID, "connectivity out of range");
+  }
   p->params = *prm;
   if (bc) {
     if (bc->n_vel_rows) {
@@ -1405,7 +1425,7 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
   const int64_t nb = pl.off[P_NODE], eb = pl.off[P_ELEM];
   const int64_t N = p->N, E = p->E;
   const std::vector<int32_t>& nn = pl.L->node_new[0];
-  const std::vector<int32_t>& eo = pl.L->elem_old[0];
+  const auto& eo = pl.L->elem_old[0];
   const int64_t EC = (int64_t)eo.size();
   std::vector<double> tmp(N);
   double* cols[4] = {b->D.su, b->D.sv, b->D.sw, b->D.sp};
