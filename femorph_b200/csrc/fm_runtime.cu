@@ -319,66 +319,77 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
   // start stays 16-byte aligned for FP32 and FP64 rows alike
   const int64_t NN = std::max<int64_t>(cap[P_NODE], 1);
   const int64_t NE = (std::max<int64_t>(cap[P_ELEM], 1) + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
-  int r = 0;
-  auto A = [&](void** p, size_t bytes) {
-    if (!r) r = dalloc(b, p, bytes);
-  };
+  // one device allocation carved into every array (256-byte aligned): the
+  // carving runs once to size the block and once to hand out the pointers
   double *x, *y, *z, *su, *sv, *sw, *sp, *pu, *pv, *pw, *pp, *ms;
-  for (double** q : {&x, &y, &z, &su, &sv, &sw, &sp, &pu, &pv, &pw, &pp, &ms}) A((void**)q, NN * sizeof(double));
   int32_t* nbc;
-  A((void**)&nbc, NN * sizeof(int32_t));
   uint16_t* conn;
-  A((void**)&conn, (size_t)NE * b->npe * sizeof(uint16_t));
-  if (b->solver == FM_SOLVER_VMS && b->precision == FM_MIXED) {
-    A((void**)&D.sdus32, (size_t)NE * 12 * sizeof(float));
-  } else if (b->solver == FM_SOLVER_VMS || b->has_history) {
-    A((void**)&D.sdus, (size_t)NE * (b->solver == FM_SOLVER_VMS ? 12 : 3 * b->npe) * sizeof(double));
-  }
-  if (b->solver == FM_SOLVER_SUPG) {
-    A((void**)&D.el_lam, NE * sizeof(double));
-    A((void**)&D.el_reg, NE * sizeof(double));
-    A((void**)&b->d_scratch, NE * sizeof(double));
-  }
   TileMeta* tiles;
-  A((void**)&tiles, std::max<int64_t>(cap[P_TILE], 1) * sizeof(TileMeta));
   int32_t *tnodes, *tcols;
-  A((void**)&tnodes, std::max<int64_t>(cap[P_TNODE], 1) * sizeof(int32_t));
-  A((void**)&tcols, std::max<int64_t>(cap[P_TCOL], 1) * sizeof(int32_t));
   uint16_t *tinc, *toff;
-  A((void**)&tinc, std::max<int64_t>(cap[P_TINC], 8) * sizeof(uint16_t));
-  A((void**)&toff, std::max<int64_t>(cap[P_TOFF], 1) * sizeof(uint16_t));
-  for (double** q : {&D.part0, &D.part1, &D.part2, &D.part3})
-    A((void**)q, std::max<int64_t>(cap[P_SLOT], 1) * sizeof(double));
   int32_t *inode, *isb, *isc, *iprob, *islots;
-  for (int32_t** q : {&inode, &isb, &isc, &iprob}) A((void**)q, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
-  A((void**)&islots, std::max<int64_t>(cap[P_ISLOT], 1) * sizeof(int32_t));
   BCRec* recs;
-  A((void**)&recs, std::max<int64_t>(cap[P_REC], 1) * sizeof(BCRec));
   int32_t *toffs, *tlens;
-  A((void**)&toffs, std::max<int64_t>(cap[P_TAB], 1) * sizeof(int32_t));
-  A((void**)&tlens, std::max<int64_t>(cap[P_TAB], 1) * sizeof(int32_t));
   double* rows;
-  A((void**)&rows, std::max<int64_t>(cap[P_ROW], 1) * 4 * sizeof(double));
   DevProb* dp;
   DevProbState* ds;
   int32_t* tg;
   double* q1;
-  const int64_t NP = std::max<int64_t>(cap[P_PROB], 1);
-  A((void**)&dp, NP * sizeof(DevProb));
-  A((void**)&ds, NP * sizeof(DevProbState));
-  A((void**)&tg, NP * sizeof(int32_t));
-  A((void**)&q1, NP * 8 * sizeof(double));
   uint32_t* done;
-  A((void**)&done, sizeof(uint32_t));
-  A((void**)&b->d_stats, std::max<int64_t>(cap[P_TILE], 256) * 11 * sizeof(double));
   int32_t* ixidx = nullptr;
+  const int64_t NP = std::max<int64_t>(cap[P_PROB], 1);
   const int64_t xcount = b->exchange ? (int64_t)b->x_slices * b->x_n * 4 : 0;
-  if (b->exchange) {
-    A((void**)&ixidx, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
-    A((void**)&D.xsend, std::max<int64_t>(xcount, 1) * sizeof(double));
-    if (b->x_external) A((void**)&D.xrecv, std::max<int64_t>(xcount, 1) * sizeof(double));
-  }
+  char* block = nullptr;
+  size_t total = 0;
+  auto A = [&](void** p, size_t bytes) {
+    const size_t off = (total + 255) & ~(size_t)255;
+    total = off + (bytes ? bytes : 16);
+    *p = block ? block + off : nullptr;
+  };
+  auto carve = [&]() {
+    total = 0;
+    for (double** q : {&x, &y, &z, &su, &sv, &sw, &sp, &pu, &pv, &pw, &pp, &ms}) A((void**)q, NN * sizeof(double));
+    A((void**)&nbc, NN * sizeof(int32_t));
+    A((void**)&conn, (size_t)NE * b->npe * sizeof(uint16_t));
+    if (b->solver == FM_SOLVER_VMS && b->precision == FM_MIXED) {
+      A((void**)&D.sdus32, (size_t)NE * 12 * sizeof(float));
+    } else if (b->solver == FM_SOLVER_VMS || b->has_history) {
+      A((void**)&D.sdus, (size_t)NE * (b->solver == FM_SOLVER_VMS ? 12 : 3 * b->npe) * sizeof(double));
+    }
+    if (b->solver == FM_SOLVER_SUPG) {
+      A((void**)&D.el_lam, NE * sizeof(double));
+      A((void**)&D.el_reg, NE * sizeof(double));
+      A((void**)&b->d_scratch, NE * sizeof(double));
+    }
+    A((void**)&tiles, std::max<int64_t>(cap[P_TILE], 1) * sizeof(TileMeta));
+    A((void**)&tnodes, std::max<int64_t>(cap[P_TNODE], 1) * sizeof(int32_t));
+    A((void**)&tcols, std::max<int64_t>(cap[P_TCOL], 1) * sizeof(int32_t));
+    A((void**)&tinc, std::max<int64_t>(cap[P_TINC], 8) * sizeof(uint16_t));
+    A((void**)&toff, std::max<int64_t>(cap[P_TOFF], 1) * sizeof(uint16_t));
+    for (double** q : {&D.part0, &D.part1, &D.part2, &D.part3})
+      A((void**)q, std::max<int64_t>(cap[P_SLOT], 1) * sizeof(double));
+    for (int32_t** q : {&inode, &isb, &isc, &iprob}) A((void**)q, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
+    A((void**)&islots, std::max<int64_t>(cap[P_ISLOT], 1) * sizeof(int32_t));
+    A((void**)&recs, std::max<int64_t>(cap[P_REC], 1) * sizeof(BCRec));
+    A((void**)&toffs, std::max<int64_t>(cap[P_TAB], 1) * sizeof(int32_t));
+    A((void**)&tlens, std::max<int64_t>(cap[P_TAB], 1) * sizeof(int32_t));
+    A((void**)&rows, std::max<int64_t>(cap[P_ROW], 1) * 4 * sizeof(double));
+    A((void**)&dp, NP * sizeof(DevProb));
+    A((void**)&ds, NP * sizeof(DevProbState));
+    A((void**)&tg, NP * sizeof(int32_t));
+    A((void**)&q1, NP * 8 * sizeof(double));
+    A((void**)&done, sizeof(uint32_t));
+    A((void**)&b->d_stats, std::max<int64_t>(cap[P_TILE], 256) * 11 * sizeof(double));
+    if (b->exchange) {
+      A((void**)&ixidx, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
+      A((void**)&D.xsend, std::max<int64_t>(xcount, 1) * sizeof(double));
+      if (b->x_external) A((void**)&D.xrecv, std::max<int64_t>(xcount, 1) * sizeof(double));
+    }
+  };
+  carve();
+  int r = dalloc(b, (void**)&block, total);
   if (r) return r;
+  carve();
   if (b->exchange) {
     D.iface_xidx = ixidx;
     D.x_n = (int32_t)b->x_n;
@@ -471,17 +482,22 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
   // node data: coordinates, initial state after the time-0 BCs, mass, BC records
   const std::vector<int32_t>& nn = L.node_new[0];
   const int64_t N = p->N;
-  std::vector<double> hx(N), hy(N), hz(N), hu(N), hv(N), hw(N), hp(N), hm(N);
-  std::vector<int32_t> hbc(N, -1);
-  std::vector<double> s0(N * 4, 0.0);
-  if (!p->init.empty()) s0 = p->init;
-  for (int64_t i = 0; i < N; ++i) {
-    const int64_t g = L.node_new[0][i];
+  hvec<double> hx(N), hy(N), hz(N), hu(N), hv(N), hw(N), hp(N), hm(N);
+  hvec<int32_t> hbc(N);
+  const bool has_init = !p->init.empty();
+  std::atomic<bool> table_miss{false};
+  // every node writes its own batch slot: in parallel on the host threads
+  parallel_blocks(N, [&](int64_t ib, int64_t ie, int) {
+  for (int64_t i = ib; i < ie; ++i) {
+    const int64_t g = nn[i];
     hx[g] = p->coords[i * 3 + 0];
     hy[g] = p->coords[i * 3 + 1];
     hz[g] = p->coords[i * 3 + 2];
-    double st[4] = {s0[i * 4 + 0], s0[i * 4 + 1], s0[i * 4 + 2], s0[i * 4 + 3]};
+    double st[4] = {0.0, 0.0, 0.0, 0.0};
+    if (has_init)
+      for (int c = 0; c < 4; ++c) st[c] = p->init[i * 4 + c];
     if (b->solver == FM_SOLVER_SUPG) st[3] = 0.0;
+    hbc[g] = -1;
     if (p->node_rec[i] >= 0) {
       const BCRec& rr = p->recs[p->node_rec[i]];
       hbc[g] = (int32_t)pl.off[P_REC] + p->node_rec[i];
@@ -499,8 +515,8 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
             if (!found) cnt++;
           }
           if (!found) {
-            for (int j = 0; j < P_COUNT; ++j) b->pools[j].release(pl.off[j], pl.len[j]);
-            return fail(FM_ERR_TABLE, "Could not find time in femUtils::interpTableData.");
+            table_miss = true;
+            continue;
           }
           const double t1 = tab[(cnt - 1) * 4 + 3], t2 = tab[cnt * 4 + 3];
           for (int c = 0; c < 3; ++c)
@@ -523,13 +539,25 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
     hp[g] = st[3];
     hm[g] = p->mass[i];
   }
+  }, 1 << 14);
+  if (table_miss) {
+    for (int j = 0; j < P_COUNT; ++j) b->pools[j].release(pl.off[j], pl.len[j]);
+    return fail(FM_ERR_TABLE, "Could not find time in femUtils::interpTableData.");
+  }
   r = r ? r : put(const_cast<double*>(D.x), noff, hx.data(), N, s);
   r = r ? r : put(const_cast<double*>(D.y), noff, hy.data(), N, s);
   r = r ? r : put(const_cast<double*>(D.z), noff, hz.data(), N, s);
-  for (double* a : {D.su, D.pu}) r = r ? r : put(a, noff, hu.data(), N, s);
-  for (double* a : {D.sv, D.pv}) r = r ? r : put(a, noff, hv.data(), N, s);
-  for (double* a : {D.sw, D.pw}) r = r ? r : put(a, noff, hw.data(), N, s);
-  for (double* a : {D.sp, D.pp}) r = r ? r : put(a, noff, hp.data(), N, s);
+  // post-BC state uploaded once, the pre-BC copies filled on the device
+  r = r ? r : put(D.su, noff, hu.data(), N, s);
+  r = r ? r : put(D.sv, noff, hv.data(), N, s);
+  r = r ? r : put(D.sw, noff, hw.data(), N, s);
+  r = r ? r : put(D.sp, noff, hp.data(), N, s);
+  if (!r)
+    for (int q = 0; q < 4; ++q) {
+      const double* src = q == 0 ? D.su : q == 1 ? D.sv : q == 2 ? D.sw : D.sp;
+      double* dst = q == 0 ? D.pu : q == 1 ? D.pv : q == 2 ? D.pw : D.pp;
+      CK(cudaMemcpyAsync(dst + noff, src + noff, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    }
   r = r ? r : put(const_cast<double*>(D.mass), noff, hm.data(), N, s);
   r = r ? r : put(const_cast<int32_t*>(D.node_bc), noff, hbc.data(), N, s);
   {

@@ -24,7 +24,9 @@ def alone(p, steps, precision):
 
 @pytest.mark.parametrize("precision", [api.FM_FP64, api.FM_MIXED])
 def test_results_same_alone_and_in_the_mix(precision):
-    reqs = serve.draw_requests(10, rate=400.0, seed=3, n_range=(3, 7), steps_range=(5, 40))
+    # arrivals close together (20,000 requests/s), so that several requests
+    # are resident at once however fast the host side admits and retires them
+    reqs = serve.draw_requests(10, rate=20000.0, seed=3, n_range=(3, 7), steps_range=(5, 40))
     srv = serve.Server(precision=precision, hbm_budget=64 << 20, max_problems=6, block=4, prepare_workers=3)
     stats = srv.run(reqs)
     srv.close()
