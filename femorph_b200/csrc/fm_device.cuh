@@ -34,7 +34,7 @@ struct DevBatch {
   const uint16_t* tile_inc;       // per tile: node -> (element*npe + corner) entries, element order
   const uint16_t* tile_off;       // per tile: n_node+1 offsets into tile_inc
   // interface
-  double *part0, *part1, *part2, *part3;
+  double2* part;                  // [slot][2]: (c0, c1) (c2, c3), one 32-byte sector a slot
   const int32_t* iface_node;
   const int32_t* iface_slot_beg;  // first partial-slot entry of each interface node
   const int32_t* iface_slot_cnt;  // number of entries

@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
       supg_node_update(B, P, st.time, g, old, acc, &status, &max_u2);
     } else {
       const int s = tm.slot_base + (l2 - tm.n_int);
-      B.part0[s] = acc[0]; B.part1[s] = acc[1]; B.part2[s] = acc[2];
+      B.part[2 * s] = make_double2(acc[0], acc[1]);
+      B.part[2 * s + 1] = make_double2(acc[2], 0.0);
     }
   }
   check_exit(B, P, pidx, max_u2, status);
@@ -182,7 +183,8 @@ __global__ void supg_iface_kernel(DevBatch B) {
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     for (int kk = k0; kk < k1; ++kk) {
       const int s = B.iface_slots[kk];
-      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s];
+      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
+      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x;
     }
     double old[3] = {B.su[g], B.sv[g], B.sw[g]};
     mask_fixed(P.glob_fixed, old[0], old[1], old[2]);
@@ -207,7 +209,8 @@ __global__ void supg_xpack_kernel(DevBatch B) {
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     for (int kk = k0; kk < k1; ++kk) {
       const int s = B.iface_slots[kk];
-      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s];
+      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
+      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x;
     }
     const int xi = B.iface_xidx[i];
     if (xi >= 0) {

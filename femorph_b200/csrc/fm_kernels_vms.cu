@@ -385,7 +385,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (M
       vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
     } else {
       const int s = tm.slot_base + (ln2 - tm.n_int);
-      B.part0[s] = acc[0]; B.part1[s] = acc[1]; B.part2[s] = acc[2]; B.part3[s] = acc[3];
+      B.part[2 * s] = make_double2(acc[0], acc[1]);
+      B.part[2 * s + 1] = make_double2(acc[2], acc[3]);
     }
   }
   if (status != FM_OK) B.pstate[pidx].status = status;
@@ -404,7 +405,8 @@ __global__ void vms_iface_kernel(DevBatch B) {
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     for (int k = k0; k < k1; ++k) {
       const int s = B.iface_slots[k];
-      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s]; acc[3] += B.part3[s];
+      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
+      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x; acc[3] += q1.y;
     }
     const double post[4] = {B.su[g], B.sv[g], B.sw[g], B.sp[g]};
     int32_t status = FM_OK;
@@ -428,7 +430,8 @@ __global__ void vms_xpack_kernel(DevBatch B) {
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     for (int k = k0; k < k1; ++k) {
       const int s = B.iface_slots[k];
-      acc[0] += B.part0[s]; acc[1] += B.part1[s]; acc[2] += B.part2[s]; acc[3] += B.part3[s];
+      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
+      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x; acc[3] += q1.y;
     }
     const int xi = B.iface_xidx[i];
     if (xi >= 0) {

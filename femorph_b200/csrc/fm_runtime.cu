@@ -366,8 +366,7 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
     A((void**)&tcols, std::max<int64_t>(cap[P_TCOL], 1) * sizeof(int32_t));
     A((void**)&tinc, std::max<int64_t>(cap[P_TINC], 8) * sizeof(uint16_t));
     A((void**)&toff, std::max<int64_t>(cap[P_TOFF], 1) * sizeof(uint16_t));
-    for (double** q : {&D.part0, &D.part1, &D.part2, &D.part3})
-      A((void**)q, std::max<int64_t>(cap[P_SLOT], 1) * sizeof(double));
+    A((void**)&D.part, std::max<int64_t>(cap[P_SLOT], 1) * 4 * sizeof(double));
     for (int32_t** q : {&inode, &isb, &isc, &iprob}) A((void**)q, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t));
     A((void**)&islots, std::max<int64_t>(cap[P_ISLOT], 1) * sizeof(int32_t));
     A((void**)&recs, std::max<int64_t>(cap[P_REC], 1) * sizeof(BCRec));

@@ -79,7 +79,7 @@ struct Carve {
 
 struct Offsets {
   size_t node[12], node_bc, recs, tab_off, tab_len, tab_rows, conn, sdus, tiles, tile_nodes, tile_cols, tile_inc,
-      tile_off, part[4], iface_node, iface_beg, iface_cnt, iface_prob, iface_slots, prob, pstate, target, q1p, done,
+      tile_off, part, iface_node, iface_beg, iface_cnt, iface_prob, iface_slots, prob, pstate, target, q1p, done,
       in_coords, in_init, in_rec, in_mass, in_node_new, out_u, out_p, total;
 };
 
@@ -100,7 +100,7 @@ Offsets plan(const fm_problem* p, const Layout& L) {
   o.tile_cols = c.take<int32_t>(L.tile_cols.size());
   o.tile_inc = c.take<uint16_t>(L.tile_inc.size());
   o.tile_off = c.take<uint16_t>(L.tile_off.size());
-  for (int k = 0; k < 4; ++k) o.part[k] = c.take<double>((size_t)L.n_slots);
+  o.part = c.take<double>((size_t)L.n_slots * 4);
   o.iface_node = c.take<int32_t>(NI);
   o.iface_beg = c.take<int32_t>(NI + 1);
   o.iface_cnt = c.take<int32_t>(NI);
@@ -235,10 +235,7 @@ extern "C" int fm_vms_solve_static(fm_problem* p, int32_t nsteps, int32_t device
   D.tile_cols = reinterpret_cast<int32_t*>(base + o.tile_cols);
   D.tile_inc = reinterpret_cast<uint16_t*>(base + o.tile_inc);
   D.tile_off = reinterpret_cast<uint16_t*>(base + o.tile_off);
-  D.part0 = reinterpret_cast<double*>(base + o.part[0]);
-  D.part1 = reinterpret_cast<double*>(base + o.part[1]);
-  D.part2 = reinterpret_cast<double*>(base + o.part[2]);
-  D.part3 = reinterpret_cast<double*>(base + o.part[3]);
+  D.part = reinterpret_cast<double2*>(base + o.part);
   D.iface_node = reinterpret_cast<int32_t*>(base + o.iface_node);
   D.iface_slot_beg = reinterpret_cast<int32_t*>(base + o.iface_beg);
   D.iface_slot_cnt = reinterpret_cast<int32_t*>(base + o.iface_cnt);
