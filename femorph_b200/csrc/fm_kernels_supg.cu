@@ -53,9 +53,20 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
 // 128-thread CTAs fit an SM (FP64 tet4: a small spill, 12% faster than two
 // CTAs at 241 registers); the FP64 hexa8 kernel keeps 255 (three CTAs spill
 // 1 KB a thread and run 30% slower).
+//
+// Accumulation of the element contributions into the tile's nodes, in the
+// order of the elements (colour-sorted) in both schemes, so both give the
+// same sums:
+//  - tet4 (GATHER): element threads write their 12 entries to shared memory,
+//    then each node's owner thread adds the entries of this chunk's elements
+//    from the node's incidence list (two barriers a chunk);
+//  - hexa8: one round per colour present in the chunk (elements of one
+//    colour share no node), a barrier after each; the 24 entries a hexa
+//    would stage cost more shared memory than the barriers cost time.
 template <int NPE, int THREADS, bool MIXED>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4) ? 3 : 1)
-    supg_tile_kernel(DevBatch B, int tn_max) {
+    supg_tile_kernel(DevBatch B, int tn_max, int inc_max) {
+  constexpr bool GATHER = NPE == 4;
   extern __shared__ double sm[];
   double* s_x = sm;
   double* s_y = s_x + tn_max;
@@ -66,7 +77,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
   double* s_a0 = s_w + tn_max;
   double* s_a1 = s_a0 + tn_max;
   double* s_a2 = s_a1 + tn_max;
-  int32_t* s_col = (int32_t*)(s_a2 + tn_max);
+  double* R = s_a2 + tn_max;                                        // GATHER: [NPE * 3][THREADS]
+  int32_t* s_col = (int32_t*)(R + (GATHER ? NPE * 3 * THREADS : 0));  // colour offsets (<= 129)
+  uint16_t* s_inc = (uint16_t*)(s_col + 130);                      // GATHER: incidence entries
+  uint16_t* s_off = s_inc + (GATHER ? inc_max : 0);                // GATHER: per-node offsets
+  uint16_t* s_cur = s_off + (GATHER ? tn_max + 1 : 0);             // GATHER: per-node cursors
   __shared__ ShapeTable<NPE, double> s_shape;
   __shared__ ShapeTable<NPE, float> s_shape_f;
 
@@ -88,6 +103,15 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
     s_a0[ln] = 0.0; s_a1[ln] = 0.0; s_a2[ln] = 0.0;
   }
   for (int c = tid; c <= tm.n_col; c += THREADS) s_col[c] = B.tile_cols[tm.col_begin + c];
+  if (GATHER) {
+    for (int i = tid; i <= tm.n_node; i += THREADS) {
+      const uint16_t o = B.tile_off[tm.off_begin + i];
+      s_off[i] = o;
+      if (i < tm.n_node) s_cur[i] = o;
+    }
+    const int ninc = tm.n_elem * NPE;
+    for (int i = tid; i < ninc; i += THREADS) s_inc[i] = B.tile_inc[tm.inc_begin + i];
+  }
   fill_shape_table<NPE, double>(&s_shape);
   if (MIXED) fill_shape_table<NPE, float>(&s_shape_f);
   __syncthreads();
@@ -140,17 +164,47 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
           }
       }
     }
-    while (c_lo < tm.n_col && s_col[c_lo + 1] <= base) ++c_lo;
-    for (int c = c_lo; c < tm.n_col && s_col[c] < base + THREADS; ++c) {
-      if (active && le >= s_col[c] && le < s_col[c + 1]) {
+    if constexpr (GATHER) {
+      if (active) {
 #pragma unroll
-        for (int a = 0; a < NPE; ++a) {
-          s_a0[ln[a]] += k[a][0];
-          s_a1[ln[a]] += k[a][1];
-          s_a2[ln[a]] += k[a][2];
-        }
+        for (int a = 0; a < NPE; ++a)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) R[(a * 3 + c) * THREADS + tid] = k[a][c];
       }
       __syncthreads();
+      // owners add this chunk's entries to their nodes, in element order
+      for (int n = tid; n < tm.n_node; n += THREADS) {
+        int c = s_cur[n];
+        const int ce = s_off[n + 1];
+        if (c >= ce) continue;
+        double a0 = s_a0[n], a1 = s_a1[n], a2 = s_a2[n];
+        while (c < ce) {
+          const int ent = s_inc[c];
+          const int col = ent / NPE - base;
+          if (col >= THREADS) break;
+          const double* Rp = R + (ent % NPE) * 3 * THREADS + col;
+          a0 += Rp[0];
+          a1 += Rp[THREADS];
+          a2 += Rp[2 * THREADS];
+          ++c;
+        }
+        s_cur[n] = (uint16_t)c;
+        s_a0[n] = a0; s_a1[n] = a1; s_a2[n] = a2;
+      }
+      __syncthreads();
+    } else {
+      while (c_lo < tm.n_col && s_col[c_lo + 1] <= base) ++c_lo;
+      for (int c = c_lo; c < tm.n_col && s_col[c] < base + THREADS; ++c) {
+        if (active && le >= s_col[c] && le < s_col[c + 1]) {
+#pragma unroll
+          for (int a = 0; a < NPE; ++a) {
+            s_a0[ln[a]] += k[a][0];
+            s_a1[ln[a]] += k[a][1];
+            s_a2[ln[a]] += k[a][2];
+          }
+        }
+        __syncthreads();
+      }
     }
   }
   __syncthreads();
@@ -291,9 +345,10 @@ __global__ void supg_pressure_kernel(DevBatch B, int tn_max, double* pres) {
   }
 }
 
-size_t supg_smem_bytes(int tn_max, int npe) {
-  (void)npe;
-  return (size_t)tn_max * 9 * sizeof(double) + 130 * sizeof(int32_t);
+size_t supg_smem_bytes(int tn_max, int inc_max, int npe, int threads) {
+  const bool gather = npe == 4;
+  return (size_t)tn_max * 9 * sizeof(double) + (gather ? (size_t)npe * 3 * threads * sizeof(double) : 0) +
+         130 * sizeof(int32_t) + (gather ? ((size_t)inc_max + 2 * (size_t)tn_max + 1) * sizeof(uint16_t) : 0);
 }
 
 // Sets kernel k's dynamic shared-memory limit to the device's opt-in
@@ -335,23 +390,23 @@ cudaError_t supg_configure(size_t smem, int npe) {
 }
 
 template <int NPE, bool MIXED>
-static void launch_supg_tile(const DevBatch& B, int tn_max, int threads, size_t smem, cudaStream_t s) {
+static void launch_supg_tile(const DevBatch& B, int tn_max, int inc_max, int threads, size_t smem, cudaStream_t s) {
   if (threads == 256)
-    supg_tile_kernel<NPE, 256, MIXED><<<B.n_tiles, 256, smem, s>>>(B, tn_max);
+    supg_tile_kernel<NPE, 256, MIXED><<<B.n_tiles, 256, smem, s>>>(B, tn_max, inc_max);
   else
-    supg_tile_kernel<NPE, 128, MIXED><<<B.n_tiles, 128, smem, s>>>(B, tn_max);
+    supg_tile_kernel<NPE, 128, MIXED><<<B.n_tiles, 128, smem, s>>>(B, tn_max, inc_max);
 }
 
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
-                             bool xpack, cudaStream_t s, cudaEvent_t* ev) {
-  const size_t smem = supg_smem_bytes(tn_max, npe);
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, int npe,
+                             bool mixed, bool xpack, cudaStream_t s, cudaEvent_t* ev) {
+  const size_t smem = supg_smem_bytes(tn_max, inc_max, npe, threads);
   if (ev) cudaEventRecord(ev[0], s);
   if (npe == 4) {
-    if (mixed) launch_supg_tile<4, true>(B, tn_max, threads, smem, s);
-    else launch_supg_tile<4, false>(B, tn_max, threads, smem, s);
+    if (mixed) launch_supg_tile<4, true>(B, tn_max, inc_max, threads, smem, s);
+    else launch_supg_tile<4, false>(B, tn_max, inc_max, threads, smem, s);
   } else {
-    if (mixed) launch_supg_tile<8, true>(B, tn_max, threads, smem, s);
-    else launch_supg_tile<8, false>(B, tn_max, threads, smem, s);
+    if (mixed) launch_supg_tile<8, true>(B, tn_max, inc_max, threads, smem, s);
+    else launch_supg_tile<8, false>(B, tn_max, inc_max, threads, smem, s);
   }
   if (ev) cudaEventRecord(ev[1], s);
   if (xpack)

@@ -33,9 +33,9 @@ cudaError_t vms_configure(int tn_max, int inc_max);
 cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
                                  bool xpack, cudaStream_t s, cudaEvent_t* ev);
 cudaError_t launch_vms_xupdate(const DevBatch& B, int blocks, cudaStream_t s);
-size_t supg_smem_bytes(int tn_max, int npe);
+size_t supg_smem_bytes(int tn_max, int inc_max, int npe, int threads);
 cudaError_t supg_configure(size_t smem, int npe);
-cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int threads, int iface_blocks, int npe, bool mixed,
+cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, int npe, bool mixed,
                              bool xpack, cudaStream_t s, cudaEvent_t* ev);
 cudaError_t launch_supg_xupdate(const DevBatch& B, int blocks, cudaStream_t s);
 cudaError_t launch_supg_pressure(const DevBatch& B, int tn_max, int npe, double* pres, cudaStream_t s);
@@ -427,7 +427,7 @@ static int configure(fm_batch* b) {
   if (b->tn_max <= b->configured_tn && b->inc_max <= b->configured_inc) return FM_OK;
   const int tn = std::max(b->tn_max, b->configured_tn), inc = std::max(b->inc_max, b->configured_inc);
   size_t smem = b->solver == FM_SOLVER_VMS ? vms_smem_bytes(tn, inc, b->threads, b->precision == FM_MIXED)
-                                           : supg_smem_bytes(tn, b->npe);
+                                           : supg_smem_bytes(tn, inc, b->npe, b->threads);
   // 227 KB opt-in limit per block, less room for the kernels' static shared memory
   if (smem + 1024 > 227 * 1024) return fail(FM_ERR_INVALID, "tile too large for shared memory; lower tile_nodes");
   cudaError_t ce = b->solver == FM_SOLVER_VMS ? vms_configure(tn, inc) : supg_configure(smem, b->npe);
@@ -1079,7 +1079,8 @@ static cudaError_t launch_first(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
   if (b->solver == FM_SOLVER_VMS)
     return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED,
                                 b->exchange, s, ev);
-  return launch_supg_step(b->D, b->tn_max, b->threads, b->iface_blocks, b->npe, b->precision == FM_MIXED, b->exchange,
+  return launch_supg_step(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->npe, b->precision == FM_MIXED,
+                          b->exchange,
                           s, ev);
 }
 static cudaError_t launch_second(fm_batch* b, cudaStream_t s) {
