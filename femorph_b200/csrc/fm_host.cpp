@@ -1,6 +1,7 @@
 // Host-side preparation: problem copies, boundary-condition resolution,
 // lumped masses and the tiled batch layout.
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -388,11 +389,23 @@ void morton_order(const fm_problem* p, hvec<int64_t>& order) {
   const int npe = p->etype;
   const int64_t E = p->E, N = p->N;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (int64_t i = 0; i < N; ++i)
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], p->coords[i * 3 + k]);
-      hi[k] = std::max(hi[k], p->coords[i * 3 + k]);
-    }
+  {
+    // bounding box: per-thread extremes combined (min / max are exact)
+    std::vector<std::array<double, 6>> part(64, {1e300, 1e300, 1e300, -1e300, -1e300, -1e300});
+    parallel_blocks(N, [&](int64_t ib, int64_t ie, int w) {
+      std::array<double, 6>& b = part[w];
+      for (int64_t i = ib; i < ie; ++i)
+        for (int k = 0; k < 3; ++k) {
+          b[k] = std::min(b[k], p->coords[i * 3 + k]);
+          b[3 + k] = std::max(b[3 + k], p->coords[i * 3 + k]);
+        }
+    }, 1 << 14);
+    for (const auto& b : part)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], b[k]);
+        hi[k] = std::max(hi[k], b[3 + k]);
+      }
+  }
   double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
   if (!(span > 0)) span = 1.0;
   hvec<uint64_t> code(E);
@@ -507,14 +520,24 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     }
     std::vector<int32_t>& nn = L.node_new[pi];
     nn.assign(N, -1);
-    int64_t next = 0;
-    for (int t = 0; t < ntile; ++t)
-      for (int32_t v : first_int[t]) nn[v] = (int32_t)(node_base + next++);
-    const int64_t iface_begin = next;
-    for (int t = 0; t < ntile; ++t)
-      for (int32_t v : first_ifc[t]) nn[v] = (int32_t)(node_base + next++);
+    // numbers in tile order from prefix offsets, written in parallel
+    std::vector<int64_t> int_at(ntile + 1, 0), ifc_at(ntile + 1, 0);
+    for (int t = 0; t < ntile; ++t) {
+      int_at[t + 1] = int_at[t] + (int64_t)first_int[t].size();
+      ifc_at[t + 1] = ifc_at[t] + (int64_t)first_ifc[t].size();
+    }
+    const int64_t iface_begin = int_at[ntile];
+    parallel_blocks(ntile, [&](int64_t tb, int64_t te2, int) {
+      for (int64_t t = tb; t < te2; ++t) {
+        int64_t k = node_base + int_at[t];
+        for (int32_t v : first_int[t]) nn[v] = (int32_t)k++;
+        k = node_base + iface_begin + ifc_at[t];
+        for (int32_t v : first_ifc[t]) nn[v] = (int32_t)k++;
+      }
+    }, 16);
     std::vector<std::vector<int32_t>>().swap(first_int);
     std::vector<std::vector<int32_t>>().swap(first_ifc);
+    int64_t next = iface_begin + ifc_at[ntile];
     for (int64_t i = 0; i < N; ++i)
       if (nn[i] < 0) nn[i] = (int32_t)(node_base + next++);  // isolated nodes
     // 4./5. tiles: local nodes, colouring, local connectivity, incidence
@@ -537,6 +560,8 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
       for (int64_t w = 0; w < nw; ++w)
         th.emplace_back([&, w] {
           std::vector<int32_t> local(N, -1);
+          std::vector<uint64_t> used;                 // per-worker scratch, reused tile by tile
+          std::vector<int32_t> col, idx, cnt, pos;
           for (int t = (int)(ntile * w / nw); t < (int)(ntile * (w + 1) / nw); ++t) {
             TileWork& W = tw[t];
             for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
@@ -556,8 +581,8 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
             const int32_t n_node = li;
             // colouring (greedy, up to 128 colours)
             const int64_t ne = tile_start[t + 1] - tile_start[t];
-            std::vector<uint64_t> used(2 * (size_t)n_node, 0);
-            std::vector<int32_t> col(ne);
+            used.assign(2 * (size_t)n_node, 0);
+            col.resize(ne);
             int ncol = 0;
             for (int64_t i = 0; i < ne; ++i) {
               const int32_t* c = &cs[(size_t)(tile_start[t] + i) * npe];
@@ -583,19 +608,21 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
             // the tile's nodes (one or two per node and chunk, which balances
             // the node-owner accumulation; the space-filling order measured
             // slower)
-            std::vector<int64_t> idx(ne);
-            std::iota(idx.begin(), idx.end(), 0);
-            std::stable_sort(idx.begin(), idx.end(), [&](int64_t x, int64_t y) { return col[x] < col[y]; });
+            // (counting sort by colour: stable, as the element order within a
+            // colour must stay the sorted order)
             W.ncol = ncol;
             W.colcnt.assign(ncol + 1, 0);
             for (int64_t i = 0; i < ne; ++i) W.colcnt[col[i] + 1]++;
             for (int k = 0; k < ncol; ++k) W.colcnt[k + 1] += W.colcnt[k];
+            idx.resize(ne);
+            pos.assign(W.colcnt.begin(), W.colcnt.end() - 1);
+            for (int64_t i = 0; i < ne; ++i) idx[pos[col[i]]++] = (int32_t)i;
             W.eo.resize(ne);
             W.conn.resize((size_t)ne * npe);
             for (int64_t i = 0; i < ne; ++i) {
-              const int64_t oe = order[tile_start[t] + idx[i]];
-              W.eo[i] = (int32_t)oe;
-              const int32_t* c = &p->conn[oe * npe];
+              const int64_t oi = tile_start[t] + idx[i];
+              W.eo[i] = (int32_t)order[oi];
+              const int32_t* c = &cs[(size_t)oi * npe];
               for (int a = 0; a < npe; ++a) W.conn[(size_t)i * npe + a] = (uint16_t)local[c[a]];
             }
             // node -> incident (element, corner) lists in element order
@@ -603,13 +630,13 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
               W.err = 2;
               continue;
             }
-            std::vector<int32_t> cnt(n_node + 1, 0);
+            cnt.assign(n_node + 1, 0);
             for (int64_t i = 0; i < ne * npe; ++i) cnt[W.conn[i] + 1]++;
             for (int k2 = 0; k2 < n_node; ++k2) cnt[k2 + 1] += cnt[k2];
             W.off.resize(n_node + 1);
             for (int k2 = 0; k2 <= n_node; ++k2) W.off[k2] = (uint16_t)cnt[k2];
             W.inc.resize((size_t)ne * npe);
-            std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
+            pos.assign(cnt.begin(), cnt.end() - 1);
             for (int64_t i = 0; i < ne; ++i)
               for (int a = 0; a < npe; ++a) W.inc[pos[W.conn[i * npe + a]]++] = (uint16_t)(i * npe + a);
           }
@@ -704,35 +731,76 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     }
     L.tiles.insert(L.tiles.end(), tms.begin(), tms.end());
     // interface nodes: one partial-sum slot per (tile, node), listed per node
-    // in tile order
+    // in tile order (per-worker counts over contiguous tile ranges give each
+    // worker its write positions, so the lists fill in parallel)
     {
       const int64_t NI = N - iface_begin;
+      const int64_t hw2 = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+      const int64_t nw = std::min<int64_t>(hw2, std::max<int64_t>(1, ntile / 64));
+      std::vector<std::vector<int32_t>> wc(nw);
+      auto node_of = [&](int32_t v) { return (int64_t)nn[v] - node_base - iface_begin; };
+      {
+        std::vector<std::thread> th;
+        for (int64_t w = 0; w < nw; ++w)
+          th.emplace_back([&, w] {
+            wc[w].assign(NI, 0);
+            for (int64_t t = ntile * w / nw; t < ntile * (w + 1) / nw; ++t)
+              for (int32_t v : tw[t].ifc) wc[w][node_of(v)]++;
+          });
+        for (auto& x : th) x.join();
+      }
       std::vector<int32_t> cnt(NI + 1, 0);
-      for (int t = 0; t < ntile; ++t)
-        for (int32_t v : tw[t].ifc) cnt[nn[v] - node_base - iface_begin + 1]++;
+      parallel_blocks(NI, [&](int64_t jb, int64_t je, int) {
+        for (int64_t j = jb; j < je; ++j) {
+          int32_t c = 0;
+          for (int64_t w = 0; w < nw; ++w) c += wc[w][j];
+          cnt[j + 1] = c;
+        }
+      }, 1 << 14);
       for (int64_t k = 0; k < NI; ++k) cnt[k + 1] += cnt[k];
+      // worker w's first position for node j: the node's start plus the
+      // counts of the workers before it
+      parallel_blocks(NI, [&](int64_t jb, int64_t je, int) {
+        for (int64_t j = jb; j < je; ++j) {
+          int32_t at = cnt[j];
+          for (int64_t w = 0; w < nw; ++w) {
+            const int32_t c = wc[w][j];
+            wc[w][j] = at;
+            at += c;
+          }
+        }
+      }, 1 << 14);
       const int64_t s0 = (int64_t)L.iface_slots.size();
       L.iface_slots.resize(s0 + cnt[NI]);
-      std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
-      for (int t = 0; t < ntile; ++t) {
-        int32_t k = 0;
-        for (int32_t v : tw[t].ifc) {
-          const int64_t j = nn[v] - node_base - iface_begin;
-          L.iface_slots[s0 + pos[j]++] = tms[t].slot_base + k++;
+      {
+        std::vector<std::thread> th;
+        for (int64_t w = 0; w < nw; ++w)
+          th.emplace_back([&, w] {
+            for (int64_t t = ntile * w / nw; t < ntile * (w + 1) / nw; ++t) {
+              int32_t k = 0;
+              for (int32_t v : tw[t].ifc) L.iface_slots[s0 + wc[w][node_of(v)]++] = tms[t].slot_base + k++;
+            }
+          });
+        for (auto& x : th) x.join();
+      }
+      const size_t i0 = L.iface_node.size();
+      L.iface_node.resize(i0 + NI);
+      L.iface_slot_beg.resize(i0 + NI);
+      L.iface_prob.resize(i0 + NI);
+      L.iface_xidx.resize(i0 + NI);
+      parallel_blocks(NI, [&](int64_t jb, int64_t je, int) {
+        for (int64_t k = jb; k < je; ++k) {
+          L.iface_node[i0 + k] = (int32_t)(node_base + iface_begin + k);
+          L.iface_slot_beg[i0 + k] = (int32_t)(s0 + cnt[k]);
+          L.iface_prob[i0 + k] = pi;
+          L.iface_xidx[i0 + k] = -1;
         }
-      }
-      for (int64_t k = 0; k < NI; ++k) {
-        L.iface_node.push_back((int32_t)(node_base + iface_begin + k));
-        L.iface_slot_beg.push_back((int32_t)(s0 + cnt[k]));
-        L.iface_prob.push_back(pi);
-      }
-      std::vector<int32_t> xi(NI, -1);
+      }, 1 << 14);
       if (!p->xidx.empty())
         for (int64_t i = 0; i < N; ++i) {
           const int64_t j = nn[i] - node_base - iface_begin;
-          if (j >= 0) xi[j] = p->xidx[i];
+          if (j >= 0) L.iface_xidx[i0 + j] = p->xidx[i];
         }
-      L.iface_xidx.insert(L.iface_xidx.end(), xi.begin(), xi.end());
     }
     node_base += N;
     e_out = (e_out + ELEM_ALIGN - 1) / ELEM_ALIGN * ELEM_ALIGN;
