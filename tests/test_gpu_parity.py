@@ -92,7 +92,7 @@ def test_vms_dual_iterations_and_ramp_table():
 
 
 def test_vms_config1_200_steps():
-    """16^3 Kuhn cavity (24,576 tets, 4,913 nodes), 200 steps."""
+    """The 16^3 Kuhn cavity (24,576 tets, 4,913 nodes), 200 steps."""
     p = mesh.cavity(16, seed=0, steps=200)
     last = None
     for s, eu, ep, es in run_pair(p, 200, check_every=20):
@@ -181,7 +181,7 @@ def test_supg_tet_cavity():
 
 def test_vms_mixed_precision_200_steps():
     """Mixed form (FP32 Gauss-point work and subscales, FP64 accumulation and
-    state) against the FP64 oracle after 200 steps of config 1: <= 1e-6."""
+    state) against the FP64 oracle after 200 steps of the 16^3 cavity: <= 1e-6."""
     p = mesh.cavity(16, seed=0, steps=200)
     g = api.GpuProblem(p, api.FM_MIXED)
     b = api.Batch([g])
