@@ -369,7 +369,10 @@ namespace fm {
 // = 0), so the Jacobian and the velocity gradient lose no digits to
 // cancellation.  Elements flagged `precise` (aspect ratio above
 // FM_MIXED_ASPECT_LIMIT) form the Jacobian and its inverse in FP64 from the
-// staged FP64 coordinates.
+// staged FP64 coordinates.  The Jacobian, the global derivatives, the
+// velocity and its gradient and the nodal terms run two components at a time
+// in paired FP32 arithmetic (sm_100 FFMA2 / FMUL2; 5% off the mixed tile
+// kernel for tet4 and hexa8).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float rcp_f(float x) {
   const float y = ptx_rcp_approx(x);
@@ -427,14 +430,18 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
     }
     float J[3][3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
+    for (int a = 0; a < 3; ++a) {
+      // (J[a][0], J[a][1]) as one pair, J[a][2] alone
+      float2 s01 = make_float2(0.0f, 0.0f);
+      float s2 = 0.0f;
 #pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        float s = 0.0f;
-#pragma unroll
-        for (int n = 1; n < NPE; ++n) s += dNv(g, n, a) * Xr[n][b];
-        J[a][b] = s;
+      for (int n = 1; n < NPE; ++n) {
+        const float d = dNv(g, n, a);
+        s01 = __ffma2_rn(make_float2(d, d), make_float2(Xr[n][0], Xr[n][1]), s01);
+        s2 += d * Xr[n][2];
       }
+      J[a][0] = s01.x; J[a][1] = s01.y; J[a][2] = s2;
+    }
     const float c00 = J[1][1] * J[2][2] - J[2][1] * J[1][2], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
                 c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
     const float det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
@@ -479,25 +486,47 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
     float inv[3][3];
     const float det = geometry(g, inv);
     float gd[NPE][3];
+    {
+      const float2 i0 = make_float2(inv[0][0], inv[1][0]), i1 = make_float2(inv[0][1], inv[1][1]),
+                   i2 = make_float2(inv[0][2], inv[1][2]);
 #pragma unroll
-    for (int a = 0; a < NPE; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b)
-        gd[a][b] = inv[b][0] * dNv(g, a, 0) + inv[b][1] * dNv(g, a, 1) + inv[b][2] * dNv(g, a, 2);
+      for (int a = 0; a < NPE; ++a) {
+        const float d0 = dNv(g, a, 0), d1 = dNv(g, a, 1), d2 = dNv(g, a, 2);
+        float2 q = __fmul2_rn(i0, make_float2(d0, d0));
+        q = __ffma2_rn(i1, make_float2(d1, d1), q);
+        q = __ffma2_rn(i2, make_float2(d2, d2), q);
+        gd[a][0] = q.x; gd[a][1] = q.y;
+        gd[a][2] = inv[2][0] * d0 + inv[2][1] * d1 + inv[2][2] * d2;
+      }
+    }
     float G[3][3];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
-    float u[3] = {U0[0], U0[1], U0[2]}, gr[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    float u[3], gr[3][3];
+    {
+      // (u0, u1) and (gr[c][0], gr[c][1]) as pairs
+      float2 u01 = make_float2(U0[0], U0[1]);
+      float u2 = U0[2];
+      float2 g01[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+      float g2[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int a = 1; a < NPE; ++a) {
-      const float Na = Nv(g, a);
+      for (int a = 1; a < NPE; ++a) {
+        const float Na = Nv(g, a);
+        u01 = __ffma2_rn(make_float2(Na, Na), make_float2(Ud[a][0], Ud[a][1]), u01);
+        u2 += Na * Ud[a][2];
+        const float2 ga = make_float2(gd[a][0], gd[a][1]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          g01[c] = __ffma2_rn(ga, make_float2(Ud[a][c], Ud[a][c]), g01[c]);
+          g2[c] += gd[a][2] * Ud[a][c];
+        }
+      }
+      u[0] = u01.x; u[1] = u01.y; u[2] = u2;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        u[c] += Na * Ud[a][c];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) gr[c][d] += gd[a][d] * Ud[a][c];
+        gr[c][0] = g01[c].x; gr[c][1] = g01[c].y; gr[c][2] = g2[c];
       }
     }
     const float div = gr[0][0] + gr[1][1] + gr[2][2];
@@ -563,23 +592,28 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
     const float sig[6] = {l2m * eps[0] + lam * eps[1] + lam * eps[2], lam * eps[0] + l2m * eps[1] + lam * eps[2],
                           lam * eps[0] + lam * eps[1] + l2m * eps[2], mu * eps[3], mu * eps[4], mu * eps[5]};
     const float c1w = rho * w, c3w = rho * tau * w, c4w = rho * nuC * div * w;
+    const float2 conv01 = make_float2(conv[0], conv[1]);
 #pragma unroll
     for (int a = 0; a < NPE; ++a) {
       const float Aa = u[0] * gd[a][0] + u[1] * gd[a][1] + u[2] * gd[a][2];
-      float f[3] = {0.0f, 0.0f, 0.0f};
+      // (f0, f1) as a pair, f2 alone
+      float2 f01 = make_float2(0.0f, 0.0f);
+      float f2v = 0.0f;
       if (iK1) {
-        const float Na = Nv(g, a);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] += c1w * Na * conv[c];
+        const float t = c1w * Nv(g, a);
+        f01 = __ffma2_rn(make_float2(t, t), conv01, f01);
+        f2v += t * conv[2];
       }
       if (iK3) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] += c3w * Aa * conv[c];
+        const float t = c3w * Aa;
+        f01 = __ffma2_rn(make_float2(t, t), conv01, f01);
+        f2v += t * conv[2];
       }
       if (iK4) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) f[c] += c4w * gd[a][c];
+        f01 = __ffma2_rn(make_float2(c4w, c4w), make_float2(gd[a][0], gd[a][1]), f01);
+        f2v += c4w * gd[a][2];
       }
+      float f[3] = {f01.x, f01.y, f2v};
       if (iK2) {
         float r0, r1, r2;
         if (NPE == 8 && bbar) {
@@ -594,8 +628,11 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
           r1 = gd[a][1] * sig[1];
           r2 = gd[a][2] * sig[2];
         }
-        f[0] += (r0 + gd[a][1] * sig[3] + gd[a][2] * sig[5]) * w;
-        f[1] += (r1 + gd[a][0] * sig[3] + gd[a][2] * sig[4]) * w;
+        // (f0, f1) as a pair
+        float2 t01 = __ffma2_rn(make_float2(gd[a][1], gd[a][0]), make_float2(sig[3], sig[3]), make_float2(r0, r1));
+        t01 = __ffma2_rn(make_float2(gd[a][2], gd[a][2]), make_float2(sig[5], sig[4]), t01);
+        const float2 n01 = __ffma2_rn(t01, make_float2(w, w), make_float2(f[0], f[1]));
+        f[0] = n01.x; f[1] = n01.y;
         f[2] += (r2 + gd[a][1] * sig[4] + gd[a][0] * sig[5]) * w;
       }
 #pragma unroll
