@@ -127,7 +127,7 @@ def algorithmic_bytes(E: int, N: int, precision: str, config: str = "cavity") ->
 # FP64 operations of one SUPG element-step (matrix-free K u over the Gauss
 # points, counting an FMA as two), from the ncu FP64 instruction counts of
 # the tile kernels (profiles/supg_tile_kernel_*.md).
-SUPG_FLOPS = {"channel": 9500, "supg": 1668}
+SUPG_FLOPS = {"channel": 9187, "supg": 1668}
 
 CONFIG_DEFAULT_N = {"cavity": 96, "supg": 96, "channel": 64}
 
