@@ -32,7 +32,7 @@ SYMBOLS = [
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
     "fm_vms_solve_static", "fm_batch_capacity_bytes", "fm_problem_velocity_extrema", "fm_problem_supg_log_stats",
     "fm_partition_elements", "fm_problem_partition", "fm_problem_part_info", "fm_problem_part_map",
-    "fm_batch_exchange_buffers", "fm_batch_exchange_begin", "fm_batch_exchange_end", "fm_batch_iterations_per_step",
+    "fm_problem_write_vtu", "fm_batch_exchange_buffers", "fm_batch_exchange_begin", "fm_batch_exchange_end", "fm_batch_iterations_per_step",
 ]
 
 
@@ -97,6 +97,7 @@ def lib():
         L.fm_problem_get_state.argtypes = [P, P, P, P, P]
         L.fm_problem_write_vtk.argtypes = [P, C.c_char_p]
         L.fm_problem_write_vtk_binary.argtypes = [P, C.c_char_p]
+        L.fm_problem_write_vtu.argtypes = [P, C.c_char_p]
         L.fm_problem_get_mass.argtypes = [P, P]
         L.fm_batch_last_timing.argtypes = [P, P, P]
         L.fm_batch_estimate_bytes.argtypes = [P, C.c_int32, P, P]
@@ -207,6 +208,10 @@ class GpuProblem:
     def write_vtk(self, path: str, binary: bool = False) -> None:
         f = lib().fm_problem_write_vtk_binary if binary else lib().fm_problem_write_vtk
         check(f(self.h, path.encode()))
+
+    def write_vtu(self, path: str) -> None:
+        """VTK XML UnstructuredGrid with raw appended binary arrays."""
+        check(lib().fm_problem_write_vtu(self.h, path.encode()))
 
     def prepare(self, tile_elems=0, tile_nodes=0, threads=0) -> None:
         """Builds the tile layout now (host only, thread-safe per problem)."""

@@ -486,3 +486,99 @@ extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
   fclose(f);
   return ok ? FM_OK : fail(FM_ERR_IO, std::string("cannot write ") + path);
 }
+
+// VTK XML UnstructuredGrid (.vtu) with the arrays raw-appended
+// (little-endian, UInt64 block sizes): the sections of the legacy writers,
+// FP64 points and data, int32 connectivity, read by ParaView and VTK without
+// any text parsing.  No counterpart in the reference (ASCII legacy VTK only).
+extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
+  static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the VTU writer emits little-endian data");
+  if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
+  if (!p->batch) return fail(FM_ERR_INVALID, "problem is not in a batch");
+  const int64_t N = p->N, E = p->E;
+  const int npe = p->etype;
+  const bool vms = p->params.solver == FM_SOLVER_VMS;
+  std::vector<double> u(N * 3), pres(vms ? N : E), e3(vms ? E * 3 : E * 2);
+  int r = fm_problem_get_state(p, u.data(), pres.data(), e3.data(), nullptr);
+  if (r) return r;
+  std::vector<double> zero((size_t)std::max(N, E) * 3, 0.0), dirbc(N, 0.0), lam, reg;
+  for (int32_t n : p->vel_node) dirbc[n] = 2.0;
+  for (int32_t n : p->pres_node) dirbc[n] = 3.0;
+  for (int32_t n : p->dir_node) dirbc[n] = 1.0;
+  if (!vms) {
+    lam.resize(E);
+    reg.resize(E);
+    for (int64_t e = 0; e < E; ++e) {
+      lam[e] = e3[e * 2];
+      reg[e] = e3[e * 2 + 1];
+    }
+  }
+  std::vector<int32_t> offs(E);
+  for (int64_t e = 0; e < E; ++e) offs[e] = (int32_t)((e + 1) * npe);
+  std::vector<uint8_t> types(E, npe == 4 ? 10 : 12);
+  struct Block {
+    std::string xml;  // DataArray attributes, without the offset
+    const void* data;
+    uint64_t bytes;
+  };
+  auto arr = [](const char* type, const char* name, int comps, const void* d, uint64_t bytes) {
+    std::string a = std::string("type=\"") + type + "\"";
+    if (name) a += std::string(" Name=\"") + name + "\"";
+    if (comps > 1) a += " NumberOfComponents=\"" + std::to_string(comps) + "\"";
+    return Block{a, d, bytes};
+  };
+  std::vector<Block> pd, cd, pts, cells;
+  const uint64_t n8 = (uint64_t)N * 8, e8 = (uint64_t)E * 8;
+  pd.push_back(arr("Float64", "DXYZ", 3, zero.data(), n8 * 3));
+  pd.push_back(arr("Float64", "velocity", 3, u.data(), n8 * 3));
+  if (vms) pd.push_back(arr("Float64", "pressure", 1, pres.data(), n8));
+  pd.push_back(arr("Float64", "dirBC", 1, dirbc.data(), n8));
+  pd.push_back(arr("Float64", "neuBC", 1, zero.data(), n8));
+  cd.push_back(arr("Float64", "normal", 3, zero.data(), e8 * 3));
+  cd.push_back(arr("Float64", "source", 1, zero.data(), e8));
+  if (vms) {
+    cd.push_back(arr("Float64", "res_v", 3, zero.data(), e8 * 3));
+    cd.push_back(arr("Float64", "res_p", 1, zero.data(), e8));
+    cd.push_back(arr("Float64", "subgrid_u", 3, e3.data(), e8 * 3));
+    cd.push_back(arr("Float64", "subgrid_p", 1, zero.data(), e8));
+  } else {
+    cd.push_back(arr("Float64", "pressure", 1, pres.data(), e8));
+    cd.push_back(arr("Float64", "lambda", 1, lam.data(), e8));
+    cd.push_back(arr("Float64", "regime", 1, reg.data(), e8));
+  }
+  pts.push_back(arr("Float64", nullptr, 3, p->coords.data(), n8 * 3));
+  cells.push_back(arr("Int32", "connectivity", 1, p->conn.data(), (uint64_t)E * npe * 4));
+  cells.push_back(arr("Int32", "offsets", 1, offs.data(), (uint64_t)E * 4));
+  cells.push_back(arr("UInt8", "types", 1, types.data(), (uint64_t)E));
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  uint64_t off = 0;
+  std::vector<const Block*> order;
+  auto section = [&](const char* tag, std::vector<Block>& bs) {
+    fprintf(f, "      <%s>\n", tag);
+    for (const Block& b : bs) {
+      fprintf(f, "        <DataArray %s format=\"appended\" offset=\"%llu\"/>\n", b.xml.c_str(),
+              (unsigned long long)off);
+      off += 8 + b.bytes;
+      order.push_back(&b);
+    }
+    fprintf(f, "      </%s>\n", tag);
+  };
+  fprintf(f, "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" "
+             "byte_order=\"LittleEndian\" header_type=\"UInt64\">\n  <UnstructuredGrid>\n"
+             "    <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"%lld\">\n",
+          (long long)N, (long long)E);
+  section("PointData", pd);
+  section("CellData", cd);
+  section("Points", pts);
+  section("Cells", cells);
+  fprintf(f, "    </Piece>\n  </UnstructuredGrid>\n  <AppendedData encoding=\"raw\">\n   _");
+  for (const Block* b : order) {
+    fwrite(&b->bytes, 8, 1, f);
+    fwrite(b->data, 1, b->bytes, f);
+  }
+  fprintf(f, "\n  </AppendedData>\n</VTKFile>\n");
+  const bool ok = ferror(f) == 0;
+  fclose(f);
+  return ok ? FM_OK : fail(FM_ERR_IO, std::string("cannot write ") + path);
+}

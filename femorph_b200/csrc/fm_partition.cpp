@@ -115,6 +115,25 @@ FM_API int fm_problem_partition(const fm_problem* full, const int32_t* elem_part
     if (!full->init.empty())
       for (int k = 0; k < 4; ++k) p->init[i * 4 + k] = full->init[(int64_t)g * 4 + k];
   }
+  // the BC rows of the part's nodes, in local ids (the BCs themselves are
+  // the resolved records above; the rows serve the output writers' dirBC
+  // markers)
+  for (size_t r = 0; r < full->vel_node.size(); ++r)
+    if (loc[full->vel_node[r]] >= 0) {
+      p->vel_node.push_back(loc[full->vel_node[r]]);
+      p->vel_dir.push_back(r < full->vel_dir.size() ? full->vel_dir[r] : 0);
+      for (int k = 0; k < 4; ++k) p->vel_vals.push_back(full->vel_vals[r * 4 + k]);
+    }
+  for (size_t r = 0; r < full->pres_node.size(); ++r)
+    if (loc[full->pres_node[r]] >= 0) {
+      p->pres_node.push_back(loc[full->pres_node[r]]);
+      p->pres_vals.push_back(full->pres_vals[r]);
+    }
+  for (size_t r = 0; r < full->dir_node.size(); ++r)
+    if (loc[full->dir_node[r]] >= 0) {
+      p->dir_node.push_back(loc[full->dir_node[r]]);
+      for (int k = 0; k < 3; ++k) p->dir_vals.push_back(full->dir_vals[r * 3 + k]);
+    }
   p->recs = full->recs;
   p->tab_off = full->tab_off;
   p->tab_len = full->tab_len;

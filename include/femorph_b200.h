@@ -306,6 +306,10 @@ FM_API int fm_problem_write_vtk(fm_problem* p, const char* path);
  * cells, float64 data); no counterpart in the reference, which writes ASCII
  * only. */
 FM_API int fm_problem_write_vtk_binary(fm_problem* p, const char* path);
+/* The same sections as VTK XML UnstructuredGrid (.vtu) with raw appended
+ * little-endian arrays (FP64 points and data, int32 connectivity); no
+ * counterpart in the reference. */
+FM_API int fm_problem_write_vtu(fm_problem* p, const char* path);
 
 /* Nodal lumped mass as the solver uses it, problem numbering: VMS n_nodes
  * (initial_assemble, femVMSExplicitFluidSolver.cpp:87-89), SUPG n_nodes x 3

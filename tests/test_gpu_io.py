@@ -125,3 +125,52 @@ def test_binary_vtk_has_the_ascii_content():
     assert np.allclose(Bn["POINTS"].reshape(-1, 3), p.coords, rtol=1e-6)
     b.close()
     g.close()
+
+
+def _read_vtu(path):
+    """Arrays of a VTU file with raw appended data (UInt64 block sizes), by name."""
+    import re
+    data = open(path, "rb").read()
+    start = data.index(b'<AppendedData encoding="raw">')
+    base = data.index(b"_", start) + 1
+    head = data[:start].decode()
+    piece = re.search(r'NumberOfPoints="(\d+)" NumberOfCells="(\d+)"', head)
+    out = {}
+    for m in re.finditer(r'<DataArray type="(\w+)"(?: Name="(\w+)")?(?: NumberOfComponents="(\d+)")? '
+                         r'format="appended" offset="(\d+)"/>', head):
+        typ, name, comps, off = m.group(1), m.group(2) or "Points", int(m.group(3) or 1), int(m.group(4))
+        n = int(np.frombuffer(data, np.uint64, 1, base + off)[0])
+        dt = {"Float64": "<f8", "Int32": "<i4", "UInt8": "u1"}[typ]
+        arr = np.frombuffer(data, dt, n // np.dtype(dt).itemsize, base + off + 8)
+        out[name] = arr.reshape(-1, comps) if comps > 1 else arr
+    return out, int(piece.group(1)), int(piece.group(2))
+
+
+@pytest.mark.parametrize("case", ["vms", "supg_hexa"])
+def test_vtu_holds_the_state_exactly(case):
+    p = mesh.cavity(5, seed=6, steps=3) if case == "vms" else mesh.channel(6, 3, 3, seed=3, steps=3, noise=1e-3)
+    g = api.GpuProblem(p)
+    b = api.Batch([g])
+    b.step(2)
+    b.sync()
+    path = os.path.join(tempfile.mkdtemp(), "s.vtu")
+    g.write_vtu(path)
+    V, n, e = _read_vtu(path)
+    assert (n, e) == (p.n_nodes, p.n_elems)
+    u, pe, el, _ = g.state()
+    assert np.array_equal(V["velocity"], u) and np.array_equal(V["pressure"], pe)
+    assert np.array_equal(V["Points"], p.coords)
+    npe = p.elem_type
+    assert np.array_equal(V["connectivity"].reshape(-1, npe), p.conn)
+    assert np.array_equal(V["offsets"], npe * np.arange(1, p.n_elems + 1))
+    assert np.all(V["types"] == (10 if npe == 4 else 12))
+    if case == "vms":
+        assert np.array_equal(V["subgrid_u"], el)
+    else:
+        assert np.array_equal(V["lambda"], el[:, 0]) and np.array_equal(V["regime"], el[:, 1])
+    # the same BC markers as the legacy binary writer
+    g.write_vtk(path + ".vtk", binary=True)
+    Bn = _read_binary_vtk(path + ".vtk", p.n_nodes, p.n_elems)
+    assert np.array_equal(V["dirBC"], Bn["dirBC"])
+    b.close()
+    g.close()
