@@ -366,8 +366,9 @@ def run_partitioned(args, rank, world, local_rank, dist, prec_name):
     p = make_problem(a2, seed=0)
     prec = api.FM_MIXED if prec_name == "mixed" else api.FM_FP64
     ps = PartitionedSolve(p, prec, device=local_rank, tile_elems=args.tile_elems, tile_nodes=args.tile_nodes,
-                          threads=args.threads)
+                          threads=args.threads, graph_steps=args.graph_steps)
     ps.step(args.warmup)
+    ps.prepare_graph()   # recorded before the timed region (no-op without --graph-steps)
     ps.sync()
     if dist:
         dist.barrier()
@@ -402,7 +403,8 @@ def partitioned_line(args, world, runs):
                        "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"one mesh, {world} part(s), one part per GPU; one all-reduce of "
                                       f"{r['count']} doubles (the shared nodes' partial sums) per dual iteration",
-                       "exchange_nodes": r["x_total"], "part_elements_rank0": r["part_elems"]},
+                       "exchange_nodes": r["x_total"], "part_elements_rank0": r["part_elems"],
+                       "graph_steps": args.graph_steps},
             "gpu_launches": 3 * args.steps, "clocks": r["clocks"]}
     if "fp64" in runs and head != "fp64":
         f = runs["fp64"]
@@ -539,6 +541,8 @@ def main():
     ap.add_argument("--tile-elems", type=int, default=0)
     ap.add_argument("--tile-nodes", type=int, default=0)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--graph-steps", type=int, default=0,
+                    help="partitioned: iterations per captured CUDA graph (0: eager loop)")
     args = ap.parse_args()
     if not args.n:
         args.n = CONFIG_DEFAULT_N.get(args.config, 96)

@@ -32,7 +32,7 @@ SYMBOLS = [
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
     "fm_vms_solve_static", "fm_batch_capacity_bytes", "fm_problem_velocity_extrema", "fm_problem_supg_log_stats",
     "fm_partition_elements", "fm_problem_partition", "fm_problem_part_info", "fm_problem_part_map",
-    "fm_problem_write_vtu", "fm_batch_exchange_buffers", "fm_batch_exchange_begin", "fm_batch_exchange_end", "fm_batch_iterations_per_step",
+    "fm_problem_write_vtu", "fm_batch_exchange_account", "fm_batch_exchange_buffers", "fm_batch_exchange_begin", "fm_batch_exchange_end", "fm_batch_iterations_per_step",
 ]
 
 
@@ -123,6 +123,7 @@ def lib():
         L.fm_batch_exchange_begin.argtypes = [P, P]
         L.fm_batch_exchange_end.argtypes = [P, P]
         L.fm_batch_iterations_per_step.argtypes = [P, P]
+        L.fm_batch_exchange_account.argtypes = [P, C.c_int32]
         _lib = L
     return _lib
 
@@ -325,6 +326,10 @@ class Batch:
 
     def exchange_end(self, stream=None) -> None:
         check(lib().fm_batch_exchange_end(self.h, stream))
+
+    def exchange_account(self, iterations: int) -> None:
+        """Counts iterations run by replaying captured begin/end pairs."""
+        check(lib().fm_batch_exchange_account(self.h, int(iterations)))
 
     def iterations_per_step(self) -> int:
         n = C.c_int32()

@@ -1255,6 +1255,24 @@ int fm_batch_iterations_per_step(fm_batch* b, int32_t* per_step) {
   return FM_OK;
 }
 
+}  // extern "C"
+
+// Host bookkeeping of `k` completed iterations of every part in the batch.
+static void count_iterations(fm_batch* b, int k) {
+  const int n = (int)b->pools[P_PROB].hwm;
+  for (int i = 0; i < n; ++i) {
+    fm_problem* p = b->slots[i].p;
+    if (!p) continue;
+    const int per = b->solver == FM_SOLVER_VMS ? std::max(0, p->params.tot_dual_steps) + 1 : 1;
+    for (int j = 0; j < k; ++j) {
+      b->iters[i] += 1;
+      if (b->iters[i] % per == 0) p->steps_done += 1;
+    }
+  }
+}
+
+extern "C" {
+
 int fm_batch_exchange_begin(fm_batch* b, void* stream) {
   if (!b) return fail(FM_ERR_INVALID, "null batch");
   if (!b->exchange) return fail(FM_ERR_INVALID, "the batch holds no partition parts");
@@ -1265,6 +1283,10 @@ int fm_batch_exchange_begin(fm_batch* b, void* stream) {
   // targets are opened once (no per-iteration copy or host wait, so the
   // host can run ahead of the GPU)
   if (!b->x_free_targets) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(FM_ERR_INVALID, "run one fm_batch_exchange_begin/end pair before capturing them in a CUDA graph");
     const int n = (int)b->pools[P_PROB].hwm;
     CK(cudaEventSynchronize(b->ev_tgt));
     for (int i = 0; i < n; ++i) b->h_targets[i] = b->slots[i].p ? INT32_MAX : 0;
@@ -1287,14 +1309,18 @@ int fm_batch_exchange_end(fm_batch* b, void* stream) {
   cudaError_t e = launch_second(b, s);
   b->x_open = false;
   if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-  const int n = (int)b->pools[P_PROB].hwm;
-  for (int i = 0; i < n; ++i) {
-    fm_problem* p = b->slots[i].p;
-    if (!p) continue;
-    b->iters[i] += 1;
-    const int per = b->solver == FM_SOLVER_VMS ? std::max(0, p->params.tot_dual_steps) + 1 : 1;
-    if (b->iters[i] % per == 0) p->steps_done += 1;
-  }
+  // a pair recorded into a CUDA graph has not run: its iterations are
+  // counted when the graph is replayed (fm_batch_exchange_account)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cs));
+  if (cs == cudaStreamCaptureStatusNone) count_iterations(b, 1);
+  return FM_OK;
+}
+
+int fm_batch_exchange_account(fm_batch* b, int32_t iterations) {
+  if (!b || iterations < 0) return fail(FM_ERR_INVALID, "bad argument");
+  if (!b->exchange) return fail(FM_ERR_INVALID, "the batch holds no partition parts");
+  count_iterations(b, iterations);
   return FM_OK;
 }
 

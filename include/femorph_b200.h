@@ -268,6 +268,11 @@ FM_API int fm_batch_exchange_buffers(fm_batch* b, double** send, double** recv, 
 FM_API int fm_batch_exchange_begin(fm_batch* b, void* stream);
 FM_API int fm_batch_exchange_end(fm_batch* b, void* stream);
 FM_API int fm_batch_iterations_per_step(fm_batch* b, int32_t* per_step);
+/* begin/end pairs may be captured in a CUDA graph together with the
+ * caller's reduction (after one pair has run outside the capture); a captured
+ * pair counts no iteration, so after replaying a graph of k pairs the caller
+ * reports them here (steps done, per-problem iteration counts). */
+FM_API int fm_batch_exchange_account(fm_batch* b, int32_t iterations);
 
 /* Velocity extrema of a problem's current state, reduced on the device
  * (get_solution_extrema, femSUPGExplicitFluidSolver.cpp:604-655; SUPG

@@ -158,6 +158,32 @@ def test_batch_rules_for_parts():
     bt.close()
 
 
+def test_partitioned_solve_graph_replay_equals_eager():
+    """One process, one part: the CUDA-graph replay of the exchange loop gives
+    the same state, bit for bit, as the eager loop, and the library counts
+    the replayed steps."""
+    from femorph_b200.partition import PartitionedSolve
+    p = mesh.cavity(10, seed=23, steps=17)
+    out = []
+    for gs in (0, 4):
+        s = PartitionedSolve(p, graph_steps=gs)
+        s.step(9)
+        s.step(8)
+        s.sync()
+        out.append(s.gather_state())
+        nn = C_steps(s.part)
+        assert nn == 17, nn
+        s.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def C_steps(part):
+    import ctypes as C
+    st = C.c_int64()
+    api.check(api.lib().fm_problem_info(part.h, None, None, None, None, C.byref(st)))
+    return st.value
+
+
 DRIVER = r"""
 import os, sys, json
 import numpy as np, torch, torch.distributed as dist
@@ -168,7 +194,7 @@ os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
 dist.init_process_group("nccl", rank=0, world_size=1)
 torch.cuda.set_device(0)
 p = mesh.cavity(10, seed=21, steps=12)
-s = PartitionedSolve(p)
+s = PartitionedSolve(p, graph_steps=int(os.environ.get("GRAPH_STEPS", "0")))
 s.step(12)
 s.sync()
 u, pr = s.gather_state()
@@ -181,14 +207,16 @@ dist.destroy_process_group()
 """
 
 
-def test_torch_distributed_driver_nccl_one_rank(tmp_path):
+@pytest.mark.parametrize("graph_steps", [0, 5])
+def test_torch_distributed_driver_nccl_one_rank(tmp_path, graph_steps):
     import json
     import socket
     sk = socket.socket()
     sk.bind(("127.0.0.1", 0))
     port = sk.getsockname()[1]
     sk.close()
-    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), NCCL_NVLS_ENABLE="0")
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), NCCL_NVLS_ENABLE="0",
+               GRAPH_STEPS=str(graph_steps))
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     r = subprocess.run([sys.executable, "-c", DRIVER], cwd=root, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
