@@ -32,7 +32,8 @@ SYMBOLS = [
     "fm_problem_prepare", "fm_batch_resident", "fm_batch_step_problems", "fm_problem_status",
     "fm_vms_solve_static", "fm_batch_capacity_bytes", "fm_problem_velocity_extrema", "fm_problem_supg_log_stats",
     "fm_partition_elements", "fm_problem_partition", "fm_problem_part_info", "fm_problem_part_map",
-    "fm_problem_write_vtu", "fm_batch_exchange_account", "fm_batch_exchange_buffers", "fm_batch_exchange_begin", "fm_batch_exchange_end", "fm_batch_iterations_per_step",
+    "fm_problem_write_vtu", "fm_batch_exchange_account", "fm_batch_exchange_buffers", "fm_batch_exchange_begin",
+    "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
 ]
 
 
@@ -98,6 +99,8 @@ def lib():
         L.fm_problem_write_vtk.argtypes = [P, C.c_char_p]
         L.fm_problem_write_vtk_binary.argtypes = [P, C.c_char_p]
         L.fm_problem_write_vtu.argtypes = [P, C.c_char_p]
+        L.fm_problem_checkpoint.argtypes = [P, C.c_char_p]
+        L.fm_problem_restore.argtypes = [P, C.c_char_p]
         L.fm_problem_get_mass.argtypes = [P, P]
         L.fm_batch_last_timing.argtypes = [P, P, P]
         L.fm_batch_estimate_bytes.argtypes = [P, C.c_int32, P, P]
@@ -213,6 +216,16 @@ class GpuProblem:
     def write_vtu(self, path: str) -> None:
         """VTK XML UnstructuredGrid with raw appended binary arrays."""
         check(lib().fm_problem_write_vtu(self.h, path.encode()))
+
+    def checkpoint(self, path: str) -> None:
+        """Writes the problem's evolving state (it must sit in a batch) to a
+        binary restart file."""
+        check(lib().fm_problem_checkpoint(self.h, path.encode()))
+
+    def restore(self, path: str) -> None:
+        """Loads a restart file of this mesh and configuration into the
+        problem (it must sit in a batch); stepping on continues that solve."""
+        check(lib().fm_problem_restore(self.h, path.encode()))
 
     def prepare(self, tile_elems=0, tile_nodes=0, threads=0) -> None:
         """Builds the tile layout now (host only, thread-safe per problem)."""

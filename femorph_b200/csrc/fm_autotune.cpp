@@ -64,6 +64,7 @@ void cache_store(const char* path, const std::string& key, const fm_tuning& t) {
 
 extern "C" int fm_autotune(fm_problem* const* probs, int32_t n, int32_t device, int32_t steps, const char* cache_path,
                            fm_tuning* best) {
+  fm::NvtxRange nvtx_range("fm_autotune");
   if (!probs || n <= 0 || !best) return fm::fail(FM_ERR_INVALID, "null argument");
   for (int i = 0; i < n; ++i)
     if (!probs[i] || probs[i]->batch) return fm::fail(FM_ERR_INVALID, "problems must exist and not be in a batch");

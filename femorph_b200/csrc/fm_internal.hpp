@@ -9,9 +9,21 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/femorph_b200.h"
 
 namespace fm {
+
+// NVTX range over a host phase of the library (preparation, placement,
+// stepping, I/O) for the lifetime of the object; without a profiler
+// attached the push and pop return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Allocator whose value-initialisation leaves trivial elements unset, so
 // large host arrays are first touched (and filled) by the host threads that

@@ -137,6 +137,7 @@ void parse_block(const char* b, const char* e, DatBlock& B) {
 // keep their order; for the single-valued keywords the last line wins, as in
 // the reference's sequential reader).
 extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t precision, fm_problem** out) {
+  NvtxRange nvtx_range("fm_problem_read_dat");
   if (!path || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
   FILE* fp = fopen(path, "rb");
@@ -311,6 +312,7 @@ void write_rows(FILE* f, int64_t n, F fmt) {
 // element loop order and carry no state); they are written as zeros.  The
 // rows are formatted on the host threads (write_rows).
 extern "C" int fm_problem_write_vtk(fm_problem* p, const char* path) {
+  NvtxRange nvtx_range("fm_problem_write_vtk");
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
   const int64_t N = p->N, E = p->E;
   const bool vms = p->params.solver == FM_SOLVER_VMS;
@@ -413,6 +415,7 @@ void put_be(FILE* f, const T* v, int64_t n) {
 // ASCII %e text at the benchmark sizes.  No counterpart in the reference,
 // which writes ASCII only.
 extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
+  NvtxRange nvtx_range("fm_problem_write_vtk_binary");
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
   if (!p->batch) return fail(FM_ERR_INVALID, "problem is not in a batch");
   const int64_t N = p->N, E = p->E;
@@ -492,6 +495,7 @@ extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
 // FP64 points and data, int32 connectivity, read by ParaView and VTK without
 // any text parsing.  No counterpart in the reference (ASCII legacy VTK only).
 extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
+  NvtxRange nvtx_range("fm_problem_write_vtu");
   static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the VTU writer emits little-endian data");
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
   if (!p->batch) return fail(FM_ERR_INVALID, "problem is not in a batch");

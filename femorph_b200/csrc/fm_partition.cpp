@@ -48,6 +48,7 @@ FM_API int fm_partition_elements(const fm_problem* full, int32_t n_parts, int32_
 
 FM_API int fm_problem_partition(const fm_problem* full, const int32_t* elem_part, int32_t n_parts, int32_t part,
                                 fm_problem** out) {
+  NvtxRange nvtx_range("fm_problem_partition");
   if (!full || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
   if (full->part >= 0) return fail(FM_ERR_INVALID, "a partition part cannot be partitioned again");

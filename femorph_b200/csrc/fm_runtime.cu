@@ -755,6 +755,7 @@ const char* fm_last_error_message(void) { return last_error(); }
 int fm_version(void) { return 101; }
 
 int fm_problem_create(const fm_mesh* m, const fm_bc* bc, const fm_params* prm, const double* init, fm_problem** out) {
+  NvtxRange nvtx_range("fm_problem_create");
   if (!m || !prm || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
   if (m->elem_type != FM_TET4 && m->elem_type != FM_HEXA8) return fail(FM_ERR_INVALID, "elem_type must be 4 or 8");
@@ -847,6 +848,7 @@ int fm_problem_get_mass(fm_problem* p, double* mass) {
 }
 
 int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning) {
+  NvtxRange nvtx_range("fm_problem_prepare");
   if (!p) return fail(FM_ERR_INVALID, "null problem");
   fm_tuning t;
   memset(&t, 0, sizeof(t));
@@ -907,6 +909,7 @@ static int new_batch(int solver, int npe, int prec, const fm_tuning* tuning, int
 }
 
 int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning, int32_t device, fm_batch** out) {
+  NvtxRange nvtx_range("fm_batch_create");
   if (!probs || n <= 0 || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
   int solver, npe, prec;
@@ -981,6 +984,7 @@ int fm_batch_create(fm_problem* const* probs, int32_t n, const fm_tuning* tuning
 }
 
 int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning, int32_t device, fm_batch** out) {
+  NvtxRange nvtx_range("fm_batch_create_empty");
   if (!cap || !out) return fail(FM_ERR_INVALID, "null argument");
   if (cap->elem_type != FM_TET4 && cap->elem_type != FM_HEXA8) return fail(FM_ERR_INVALID, "bad element type");
   if (cap->max_elems <= 0 || cap->max_nodes <= 0 || cap->max_problems <= 0) return fail(FM_ERR_INVALID, "bad capacity");
@@ -1015,6 +1019,7 @@ int fm_batch_capacity_bytes(const fm_capacity* cap, const fm_tuning* tuning, int
 }
 
 int fm_batch_add(fm_batch* b, fm_problem* p) {
+  NvtxRange nvtx_range("fm_batch_add");
   if (!b || !p) return fail(FM_ERR_INVALID, "null argument");
   if (p->batch) return fail(FM_ERR_INVALID, "problem already belongs to a batch");
   if (p->part >= 0 || b->exchange)
@@ -1032,6 +1037,7 @@ int fm_batch_add(fm_batch* b, fm_problem* p) {
 }
 
 int fm_batch_remove(fm_batch* b, fm_problem* p) {
+  NvtxRange nvtx_range("fm_batch_remove");
   if (!b || !p || p->batch != b) return fail(FM_ERR_INVALID, "problem is not in this batch");
   if (b->exchange) return fail(FM_ERR_INVALID, "partition parts stay in their batch until it is destroyed");
   CK(cudaSetDevice(b->device));
@@ -1099,6 +1105,7 @@ static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
 // device times are summed into prof[0] (tile kernel) and prof[1] (interface
 // kernel), in milliseconds.
 static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cudaStream_t s, double* prof = nullptr) {
+  NvtxRange nvtx_range("fm_batch_step");
   if (b->x_external)
     return fail(FM_ERR_INVALID,
                 "the batch holds partition parts whose other parts run elsewhere: advance it with "
@@ -1274,6 +1281,7 @@ static void count_iterations(fm_batch* b, int k) {
 extern "C" {
 
 int fm_batch_exchange_begin(fm_batch* b, void* stream) {
+  NvtxRange nvtx_range("fm_batch_exchange_begin");
   if (!b) return fail(FM_ERR_INVALID, "null batch");
   if (!b->exchange) return fail(FM_ERR_INVALID, "the batch holds no partition parts");
   if (b->x_open) return fail(FM_ERR_INVALID, "fm_batch_exchange_begin called twice without fm_batch_exchange_end");
@@ -1302,6 +1310,7 @@ int fm_batch_exchange_begin(fm_batch* b, void* stream) {
 }
 
 int fm_batch_exchange_end(fm_batch* b, void* stream) {
+  NvtxRange nvtx_range("fm_batch_exchange_end");
   if (!b) return fail(FM_ERR_INVALID, "null batch");
   if (!b->x_open) return fail(FM_ERR_INVALID, "fm_batch_exchange_end called without fm_batch_exchange_begin");
   CK(cudaSetDevice(b->device));
@@ -1325,6 +1334,7 @@ int fm_batch_exchange_account(fm_batch* b, int32_t iterations) {
 }
 
 int fm_batch_profile(fm_batch* b, int32_t nsteps, double* kernel_ms, int64_t* launches) {
+  NvtxRange nvtx_range("fm_batch_profile");
   if (!b || nsteps < 0) return fail(FM_ERR_INVALID, "bad argument");
   CK(cudaSetDevice(b->device));
   const int n = (int)b->pools[P_PROB].hwm;
@@ -1470,6 +1480,7 @@ int fm_batch_resident(fm_batch* b, int32_t* problems, int64_t* elems, int64_t* f
 }
 
 int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, double* sdus) {
+  NvtxRange nvtx_range("fm_problem_get_state");
   if (!p) return fail(FM_ERR_INVALID, "null problem");
   fm_batch* b = p->batch;
   if (!b) return fail(FM_ERR_INVALID, "problem is not in a batch");
@@ -1544,6 +1555,213 @@ int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, 
       }
     }
   }
+  return FM_OK;
+}
+
+}  // extern "C"
+
+// ---- checkpoint / restart ----
+// File layout (little-endian): CkptHeader, then in the problem's own
+// numbering
+//   8 node columns of n_nodes doubles: u v w p after BCs, u v w p before BCs;
+//   n_sd_cols element columns of n_elems values of sd_bytes each (VMS: the
+//     12 Gauss-point subscales [gp*3+c], FP32 in the mixed form; SUPG: the
+//     3*npe AB2 history columns of a problem without EXOPTS euler);
+//   n_diag_cols element columns of n_elems doubles (SUPG: lambda, regime).
+namespace {
+struct CkptHeader {
+  char magic[8];  // "FMSTATE1"
+  int32_t version, solver, precision, npe;
+  int64_t n_nodes, n_elems;
+  int32_t n_sd_cols, sd_bytes, n_diag_cols, iter;
+  int32_t status, reserved;
+  int64_t steps_done;
+  double time, max_u2;
+  double q1p[8];  // pre-BC pressures of nodes 0..3, both iteration parities
+  uint64_t mesh_hash;
+};
+static_assert(sizeof(CkptHeader) == 160, "checkpoint header size");
+
+// FNV-1a over the 64-bit words of the coordinates, then the connectivity.
+uint64_t mesh_hash(const fm_problem* p) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t w) { h = (h ^ w) * 1099511628211ull; };
+  for (int64_t i = 0; i < p->N * 3; ++i) {
+    uint64_t w;
+    memcpy(&w, &p->coords[i], 8);
+    mix(w);
+  }
+  const int64_t nc = p->E * p->etype;
+  for (int64_t i = 0; i < nc; ++i) mix((uint64_t)(uint32_t)p->conn[i]);
+  mix((uint64_t)p->N);
+  mix((uint64_t)p->E);
+  return h;
+}
+
+struct CkptCols {
+  int n_sd = 0, sd_bytes = 8, n_diag = 0;
+};
+CkptCols ckpt_cols(const fm_batch* b, const fm_problem* p) {
+  CkptCols c;
+  if (b->solver == FM_SOLVER_VMS) {
+    c.n_sd = 12;
+    c.sd_bytes = b->D.sdus32 ? 4 : 8;
+  } else {
+    c.n_sd = p->params.ex_opts[0] == 0 ? 3 * b->npe : 0;  // only AB2 reads its history
+    c.n_diag = 2;
+  }
+  return c;
+}
+
+// Device address of element column q of slot range eb (subscales or
+// history first, then lambda and regime).
+void* ckpt_elem_col(const fm_batch* b, const CkptCols& cc, int q, int64_t eb) {
+  if (q >= cc.n_sd) return (q == cc.n_sd ? b->D.el_lam : b->D.el_reg) + eb;
+  if (cc.sd_bytes == 4) return b->D.sdus32 + (int64_t)q * b->D.E + eb;
+  return b->D.sdus + (int64_t)q * b->D.E + eb;
+}
+
+struct FileCloser {
+  FILE* f;
+  ~FileCloser() {
+    if (f) fclose(f);
+  }
+};
+}  // namespace
+
+extern "C" {
+
+int fm_problem_checkpoint(fm_problem* p, const char* path) {
+  NvtxRange nvtx_range("fm_problem_checkpoint");
+  if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
+  fm_batch* b = p->batch;
+  if (!b) return fail(FM_ERR_INVALID, "problem is not in a batch");
+  if (b->x_open) return fail(FM_ERR_INVALID, "an exchange is open: checkpoint after fm_batch_exchange_end");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const int ps = p->index;
+  const Placement& pl = b->slots[ps];
+  const int64_t nb = pl.off[P_NODE], eb = pl.off[P_ELEM];
+  const int64_t N = p->N, E = p->E;
+  const std::vector<int32_t>& nn = pl.L->node_new[0];
+  const auto& eo = pl.L->elem_old[0];
+  const int64_t EC = (int64_t)eo.size();
+  const CkptCols cc = ckpt_cols(b, p);
+
+  CkptHeader h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, "FMSTATE1", 8);
+  h.version = 1;
+  h.solver = b->solver;
+  h.precision = b->precision;
+  h.npe = b->npe;
+  h.n_nodes = N;
+  h.n_elems = E;
+  h.n_sd_cols = cc.n_sd;
+  h.sd_bytes = cc.sd_bytes;
+  h.n_diag_cols = cc.n_diag;
+  DevProbState st;
+  CK(cudaMemcpy(&st, b->D.pstate + ps, sizeof(st), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(h.q1p, b->D.q1p + (int64_t)ps * 8, sizeof(h.q1p), cudaMemcpyDeviceToHost));
+  h.iter = st.iter;
+  h.status = st.status;
+  h.time = st.time;
+  h.max_u2 = st.max_u2;
+  h.steps_done = p->steps_done;
+  h.mesh_hash = mesh_hash(p);
+
+  FileCloser fc{fopen(path, "wb")};
+  if (!fc.f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  bool ok = fwrite(&h, sizeof(h), 1, fc.f) == 1;
+  std::vector<double> tmp(N), out(N);
+  double* cols[8] = {b->D.su, b->D.sv, b->D.sw, b->D.sp, b->D.pu, b->D.pv, b->D.pw, b->D.pp};
+  for (int c = 0; c < 8 && ok; ++c) {
+    CK(cudaMemcpy(tmp.data(), cols[c] + nb, sizeof(double) * N, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < N; ++i) out[i] = tmp[nn[i]];
+    ok = fwrite(out.data(), sizeof(double), N, fc.f) == (size_t)N;
+  }
+  // element columns: device slot k holds problem element eo[k] (padding < 0)
+  std::vector<char> col((size_t)EC * 8), eout((size_t)E * 8);
+  for (int q = 0; q < cc.n_sd + cc.n_diag && ok; ++q) {
+    const int bytes = q < cc.n_sd ? cc.sd_bytes : 8;
+    CK(cudaMemcpy(col.data(), ckpt_elem_col(b, cc, q, eb), (size_t)EC * bytes, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < EC; ++k)
+      if (eo[k] >= 0) memcpy(&eout[(size_t)eo[k] * bytes], &col[(size_t)k * bytes], bytes);
+    ok = fwrite(eout.data(), bytes, E, fc.f) == (size_t)E;
+  }
+  if (!ok || fflush(fc.f) != 0) return fail(FM_ERR_IO, std::string("cannot write ") + path);
+  return FM_OK;
+}
+
+int fm_problem_restore(fm_problem* p, const char* path) {
+  NvtxRange nvtx_range("fm_problem_restore");
+  if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
+  fm_batch* b = p->batch;
+  if (!b) return fail(FM_ERR_INVALID, "problem is not in a batch");
+  if (b->x_open) return fail(FM_ERR_INVALID, "an exchange is open: restore after fm_batch_exchange_end");
+  FileCloser fc{fopen(path, "rb")};
+  if (!fc.f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  CkptHeader h;
+  if (fread(&h, sizeof(h), 1, fc.f) != 1 || memcmp(h.magic, "FMSTATE1", 8) != 0 || h.version != 1)
+    return fail(FM_ERR_INVALID, std::string(path) + " is not a femorph_b200 checkpoint");
+  const CkptCols cc = ckpt_cols(b, p);
+  if (h.solver != b->solver || h.precision != b->precision || h.npe != b->npe)
+    return fail(FM_ERR_INVALID, "checkpoint of another solver, precision or element type");
+  if (h.n_nodes != p->N || h.n_elems != p->E || h.mesh_hash != mesh_hash(p))
+    return fail(FM_ERR_INVALID, "checkpoint of another mesh");
+  if (h.n_sd_cols != cc.n_sd || h.sd_bytes != cc.sd_bytes || h.n_diag_cols != cc.n_diag)
+    return fail(FM_ERR_INVALID, "checkpoint element columns differ (SUPG AB2 history or not)");
+  if (h.iter < 0 || h.steps_done < 0) return fail(FM_ERR_INVALID, "checkpoint counters out of range");
+  const int64_t N = p->N, E = p->E;
+  // read everything before touching the device, so a bad file leaves the
+  // problem's state as it was
+  std::vector<double> nodes((size_t)N * 8);
+  if (fread(nodes.data(), sizeof(double), nodes.size(), fc.f) != nodes.size())
+    return fail(FM_ERR_IO, std::string("truncated checkpoint ") + path);
+  const int ncols = cc.n_sd + cc.n_diag;
+  std::vector<std::vector<char>> ecols(ncols);
+  for (int q = 0; q < ncols; ++q) {
+    const int bytes = q < cc.n_sd ? cc.sd_bytes : 8;
+    ecols[q].resize((size_t)E * bytes);
+    if (fread(ecols[q].data(), bytes, E, fc.f) != (size_t)E)
+      return fail(FM_ERR_IO, std::string("truncated checkpoint ") + path);
+  }
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const int ps = p->index;
+  const Placement& pl = b->slots[ps];
+  const int64_t nb = pl.off[P_NODE], eb = pl.off[P_ELEM];
+  const std::vector<int32_t>& nn = pl.L->node_new[0];
+  const auto& eo = pl.L->elem_old[0];
+  const int64_t EC = (int64_t)eo.size();
+  std::vector<double> tmp(N);
+  double* cols[8] = {b->D.su, b->D.sv, b->D.sw, b->D.sp, b->D.pu, b->D.pv, b->D.pw, b->D.pp};
+  for (int c = 0; c < 8; ++c) {
+    const double* in = nodes.data() + (size_t)c * N;
+    for (int64_t i = 0; i < N; ++i) tmp[nn[i]] = in[i];
+    CK(cudaMemcpy(cols[c] + nb, tmp.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  }
+  // element columns: padding slots keep their device values
+  std::vector<char> col((size_t)EC * 8);
+  for (int q = 0; q < ncols; ++q) {
+    const int bytes = q < cc.n_sd ? cc.sd_bytes : 8;
+    void* dev = ckpt_elem_col(b, cc, q, eb);
+    CK(cudaMemcpy(col.data(), dev, (size_t)EC * bytes, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < EC; ++k)
+      if (eo[k] >= 0) memcpy(&col[(size_t)k * bytes], &ecols[q][(size_t)eo[k] * bytes], bytes);
+    CK(cudaMemcpy(dev, col.data(), (size_t)EC * bytes, cudaMemcpyHostToDevice));
+  }
+  DevProbState st;
+  memset(&st, 0, sizeof(st));
+  st.iter = h.iter;
+  st.status = h.status;
+  st.time = h.time;
+  st.max_u2 = h.max_u2;
+  CK(cudaMemcpy(b->D.pstate + ps, &st, sizeof(st), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->D.q1p + (int64_t)ps * 8, h.q1p, sizeof(h.q1p), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(const_cast<int32_t*>(b->D.target) + ps, &h.iter, sizeof(int32_t), cudaMemcpyHostToDevice));
+  b->iters[ps] = h.iter;
+  p->steps_done = h.steps_done;
   return FM_OK;
 }
 

@@ -185,6 +185,7 @@ static cudaError_t up(unsigned char* base, size_t off, const T* src, size_t n, c
 
 extern "C" int fm_vms_solve_static(fm_problem* p, int32_t nsteps, int32_t device, double* u, double* pres,
                                    void* stream) {
+  NvtxRange nvtx_range("fm_vms_solve_static");
   if (!p || nsteps < 0) return fail(FM_ERR_INVALID, "null problem or negative step count");
   if (p->params.solver != FM_SOLVER_VMS || p->etype != FM_TET4)
     return fail(FM_ERR_INVALID, "fm_vms_solve_static runs the VMS tet4 solver only");

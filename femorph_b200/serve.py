@@ -13,6 +13,13 @@ waiting for them to finish.  A problem's result does not depend on which other
 problems share the batch (tiles never span problems; every launch is
 deterministic).
 
+Preemption (optional, `preempt_after` seconds): when the oldest prepared
+request has waited that long for room, the resident solve with the most
+steps left (among those that ran at least one round since admission) is
+checkpointed to `spill_dir` (fm_problem_checkpoint), removed, and queued
+behind the waiting requests; re-admitted, it is restored
+(fm_problem_restore) and continues bit for bit.
+
 The reference solves one model per process (femVMSExplicitFluidSolver::solve,
 src/femVMSExplicitFluidSolver.cpp:842-1334); this loop has no counterpart
 there.
@@ -22,6 +29,7 @@ from __future__ import annotations
 import collections
 import concurrent.futures as cf
 import dataclasses
+import os
 import time
 
 import numpy as np
@@ -44,6 +52,9 @@ class Request:
     result: tuple | None = None     # (u (N,3), p (N,)) after `steps` steps
     status: int = 0                 # FM_OK, or the device status that retired it early
     steps_done: int = 0
+    preemptions: int = 0
+    spill: str | None = None        # checkpoint of a preempted solve, until re-admitted
+    blocked: float | None = None    # when it first found no room at the head of the queue
 
     @property
     def latency(self) -> float:
@@ -59,9 +70,13 @@ class Server:
 
     def __init__(self, precision: int = api.FM_MIXED, hbm_budget: int = 16 << 30, max_problems: int = 512,
                  block: int = 50, device: int = 0, prepare_workers: int = 0, tuning: dict | None = None,
-                 keep_results: bool = True):
+                 keep_results: bool = True, preempt_after: float | None = None, spill_dir: str | None = None):
         self.precision = precision
         self.block = block
+        self.preempt_after = preempt_after
+        self.spill_dir = spill_dir
+        if preempt_after is not None and spill_dir is None:
+            raise ValueError("preemption checkpoints to spill_dir")
         self.hbm_budget = hbm_budget
         self.keep_results = keep_results
         self.tuning = dict(tuning or {})
@@ -75,7 +90,6 @@ class Server:
         self.pool = api.Pool(mesh.VMS, 4, max_problems=max_problems, max_elems=max_elems, max_nodes=max_nodes,
                              precision=precision, device=device, **self.tuning)
         self.capacity = dict(max_elems=max_elems, max_nodes=max_nodes, max_problems=max_problems)
-        import os
         self.exec = cf.ThreadPoolExecutor(max_workers=prepare_workers or min(32, os.cpu_count() or 4))
 
     def _prepare(self, req: Request):
@@ -89,8 +103,9 @@ class Server:
         run statistics.  Blocks until every request is done."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         preparing: collections.deque = collections.deque()   # (req, future) in arrival order
-        resident: list = []                                    # [req, GpuProblem, remaining steps]
+        resident: list = []                  # [req, GpuProblem, remaining steps, steps since admission]
         rounds = 0
+        preemptions = 0
         busy = 0.0
         peak_resident = 0
         t0 = clock()
@@ -107,10 +122,34 @@ class Server:
                     if not resident:
                         raise RuntimeError(f"request {r.rid} ({r.problem.n_elems} elements) does not fit the "
                                            f"server's pools {self.capacity}")
+                    if r.blocked is None:
+                        r.blocked = now
                     break
                 preparing.popleft()
-                r.admitted = clock() - t0
-                resident.append([r, g, r.steps])
+                r.blocked = None
+                if r.spill is not None:
+                    g.restore(r.spill)
+                    os.remove(r.spill)
+                    r.spill = None
+                if r.admitted is None:
+                    r.admitted = clock() - t0
+                resident.append([r, g, r.steps - r.steps_done, 0])
+            if (self.preempt_after is not None and preparing and preparing[0][0].blocked is not None
+                    and now - preparing[0][0].blocked >= self.preempt_after):
+                movable = [item for item in resident if item[3] >= self.block]
+                if movable:
+                    victim = max(movable, key=lambda item: item[2] * item[0].problem.n_elems)
+                    v, g, _, _ = victim
+                    v.spill = os.path.join(self.spill_dir, f"request{v.rid}.fmck")
+                    g.checkpoint(v.spill)
+                    self.pool.remove(g)
+                    resident.remove(victim)
+                    v.preemptions += 1
+                    preemptions += 1
+                    fut: cf.Future = cf.Future()
+                    fut.set_result(g)
+                    preparing.append((v, fut))
+                    continue
             if not resident:
                 # idle: wait for the next arrival or preparation
                 if preparing:
@@ -119,16 +158,17 @@ class Server:
                     time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
                 continue
             peak_resident = max(peak_resident, len(resident))
-            steps = [min(self.block, rem) for _, _, rem in resident]
+            steps = [min(self.block, item[2]) for item in resident]
             ts = clock()
-            self.pool.step([g for _, g, _ in resident], steps)
+            self.pool.step([item[1] for item in resident], steps)
             failed = self.pool.wait()   # True when some problem reported a device error
             busy += clock() - ts
             rounds += 1
             still = []
             for item, k in zip(resident, steps):
                 item[2] -= k
-                r, g, rem = item
+                item[3] += k
+                r, g, rem, _ = item
                 r.steps_done += k
                 status = g.status() if failed else api.FM_OK
                 if rem > 0 and status == api.FM_OK:
@@ -153,7 +193,7 @@ class Server:
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                 "mean_latency_s": float(lat.mean()), "element_steps": int(work),
                 "element_steps_per_s": work / (last - first), "peak_resident": peak_resident,
-                "failed": sum(1 for r in requests if r.status != 0)}
+                "failed": sum(1 for r in requests if r.status != 0), "preemptions": preemptions}
 
     def close(self):
         self.exec.shutdown(wait=True)

@@ -316,6 +316,23 @@ FM_API int fm_problem_write_vtk_binary(fm_problem* p, const char* path);
  * counterpart in the reference. */
 FM_API int fm_problem_write_vtu(fm_problem* p, const char* path);
 
+/* Checkpoint and restart (no counterpart in the reference, whose VTK output
+ * keeps six digits and cannot restart a solve).  fm_problem_checkpoint
+ * writes everything the next iteration reads of a problem in a batch, in
+ * the problem's own node / element numbering: the state after and before
+ * BCs, the element state (VMS subscales, FP64 or FP32 as the precision
+ * keeps them; SUPG history and lambda / regime), the iteration and step
+ * counters, time, status and the pressures of nodes 0..3 (little-endian,
+ * a 160-byte header then columns; layout in fm_runtime.cu).
+ * fm_problem_restore loads such a file into a problem of the same mesh,
+ * solver and precision that sits in a batch (any batch, any slot); stepping
+ * on continues the solve: bit for bit the uninterrupted one when the batch
+ * has the same tile sizes and threads.  Either call waits for the batch's
+ * stream; neither may run while an exchange is open.  FM_ERR_IO for a file
+ * error, FM_ERR_INVALID for a file of another mesh or configuration. */
+FM_API int fm_problem_checkpoint(fm_problem* p, const char* path);
+FM_API int fm_problem_restore(fm_problem* p, const char* path);
+
 /* Nodal lumped mass as the solver uses it, problem numbering: VMS n_nodes
  * (initial_assemble, femVMSExplicitFluidSolver.cpp:87-89), SUPG n_nodes x 3
  * (form_lumped_mass, femSUPGExplicitFluidSolver.cpp:507-598). */

@@ -183,3 +183,16 @@ def test_dat_reader_multi_block_file_equals_in_memory_problem(tmp_path):
     api.check(api.lib().fm_problem_get_mass(h, m.ctypes.data))
     assert np.array_equal(m, api.GpuProblem(p).mass())
     api.lib().fm_problem_destroy(h)
+
+
+def test_checkpoint_needs_a_batch(tmp_path):
+    """Checkpoint and restore refuse a problem outside a batch before any
+    file or device access."""
+    q = api.GpuProblem(mesh.cavity(2, seed=0, steps=1))
+    path = str(tmp_path / "state.fmck")
+    for f in (q.checkpoint, q.restore):
+        with pytest.raises(api.FmError) as ei:
+            f(path)
+        assert ei.value.code == api.FM_ERR_INVALID
+    assert not os.path.exists(path)
+    q.close()

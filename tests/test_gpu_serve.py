@@ -60,3 +60,26 @@ def test_budget_admission_waits_for_room():
     admitted = sorted(r.admitted for r in reqs)
     done = sorted(r.done for r in reqs)
     assert admitted[-1] >= done[0]   # the last admission had to wait for a retirement
+
+
+@pytest.mark.parametrize("precision", [api.FM_FP64, api.FM_MIXED])
+def test_preempted_solves_resume_bit_for_bit(tmp_path, precision):
+    # room for about two of these problems; with preempt_after = 0 a waiting
+    # request evicts the resident solve with the most work left after every
+    # round, so solves are checkpointed, removed, restored and resumed many
+    # times; each result must still equal the request solved alone
+    reqs = serve.draw_requests(5, rate=1000.0, seed=9, n_range=(6, 6), steps_range=(24, 40))
+    per = api.capacity_bytes(mesh.VMS, 4, 4, 3000, 600, precision)
+    srv = serve.Server(precision=precision, hbm_budget=per, max_problems=4, block=4, prepare_workers=2,
+                       preempt_after=0.0, spill_dir=str(tmp_path))
+    stats = srv.run(reqs)
+    srv.close()
+    assert stats["failed"] == 0
+    assert stats["preemptions"] >= 2 and stats["peak_resident"] <= 2
+    assert sum(r.preemptions for r in reqs) == stats["preemptions"]
+    assert not list(tmp_path.iterdir())   # every spilled checkpoint was restored and removed
+    for r in reqs:
+        assert r.steps_done == r.steps
+        u0, p0 = alone(r.problem, r.steps, precision)
+        u, p = r.result
+        assert np.array_equal(u, u0) and np.array_equal(p, p0), r.rid
