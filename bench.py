@@ -155,7 +155,8 @@ def run_ours(args, rank, world, local_rank, dist):
     p = make_problem(args, seed=rank)
     E, N = p.n_elems, p.n_nodes
     g = api.GpuProblem(p, prec)
-    tune = dict(tile_elems=args.tile_elems, tile_nodes=args.tile_nodes, threads=args.threads)
+    tune = dict(tile_elems=args.tile_elems, tile_nodes=args.tile_nodes, threads=args.threads,
+                ctas_per_sm=args.ctas_per_sm)
     b = api.Batch([g], device=local_rank, **tune)
     b.step(args.warmup)
     b.sync()
@@ -288,7 +289,7 @@ def batched_line(args, world, rb):
                        "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"problems sharded over {world} GPU(s) by LPT on element count"},
             "roofline": m["roofline"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
-            "fp64": out["fp64"], "mixed_over_fp64": m["value"] / out["fp64"]["value"],
+            "tuning": m["tuning"], "fp64": out["fp64"], "mixed_over_fp64": m["value"] / out["fp64"]["value"],
             "mixed_vs_fp64_rel_l2": {"u_max_over_problems": rb["err"][0], "p_max_over_problems": rb["err"][1],
                                      "after_steps": args.warmup + args.steps + min(args.steps, 50)}}
 
@@ -541,6 +542,8 @@ def main():
     ap.add_argument("--tile-elems", type=int, default=0)
     ap.add_argument("--tile-nodes", type=int, default=0)
     ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0,
+                    help="VMS register budget: tile kernel variant for this many resident CTAs an SM (0: default)")
     ap.add_argument("--graph-steps", type=int, default=0,
                     help="partitioned: iterations per captured CUDA graph (0: eager loop)")
     args = ap.parse_args()

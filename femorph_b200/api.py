@@ -57,7 +57,7 @@ class FmParams(C.Structure):
 
 class FmTuning(C.Structure):
     _fields_ = [("tile_elems", C.c_int32), ("tile_nodes", C.c_int32), ("threads", C.c_int32),
-                ("graph_steps", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("graph_steps", C.c_int32), ("ctas_per_sm", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class FmCapacity(C.Structure):
@@ -295,11 +295,11 @@ class _DeviceArray:
 class Batch:
     """Device-resident batch of GpuProblems (all share solver and element type)."""
 
-    def __init__(self, problems, tile_elems=0, tile_nodes=0, threads=0, graph_steps=0, device=0):
+    def __init__(self, problems, tile_elems=0, tile_nodes=0, threads=0, graph_steps=0, device=0, ctas_per_sm=0):
         L = lib()
         self.problems = list(problems)
         arr = (C.c_void_p * len(self.problems))(*[q.h.value for q in self.problems])
-        t = FmTuning(tile_elems, tile_nodes, threads, graph_steps)
+        t = FmTuning(tile_elems, tile_nodes, threads, graph_steps, ctas_per_sm)
         h = C.c_void_p()
         check(L.fm_batch_create(arr, len(self.problems), C.byref(t), device, C.byref(h)))
         self.h = h
@@ -381,9 +381,9 @@ class Pool:
     launches (continuous batching)."""
 
     def __init__(self, solver, elem_type, max_problems, max_elems, max_nodes, precision=FM_FP64,
-                 max_table_rows=0, tile_elems=0, tile_nodes=0, threads=0, graph_steps=0, device=0):
+                 max_table_rows=0, tile_elems=0, tile_nodes=0, threads=0, graph_steps=0, device=0, ctas_per_sm=0):
         cap = FmCapacity(solver, elem_type, precision, max_problems, max_elems, max_nodes, max_table_rows)
-        t = FmTuning(tile_elems, tile_nodes, threads, graph_steps)
+        t = FmTuning(tile_elems, tile_nodes, threads, graph_steps, ctas_per_sm)
         h = C.c_void_p()
         check(lib().fm_batch_create_empty(C.byref(cap), C.byref(t), device, C.byref(h)))
         self.h = h
@@ -452,7 +452,7 @@ def autotune(problems, device: int = 0, steps: int = 10, cache_path: str | None 
     t = FmTuning()
     check(lib().fm_autotune(arr, len(problems), device, steps, cache_path.encode() if cache_path else None,
                             C.byref(t)))
-    return dict(tile_elems=t.tile_elems, tile_nodes=t.tile_nodes, threads=t.threads)
+    return dict(tile_elems=t.tile_elems, tile_nodes=t.tile_nodes, threads=t.threads, ctas_per_sm=t.ctas_per_sm)
 
 
 def solve(p: "_mesh.Problem", steps: int | None = None, precision: int = FM_FP64, **tuning):

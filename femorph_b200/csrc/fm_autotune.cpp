@@ -1,4 +1,6 @@
-// Launch-shape autotuner with a persisted cache.
+// Launch-shape autotuner with a persisted cache: tile size (elements per
+// CTA), threads per CTA and, for VMS, the register budget (the tile kernel
+// variant compiled for 3 or 4 resident 128-thread CTAs an SM, ...).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -9,6 +11,11 @@
 #include <vector>
 
 #include "fm_internal.hpp"
+
+namespace fm {
+int vms_default_ctas(int threads, bool mixed);
+bool vms_variant_exists(int threads, bool mixed, int ctas);
+}  // namespace fm
 
 namespace {
 
@@ -31,16 +38,20 @@ std::string cache_key(fm_problem* const* probs, int n, int device) {
 bool cache_lookup(const char* path, const std::string& key, fm_tuning* t) {
   if (!path) return false;
   std::ifstream f(path);
-  std::string k;
-  int te, tn, th;
-  while (f >> k >> te >> tn >> th)
-    if (k == key) {
-      memset(t, 0, sizeof(*t));
-      t->tile_elems = te;
-      t->tile_nodes = tn;
-      t->threads = th;
-      return true;
-    }
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream l(line);
+    std::string k;
+    int te = 0, tn = 0, th = 0, ctas = 0;
+    if (!(l >> k >> te >> tn >> th) || k != key) continue;
+    l >> ctas;  // absent in lines written before the register budget was tuned
+    memset(t, 0, sizeof(*t));
+    t->tile_elems = te;
+    t->tile_nodes = tn;
+    t->threads = th;
+    t->ctas_per_sm = ctas;
+    return true;
+  }
   return false;
 }
 
@@ -54,7 +65,7 @@ void cache_store(const char* path, const std::string& key, const fm_tuning& t) {
       if (line.compare(0, key.size() + 1, key + " ") != 0 && !line.empty()) lines.push_back(line);
   }
   std::ostringstream l;
-  l << key << " " << t.tile_elems << " " << t.tile_nodes << " " << t.threads;
+  l << key << " " << t.tile_elems << " " << t.tile_nodes << " " << t.threads << " " << t.ctas_per_sm;
   lines.push_back(l.str());
   std::ofstream f(path, std::ios::trunc);
   for (auto& s : lines) f << s << "\n";
@@ -73,18 +84,24 @@ extern "C" int fm_autotune(fm_problem* const* probs, int32_t n, int32_t device, 
   const bool hexa = probs[0]->etype == 8;
   const bool vms = probs[0]->params.solver == FM_SOLVER_VMS;
   struct Cand {
-    int te, tn, th;
+    int te, tn, th, ctas;
   };
   std::vector<Cand> cands;
   if (vms) {
-    for (int th : {128, 256})
-      for (int te : {384, 512, 768, 1024}) cands.push_back({te, FM_MAX_TILE_NODES, th});
+    const bool mixed = probs[0]->params.precision == FM_MIXED;
+    for (int th : {128, 256}) {
+      const int c0 = fm::vms_default_ctas(th, mixed);
+      for (int ctas : {c0, c0 + 1}) {
+        if (!fm::vms_variant_exists(th, mixed, ctas)) continue;
+        for (int te : {384, 512, 768, 1024}) cands.push_back({te, FM_MAX_TILE_NODES, th, ctas});
+      }
+    }
   } else if (hexa) {
     for (int th : {128, 256})
-      for (int te : {128, 256, 384, 512}) cands.push_back({te, 2 * te + 256, th});
+      for (int te : {128, 256, 384, 512}) cands.push_back({te, 2 * te + 256, th, 0});
   } else {
     for (int th : {128, 256})
-      for (int te : {512, 1024, 2048}) cands.push_back({te, te / 2 + 128, th});
+      for (int te : {512, 1024, 2048}) cands.push_back({te, te / 2 + 128, th, 0});
   }
   double best_ms = 1e300;
   fm_tuning bt;
@@ -96,6 +113,7 @@ extern "C" int fm_autotune(fm_problem* const* probs, int32_t n, int32_t device, 
     t.tile_elems = c.te;
     t.tile_nodes = c.tn;
     t.threads = c.th;
+    t.ctas_per_sm = c.ctas;
     fm_batch* b = nullptr;
     if (fm_batch_create(probs, n, &t, device, &b) != FM_OK) continue;
     double ms[2] = {0, 0};

@@ -186,9 +186,9 @@ __host__ __device__ constexpr size_t vms_stage_buffer_bytes() {
   return MIXED ? (size_t)12 * THREADS * sizeof(float) + (size_t)THREADS * 8 : (size_t)16 * THREADS * 8;
 }
 
-template <int THREADS, bool MIXED>
-__global__ void __launch_bounds__(THREADS, THREADS == 128 ? (MIXED ? 4 : 3) : (MIXED ? 2 : 1))
-    vms_tile_kernel(DevBatch B, int tn_max, int inc_max) {
+// MINB: resident CTAs an SM the variant is compiled for (its register budget).
+template <int THREADS, bool MIXED, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int tn_max, int inc_max) {
   using S = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) double sm[];
   const int tn_pad = (tn_max + 1) & ~1;
@@ -477,23 +477,37 @@ size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed) {
   return tn_pad * 12 * sizeof(double) + stage + (size_t)inc_max * sizeof(uint16_t) + (tn_pad + 2) * sizeof(uint16_t);
 }
 
+// Register-budget variants of the tile kernel: (threads, mixed, CTAs an SM).
+// The first variant of each (threads, mixed) pair is the default.
+#define FM_VMS_VARIANTS(X) \
+  X(128, false, 3) X(128, false, 4) X(128, true, 4) X(128, true, 5) X(256, false, 1) X(256, false, 2) X(256, true, 2)
+
+int vms_default_ctas(int threads, bool mixed) { return threads == 256 ? (mixed ? 2 : 1) : (mixed ? 4 : 3); }
+
+bool vms_variant_exists(int threads, bool mixed, int ctas) {
+#define FM_VMS_HAS(T, M, C) \
+  if (threads == T && mixed == M && ctas == C) return true;
+  FM_VMS_VARIANTS(FM_VMS_HAS)
+#undef FM_VMS_HAS
+  return false;
+}
+
 // One dual iteration: tile kernel, then the interface pass (xpack: its first
 // half for a batch of partition parts; launch_vms_xupdate completes it).
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
-                                 bool xpack, cudaStream_t s, cudaEvent_t* ev) {
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int ctas, int iface_blocks,
+                                 bool mixed, bool xpack, cudaStream_t s, cudaEvent_t* ev) {
   const size_t smem = vms_smem_bytes(tn_max, inc_max, threads, mixed);
+  if (ctas <= 0) ctas = vms_default_ctas(threads, mixed);
   if (ev) cudaEventRecord(ev[0], s);
-  if (mixed) {
-    if (threads == 256)
-      vms_tile_kernel<256, true><<<B.n_tiles, 256, smem, s>>>(B, tn_max, inc_max);
-    else
-      vms_tile_kernel<128, true><<<B.n_tiles, 128, smem, s>>>(B, tn_max, inc_max);
-  } else {
-    if (threads == 256)
-      vms_tile_kernel<256, false><<<B.n_tiles, 256, smem, s>>>(B, tn_max, inc_max);
-    else
-      vms_tile_kernel<128, false><<<B.n_tiles, 128, smem, s>>>(B, tn_max, inc_max);
+  bool launched = false;
+#define FM_VMS_LAUNCH(T, M, C)                                                       \
+  if (!launched && threads == T && mixed == M && ctas == C) {                        \
+    vms_tile_kernel<T, M, C><<<B.n_tiles, T, smem, s>>>(B, tn_max, inc_max);         \
+    launched = true;                                                                 \
   }
+  FM_VMS_VARIANTS(FM_VMS_LAUNCH)
+#undef FM_VMS_LAUNCH
+  if (!launched) return cudaErrorInvalidValue;
   if (ev) cudaEventRecord(ev[1], s);
   if (xpack)
     vms_xpack_kernel<<<iface_blocks, 256, 0, s>>>(B);
@@ -529,10 +543,10 @@ cudaError_t vms_configure(int tn_max, int inc_max) {
   if (e != cudaSuccess) return e;
   (void)tn_max;  // sizes are checked against the limit by the caller
   (void)inc_max;
-  e = raise_dyn_smem(vms_tile_kernel<256, false>, optin);
-  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<128, false>, optin);
-  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<256, true>, optin);
-  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<128, true>, optin);
+#define FM_VMS_RAISE(T, M, C) \
+  if (e == cudaSuccess) e = raise_dyn_smem(vms_tile_kernel<T, M, C>, optin);
+  FM_VMS_VARIANTS(FM_VMS_RAISE)
+#undef FM_VMS_RAISE
   return e;
 }
 

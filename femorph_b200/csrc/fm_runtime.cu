@@ -30,8 +30,10 @@ namespace fm {
 const char* last_error();
 size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed);
 cudaError_t vms_configure(int tn_max, int inc_max);
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
-                                 bool xpack, cudaStream_t s, cudaEvent_t* ev);
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int ctas, int iface_blocks,
+                                 bool mixed, bool xpack, cudaStream_t s, cudaEvent_t* ev);
+int vms_default_ctas(int threads, bool mixed);
+bool vms_variant_exists(int threads, bool mixed, int ctas);
 cudaError_t launch_vms_xupdate(const DevBatch& B, int blocks, cudaStream_t s);
 size_t supg_smem_bytes(int tn_max, int inc_max, int npe, int threads);
 cudaError_t supg_configure(size_t smem, int npe);
@@ -890,6 +892,11 @@ static int check_same(fm_problem* const* probs, int n, int* solver, int* npe, in
 }
 
 static int new_batch(int solver, int npe, int prec, const fm_tuning* tuning, int32_t device, fm_batch** out) {
+  if (tuning && tuning->ctas_per_sm != 0 && solver == FM_SOLVER_VMS) {
+    const int th = tuning->threads == 256 ? 256 : 128;
+    if (!vms_variant_exists(th, prec == FM_MIXED, tuning->ctas_per_sm))
+      return fail(FM_ERR_INVALID, "no VMS tile kernel variant for this ctas_per_sm, threads and precision");
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FM_ERR_NODEVICE, "no CUDA device");
   if (device < 0 || device >= ndev) return fail(FM_ERR_INVALID, "bad device ordinal");
@@ -903,6 +910,7 @@ static int new_batch(int solver, int npe, int prec, const fm_tuning* tuning, int
   b->npe = npe;
   b->precision = prec;
   b->threads = b->tune.threads;
+  if (solver == FM_SOLVER_VMS && b->tune.ctas_per_sm == 0) b->tune.ctas_per_sm = vms_default_ctas(b->threads, prec == FM_MIXED);
   b->graph_steps = b->tune.graph_steps;
   *out = b;
   return FM_OK;
@@ -1083,8 +1091,8 @@ int fm_batch_destroy(fm_batch* b) {
 // again after it).
 static cudaError_t launch_first(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
   if (b->solver == FM_SOLVER_VMS)
-    return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->precision == FM_MIXED,
-                                b->exchange, s, ev);
+    return launch_vms_iteration(b->D, b->tn_max, b->inc_max, b->threads, b->tune.ctas_per_sm, b->iface_blocks,
+                                b->precision == FM_MIXED, b->exchange, s, ev);
   return launch_supg_step(b->D, b->tn_max, b->inc_max, b->threads, b->iface_blocks, b->npe, b->precision == FM_MIXED,
                           b->exchange,
                           s, ev);

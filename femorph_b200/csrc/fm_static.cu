@@ -35,8 +35,8 @@
 namespace fm {
 cudaError_t vms_configure(int tn_max, int inc_max);
 size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed);
-cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, bool mixed,
-                                 bool xpack, cudaStream_t s, cudaEvent_t* ev);
+cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int threads, int ctas, int iface_blocks,
+                                 bool mixed, bool xpack, cudaStream_t s, cudaEvent_t* ev);
 }  // namespace fm
 
 using namespace fm;
@@ -318,7 +318,7 @@ extern "C" int fm_vms_solve_static(fm_problem* p, int32_t nsteps, int32_t device
   CKS(cudaGetLastError());
   const int iface_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((D.n_iface + 255) / 256, 148 * 8));
   for (int32_t it = 0; it < target; ++it)
-    CKS(launch_vms_iteration(D, tn_max, inc_max, threads, iface_blocks, false, false, s, nullptr));
+    CKS(launch_vms_iteration(D, tn_max, inc_max, threads, 0, iface_blocks, false, false, s, nullptr));
   double* du = reinterpret_cast<double*>(base + o.out_u);
   double* dp = reinterpret_cast<double*>(base + o.out_p);
   static_gather_kernel<<<blocks, 256, 0, s>>>(D, reinterpret_cast<const int32_t*>(base + o.in_node_new), (int32_t)N,

@@ -110,7 +110,12 @@ typedef struct fm_tuning {
   int32_t tile_nodes;      /* max distinct nodes per tile (shared memory) */
   int32_t threads;         /* threads per CTA */
   int32_t graph_steps;     /* time steps captured per CUDA graph (0: no graph) */
-  int32_t reserved[4];
+  int32_t ctas_per_sm;     /* VMS register budget: the tile kernel variant compiled for at least this
+                            * many resident CTAs an SM (registers a thread <= 65536 / (threads x
+                            * ctas_per_sm)); 0 takes the default.  128 threads: FP64 3 (default) or 4,
+                            * mixed 4 (default) or 5; 256 threads: FP64 1 (default) or 2, mixed 2.
+                            * SUPG ignores it. */
+  int32_t reserved[3];
 } fm_tuning;
 
 /* Pool capacities of a batch created empty (fm_batch_create_empty).  The

@@ -196,3 +196,12 @@ def test_checkpoint_needs_a_batch(tmp_path):
         assert ei.value.code == api.FM_ERR_INVALID
     assert not os.path.exists(path)
     q.close()
+
+
+def test_unknown_register_budget_rejected_before_device():
+    g = api.GpuProblem(mesh.cavity(2, seed=0, steps=1))
+    for threads, ctas in ((128, 7), (256, 3), (128, 1)):
+        with pytest.raises(api.FmError) as ei:
+            api.Batch([g], threads=threads, ctas_per_sm=ctas)
+        assert ei.value.code == api.FM_ERR_INVALID
+    g.close()

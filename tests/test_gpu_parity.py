@@ -306,3 +306,29 @@ def test_device_extrema_and_supg_log_stats():
     assert st[7] > 0 and st[8] < 1e3 * E.max()
     b.close()
     g.close()
+
+
+@pytest.mark.parametrize("threads,precision,ctas", [(128, api.FM_FP64, 4), (256, api.FM_FP64, 2),
+                                                   (128, api.FM_MIXED, 5)])
+def test_register_budget_variants(threads, precision, ctas):
+    """The tile kernel compiled for a tighter register budget (more resident
+    CTAs an SM, spilling where it must) does the same arithmetic: bitwise the
+    default variant's state, and the FP64 one within the per-step tolerance
+    of the oracle."""
+    p = mesh.cavity(6, seed=41, steps=6, lid=0.8)
+    out = []
+    for c in (0, ctas):
+        g = api.GpuProblem(p, precision)
+        b = api.Batch([g], threads=threads, tile_elems=384, ctas_per_sm=c)
+        b.step(6)
+        b.sync()
+        out.append(g.state())
+        b.close()
+        g.close()
+    for x, y in zip(out[0], out[1]):
+        assert np.array_equal(x, y)
+    if precision == api.FM_FP64:
+        o = oracle_b.OracleSolve(p)
+        o.step(6)
+        st, _, _, _ = o.state()
+        assert rel(out[1][0], st[:, :3]) <= TOL_STEP and rel(out[1][1], st[:, 3]) <= TOL_STEP
