@@ -106,7 +106,25 @@ struct Session {
 
 }  // namespace
 
-femVMSExplicitFluidSolverGPU::femVMSExplicitFluidSolverGPU(int device, bool mixed) : device_(device), mixed_(mixed) {}
+femVMSExplicitFluidSolverGPU::femVMSExplicitFluidSolverGPU(int device, bool mixed, bool log)
+    : device_(device), mixed_(mixed), log_(log) {}
+
+namespace {
+// Prints the queued diagnostics rows as the reference's log lines
+// (src/femVMSExplicitFluidSolver.cpp:1215).  Its time loop counts steps from
+// 1 (:1025), so the header it guards with loopTime == 0 (:1211-1214) is
+// never printed, and neither is it here.
+void print_vms_log(fm_problem* p) {
+  int32_t n = 0;
+  fm_check(fm_problem_vms_log(p, nullptr, 0, &n));
+  std::vector<double> rows((size_t)n * 6);
+  if (n > 0) fm_check(fm_problem_vms_log(p, rows.data(), n, &n));
+  for (int32_t i = 0; i < n; ++i) {
+    const double* r = &rows[(size_t)i * 6];
+    printf("%4d.%-4d %20.8f %20.3e %20.3e %10.3f\n", (int)r[0] + 1, (int)r[1], r[2], r[3], r[4], r[5]);
+  }
+}
+}  // namespace
 
 // femVMSExplicitFluidSolver::solve (src/femVMSExplicitFluidSolver.cpp:842-1334).
 void femVMSExplicitFluidSolverGPU::solve(femModel* model) {
@@ -128,8 +146,9 @@ void femVMSExplicitFluidSolverGPU::solve(femModel* model) {
   Session s;
   fm_check(fm_problem_create(&mesh, &bc, &prm, nullptr, &s.p));
   fm_check(fm_batch_create(&s.p, 1, nullptr, device_, &s.b));
+  if (log_) fm_check(fm_batch_set_diagnostics(s.b, 1));
   const size_t N = (size_t)mesh.n_nodes, E = (size_t)mesh.n_elems;
-  std::vector<double> u(N * 3), pr(N), sg(E * 3);
+  std::vector<double> u(N * 3), pr(N), sg(E * 3), ru(log_ ? E * 3 : 0), rp(log_ ? E : 0);
   fm_check(fm_problem_get_state(s.p, u.data(), pr.data(), nullptr, nullptr));
   model->resultList.push_back(make_result("velocity", frNode, 3, u.data(), N, 3));
   model->resultList.push_back(make_result("pressure", frNode, 1, pr.data(), N, 1));
@@ -141,16 +160,18 @@ void femVMSExplicitFluidSolverGPU::solve(femModel* model) {
     while (next < steps && !is_save_step(next, model->saveEvery)) ++next;
     fm_check(fm_batch_step(s.b, (int32_t)(next - done), nullptr));
     fm_check(fm_batch_sync(s.b));
+    if (log_) print_vms_log(s.p);
     done = next;
     if (is_save_step(done, model->saveEvery)) {
       fm_check(fm_problem_get_state(s.p, u.data(), pr.data(), sg.data(), nullptr));
+      if (log_) fm_check(fm_problem_vms_residuals(s.p, ru.data(), rp.data()));
       model->resultList.clear();
       model->resultList.push_back(make_result("velocity", frNode, 3, u.data(), N, 3));
       model->resultList.push_back(make_result("pressure", frNode, 1, pr.data(), N, 1));
-      // res_v / res_p: the reference's centroid averages of a partially
-      // assembled residual (element-order dependent diagnostics), not kept.
-      model->resultList.push_back(make_result("res_v", frElement, 3, nullptr, E, 3));
-      model->resultList.push_back(make_result("res_p", frElement, 1, nullptr, E, 1));
+      // res_v / res_p: centroid averages of the partially assembled residual
+      // of the last dual iteration (zero without the diagnostics)
+      model->resultList.push_back(make_result("res_v", frElement, 3, log_ ? ru.data() : nullptr, E, 3));
+      model->resultList.push_back(make_result("res_p", frElement, 1, log_ ? rp.data() : nullptr, E, 1));
       model->resultList.push_back(make_result("subgrid_u", frElement, 3, sg.data(), E, 3));
       model->resultList.push_back(make_result("subgrid_p", frElement, 1, nullptr, E, 1));
       model->ExportToVTKLegacy(std::string("out_Step_" + femUtils::intToStr(done) + ".vtk"), false);

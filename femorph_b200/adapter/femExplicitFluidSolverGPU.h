@@ -19,12 +19,15 @@
 
 class femVMSExplicitFluidSolverGPU : public femSolver {
  public:
-  femVMSExplicitFluidSolverGPU(int device = 0, bool mixed = false);
+  // log: print the reference's per-dual-iteration line and write its res_v /
+  // res_p fields (device diagnostics, which slow the solve); off: neither.
+  femVMSExplicitFluidSolverGPU(int device = 0, bool mixed = false, bool log = true);
   virtual void solve(femModel* model);
 
  private:
   int device_;
   bool mixed_;
+  bool log_;
 };
 
 class femSUPGExplicitFluidSolverGPU : public femSolver {

@@ -34,6 +34,7 @@ SYMBOLS = [
     "fm_partition_elements", "fm_problem_partition", "fm_problem_part_info", "fm_problem_part_map",
     "fm_problem_write_vtu", "fm_batch_exchange_account", "fm_batch_exchange_buffers", "fm_batch_exchange_begin",
     "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
+    "fm_batch_set_diagnostics", "fm_problem_vms_log", "fm_problem_vms_residuals",
 ]
 
 
@@ -100,6 +101,9 @@ def lib():
         L.fm_problem_write_vtk_binary.argtypes = [P, C.c_char_p]
         L.fm_problem_write_vtu.argtypes = [P, C.c_char_p]
         L.fm_problem_checkpoint.argtypes = [P, C.c_char_p]
+        L.fm_batch_set_diagnostics.argtypes = [P, C.c_int32]
+        L.fm_problem_vms_log.argtypes = [P, P, C.c_int32, P]
+        L.fm_problem_vms_residuals.argtypes = [P, P, P]
         L.fm_problem_restore.argtypes = [P, C.c_char_p]
         L.fm_problem_get_mass.argtypes = [P, P]
         L.fm_batch_last_timing.argtypes = [P, P, P]
@@ -217,6 +221,22 @@ class GpuProblem:
         """VTK XML UnstructuredGrid with raw appended binary arrays."""
         check(lib().fm_problem_write_vtu(self.h, path.encode()))
 
+    def vms_log(self):
+        """Queued VMS diagnostics rows (rows, 6): step, dual iteration, time,
+        max centroid |res_u|, max |res_p|, CFL; the queue is emptied."""
+        n = C.c_int32()
+        check(lib().fm_problem_vms_log(self.h, None, 0, C.byref(n)))
+        rows = np.zeros((n.value, 6))
+        if n.value:
+            check(lib().fm_problem_vms_log(self.h, _p(rows), n.value, C.byref(n)))
+        return rows[: n.value]
+
+    def vms_residuals(self):
+        """Centroid residuals of the last recorded iteration: (res_u (E,3), res_p (E,))."""
+        ru, rp = np.zeros((self.n_elems, 3)), np.zeros(self.n_elems)
+        check(lib().fm_problem_vms_residuals(self.h, _p(ru), _p(rp)))
+        return ru, rp
+
     def checkpoint(self, path: str) -> None:
         """Writes the problem's evolving state (it must sit in a batch) to a
         binary restart file."""
@@ -306,6 +326,11 @@ class Batch:
 
     def step(self, n: int = 1, stream=None) -> None:
         check(lib().fm_batch_step(self.h, int(n), stream))
+
+    def set_diagnostics(self, enable: bool = True) -> None:
+        """VMS: record the reference's log row and centroid residuals every
+        dual iteration (GpuProblem.vms_log / vms_residuals)."""
+        check(lib().fm_batch_set_diagnostics(self.h, 1 if enable else 0))
 
     def step_ragged(self, steps, stream=None) -> None:
         a = np.ascontiguousarray(steps, np.int32)

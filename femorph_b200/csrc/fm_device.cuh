@@ -25,6 +25,7 @@ struct DevBatch {
   float* sdus32;                  // VMS mixed: FP32 subscales [12][E]
   double* el_lam;                 // SUPG per-element lambda / regime (diagnostics)
   double* el_reg;
+  double* diag_res;               // VMS diagnostics on: [16][E] residual entries of the last iteration (else null)
   int64_t E;
   // tiles
   const TileMeta* tiles;

@@ -154,6 +154,12 @@ struct fm_problem {
   fm_batch* batch = nullptr;
   int32_t index = -1;
   int64_t steps_done = 0;
+  // VMS diagnostics (fm_batch_set_diagnostics): queued log rows, 6 doubles
+  // each, the smallest element length, and the last step whose time was formed
+  std::vector<double> diag_rows;
+  double diag_min_h = 0.0;
+  int64_t diag_step = -1;
+  double diag_time = 0.0;
 };
 
 namespace fm {

@@ -17,6 +17,7 @@
 // applies the same node update, then advances the problems' iteration.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "fm_device.cuh"
@@ -328,6 +329,10 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
       double lres[4][4];
       vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, precise, s_rec, sd_in, pq, pending, first_dual, inv_dt,
                             c1nu, nu4, lres);
+      if (B.diag_res) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) B.diag_res[(int64_t)r * E + tm.elem_begin + le] = lres[r >> 2][r & 3];
+      }
       // FP64: this thread's column held only its own inputs, read above
 #pragma unroll
       for (int r = 0; r < 16; ++r) R[r * THREADS + tid] = lres[r >> 2][r & 3];
@@ -468,6 +473,103 @@ __global__ void vms_xupdate_kernel(DevBatch B) {
     if (status != FM_OK) B.pstate[pidx].status = status;
   }
   finish_iteration(B);
+}
+
+// ---- diagnostics of the reference's VMS log line and res_v / res_p output ----
+// eval_centroid_residuals (src/femVMSExplicitFluidSolver.cpp:699-711) reads
+// the nodal residual right after each element's assembly, so element e sees,
+// at each of its nodes, the sum of the contributions of the elements up to e
+// in the reference's element order.  ent lists, per problem node, its
+// (batch element slot * 4 + corner) entries in that order; cres receives the
+// running sum at every entry.
+__global__ void vms_diag_prefix_kernel(const double* res, int64_t E, const int32_t* off, const int32_t* ent,
+                                       int32_t n_nodes, double* cres) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_nodes; i += gridDim.x * blockDim.x) {
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j = off[i]; j < off[i + 1]; ++j) {
+      const int32_t q = ent[j];
+      const int64_t k = q >> 2;
+      const int c = q & 3;
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        a[d] += res[(int64_t)(c * 4 + d) * E + k];
+        cres[(k * 4 + c) * 4 + d] = a[d];
+      }
+    }
+  }
+}
+
+// Centroid residuals (the quarter-weighted running sums at the element's four
+// nodes, in corner order) into el (problem element order, 4 values each), and
+// the block maxima of |res_u| and |res_p| (eval_residual_norms, src lines
+// 774-793) into blk[2 * block].
+__global__ void vms_diag_centroid_kernel(const double* cres, const int32_t* eo, int64_t eb, int64_t ec, double* el,
+                                         double* blk) {
+  __shared__ double s_u[256], s_p[256];
+  double mu = 0.0, mp = 0.0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < ec; k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t e = eo[k];
+    if (e < 0) continue;
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* c = cres + (eb + k) * 16;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int d = 0; d < 4; ++d) r[d] += c[a * 4 + d] * 0.25;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) el[(int64_t)e * 4 + d] = r[d];
+    const double nu = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    mu = nu > mu ? nu : mu;
+    mp = fabs(r[3]) > mp ? fabs(r[3]) : mp;
+  }
+  s_u[threadIdx.x] = mu;
+  s_p[threadIdx.x] = mp;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s_u[threadIdx.x] = fmax(s_u[threadIdx.x], s_u[threadIdx.x + w]);
+      s_p[threadIdx.x] = fmax(s_p[threadIdx.x], s_p[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    blk[2 * blockIdx.x] = s_u[0];
+    blk[2 * blockIdx.x + 1] = s_p[0];
+  }
+}
+
+// Largest nodal velocity magnitude of the state before BCs (the CFL of the
+// reference's log line reads sol_n after update_dual_solution, src lines
+// 1202-1208); block maxima into blk[block].
+__global__ void vms_diag_vmax_kernel(DevBatch B, int64_t nb, int64_t n, double* blk) {
+  __shared__ double s_m[256];
+  double m = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = nb + i;
+    const bool bc = B.node_bc[g] >= 0;
+    const double u = bc ? B.pu[g] : B.su[g], v = bc ? B.pv[g] : B.sv[g], w = bc ? B.pw[g] : B.sw[g];
+    const double a = sqrt(u * u + v * v + w * w);
+    m = a > m ? a : m;
+  }
+  s_m[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) s_m[threadIdx.x] = fmax(s_m[threadIdx.x], s_m[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) blk[blockIdx.x] = s_m[0];
+}
+
+// One problem's diagnostics after an iteration: out[0 .. 2*blocks) the
+// centroid maxima per block, out[2*blocks .. 3*blocks) the velocity maxima.
+cudaError_t launch_vms_diagnostics(const DevBatch& B, const double* cres_buf, const int32_t* off, const int32_t* ent,
+                                   int32_t n_nodes, const int32_t* eo, int64_t eb, int64_t ec, int64_t nb,
+                                   double* el, double* out, int blocks, cudaStream_t s) {
+  const int pb = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n_nodes + 255) / 256, 148 * 8));
+  vms_diag_prefix_kernel<<<pb, 256, 0, s>>>(B.diag_res, B.E, off, ent, n_nodes, const_cast<double*>(cres_buf));
+  vms_diag_centroid_kernel<<<blocks, 256, 0, s>>>(cres_buf, eo, eb, ec, el, out);
+  vms_diag_vmax_kernel<<<blocks, 256, 0, s>>>(B, nb, n_nodes, out + 2 * blocks);
+  return cudaGetLastError();
 }
 
 size_t vms_smem_bytes(int tn_max, int inc_max, int threads, bool mixed) {

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <string>
@@ -35,6 +36,9 @@ cudaError_t launch_vms_iteration(const DevBatch& B, int tn_max, int inc_max, int
 int vms_default_ctas(int threads, bool mixed);
 bool vms_variant_exists(int threads, bool mixed, int ctas);
 cudaError_t launch_vms_xupdate(const DevBatch& B, int blocks, cudaStream_t s);
+cudaError_t launch_vms_diagnostics(const DevBatch& B, const double* cres_buf, const int32_t* off, const int32_t* ent,
+                                   int32_t n_nodes, const int32_t* eo, int64_t eb, int64_t ec, int64_t nb,
+                                   double* el, double* out, int blocks, cudaStream_t s);
 size_t supg_smem_bytes(int tn_max, int inc_max, int npe, int threads);
 cudaError_t supg_configure(size_t smem, int npe);
 cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int inc_max, int threads, int iface_blocks, int npe, bool mixed,
@@ -163,7 +167,15 @@ struct Placement {
   int64_t len[P_COUNT] = {0};
   int32_t tn_max = 0, inc_max = 0;
   std::shared_ptr<Layout> L;  // the problem's layout (node and element numbering)
+  // VMS diagnostics (device, own allocations): per problem node its
+  // (element slot * 4 + corner) entries in the problem's element order, the
+  // problem element of each slot, and the centroid residuals (E x 4)
+  int32_t *dg_off = nullptr, *dg_ent = nullptr, *dg_eo = nullptr;
+  double* dg_el = nullptr;
 };
+
+// Blocks of the diagnostics reductions.
+constexpr int DIAG_BLOCKS = 148 * 4;
 
 }  // namespace fm
 
@@ -200,6 +212,11 @@ struct fm_batch {
   int32_t x_slices = 0, x_blocks = 1;
   int64_t x_n = 0;
   std::vector<int32_t> x_slice_of;  // by problem slot
+  // VMS diagnostics (fm_batch_set_diagnostics): residual entries of the last
+  // iteration (16 x element slots), running sums (element slots x 16),
+  // per-block maxima and their pinned host copy
+  bool diag = false;
+  double *d_diag_res = nullptr, *d_cres = nullptr, *d_diag_out = nullptr, *h_diag = nullptr;
 };
 
 #define CK(x)                                                                                     \
@@ -461,6 +478,78 @@ static void refresh_extent(fm_batch* b) {
 
 // Places a prepared problem into the pools; FM_ERR_OOM if some pool has no
 // room (nothing is changed then).
+// ---- VMS diagnostics resources ----
+static void diag_free_problem(Placement& pl) {
+  cudaFree(pl.dg_off);
+  cudaFree(pl.dg_ent);
+  cudaFree(pl.dg_eo);
+  cudaFree(pl.dg_el);
+  pl.dg_off = pl.dg_ent = pl.dg_eo = nullptr;
+  pl.dg_el = nullptr;
+}
+
+static void diag_free(fm_batch* b) {
+  for (Placement& pl : b->slots) diag_free_problem(pl);
+  cudaFree(b->d_diag_res);
+  cudaFree(b->d_cres);
+  cudaFree(b->d_diag_out);
+  if (b->h_diag) cudaFreeHost(b->h_diag);
+  b->d_diag_res = b->d_cres = b->d_diag_out = b->h_diag = nullptr;
+  b->D.diag_res = nullptr;
+  b->diag = false;
+}
+
+// The problem's reference-order incidence lists and output array.
+static int diag_prepare_problem(fm_batch* b, Placement& pl) {
+  const fm_problem* p = pl.p;
+  const Layout& L = *pl.L;
+  const auto& eo = L.elem_old[0];
+  const int64_t N = p->N, E = p->E, EC = (int64_t)eo.size();
+  if ((pl.off[P_ELEM] + EC) * 4 >= (int64_t)INT32_MAX)
+    return fail(FM_ERR_INVALID, "diagnostics index element slots in 32 bits: batch too large");
+  std::vector<int32_t> slot_of(E, -1), off(N + 1, 0), ent((size_t)E * 4), eo32(EC);
+  for (int64_t k = 0; k < EC; ++k) {
+    eo32[k] = eo[k];
+    if (eo[k] >= 0) slot_of[eo[k]] = (int32_t)(pl.off[P_ELEM] + k);
+  }
+  for (int64_t q = 0; q < E * 4; ++q) off[p->conn[q] + 1]++;
+  for (int64_t i = 0; i < N; ++i) off[i + 1] += off[i];
+  std::vector<int32_t> pos(off.begin(), off.end() - 1);
+  for (int64_t e = 0; e < E; ++e)
+    for (int a = 0; a < 4; ++a) ent[pos[p->conn[e * 4 + a]]++] = slot_of[e] * 4 + a;
+  // smallest pow(6 V, 1/3) over the elements (src/femVMSExplicitFluidSolver.cpp:947-952)
+  double hmin = std::numeric_limits<double>::max();
+  for (int64_t e = 0; e < E; ++e) {
+    const double* x0 = &p->coords[(size_t)p->conn[e * 4] * 3];
+    double j[3][3];
+    for (int k = 0; k < 3; ++k) {
+      const double* xk = &p->coords[(size_t)p->conn[e * 4 + k + 1] * 3];
+      for (int i = 0; i < 3; ++i) j[i][k] = xk[i] - x0[i];
+    }
+    const double det = j[0][0] * (j[1][1] * j[2][2] - j[2][1] * j[1][2]) +
+                       j[0][1] * (j[2][0] * j[1][2] - j[1][0] * j[2][2]) +
+                       j[0][2] * (j[1][0] * j[2][1] - j[2][0] * j[1][1]);
+    hmin = std::min(hmin, std::pow(6.0 * (det / 6.0), 1.0 / 3.0));
+  }
+  pl.p->diag_min_h = hmin;
+  pl.p->diag_step = -1;
+  auto al = [&](void** q, size_t bytes) { return cudaMalloc(q, bytes ? bytes : 16); };
+  cudaError_t e = al((void**)&pl.dg_off, (N + 1) * sizeof(int32_t));
+  if (e == cudaSuccess) e = al((void**)&pl.dg_ent, (size_t)E * 4 * sizeof(int32_t));
+  if (e == cudaSuccess) e = al((void**)&pl.dg_eo, EC * sizeof(int32_t));
+  if (e == cudaSuccess) e = al((void**)&pl.dg_el, (size_t)E * 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(pl.dg_off, off.data(), (N + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pl.dg_ent, ent.data(), (size_t)E * 4 * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pl.dg_eo, eo32.data(), EC * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(pl.dg_el, 0, (size_t)E * 4 * sizeof(double));
+  if (e != cudaSuccess) {
+    diag_free_problem(pl);
+    return fail(e == cudaErrorMemoryAllocation ? FM_ERR_OOM : FM_ERR_CUDA,
+                std::string("diagnostics: ") + cudaGetErrorString(e));
+  }
+  return FM_OK;
+}
+
 static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) {
   const Layout& L = *Lp;
   Placement pl;
@@ -690,6 +779,10 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
   p->steps_done = 0;
   b->slots[ps] = std::move(pl);
   refresh_extent(b);
+  if (b->diag) {
+    r = diag_prepare_problem(b, b->slots[ps]);
+    if (r) return r;
+  }
   return configure(b);
 }
 
@@ -1060,6 +1153,7 @@ int fm_batch_remove(fm_batch* b, fm_problem* p) {
   CK(cudaMemset(D.pstate + ps, 0, sizeof(DevProbState)));
   for (int k = 0; k < P_COUNT; ++k) b->pools[k].release(pl.off[k], pl.len[k]);
   b->iters[ps] = 0;
+  diag_free_problem(pl);
   pl = Placement();
   p->batch = nullptr;
   p->index = -1;
@@ -1076,6 +1170,7 @@ int fm_batch_destroy(fm_batch* b) {
       pl.p->batch = nullptr;
       pl.p->index = -1;
     }
+  diag_free(b);
   release_all(b);
   delete b;
   return FM_OK;
@@ -1106,6 +1201,49 @@ static cudaError_t launch_one(fm_batch* b, cudaStream_t s, cudaEvent_t* ev) {
   e = launch_second(b, s);
   if (ev) cudaEventRecord(ev[2], s);
   return e;
+}
+
+// VMS diagnostics after iteration `it` of a launch sequence: for every
+// problem that took part, the reference's log row (step, dual iteration,
+// time, max centroid |res_u|, max |res_p|, CFL) is queued on the problem.
+static int record_diagnostics(fm_batch* b, const std::vector<int32_t>& add_iters, int it, cudaStream_t s) {
+  const int n = (int)add_iters.size();
+  for (int i = 0; i < n; ++i) {
+    Placement& pl = b->slots[i];
+    fm_problem* p = pl.p;
+    if (!p || it >= add_iters[i] || !pl.dg_el) continue;
+    const int64_t EC = (int64_t)pl.L->elem_old[0].size();
+    cudaError_t e = launch_vms_diagnostics(b->D, b->d_cres, pl.dg_off, pl.dg_ent, (int32_t)p->N, pl.dg_eo,
+                                           pl.off[P_ELEM], EC, pl.off[P_NODE], pl.dg_el, b->d_diag_out, DIAG_BLOCKS, s);
+    if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("diagnostics: ") + cudaGetErrorString(e));
+    CK(cudaMemcpyAsync(b->h_diag, b->d_diag_out, 3 * DIAG_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double mu = 0.0, mp = 0.0, mv = 0.0;
+    for (int k = 0; k < DIAG_BLOCKS; ++k) {
+      mu = std::max(mu, b->h_diag[2 * k]);
+      mp = std::max(mp, b->h_diag[2 * k + 1]);
+      mv = std::max(mv, b->h_diag[2 * DIAG_BLOCKS + k]);
+    }
+    // the iteration just done; the step's time accumulates like the
+    // reference's currentTime (src/femVMSExplicitFluidSolver.cpp:1028)
+    const int64_t per = std::max(0, p->params.tot_dual_steps) + 1;
+    const int64_t idx = (int64_t)b->iters[i] + it;
+    const int64_t step = idx / per;
+    const double dt = p->params.time_step;
+    if (step != p->diag_step) {
+      if (step == p->diag_step + 1 && p->diag_step >= 0) {
+        p->diag_time += dt;
+      } else {
+        double t = 0.0;
+        for (int64_t q = 0; q <= step; ++q) t += dt;
+        p->diag_time = t;
+      }
+      p->diag_step = step;
+    }
+    const double row[6] = {(double)step, (double)(idx % per + 1), p->diag_time, mu, mp, mv * dt / p->diag_min_h};
+    p->diag_rows.insert(p->diag_rows.end(), row, row + 6);
+  }
+  return FM_OK;
 }
 
 // Sets per-slot targets (iterations) and launches enough iterations.  With
@@ -1144,7 +1282,7 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
   // (the per-slot targets live in device memory, so the same graph serves
   // every block and every ragged step pattern; it is re-captured when the
   // batch's extent changes)
-  if (!prof && b->graph_steps > 0 && maxit >= b->graph_steps) {
+  if (!prof && !b->diag && b->graph_steps > 0 && maxit >= b->graph_steps) {
     if (!b->graph) {
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1170,6 +1308,10 @@ static int run_iterations(fm_batch* b, const std::vector<int32_t>& add_iters, cu
     cudaError_t e = launch_one(b, s, ev);
     if (e != cudaSuccess) return fail(FM_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     launches += b->exchange ? 3 : 2;
+    if (b->diag) {
+      int r = record_diagnostics(b, add_iters, it, s);
+      if (r) return r;
+    }
   }
   CK(cudaEventRecord(b->ev1, s));
   if (prof) {
@@ -1770,6 +1912,87 @@ int fm_problem_restore(fm_problem* p, const char* path) {
   CK(cudaMemcpy(const_cast<int32_t*>(b->D.target) + ps, &h.iter, sizeof(int32_t), cudaMemcpyHostToDevice));
   b->iters[ps] = h.iter;
   p->steps_done = h.steps_done;
+  return FM_OK;
+}
+
+}  // extern "C"
+
+// ---- VMS diagnostics (the reference's log line and res_v / res_p) ----
+extern "C" {
+
+int fm_batch_set_diagnostics(fm_batch* b, int32_t enable) {
+  NvtxRange nvtx_range("fm_batch_set_diagnostics");
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  if (b->solver != FM_SOLVER_VMS) return fail(FM_ERR_INVALID, "diagnostics are those of the VMS solver");
+  if (b->exchange) return fail(FM_ERR_INVALID, "diagnostics are not kept for partition parts");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  // captured graphs hold the batch view with or without the residual buffer
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (!enable) {
+    diag_free(b);
+    return FM_OK;
+  }
+  if (b->diag) return FM_OK;
+  const size_t ecap = (size_t)std::max<int64_t>(b->D.E, 1);
+  cudaError_t e = cudaMalloc((void**)&b->d_diag_res, ecap * 16 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_cres, ecap * 16 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_diag_out, 3 * DIAG_BLOCKS * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_diag, 3 * DIAG_BLOCKS * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(b->d_diag_res, 0, ecap * 16 * sizeof(double));
+  if (e != cudaSuccess) {
+    diag_free(b);
+    return fail(e == cudaErrorMemoryAllocation ? FM_ERR_OOM : FM_ERR_CUDA,
+                std::string("diagnostics: ") + cudaGetErrorString(e));
+  }
+  b->D.diag_res = b->d_diag_res;
+  b->diag = true;
+  for (Placement& pl : b->slots)
+    if (pl.p) {
+      int r = diag_prepare_problem(b, pl);
+      if (r) {
+        diag_free(b);
+        return r;
+      }
+    }
+  return FM_OK;
+}
+
+int fm_problem_vms_log(fm_problem* p, double* rows, int32_t max_rows, int32_t* n_rows) {
+  if (!p || !n_rows) return fail(FM_ERR_INVALID, "null argument");
+  const int64_t queued = (int64_t)p->diag_rows.size() / 6;
+  if (!rows) {
+    *n_rows = (int32_t)std::min<int64_t>(queued, INT32_MAX);
+    return FM_OK;
+  }
+  const int64_t n = std::min<int64_t>(queued, std::max(0, max_rows));
+  if (n > 0) {
+    memcpy(rows, p->diag_rows.data(), (size_t)n * 6 * sizeof(double));
+    p->diag_rows.erase(p->diag_rows.begin(), p->diag_rows.begin() + n * 6);
+  }
+  *n_rows = (int32_t)n;
+  return FM_OK;
+}
+
+int fm_problem_vms_residuals(fm_problem* p, double* res_u, double* res_p) {
+  if (!p) return fail(FM_ERR_INVALID, "null problem");
+  fm_batch* b = p->batch;
+  if (!b || !b->diag) return fail(FM_ERR_INVALID, "problem is not in a batch with diagnostics on");
+  const Placement& pl = b->slots[p->index];
+  if (!pl.dg_el) return fail(FM_ERR_INVALID, "no diagnostics for this problem");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  const int64_t E = p->E;
+  std::vector<double> el((size_t)E * 4);
+  CK(cudaMemcpy(el.data(), pl.dg_el, el.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int64_t e = 0; e < E; ++e) {
+    if (res_u)
+      for (int c = 0; c < 3; ++c) res_u[e * 3 + c] = el[(size_t)e * 4 + c];
+    if (res_p) res_p[e] = el[(size_t)e * 4 + 3];
+  }
   return FM_OK;
 }
 

@@ -294,6 +294,24 @@ FM_API int fm_problem_velocity_extrema(fm_problem* p, double* out);
  * prints its log keeps that running maximum.) */
 FM_API int fm_problem_supg_log_stats(fm_problem* p, double* out);
 
+/* VMS diagnostics: the reference's per-dual-iteration log line and its
+ * res_v / res_p output (femVMSExplicitFluidSolver.cpp:699-711,
+ * 774-793, 1202-1215; the centroid residuals are quarter-weighted nodal
+ * residuals read right after each element's assembly, i.e. running sums in
+ * the reference's element order, rebuilt on the device from the
+ * iteration's element residuals).  fm_batch_set_diagnostics(b, 1) makes
+ * every later dual iteration of the batch's VMS problems record them
+ * (slower: no CUDA graphs, extra passes and a host read per iteration;
+ * 0 turns it off and frees the buffers).  fm_problem_vms_log pops up to
+ * max_rows queued rows, oldest first, 6 doubles each: step (0-based),
+ * dual iteration (1-based), time, max centroid |res_u|, max |res_p|, CFL;
+ * rows NULL only reports the queued count in n_rows.
+ * fm_problem_vms_residuals copies the last recorded iteration's centroid
+ * residuals (res_u n_elems x 3, res_p n_elems; either may be NULL). */
+FM_API int fm_batch_set_diagnostics(fm_batch* b, int32_t enable);
+FM_API int fm_problem_vms_log(fm_problem* p, double* rows, int32_t max_rows, int32_t* n_rows);
+FM_API int fm_problem_vms_residuals(fm_problem* p, double* res_u, double* res_p);
+
 /* Device status of one problem of a batch (FM_OK, FM_ERR_DIVERGED,
  * FM_ERR_TABLE, FM_ERR_TIMEOUT); waits for the batch's stream. */
 FM_API int fm_problem_status(fm_problem* p);
