@@ -180,43 +180,54 @@ def run_ours(args, rank, world, local_rank, dist):
     g.close()
     res = dict(E=E, N=N, ms=ms, launches=launches, clocks=clk.summary(), kprof=kprof, klaunch=klaunch, layout=lay,
                state=state, steps_total=args.warmup + args.steps + min(args.steps, 50), p=p)
-    # end to end through the C ABI: host buffers in, state out
+    # end to end through the C ABI: the whole solve of the configured
+    # problem (its own step count) from host buffers to the state read back
     if rank == 0:
+        e2e_steps = p.steps
         t0 = time.perf_counter()
         g2 = api.GpuProblem(p, prec)
         b2 = api.Batch([g2], device=local_rank, **tune)
-        b2.step(args.steps)
+        b2.step(e2e_steps)
         b2.sync()
         u, pr, _, _ = g2.state(elements=False)
         t1 = time.perf_counter()
         b2.close()
         g2.close()
         res["e2e_s"] = t1 - t0
+        res["e2e_steps"] = e2e_steps
         res["h2d"] = p.coords.nbytes + p.conn.nbytes + p.init_state.nbytes
         res["d2h"] = u.nbytes + pr.nbytes
     return res
 
 
-# Time step of the batched cavities: dt = 0.05 h_min / (lid + sqrt(invEps)).
-# At the CFL 0.2 of the single cavity, some of the 256 cavities (high lid
-# speed, low viscosity) grow without bound within the ~1000 steps of a bench
-# run - a property of the explicit scheme (the CPU restatement of the
-# reference's solver diverges the same way) - so the batched and served
-# streams run at CFL 0.05.
-BATCHED_CFL = 0.05
+def accuracy_run(args, local_rank, steps: int):
+    """Mixed form against the FP64 form on the GPU after `steps` steps of
+    the configured workload (fresh solves of the same problem)."""
+    from femorph_b200 import api
+    p = make_problem(args, seed=0)
+    out = {}
+    for pn, prec in (("fp64", api.FM_FP64), ("mixed", api.FM_MIXED)):
+        g = api.GpuProblem(p, prec)
+        b = api.Batch([g], device=local_rank)
+        b.step(steps)
+        b.sync()
+        out[pn] = g.state(elements=False)[:2]
+        b.close()
+        g.close()
+    (um, pm), (ud, pd) = out["mixed"], out["fp64"]
+    return {"u": float(np.linalg.norm(um - ud) / np.linalg.norm(ud)),
+            "p": float(np.linalg.norm(pm - pd) / max(np.linalg.norm(pd), 1e-300)),
+            "after_steps": steps,
+            "reference": "the FP64 GPU path (itself within 1e-10 of the oracle after 200 steps of this "
+                         "workload, tests/test_gpu_fullsize.py)"}
 
 
-def batched_problems(count: int = 256, seed: int = 0, n_lo: int = 8, n_hi: int = 48):
-    """Batched workload: `count` independent cavities, each with its own seed;
-    n ~ U{n_lo..n_hi}, viscosity log-uniform in [1e-3, 1e-1] (rho = 1), lid
-    speed uniform in [0.5, 2], CFL 0.05."""
+def batched_problems(count: int = 256, seed: int = 0):
+    """Batched workload (femorph_b200.mesh.batched_cavities): `count`
+    independent cavities, n ~ U{8..48}, viscosity log-uniform in
+    [1e-3, 1e-1], lid speed uniform in [0.5, 2], CFL 0.05."""
     from femorph_b200 import mesh
-    rng = np.random.default_rng(seed)
-    ns = rng.integers(n_lo, n_hi + 1, count)
-    nus = np.exp(rng.uniform(np.log(1e-3), np.log(1e-1), count))
-    lids = rng.uniform(0.5, 2.0, count)
-    return [mesh.cavity(int(n), seed=seed * 100003 + i, mu=float(nu), lid=float(lid), steps=200, cfl=BATCHED_CFL)
-            for i, (n, nu, lid) in enumerate(zip(ns, nus, lids))]
+    return mesh.batched_cavities(count, seed=seed)
 
 
 def run_batched(args, rank, world, local_rank, dist):
@@ -278,18 +289,20 @@ def batched_line(args, world, rb):
                                 "frac": ab / (tile_ms * 1e-3) / 1e9 / peak, "traffic": None,
                                 "peak_source": peak_kind, "kernel": "vms_tile_kernel",
                                 "algorithmic_bytes_per_launch": ab, "avg_launch_ms": tile_ms}}
-    m = out["mixed"]
-    return {"metric": "VMS element-steps/s, batched cavities (mixed; FP64 beside)", "value": m["value"],
+    from femorph_b200 import mesh
+    m = out["fp64"]
+    return {"metric": "VMS element-steps/s, batched cavities (FP64; mixed beside)", "value": m["value"],
             "unit": "element-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64", "data": "synthetic",
+            "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{args.batch_count} independent VMS cavities per GPU job, n~U{{8..48}}, "
-                                   f"nu log-U[1e-3,1e-1], lid U[0.5,2], CFL {BATCHED_CFL}, one launch pair per step for all, "
+                                   f"nu log-U[1e-3,1e-1], lid U[0.5,2], CFL {mesh.BATCHED_CFL}, one launch pair per step for all, "
                                    f"50-step CUDA graphs, autotuned tiles", "elements": rb["E_total"],
                        "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"problems sharded over {world} GPU(s) by LPT on element count"},
             "roofline": m["roofline"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
-            "tuning": m["tuning"], "fp64": out["fp64"], "mixed_over_fp64": m["value"] / out["fp64"]["value"],
+            "tuning": m["tuning"], "mixed": dict(out["mixed"], dtype="f32+f64"),
+            "mixed_over_fp64": out["mixed"]["value"] / m["value"],
             "mixed_vs_fp64_rel_l2": {"u_max_over_problems": rb["err"][0], "p_max_over_problems": rb["err"][1],
                                      "after_steps": args.warmup + args.steps + min(args.steps, 50)}}
 
@@ -434,20 +447,24 @@ def cpu_sample_n(args) -> int:
     return 16 if args.config == "channel" else args.n
 
 
-def cpu_baseline(args, steps: int = 1):
-    """Oracle B (plain-C restatement, single thread) on `steps` steps of the
+def cpu_baseline(args, steps: int = 2):
+    """Oracle B (plain-C restatement, element loops on all host threads,
+    nodal sums in the reference's element order) on `steps` steps of the
     workload (or of the bounded sample of cpu_sample_n)."""
     from oracle import oracle_b
     n = cpu_sample_n(args)
     p = make_problem(args, seed=0, n=n)
     o = oracle_b.OracleSolve(p)
+    threads = oracle_b.get_threads()
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
     solver = "femVMSExplicitFluidSolver" if args.config == "cavity" else "femSUPGExplicitFluidSolver"
-    return {"value": p.n_elems * steps / dt, "unit": "element-steps/s", "cores": 1, "kind": "port", "host": host_cpu(),
+    host = dict(host_cpu(), cores_used=threads)
+    return {"value": p.n_elems * steps / dt, "unit": "element-steps/s", "cores": threads, "kind": "port",
+            "host": host,
             "sample": f"{steps} time step(s) of {workload_name(args, n)} ({p.n_elems} elements) with the "
-                      f"single-threaded C restatement of {solver}, setup excluded"}
+                      f"C restatement of {solver} on {threads} host threads, setup excluded"}
 
 
 def run_reference(args):
@@ -592,7 +609,8 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
-    precs = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    # FP64 (the reference's precision) is the headline; the mixed form beside it
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
     runs = {}
     for pn in precs:
         a2 = argparse.Namespace(**vars(args))
@@ -616,8 +634,17 @@ def main():
                 # the SUPG element work is FP64-pipe bound: FLOP rate beside the bytes
                 roof["fp64_tflops"] = SUPG_FLOPS[args.config] * E / (tile_ms * 1e-3) / 1e12
                 roof["fp64_flops_per_element_step"] = SUPG_FLOPS[args.config]
-            return {"value": world * E * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
-                    "roofline": roof}
+            out = {"value": world * E * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
+                   "roofline": roof, "gpu_launches": r["launches"], "clocks": r["clocks"]}
+            if "e2e_s" in r:
+                k = r["e2e_steps"]
+                out["e2e"] = {"value": E * k / r["e2e_s"], "unit": "element-steps/s",
+                              "h2d_bytes_per_step": r["h2d"] / k, "d2h_bytes_per_step": r["d2h"] / k,
+                              "steps": k,
+                              "note": f"one whole {k}-step solve of the workload through the C ABI: problem "
+                                      f"create + batch create (host layout, H2D of mesh and initial state) + "
+                                      f"{k} steps + state readback (D2H), wall clock"}
+            return out
 
         head = precs[0]
         r = runs[head]
@@ -633,24 +660,16 @@ def main():
             "roofline": s["roofline"],
             "gpu_launches": r["launches"], "clocks": r["clocks"], "layout": r["layout"],
         }
-        if "fp64" in runs and head != "fp64":
-            sd = summary("fp64", runs["fp64"])
-            (um, pm), (ud, pd) = runs[head]["state"], runs["fp64"]["state"]
-            line["fp64"] = sd
-            line["mixed_over_fp64"] = s["value"] / sd["value"]
-            line["mixed_vs_fp64_rel_l2"] = {
-                "u": float(np.linalg.norm(um - ud) / np.linalg.norm(ud)),
-                "p": float(np.linalg.norm(pm - pd) / max(np.linalg.norm(pd), 1e-300)),
-                "after_steps": r["steps_total"],
-                "reference": "the FP64 GPU path (itself <= 1e-10 of the oracle after 200 steps of the 16^3 cavity)"}
-        if "e2e_s" in r:
-            line["e2e"] = {"value": E * args.steps / r["e2e_s"], "unit": "element-steps/s",
-                           "h2d_bytes_per_step": r["h2d"] / args.steps, "d2h_bytes_per_step": r["d2h"] / args.steps,
-                           "note": "problem create + batch create (host layout, H2D) + K steps + state readback, "
-                                   "wall clock"}
+        if "e2e" in s:
+            line["e2e"] = s["e2e"]
+        if "mixed" in runs and head != "mixed":
+            sm = summary("mixed", runs["mixed"])
+            line["mixed"] = dict(sm, dtype="f32+f64")
+            line["mixed_over_fp64"] = sm["value"] / s["value"]
+            line["mixed_vs_fp64_rel_l2"] = accuracy_run(args, local_rank, 200)
         if world == 1 and not args.no_cpu:
             try:
-                line["cpu_baseline"] = cpu_baseline(args, 1)
+                line["cpu_baseline"] = cpu_baseline(args)
             except Exception as e:  # the baseline is reported, not required
                 line["cpu_baseline"] = {"error": str(e)}
         print(json.dumps(line), flush=True)

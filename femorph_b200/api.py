@@ -102,6 +102,8 @@ def lib():
         L.fm_problem_write_vtu.argtypes = [P, C.c_char_p]
         L.fm_problem_checkpoint.argtypes = [P, C.c_char_p]
         L.fm_batch_set_diagnostics.argtypes = [P, C.c_int32]
+        L.fm_batch_set_wait_limit.argtypes = [P, C.c_uint32]
+        L.fm_math_check.argtypes = [P, C.c_int64, P]
         L.fm_problem_vms_log.argtypes = [P, P, C.c_int32, P]
         L.fm_problem_vms_residuals.argtypes = [P, P, P]
         L.fm_problem_restore.argtypes = [P, C.c_char_p]
@@ -326,6 +328,10 @@ class Batch:
 
     def step(self, n: int = 1, stream=None) -> None:
         check(lib().fm_batch_step(self.h, int(n), stream))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of the VMS tile kernel's bounded chunk waits before FM_ERR_TIMEOUT."""
+        check(lib().fm_batch_set_wait_limit(self.h, int(polls)))
 
     def set_diagnostics(self, enable: bool = True) -> None:
         """VMS: record the reference's log row and centroid residuals every

@@ -57,6 +57,9 @@ struct DevBatch {
   int32_t x_slices;               // one slice per part in the batch
   double* xsend;                  // [x_slices][x_n][4] partial sums of this batch's parts
   const double* xrecv;            // the same, summed over all processes (xsend when all parts are here)
+  // polls of a tile CTA's wait for one chunk's bulk copies before it gives
+  // up with FM_ERR_TIMEOUT (FM_WAIT_LIMIT unless fm_batch_set_wait_limit)
+  uint32_t wait_limit;
 };
 
 // Sum over the part slices of exchange entry xi (component c).
@@ -98,8 +101,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 // Polls at most `limit` times (each try_wait may itself suspend for a
 // bounded, hardware-defined time); false when the phase did not complete.
-constexpr uint32_t FM_WAIT_LIMIT = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit = FM_WAIT_LIMIT) {
+// FM_WAIT_LIMIT (fm_internal.hpp) is the default limit of the chunk waits.
+constexpr uint32_t FM_DRAIN_LIMIT = 1u << 16;  // a timed-out CTA's wait for its own copies
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
   for (uint32_t i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
@@ -214,7 +218,10 @@ __device__ __forceinline__ void apply_bc(const DevBatch& B, int32_t rec, double 
 
 // Marks the end of one pass over the interface nodes.  The last block to
 // finish (counter pattern: fence, ticket, no waiting) advances every active
-// problem by one iteration and its time at the start of a new step.
+// problem by one iteration and its time at the start of a new step.  A
+// problem with a device error (status != FM_OK) stops where it is: the
+// kernels skip it from then on, so its state stays that of the failed
+// iteration.
 __device__ __forceinline__ void finish_iteration(const DevBatch& B) {
   __shared__ bool s_last;
   __syncthreads();
@@ -228,7 +235,7 @@ __device__ __forceinline__ void finish_iteration(const DevBatch& B) {
   __threadfence();
   for (int p = threadIdx.x; p < B.n_probs; p += blockDim.x) {
     DevProbState st = B.pstate[p];
-    if (st.iter < B.target[p]) {
+    if (st.iter < B.target[p] && st.status == FM_OK) {
       const int per_step = B.probs[p].ndual + 1;
       st.iter += 1;
       if (st.iter % per_step == 0) st.time = st.time + B.probs[p].dt;

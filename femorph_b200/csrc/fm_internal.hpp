@@ -98,6 +98,10 @@ struct DevProb {
 // iterations (VMS) or steps (SUPG); a pass only works on problems with
 // iter < target[p] (a separate array, set by the host per launch block).  time is the physical time of the step iter belongs to,
 // accumulated by repeated addition like the reference's currentTime.
+// Default polls of a tile CTA's bounded wait for one chunk's bulk copies
+// (each mbarrier try_wait may itself suspend for a bounded time).
+constexpr uint32_t FM_WAIT_LIMIT = 1u << 22;
+
 struct DevProbState {
   int32_t iter;
   int32_t status;   // FM_OK or an FM_ERR_* raised on the device

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
   const int pidx = tm.problem;
   if (pidx < 0) return;  // free tile slot
   const DevProbState st = B.pstate[pidx];
-  if (st.iter >= B.target[pidx]) return;
+  if (st.iter >= B.target[pidx] || st.status != FM_OK) return;
   const DevProb& P = B.probs[pidx];
   const bool euler = (P.ex_mask & 1) || st.iter == 0;
   const bool ab2 = !(P.ex_mask & 1);
@@ -230,7 +230,7 @@ __global__ void supg_iface_kernel(DevBatch B) {
     const int pidx = B.iface_prob[i];
     if (pidx < 0) continue;  // free interface entry
     const DevProbState st = B.pstate[pidx];
-    if (st.iter >= B.target[pidx]) continue;
+    if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     const int g = B.iface_node[i];
     double acc[3] = {0.0, 0.0, 0.0};
@@ -257,7 +257,7 @@ __global__ void supg_xpack_kernel(DevBatch B) {
     const int pidx = B.iface_prob[i];
     if (pidx < 0) continue;
     const DevProbState st = B.pstate[pidx];
-    if (st.iter >= B.target[pidx]) continue;
+    if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     double acc[3] = {0.0, 0.0, 0.0};
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
@@ -288,7 +288,7 @@ __global__ void supg_xupdate_kernel(DevBatch B) {
     const int pidx = B.iface_prob[i];
     if (pidx < 0) continue;
     const DevProbState st = B.pstate[pidx];
-    if (st.iter >= B.target[pidx]) continue;
+    if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     const int xi = B.iface_xidx[i];
     const double acc[3] = {exchange_sum(B, xi, 0), exchange_sum(B, xi, 1), exchange_sum(B, xi, 2)};

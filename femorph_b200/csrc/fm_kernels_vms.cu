@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   const int pidx = tm.problem;
   if (pidx < 0) return;  // free tile slot
   const DevProbState st = B.pstate[pidx];
-  if (st.iter >= B.target[pidx]) return;
+  if (st.iter >= B.target[pidx] || st.status != FM_OK) return;
   const DevProb& P = B.probs[pidx];
   const int per_step = P.ndual + 1;
   const bool first_dual = (st.iter % per_step) == 0;
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
     // each thread waits for the chunk itself (the mbarrier phase makes the
     // bulk-copied bytes visible to it); a timed-out wait skips the chunk and
     // is agreed on at the end-of-chunk barrier
-    const bool arrived = mbar_wait_bounded(&bars[k & 1], (uint32_t)((k >> 1) & 1));
+    const bool arrived = mbar_wait_bounded(&bars[k & 1], (uint32_t)((k >> 1) & 1), B.wait_limit);
     const int base = k * THREADS;
     const int le = base + tid;
     const bool active = arrived && le < tm.n_elem;
@@ -396,7 +396,8 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
     // a copy never completed: wait (bounded) for the copies this CTA issued,
     // report, and leave the tile's nodes untouched
     if (tid == 0) {
-      for (int j = k; j < nchunks && j <= k + 1; ++j) mbar_wait_bounded(&bars[j & 1], (uint32_t)((j >> 1) & 1), 1u << 16);
+      for (int j = k; j < nchunks && j <= k + 1; ++j)
+        mbar_wait_bounded(&bars[j & 1], (uint32_t)((j >> 1) & 1), FM_DRAIN_LIMIT);
       B.pstate[pidx].status = FM_ERR_TIMEOUT;
     }
     return;
@@ -426,7 +427,7 @@ __global__ void vms_iface_kernel(DevBatch B) {
     const int pidx = B.iface_prob[i];
     if (pidx < 0) continue;  // free interface entry
     const DevProbState st = B.pstate[pidx];
-    if (st.iter >= B.target[pidx]) continue;
+    if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     const bool first_dual = (st.iter % (P.ndual + 1)) == 0;
     const int g = B.iface_node[i];
@@ -453,7 +454,7 @@ __global__ void vms_xpack_kernel(DevBatch B) {
     const int pidx = B.iface_prob[i];
     if (pidx < 0) continue;
     const DevProbState st = B.pstate[pidx];
-    if (st.iter >= B.target[pidx]) continue;
+    if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
@@ -485,7 +486,7 @@ __global__ void vms_xupdate_kernel(DevBatch B) {
     const int pidx = B.iface_prob[i];
     if (pidx < 0) continue;
     const DevProbState st = B.pstate[pidx];
-    if (st.iter >= B.target[pidx]) continue;
+    if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     const int xi = B.iface_xidx[i];
     const double acc[4] = {exchange_sum(B, xi, 0), exchange_sum(B, xi, 1), exchange_sum(B, xi, 2), exchange_sum(B, xi, 3)};

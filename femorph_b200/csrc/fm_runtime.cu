@@ -424,6 +424,7 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
   D.iface_node = inode; D.iface_slot_beg = isb; D.iface_slot_cnt = isc; D.iface_prob = iprob; D.iface_slots = islots;
   D.recs = recs; D.tab_off = toffs; D.tab_len = tlens; D.tab_rows = rows;
   D.probs = dp; D.pstate = ds; D.target = tg; D.q1p = q1; D.done = done;
+  D.wait_limit = FM_WAIT_LIMIT;
   // every slot starts inactive
   CK(cudaMemset(tiles, 0xff, std::max<int64_t>(cap[P_TILE], 1) * sizeof(TileMeta)));
   CK(cudaMemset(iprob, 0xff, std::max<int64_t>(cap[P_IFACE], 1) * sizeof(int32_t)));
@@ -1728,23 +1729,44 @@ struct CkptHeader {
   int64_t steps_done;
   double time, max_u2;
   double q1p[8];  // pre-BC pressures of nodes 0..3, both iteration parities
-  uint64_t mesh_hash;
+  uint64_t setup_hash;  // setup_hash(): mesh, parameters, BCs
 };
 static_assert(sizeof(CkptHeader) == 160, "checkpoint header size");
 
-// FNV-1a over the 64-bit words of the coordinates, then the connectivity.
-uint64_t mesh_hash(const fm_problem* p) {
+// FNV-1a over the 64-bit words of the coordinates, then the connectivity,
+// then everything else that shapes the solve: the physical and time-stepping
+// parameters and the BC records and tables.  A checkpoint restores only into
+// a problem with the same hash.
+uint64_t setup_hash(const fm_problem* p) {
   uint64_t h = 1469598103934665603ull;
   auto mix = [&](uint64_t w) { h = (h ^ w) * 1099511628211ull; };
-  for (int64_t i = 0; i < p->N * 3; ++i) {
+  auto mixd = [&](double d) {
     uint64_t w;
-    memcpy(&w, &p->coords[i], 8);
+    memcpy(&w, &d, 8);
     mix(w);
-  }
+  };
+  auto mixbytes = [&](const void* data, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) mix(c[i]);
+  };
+  for (int64_t i = 0; i < p->N * 3; ++i) mixd(p->coords[i]);
   const int64_t nc = p->E * p->etype;
   for (int64_t i = 0; i < nc; ++i) mix((uint64_t)(uint32_t)p->conn[i]);
   mix((uint64_t)p->N);
   mix((uint64_t)p->E);
+  const fm_params& q = p->params;
+  for (int i = 0; i < 5; ++i) mixd(q.props[i]);
+  mixd(q.time_step);
+  mixd(q.dual_step);
+  mixd(q.exit_condition);
+  mix((uint64_t)(uint32_t)q.tot_dual_steps);
+  for (int i = 0; i < 6; ++i) mix((uint64_t)(uint32_t)q.ex_opts[i]);
+  mix((uint64_t)(uint32_t)q.glob_fixed);
+  mixbytes(p->node_rec.data(), p->node_rec.size() * sizeof(int32_t));
+  mixbytes(p->recs.data(), p->recs.size() * sizeof(BCRec));
+  mixbytes(p->tab_off.data(), p->tab_off.size() * sizeof(int32_t));
+  mixbytes(p->tab_len.data(), p->tab_len.size() * sizeof(int32_t));
+  for (double d : p->tab_rows) mixd(d);
   return h;
 }
 
@@ -1801,7 +1823,7 @@ int fm_problem_checkpoint(fm_problem* p, const char* path) {
   CkptHeader h;
   memset(&h, 0, sizeof(h));
   memcpy(h.magic, "FMSTATE1", 8);
-  h.version = 1;
+  h.version = 2;
   h.solver = b->solver;
   h.precision = b->precision;
   h.npe = b->npe;
@@ -1818,10 +1840,13 @@ int fm_problem_checkpoint(fm_problem* p, const char* path) {
   h.time = st.time;
   h.max_u2 = st.max_u2;
   h.steps_done = p->steps_done;
-  h.mesh_hash = mesh_hash(p);
+  h.setup_hash = setup_hash(p);
 
-  FileCloser fc{fopen(path, "wb")};
-  if (!fc.f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  // written to path.tmp and renamed over path once complete, so a failed or
+  // short write never replaces an earlier good checkpoint
+  const std::string tmp_path = std::string(path) + ".tmp";
+  FileCloser fc{fopen(tmp_path.c_str(), "wb")};
+  if (!fc.f) return fail(FM_ERR_IO, std::string("cannot open ") + tmp_path);
   bool ok = fwrite(&h, sizeof(h), 1, fc.f) == 1;
   std::vector<double> tmp(N), out(N);
   double* cols[8] = {b->D.su, b->D.sv, b->D.sw, b->D.sp, b->D.pu, b->D.pv, b->D.pw, b->D.pp};
@@ -1839,7 +1864,13 @@ int fm_problem_checkpoint(fm_problem* p, const char* path) {
       if (eo[k] >= 0) memcpy(&eout[(size_t)eo[k] * bytes], &col[(size_t)k * bytes], bytes);
     ok = fwrite(eout.data(), bytes, E, fc.f) == (size_t)E;
   }
-  if (!ok || fflush(fc.f) != 0) return fail(FM_ERR_IO, std::string("cannot write ") + path);
+  ok = ok && fflush(fc.f) == 0;
+  ok = (fclose(fc.f) == 0) && ok;
+  fc.f = nullptr;
+  if (!ok || rename(tmp_path.c_str(), path) != 0) {
+    remove(tmp_path.c_str());
+    return fail(FM_ERR_IO, std::string("cannot write ") + path);
+  }
   return FM_OK;
 }
 
@@ -1852,13 +1883,13 @@ int fm_problem_restore(fm_problem* p, const char* path) {
   FileCloser fc{fopen(path, "rb")};
   if (!fc.f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
   CkptHeader h;
-  if (fread(&h, sizeof(h), 1, fc.f) != 1 || memcmp(h.magic, "FMSTATE1", 8) != 0 || h.version != 1)
+  if (fread(&h, sizeof(h), 1, fc.f) != 1 || memcmp(h.magic, "FMSTATE1", 8) != 0 || h.version != 2)
     return fail(FM_ERR_INVALID, std::string(path) + " is not a femorph_b200 checkpoint");
   const CkptCols cc = ckpt_cols(b, p);
   if (h.solver != b->solver || h.precision != b->precision || h.npe != b->npe)
     return fail(FM_ERR_INVALID, "checkpoint of another solver, precision or element type");
-  if (h.n_nodes != p->N || h.n_elems != p->E || h.mesh_hash != mesh_hash(p))
-    return fail(FM_ERR_INVALID, "checkpoint of another mesh");
+  if (h.n_nodes != p->N || h.n_elems != p->E || h.setup_hash != setup_hash(p))
+    return fail(FM_ERR_INVALID, "checkpoint of another mesh, parameter set or BC set");
   if (h.n_sd_cols != cc.n_sd || h.sd_bytes != cc.sd_bytes || h.n_diag_cols != cc.n_diag)
     return fail(FM_ERR_INVALID, "checkpoint element columns differ (SUPG AB2 history or not)");
   if (h.iter < 0 || h.steps_done < 0) return fail(FM_ERR_INVALID, "checkpoint counters out of range");
@@ -1919,6 +1950,19 @@ int fm_problem_restore(fm_problem* p, const char* path) {
 
 // ---- VMS diagnostics (the reference's log line and res_v / res_p) ----
 extern "C" {
+
+int fm_batch_set_wait_limit(fm_batch* b, uint32_t polls) {
+  if (!b) return fail(FM_ERR_INVALID, "null batch");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  // captured graphs hold the batch view (and so the limit) by value
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->D.wait_limit = polls;
+  return FM_OK;
+}
 
 int fm_batch_set_diagnostics(fm_batch* b, int32_t enable) {
   NvtxRange nvtx_range("fm_batch_set_diagnostics");

@@ -177,6 +177,19 @@ __global__ void static_gather_kernel(DevBatch B, const int32_t* node_new, int32_
     if (_e != cudaSuccess) return fail(FM_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
+// Puts the caller's current device back on every return path: the entry
+// point selects the requested device, and callers that run inside another
+// framework's device and stream management must find theirs unchanged.
+struct DeviceRestore {
+  int prev = -1;
+  DeviceRestore() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceRestore() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 template <class T>
 static cudaError_t up(unsigned char* base, size_t off, const T* src, size_t n, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
@@ -207,6 +220,7 @@ extern "C" int fm_vms_solve_static(fm_problem* p, int32_t nsteps, int32_t device
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(FM_ERR_NODEVICE, "no CUDA device");
   if (device < 0 || device >= ndev || device >= kMaxDevices) return fail(FM_ERR_INVALID, "bad device ordinal");
+  DeviceRestore restore_device;
   CKS(cudaSetDevice(device));
   unsigned char* base = nullptr;
   int r = scratch_address(device, &base);
@@ -249,6 +263,7 @@ extern "C" int fm_vms_solve_static(fm_problem* p, int32_t nsteps, int32_t device
   D.q1p = reinterpret_cast<double*>(base + o.q1p);
   D.n_probs = 1;
   D.done = reinterpret_cast<unsigned int*>(base + o.done);
+  D.wait_limit = FM_WAIT_LIMIT;
 
   // problem constants and progress (as fm_batch_create sets them)
   const fm_params& pr = p->params;

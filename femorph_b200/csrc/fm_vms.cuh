@@ -22,9 +22,12 @@ namespace fm {
 #define FM_PR (FM_VB * (FM_VS + (FM_VA - FM_VB)) / FM_VS)
 #define FM_PG1 ((FM_VA - FM_VB) * (FM_VA - FM_VB) / FM_VS - 1.0)
 
-// Element geometry: initial_assemble (src lines 21-91).  Products are
-// rounded individually (no FMA contraction) so DN and V are bit-identical to
-// the reference's.
+// Element geometry: initial_assemble (src lines 21-91).  The cofactors and
+// the determinant round each product individually, as the reference's
+// uncontracted expressions do.  DN and V can still differ from the
+// reference's in the last bit: 1/det comes from rcp_nr (within about one ulp
+// of the correctly rounded 1.0 / detJ of src line 64) and V = det * (1/6)
+// where the reference divides detJ / 6.0 (src line 73).
 struct TetGeom {
   double DN[3][4];
   double V;

@@ -217,6 +217,27 @@ def channel(nx: int = 256, ny: int = 64, nz: int = 64, seed: int = 0, mu: float 
         name=f"channel{nx}x{ny}x{nz}_s{seed}")
 
 
+# Time step of the batched cavities: dt = 0.05 h_min / (lid + sqrt(invEps)).
+# At CFL 0.2 some of the 256 cavities (high lid speed, low viscosity) grow
+# without bound within ~1000 steps - a property of the explicit scheme (the
+# CPU restatement of the reference's solver diverges the same way) - so the
+# batched workload runs at CFL 0.05.
+BATCHED_CFL = 0.05
+
+
+def batched_cavities(count: int = 256, seed: int = 0, n_lo: int = 8, n_hi: int = 48,
+                     steps: int = 200) -> list:
+    """The batched workload: `count` independent VMS cavities, each with its
+    own seed; n ~ U{n_lo..n_hi} (6 n^3 tets), viscosity log-uniform in
+    [1e-3, 1e-1] (rho = 1), lid speed uniform in [0.5, 2], CFL 0.05."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_lo, n_hi + 1, count)
+    nus = np.exp(rng.uniform(np.log(1e-3), np.log(1e-1), count))
+    lids = rng.uniform(0.5, 2.0, count)
+    return [cavity(int(n), seed=seed * 100003 + i, mu=float(nu), lid=float(lid), steps=steps, cfl=BATCHED_CFL)
+            for i, (n, nu, lid) in enumerate(zip(ns, nus, lids))]
+
+
 def _fmt_rows(prefix: str, first: np.ndarray, vals: np.ndarray | None = None, ints: np.ndarray | None = None) -> str:
     cols = [np.char.add(prefix, first.astype(str))]
     if vals is not None:

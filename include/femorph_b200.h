@@ -309,6 +309,28 @@ FM_API int fm_problem_supg_log_stats(fm_problem* p, double* out);
  * fm_problem_vms_residuals copies the last recorded iteration's centroid
  * residuals (res_u n_elems x 3, res_p n_elems; either may be NULL). */
 FM_API int fm_batch_set_diagnostics(fm_batch* b, int32_t enable);
+
+/* Failure detection (femSUPGExplicitFluidSolver.cpp:1635-1643 is the
+ * reference's only failure exit; it has no device waits).  The VMS tile
+ * kernel's waits for each chunk's bulk copies are bounded: after `polls`
+ * unsuccessful mbarrier polls (default 4,194,304) the CTA waits, again
+ * bounded, for the copies it issued, leaves its nodes untouched and sets the
+ * problem's status to FM_ERR_TIMEOUT, which fm_batch_sync reports.  A
+ * problem whose status is not FM_OK stops there: the kernels skip it from
+ * then on.  A small limit (0: give up at once) makes the timeout path run on
+ * demand, which is how it is tested; 0 is not for production use.  Drops
+ * the batch's captured CUDA graph (it holds the old limit). */
+FM_API int fm_batch_set_wait_limit(fm_batch* b, uint32_t polls);
+
+/* Self-check of the device arithmetic that stands in for CUDA's division,
+ * rcbrt and sqrt in the element kernels (Newton-Raphson from the PTX
+ * approximate FP32 instructions).  No reference counterpart: the reference
+ * computes 1.0 / detJ, pow(6V, 1/3) and sqrt on the host
+ * (femVMSExplicitFluidSolver.cpp:64, 75, 585).  For each x[i] writes
+ * out[i*8 .. i*8+7] = rcp_nr(x), 1.0/x, rcbrt_nr(x), rcbrt(x), sqrt_nr(x),
+ * sqrt(x), rcbrt_nr((float)x), rcbrtf((float)x), computed on device 0
+ * (allocates; for tests). */
+FM_API int fm_math_check(const double* x, int64_t n, double* out);
 FM_API int fm_problem_vms_log(fm_problem* p, double* rows, int32_t max_rows, int32_t* n_rows);
 FM_API int fm_problem_vms_residuals(fm_problem* p, double* res_u, double* res_p);
 
@@ -347,8 +369,12 @@ FM_API int fm_problem_write_vtu(fm_problem* p, const char* path);
  * keeps them; SUPG history and lambda / regime), the iteration and step
  * counters, time, status and the pressures of nodes 0..3 (little-endian,
  * a 160-byte header then columns; layout in fm_runtime.cu).
+ * The file is written to path.tmp and renamed over path when complete, so
+ * a failed write leaves an earlier checkpoint at path intact.
  * fm_problem_restore loads such a file into a problem of the same mesh,
- * solver and precision that sits in a batch (any batch, any slot); stepping
+ * parameters (properties, time and dual step, dual iterations, EXOPTS,
+ * fixed dofs, exit condition), BC rows and tables, solver and precision
+ * that sits in a batch (any batch, any slot); stepping
  * on continues the solve: bit for bit the uninterrupted one when the batch
  * has the same tile sizes and threads.  Either call waits for the batch's
  * stream; neither may run while an exchange is open.  FM_ERR_IO for a file

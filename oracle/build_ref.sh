@@ -4,10 +4,11 @@
 # oracle/shim, linked with oracle/refdrv.cpp (driver + full-precision state
 # hooks).  Outputs go to oracle/_ref/ only.  Needs the reference tree; the GPU
 # host only runs the prebuilt oracle/_ref/fm_refdrv.
-#   REF=<path to the reference project>  (default /root/reference)
+#   FEMORPH_REFERENCE=<path to the reference project>  (default /root/reference)
+# Exit status 2: the reference sources are not there (nothing is built).
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-SRC=${REF:-/root/reference}/src
+SRC=${FEMORPH_REFERENCE:-/root/reference}/src
 OUT=$HERE/_ref
 OBJ=$OUT/obj
 [ -d "$SRC" ] || { echo "reference sources not found at $SRC" >&2; exit 2; }

@@ -25,11 +25,24 @@
  *          unique node), 4581-4643 (setNodeVelocity, setDirichletBC).
  * Diagnostics that do not feed the state (norms, CFL, logs) are left out,
  * except the VMS centroid subgrid average that the reference writes out.
+ *
+ * Host threads.  The element loops run in parallel over element ranges; the
+ * reference's nodal scatters (rhs[node] += lRes in element order, the SUPG
+ * solN and l_M sums) are computed per node, each walking its incident
+ * (element, corner) entries in increasing element order, so every nodal sum
+ * is formed from the same terms in the same order as the reference's serial
+ * loop and the results do not depend on the thread count (bit for bit).
+ * FMO_THREADS (environment) or fmo_set_threads() sets the thread count;
+ * default: the CPUs this process may run on.
  */
+#define _GNU_SOURCE
 #include <math.h>
+#include <pthread.h>
+#include <sched.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #define FMO_OK 0
 #define FMO_ERR_INVALID 1
@@ -67,7 +80,86 @@ typedef struct {
   double *el_u_sdus; /* centroid subgrid velocity (E x 3) of the last dual pass */
   /* SUPG */
   double *sol_p, *solN, *l_M, *k_p, *k_pp, *el_lam, *el_regime, *pres_n;
+  /* node -> incident (element * npe + corner) entries, increasing element order */
+  int64_t* inc_off;
+  int64_t* inc_ent;
+  double* lres; /* VMS: [E][16] element residuals of the current pass; SUPG: [E][24] mass row sums */
+  const double* pres_src; /* SUPG: the state compute_pressure reads */
 } fmo_ctx;
+
+/* ------------------------------------------------------------------ */
+/* Host threads                                                        */
+/* ------------------------------------------------------------------ */
+#define FMO_MAX_THREADS 256
+static int g_threads = 0;
+
+void fmo_set_threads(int n) { g_threads = n < 1 ? 1 : (n > FMO_MAX_THREADS ? FMO_MAX_THREADS : n); }
+
+int fmo_get_threads(void) {
+  if (g_threads > 0) return g_threads;
+  const char* s = getenv("FMO_THREADS");
+  int n = s ? atoi(s) : 0;
+  if (n <= 0) {
+    cpu_set_t set;
+    n = sched_getaffinity(0, sizeof(set), &set) == 0 ? CPU_COUNT(&set) : (int)sysconf(_SC_NPROCESSORS_ONLN);
+  }
+  fmo_set_threads(n);
+  return g_threads;
+}
+
+typedef void (*fmo_range_fn)(fmo_ctx* c, int64_t b, int64_t e);
+typedef struct {
+  fmo_range_fn fn;
+  fmo_ctx* c;
+  int64_t b, e;
+} fmo_job;
+
+static void* fmo_job_run(void* p) {
+  fmo_job* j = (fmo_job*)p;
+  j->fn(j->c, j->b, j->e);
+  return NULL;
+}
+
+/* fn(c, b, e) over [0, n) split into contiguous ranges, one per thread. */
+static void par_for(fmo_ctx* c, int64_t n, fmo_range_fn fn) {
+  int T = fmo_get_threads();
+  if ((int64_t)T > n / 64) T = (int)(n / 64);
+  if (T <= 1) {
+    fn(c, 0, n);
+    return;
+  }
+  pthread_t th[FMO_MAX_THREADS];
+  fmo_job job[FMO_MAX_THREADS];
+  int started[FMO_MAX_THREADS];
+  for (int t = 0; t < T; ++t) {
+    job[t].fn = fn;
+    job[t].c = c;
+    job[t].b = n * t / T;
+    job[t].e = n * (t + 1) / T;
+  }
+  for (int t = 1; t < T; ++t) started[t] = pthread_create(&th[t], NULL, fmo_job_run, &job[t]) == 0;
+  fmo_job_run(&job[0]);
+  for (int t = 1; t < T; ++t) {
+    if (started[t])
+      pthread_join(th[t], NULL);
+    else
+      fmo_job_run(&job[t]); /* no thread: run the range here */
+  }
+}
+
+/* Node incidence lists in element order (counting sort of conn). */
+static void build_incidence(fmo_ctx* c) {
+  int64_t N = c->N, E = c->E;
+  int npe = c->npe;
+  c->inc_off = (int64_t*)calloc(N + 1, sizeof(int64_t));
+  c->inc_ent = (int64_t*)malloc(sizeof(int64_t) * (E * npe + 1));
+  for (int64_t q = 0; q < E * npe; ++q) c->inc_off[c->conn[q] + 1]++;
+  for (int64_t n = 0; n < N; ++n) c->inc_off[n + 1] += c->inc_off[n];
+  int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (N + 1));
+  memcpy(fill, c->inc_off, sizeof(int64_t) * (N + 1));
+  for (int64_t q = 0; q < E * npe; ++q) c->inc_ent[fill[c->conn[q]]++] = q;
+  free(fill);
+}
 
 /* ------------------------------------------------------------------ */
 /* Boundary conditions                                                 */
@@ -207,7 +299,21 @@ static void vms_initial_assemble(fmo_ctx* c, int64_t e) {
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 4; ++j)
       c->DNs[(i * 4 + j) * E + e] = V_lDN[0][j] * inv[0][i] + V_lDN[1][j] * inv[1][i] + V_lDN[2][j] * inv[2][i];
-  for (int i = 0; i < 4; ++i) c->nd_mass[ids[i]] += c->volumes[e] / 4.0;
+  /* nd_mass[ids[i]] += volumes[e] / 4.0 is summed per node in element order
+     (vms_mass_nodes) */
+}
+
+static void vms_initial_range(fmo_ctx* c, int64_t b, int64_t e) {
+  for (int64_t k = b; k < e; ++k) vms_initial_assemble(c, k);
+}
+
+/* femVMSExplicitFluidSolver.cpp:89 (nd_mass scatter) per node */
+static void vms_mass_nodes(fmo_ctx* c, int64_t b, int64_t e) {
+  for (int64_t n = b; n < e; ++n) {
+    double acc = 0.0;
+    for (int64_t j = c->inc_off[n]; j < c->inc_off[n + 1]; ++j) acc += c->volumes[c->inc_ent[j] >> 2] / 4.0;
+    c->nd_mass[n] = acc;
+  }
 }
 
 /* femVMSExplicitFluidSolver.cpp:93-399 (sol_n := sol_tau, sol_prev := sol_n) */
@@ -282,10 +388,38 @@ static void vms_assemble_rhs(fmo_ctx* c, int64_t e, const double* soln, const do
       lRes[a][3] += -wGp * sduhDN * invEpsilon;
     }
   }
+  /* rhs[ids[a]*4+i] += lRes[a][i] (src lines 393-396): kept per element
+     and summed per node in element order (vms_rhs_nodes) */
   for (int a = 0; a < 4; ++a)
-    for (int i = 0; i < 4; ++i) c->rhs[ids[a] * 4 + i] += lRes[a][i];
+    for (int i = 0; i < 4; ++i) c->lres[e * 16 + a * 4 + i] = lRes[a][i];
   for (int a = 0; a < 4; ++a)
     for (int i = 0; i < 3; ++i) sdu_out[a][i] = sdu[a][i];
+}
+
+static void vms_rhs_range(fmo_ctx* c, int64_t b, int64_t e) {
+  for (int64_t k = b; k < e; ++k) {
+    double sdu[4][3];
+    vms_assemble_rhs(c, k, c->sol_tau, c->sol_n, sdu);
+    for (int j = 0; j < 3; ++j) c->el_u_sdus[k * 3 + j] = 0.0;
+    for (int a = 0; a < 4; ++a)
+      for (int j = 0; j < 3; ++j) c->el_u_sdus[k * 3 + j] += sdu[a][j] * 0.25;
+  }
+}
+
+/* The nodal scatter of assemble_RHS per node, then update_dual_solution
+   (src lines 754-772) on the node. */
+static void vms_rhs_nodes(fmo_ctx* c, int64_t b, int64_t e) {
+  for (int64_t n = b; n < e; ++n) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t j = c->inc_off[n]; j < c->inc_off[n + 1]; ++j) {
+      const double* r = c->lres + (c->inc_ent[j] >> 2) * 16 + (c->inc_ent[j] & 3) * 4;
+      for (int i = 0; i < 4; ++i) acc[i] += r[i];
+    }
+    for (int i = 0; i < 4; ++i) {
+      c->rhs[n * 4 + i] = acc[i];
+      c->sol_tau[n * 4 + i] = c->sol_n[n * 4 + i] - c->ds * acc[i] / c->nd_mass[n];
+    }
+  }
 }
 
 /* femVMSExplicitFluidSolver.cpp:406-588 (proj_res_at_nodes = false) */
@@ -347,8 +481,10 @@ static void vms_assemble_proj(fmo_ctx* c, int64_t e, const double* soln) {
       proj_den[a][3] += wGp * V_lN[g][a];
     }
   }
+  /* projRHS is zeroed before each pass (src line 1047) and receives one
+     term an entry: 0.0 + x */
   for (int a = 0; a < 4; ++a)
-    for (int i = 0; i < 4; ++i) c->projRHS[(a * 4 + i) * E + e] += projL[a][i] / proj_den[a][i];
+    for (int i = 0; i < 4; ++i) c->projRHS[(a * 4 + i) * E + e] = 0.0 + projL[a][i] / proj_den[a][i];
   double tau_u = 1.0 / (c1 * nu / (insDiameter * insDiameter) + c2 * maxA / insDiameter);
   double tau_p = (insDiameter * insDiameter) / (c1 * tau_u);
   c->elmTaus[0 * E + e] = 1.0 / (1.0 / dt + 1.0 / tau_u);
@@ -371,6 +507,14 @@ static void vms_update_subscales(fmo_ctx* c, int64_t e) {
   }
 }
 
+static void vms_proj_range(fmo_ctx* c, int64_t b, int64_t e) {
+  for (int64_t k = b; k < e; ++k) vms_assemble_proj(c, k, c->sol_tau);
+}
+
+static void vms_subscale_range(fmo_ctx* c, int64_t b, int64_t e) {
+  for (int64_t k = b; k < e; ++k) vms_update_subscales(c, k);
+}
+
 /* One time step of femVMSExplicitFluidSolver::solve (src lines 1025-1234). */
 static void vms_step(fmo_ctx* c) {
   int64_t N = c->N, E = c->E;
@@ -378,21 +522,14 @@ static void vms_step(fmo_ctx* c) {
   int loopTau = 0, conv = 0;
   while (!conv) {
     loopTau++;
-    memset(c->rhs, 0, sizeof(double) * N * 4);
-    memset(c->projRHS, 0, sizeof(double) * E * 16);
-    memset(c->el_u_sdus, 0, sizeof(double) * E * 3);
-    for (int64_t e = 0; e < E; ++e) {
-      double sdu[4][3];
-      vms_assemble_rhs(c, e, c->sol_tau, c->sol_n, sdu);
-      for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 3; ++b) c->el_u_sdus[e * 3 + b] += sdu[a][b] * 0.25;
-    }
-    /* update_dual_solution, src lines 754-772 */
-    for (int64_t i = 0; i < N; ++i)
-      for (int j = 0; j < 4; ++j) c->sol_tau[i * 4 + j] = c->sol_n[i * 4 + j] - c->ds * c->rhs[i * 4 + j] / c->nd_mass[i];
+    par_for(c, E, vms_rhs_range);
+    /* nodal sums + update_dual_solution, src lines 754-772 */
+    par_for(c, N, vms_rhs_nodes);
     memcpy(c->sol_n, c->sol_tau, sizeof(double) * N * 4);
-    for (int64_t e = 0; e < E; ++e) vms_assemble_proj(c, e, c->sol_tau);
-    for (int64_t e = 0; e < E; ++e) vms_update_subscales(c, e);
+    /* the pressures of nodes 0..3 that every element reads (quirk Q1) are
+       final here: the element passes below do not write the state */
+    par_for(c, E, vms_proj_range);
+    par_for(c, E, vms_subscale_range);
     set_node_velocity(c, c->cur_time, c->sol_tau, 4);
     apply_zero_traction(c, c->sol_tau);
     set_dirichlet(c, c->sol_tau, 4);
@@ -508,15 +645,14 @@ static void elem_coords(fmo_ctx* c, int64_t e, double xe[8][3]) {
 /* SUPG                                                                */
 /* ------------------------------------------------------------------ */
 /* femSUPGExplicitFluidSolver.cpp:507-598 */
-static void supg_lumped_mass(fmo_ctx* c) {
+static void supg_lumped_mass_range(fmo_ctx* c, int64_t eb, int64_t ee) {
   double rho = c->props[0];
   int npe = c->npe, nd = npe * 3;
   int ngp;
   double gps[8][3], gpw[8];
   gauss_rule(npe, &ngp, gps, gpw);
-  memset(c->l_M, 0, sizeof(double) * c->N * 3);
-  static double BM[24][24];
-  for (int64_t e = 0; e < c->E; ++e) {
+  double BM[24][24];
+  for (int64_t e = eb; e < ee; ++e) {
     double xe[8][3];
     elem_coords(c, e, xe);
     for (int a = 0; a < nd; ++a)
@@ -535,21 +671,42 @@ static void supg_lumped_mass(fmo_ctx* c) {
           BM[a][b] += t;
         }
     }
+    /* l_M[conn[e][a/3]*3 + a%3] += row sum a: kept per element and summed
+       per node in element order (supg_mass_nodes) */
     for (int a = 0; a < nd; ++a) {
       double t = 0.0;
       for (int b = 0; b < nd; ++b) t += BM[a][b];
-      c->l_M[(int64_t)c->conn[e * npe + a / 3] * 3 + a % 3] += t;
+      c->lres[e * 24 + a] = t;
     }
   }
 }
 
+static void supg_mass_nodes(fmo_ctx* c, int64_t b, int64_t e) {
+  int npe = c->npe;
+  for (int64_t n = b; n < e; ++n) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t j = c->inc_off[n]; j < c->inc_off[n + 1]; ++j) {
+      int64_t q = c->inc_ent[j];
+      const double* r = c->lres + (q / npe) * 24 + (q % npe) * 3;
+      for (int d = 0; d < 3; ++d) acc[d] += r[d];
+    }
+    for (int d = 0; d < 3; ++d) c->l_M[n * 3 + d] = acc[d];
+  }
+}
+
+static void supg_lumped_mass(fmo_ctx* c) {
+  par_for(c, c->E, supg_lumped_mass_range);
+  par_for(c, c->N, supg_mass_nodes);
+}
+
 /* femSUPGExplicitFluidSolver.cpp:446-501 */
-static void supg_compute_pressure(fmo_ctx* c, const double* sol) {
+static void supg_pressure_range(fmo_ctx* c, int64_t eb, int64_t ee) {
+  const double* sol = c->pres_src;
   int npe = c->npe;
   int ngp;
   double gps[8][3], gpw[8];
   gauss_rule(npe, &ngp, gps, gpw);
-  for (int64_t e = 0; e < c->E; ++e) {
+  for (int64_t e = eb; e < ee; ++e) {
     double xe[8][3], es[24];
     elem_coords(c, e, xe);
     for (int a = 0; a < npe; ++a)
@@ -565,6 +722,11 @@ static void supg_compute_pressure(fmo_ctx* c, const double* sol) {
     }
     c->pres_n[e] = -c->el_lam[e] * (num / den);
   }
+}
+
+static void supg_compute_pressure(fmo_ctx* c, const double* sol) {
+  c->pres_src = sol;
+  par_for(c, c->E, supg_pressure_range);
 }
 
 /* femSUPGExplicitFluidSolver.cpp:660-707 (hexa8 only; tet4 reads out of
@@ -588,22 +750,20 @@ static void supg_avg_shape_deriv(fmo_ctx* c, const double xe[8][3], double avg[8
     for (int b = 0; b < 3; ++b) avg[a][b] = avg[a][b] / den[a][b];
 }
 
-/* One time step of femSUPGExplicitFluidSolver::solve (src lines 1034-1591). */
-static void supg_step(fmo_ctx* c) {
-  int64_t N = c->N, E = c->E;
+/* The element loop of femSUPGExplicitFluidSolver::solve (src lines
+   1095-1472) over elements [eb, ee): k_p, el_lam, el_regime. */
+static void supg_element_range(fmo_ctx* c, int64_t eb, int64_t ee) {
+  int64_t E = c->E;
   int npe = c->npe, nd = npe * 3;
   double rho = c->props[0], mu = c->props[1], alpha = c->props[2], cI = c->props[3];
-  int use_euler = c->ex_opts[0], use_B_hat = c->ex_opts[1];
+  int use_B_hat = c->ex_opts[1];
   int iK1 = c->ex_opts[2], iK2 = c->ex_opts[3], iK3 = c->ex_opts[4], iK4 = c->ex_opts[5];
   double dt = c->dt;
   int ngp;
   double gps[8][3], gpw[8];
   gauss_rule(npe, &ngp, gps, gpw);
-  c->step++;
-  c->cur_time += dt;
-  for (int64_t i = 0; i < N * 3; ++i) c->solN[i] = 0.0;
-  static double K1[24][24], K2[24][24], K3[24][24], K4[24][24], K[24][24];
-  for (int64_t e = 0; e < E; ++e) {
+  double K1[24][24], K2[24][24], K3[24][24], K4[24][24], K[24][24];
+  for (int64_t e = eb; e < ee; ++e) {
     double xe[8][3], es[24], sd0[8][3];
     elem_coords(c, e, xe);
     for (int a = 0; a < npe; ++a)
@@ -745,19 +905,40 @@ static void supg_step(fmo_ctx* c) {
       *kp = 0.0;
       for (int b = 0; b < nd; ++b) *kp += -dt * K[a][b] * es[b];
     }
-    for (int a = 0; a < npe; ++a) {
-      int64_t n = c->conn[e * npe + a];
+  }
+}
+
+/* The scatter of k_p into solN (src lines 1475-1498: Euler, or AB2 after the
+   first step), per node in element order, then the update u^{n+1} = u^n +
+   solN / l_M (src lines 1510-1514). */
+static void supg_update_nodes(fmo_ctx* c, int64_t b, int64_t e) {
+  int64_t E = c->E;
+  int npe = c->npe;
+  int euler = c->ex_opts[0] || c->step == 1;
+  for (int64_t n = b; n < e; ++n) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int64_t j = c->inc_off[n]; j < c->inc_off[n + 1]; ++j) {
+      int64_t q = c->inc_ent[j], el = q / npe;
+      int a = (int)(q % npe);
       for (int d = 0; d < 3; ++d) {
-        double kp = c->k_p[(int64_t)(a * 3 + d) * E + e];
-        if (use_euler || c->step == 1)
-          c->solN[n * 3 + d] += kp;
+        double kp = c->k_p[(int64_t)(a * 3 + d) * E + el];
+        if (euler)
+          acc[d] += kp;
         else
-          c->solN[n * 3 + d] += (3.0 / 2.0) * kp - (1.0 / 2.0) * c->k_pp[(int64_t)(a * 3 + d) * E + e];
+          acc[d] += (3.0 / 2.0) * kp - (1.0 / 2.0) * c->k_pp[(int64_t)(a * 3 + d) * E + el];
       }
     }
+    for (int d = 0; d < 3; ++d) c->solN[n * 3 + d] = c->sol_p[n * 3 + d] + (1.0 / c->l_M[n * 3 + d]) * acc[d];
   }
-  for (int64_t i = 0; i < N; ++i)
-    for (int d = 0; d < 3; ++d) c->solN[i * 3 + d] = c->sol_p[i * 3 + d] + (1.0 / c->l_M[i * 3 + d]) * c->solN[i * 3 + d];
+}
+
+/* One time step of femSUPGExplicitFluidSolver::solve (src lines 1034-1591). */
+static void supg_step(fmo_ctx* c) {
+  int64_t N = c->N, E = c->E;
+  c->step++;
+  c->cur_time += c->dt;
+  par_for(c, E, supg_element_range);
+  par_for(c, N, supg_update_nodes);
   set_node_velocity(c, c->cur_time, c->solN, 3);
   set_dirichlet(c, c->solN, 3);
   supg_compute_pressure(c, c->solN);
@@ -804,13 +985,16 @@ void* fmo_create(int64_t N, int64_t E, int npe, const double* x, const int32_t* 
     c->elmTaus = (double*)calloc(E * 2, sizeof(double));
     c->projRHS = (double*)calloc(E * 16, sizeof(double));
     c->el_u_sdus = (double*)calloc(E * 3, sizeof(double));
+    c->lres = (double*)malloc(sizeof(double) * (E * 16 + 1));
+    build_incidence(c);
     if (init) memcpy(c->sol_tau, init, sizeof(double) * N * 4);
     set_node_velocity(c, 0.0, c->sol_tau, 4);
     apply_zero_traction(c, c->sol_tau);
     set_dirichlet(c, c->sol_tau, 4);
     memcpy(c->sol_prev, c->sol_tau, sizeof(double) * N * 4);
     memcpy(c->sol_n, c->sol_tau, sizeof(double) * N * 4);
-    for (int64_t e = 0; e < E; ++e) vms_initial_assemble(c, e);
+    par_for(c, E, vms_initial_range);
+    par_for(c, N, vms_mass_nodes);
   } else {
     c->sol_p = (double*)calloc(N * 3, sizeof(double));
     c->solN = (double*)calloc(N * 3, sizeof(double));
@@ -820,6 +1004,8 @@ void* fmo_create(int64_t N, int64_t E, int npe, const double* x, const int32_t* 
     c->el_lam = (double*)calloc(E, sizeof(double));
     c->el_regime = (double*)calloc(E, sizeof(double));
     c->pres_n = (double*)calloc(E, sizeof(double));
+    c->lres = (double*)malloc(sizeof(double) * (E * 24 + 1));
+    build_incidence(c);
     if (init)
       for (int64_t i = 0; i < N; ++i)
         for (int d = 0; d < 3; ++d) c->sol_p[i * 3 + d] = init[i * 4 + d];
@@ -882,7 +1068,7 @@ void fmo_destroy(void* h) {
   void* ptrs[] = {c->vel_node, c->vel_off, c->vel_len, c->vel_tab, c->vel_dir, c->dir_node, c->dir_vals, c->pres_node,
                   c->pres_vals, c->sol_n, c->sol_prev, c->sol_tau, c->rhs, c->sdus, c->sgps, c->volumes, c->DNs,
                   c->char_length, c->nd_mass, c->elmTaus, c->projRHS, c->el_u_sdus, c->sol_p, c->solN, c->l_M,
-                  c->k_p, c->k_pp, c->el_lam, c->el_regime, c->pres_n};
+                  c->k_p, c->k_pp, c->el_lam, c->el_regime, c->pres_n, c->inc_off, c->inc_ent, c->lres};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
   free(c);
 }

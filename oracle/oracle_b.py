@@ -38,8 +38,19 @@ def lib():
         L.fmo_step.argtypes = [P, C.c_int]
         L.fmo_get.argtypes = [P, P, P, P, P]
         L.fmo_destroy.argtypes = [P]
+        L.fmo_set_threads.argtypes = [C.c_int]
+        L.fmo_get_threads.restype = C.c_int
         _lib = L
     return _lib
+
+
+def set_threads(n: int) -> None:
+    """Host threads of the element loops (results do not depend on it)."""
+    lib().fmo_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().fmo_get_threads())
 
 
 def _ptr(a):

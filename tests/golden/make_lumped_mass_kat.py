@@ -13,6 +13,7 @@ the nodes whose every incident element lies in that block (those values are
 complete within the block).  The resulting fixture is a few tens of KB.
 
 Run from the repository root:  python tests/golden/make_lumped_mass_kat.py [reference_root]
+(default: $FEMORPH_REFERENCE, else /root/reference)
 """
 import base64
 import os
@@ -22,7 +23,7 @@ import zlib
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FEMORPH_REFERENCE", "/root/reference")
 EX = os.path.join(REF, "examples/02_explicit_fluid_VMS/06_2D_hexa_lid_driven_cavity")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lumped_mass_kat.npz")
 

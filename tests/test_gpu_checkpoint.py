@@ -132,6 +132,21 @@ def test_foreign_and_truncated_files_refused(tmp_path):
     assert ei.value.code == api.FM_ERR_INVALID
     bh.close()
     h.close()
+    # the same mesh with another time step, and with another lid speed
+    for change in ("dt", "lid"):
+        q = vms_problem()
+        if change == "dt":
+            q.time_step *= 1.5
+        else:
+            q.vel_vals = np.array(q.vel_vals) * 1.1
+        h = api.GpuProblem(q)
+        bh = api.Batch([h])
+        with pytest.raises(api.FmError) as ei:
+            h.restore(path)
+        assert ei.value.code == api.FM_ERR_INVALID, change
+        bh.close()
+        h.close()
+    assert not os.path.exists(path + ".tmp")
     # the same mesh in the other precision
     m = api.GpuProblem(vms_problem(), api.FM_MIXED)
     bm = api.Batch([m])

@@ -19,6 +19,7 @@ import pytest
 
 from femorph_b200 import api, mesh
 from femorph_b200.partition import assemble
+from oracle import oracle_b
 
 pytestmark = pytest.mark.gpu
 
@@ -95,6 +96,32 @@ def test_supg_tet_custom_split():
     u0, p0 = whole(p, 20)
     u1, p1 = split_one_batch(p, 3, 20, elem_part=ep)
     assert rel(u1, u0) < TOL and rel(p1, p0) < TOL
+
+
+def test_vms_parts_against_oracle():
+    """The split solve (3 Morton-band parts, one exchange per iteration)
+    against the oracle directly: FP64 within 1e-10 after 40 steps."""
+    p = mesh.cavity(16, seed=5, steps=40)
+    o = oracle_b.OracleSolve(p)
+    o.step(40)
+    st = o.state()[0]
+    u1, p1 = split_one_batch(p, 3, 40)
+    eu, ep = rel(u1, st[:, :3]), rel(p1, st[:, 3])
+    print(f"[parity] vms16 in 3 parts, step 40 vs oracle: u {eu:.3e} p {ep:.3e}")
+    assert eu <= 1e-10 and ep <= 1e-10, (eu, ep)
+
+
+def test_supg_hexa_parts_against_oracle():
+    """SUPG hexa8 (AB2, B-bar) split in 3 parts against the oracle: velocity
+    and element pressure within 1e-10 after 20 steps."""
+    p = mesh.channel(16, 6, 5, seed=6, steps=20, ex_opts=(0, 1, 1, 1, 1, 1))
+    o = oracle_b.OracleSolve(p)
+    o.step(20)
+    st, oel, _, _ = o.state()
+    u1, p1 = split_one_batch(p, 3, 20)
+    eu, ep = rel(u1, st[:, :3]), rel(p1, oel[:, 0])
+    print(f"[parity] channel16x6x5 in 3 parts, step 20 vs oracle: u {eu:.3e} element p {ep:.3e}")
+    assert eu <= 1e-10 and ep <= 1e-10, (eu, ep)
 
 
 def test_two_batches_external_exchange():

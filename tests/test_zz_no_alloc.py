@@ -4,8 +4,10 @@ on which cudaMalloc/cudaFree's device-wide synchronisation is not
 acceptable).  It keeps everything in one fixed device array, so two calls
 in a row must not see each other's leftovers.  Each call is checked, through
 the C ABI, against the allocating path (fm_batch_create + fm_batch_step +
-fm_problem_get_state) with the per-step tolerance of the parity tests; the
-two paths run the same kernels on the same tile layout.
+fm_problem_get_state): the two paths run the same kernels on the same tile
+layout in the same order, so their results must be equal bit for bit (any
+leftover state of the previous call would break that).  Each call is also
+checked against the oracle with the per-step tolerance of the parity tests.
 
 This file sorts last so that a run stopping at the first failure has run
 every other test before it."""
@@ -15,6 +17,7 @@ import numpy as np
 import pytest
 
 from femorph_b200 import api, mesh
+from oracle import oracle_b
 
 pytestmark = pytest.mark.gpu
 
@@ -66,7 +69,12 @@ def test_two_calls_in_a_row_match_allocating_path():
         u, pr = static_path(p, steps)
         u0, pr0 = allocating_path(p, steps)
         assert np.isfinite(u).all() and np.isfinite(pr).all()
-        assert rel(u, u0) <= TOL and rel(pr, pr0) <= TOL, (rel(u, u0), rel(pr, pr0))
+        assert np.array_equal(u, u0) and np.array_equal(pr, pr0), (rel(u, u0), rel(pr, pr0))
+        o = oracle_b.OracleSolve(p)
+        o.step(steps)
+        st = o.state()[0]
+        o.close()
+        assert rel(u, st[:, :3]) <= TOL and rel(pr, st[:, 3]) <= TOL, (rel(u, st[:, :3]), rel(pr, st[:, 3]))
 
 
 def test_rejects_problems_beyond_the_array():
