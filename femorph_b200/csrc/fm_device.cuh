@@ -161,14 +161,17 @@ __device__ __forceinline__ float rcbrt_nr(float x) {
   const float e = fmaf(-x, y * y * y, 1.0f);
   return fmaf(y * (1.0f / 3.0f), e, y);
 }
-// sqrt(x) for x >= 0 via 1/sqrt: Newton y <- y (3 - x y^2) / 2, then x y.
+// sqrt(x) for x >= 0: one Newton step on y = 1/sqrt(x),
+// y <- y (3 - x y^2) / 2 (relative error ~2^-44), then s = x y and one
+// Newton step on s itself with the exact residual x - s^2 (an FMA),
+// s <- s + (x - s^2) y / 2, which leaves s within an ulp of sqrt(x).
 __device__ __forceinline__ double sqrt_nr(double x) {
   if (!(x > 0.0)) return 0.0;
   if (!(x > 1e-37 && x < 1e37)) return sqrt(x);
   double y = (double)ptx_rsqrt_approx((float)x);
-#pragma unroll
-  for (int i = 0; i < 2; ++i) y = y * fma(-0.5 * x, y * y, 1.5);
-  return x * y;
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  const double s = x * y;
+  return fma(fma(-s, s, x), 0.5 * y, s);
 }
 
 // femUtils.cpp:830-871 (interpTableData) with femUtils.cpp:818-828

@@ -7,9 +7,11 @@
 //      geometry from the staged coordinates, the pending subscale update of
 //      the previous iteration (assemble_projRes_explicit +
 //      update_subscales_explicit), the element residual (assemble_RHS);
-//   3. add the 16 residual entries to shared-memory node accumulators, one
-//      colour at a time (elements of a colour share no node), so every node
-//      receives its contributions in a fixed order - no atomics;
+//   3. stage the chunk's 16 residual entries an element in shared memory;
+//      after one barrier each thread adds, for the nodes it owns, the
+//      chunk's contributions to its shared-memory accumulators, walking the
+//      node's incidence list in element order, so every node receives its
+//      contributions in a fixed order - no atomics;
 //   4. nodes interior to the tile are complete: dual update
 //      (update_dual_solution), BCs (setNodeVelocity, apply_zeroTraction,
 //      setDirichletBC) and store; interface nodes store their tile partial.

@@ -45,7 +45,7 @@ def test_newton_raphson_math_within_ulps_of_cuda():
     # against extended-precision values on the host (CUDA's rcbrt is itself
     # within about an ulp)
     ld = np.asarray(x[pos], np.longdouble)
-    exact = np.asarray(ld ** np.longdouble(-1.0 / 3.0) if hasattr(np, "longdouble") else ld, np.float64)
+    exact = np.asarray(ld ** (np.longdouble(-1) / np.longdouble(3)), np.float64)
     r_cbrt_exact = ulps(out[pos, 2], exact).max()
     print(f"[math] max ulps: rcp_nr vs 1/x {r_rcp:.2f}, rcbrt_nr vs rcbrt {r_cbrt:.2f} "
           f"(vs extended {r_cbrt_exact:.2f}), sqrt_nr vs sqrt {r_sqrt:.2f}, rcbrt_nr(float) vs rcbrtf {r_cbrtf:.2f}")
