@@ -32,7 +32,25 @@ namespace fm {
 // differs at BC nodes).  The dual update starts from sol_n, which is the
 // post-BC state at the first dual iteration of a step (update_solution,
 // src lines 726-752) and the pre-BC state afterwards.
-__device__ __forceinline__ void vms_node_update(const DevBatch& B, const DevProb& P, int pidx, int iter, double time,
+// The problem constants the element and node passes read, copied into
+// registers once per CTA (read through the DevProb in global memory they
+// would be reloaded for every element: the compiler cannot prove that the
+// kernel's own stores leave them unchanged).
+struct VmsConsts {
+  double ds, c2, inv_eps;
+  int32_t q1[4];
+};
+__device__ __forceinline__ VmsConsts vms_consts(const DevProb& P) {
+  VmsConsts c;
+  c.ds = P.ds;
+  c.c2 = P.c2;
+  c.inv_eps = P.inv_eps;
+  c.q1[0] = P.q1[0]; c.q1[1] = P.q1[1]; c.q1[2] = P.q1[2]; c.q1[3] = P.q1[3];
+  return c;
+}
+
+template <class PROB>  // DevProb or VmsConsts: reads ds and q1[]
+__device__ __forceinline__ void vms_node_update(const DevBatch& B, const PROB& P, int pidx, int iter, double time,
                                                 int64_t g, const double post[4], const double acc[4], bool first_dual,
                                                 int32_t* status) {
   const int32_t rec = B.node_bc[g];
@@ -57,29 +75,34 @@ __device__ __forceinline__ void vms_node_update(const DevBatch& B, const DevProb
 }
 
 // Node records in shared memory: four 16-byte pieces per node, (x, y)
-// (z, u) (v, w) (p, BC tag), piece k of node ln stored at position
+// (z, u) (v, w) (p, tag), piece k of node ln stored at position
 // k ^ ((ln >> 1) & 3).  With 64-byte records the unswizzled piece k of every
 // node falls in one of only two 4-bank groups, so a warp's 16-byte loads of
 // 32 different nodes serialise up to 16-fold; the swizzle spreads them over
 // all eight groups.
 __device__ __forceinline__ int rec_index(int ln, int k) { return ln * 4 + (k ^ ((ln >> 1) & 3)); }
 
+// Node record piece 3 = (p, tag): tag = batch node id, with bit 62 set when
+// the node carries a BC (its pre-BC values are then read from memory).
+constexpr long long FM_TAG_BC = 1ll << 62;
+
 // Per-element VMS work for one chunk slot: pending subscale update (written
 // back to global memory) and the element residual lres.  S: subscale storage
 // type (double, or float in the mixed form).
 template <bool MIXED, typename S>
-__device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P, int64_t e, const int ln[4],
+__device__ __forceinline__ void vms_element(const DevBatch& B, const VmsConsts& P, int64_t e, const int ln[4],
                                             bool precise, const double2* s_rec, const S sd_in[12],
                                             const double pq[4], bool pending, bool first_dual, double inv_dt,
                                             double c1nu, double nu4, double lres[4][4]) {
   const int64_t E = B.E;
   // Pass 1 reads the coordinates and Q, the velocity before the last BC
-  // application (it differs from the staged state only at BC nodes, tag >= 0
-  // = the node's global id, and is read from memory there).  FP64: pass 2
+  // application (it differs from the staged state only at BC nodes, whose
+  // tag has FM_TAG_BC set beside the node's batch id, and is read from
+  // memory there).  FP64: pass 2
   // re-reads the post-BC velocity U and pressure from shared memory, so the
   // two velocity sets are never held in registers at the same time (the
   // FP32 form, with fewer live registers, reads them in pass 1).
-  // Node record: (x, y) (z, u) (v, w) (p, BC tag).
+  // Node record: (x, y) (z, u) (v, w) (p, tag).
   double X[4][3], Q[4][3], U[4][3], Pn[4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
@@ -90,8 +113,9 @@ __device__ __forceinline__ void vms_element(const DevBatch& B, const DevProb& P,
       U[a][0] = r1.y; U[a][1] = r2.x; U[a][2] = r2.y;
       Pn[a] = r3.x;
     }
-    const long long g = __double_as_longlong(r3.y);
-    if (g >= 0) {
+    const long long tag = __double_as_longlong(r3.y);
+    if (tag & FM_TAG_BC) {
+      const long long g = tag & 0x7fffffffll;
       Q[a][0] = B.pu[g]; Q[a][1] = B.pv[g]; Q[a][2] = B.pw[g];
     } else {
       Q[a][0] = r1.y; Q[a][1] = r2.x; Q[a][2] = r2.y;
@@ -195,7 +219,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   using S = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(16) double sm[];
   const int tn_pad = (tn_max + 1) & ~1;
-  double2* s_rec = reinterpret_cast<double2*>(sm);  // per node: (x,y) (z,u) (v,w) (p,BC tag)
+  double2* s_rec = reinterpret_cast<double2*>(sm);  // per node: (x,y) (z,u) (v,w) (p,tag)
   double* s_a0 = sm + 8 * tn_pad;  // residual accumulators (each node owned by one thread)
   double* s_a1 = s_a0 + tn_pad;
   double* s_a2 = s_a1 + tn_pad;
@@ -214,6 +238,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   const DevProbState st = B.pstate[pidx];
   if (st.iter >= B.target[pidx] || st.status != FM_OK) return;
   const DevProb& P = B.probs[pidx];
+  const VmsConsts PC = vms_consts(P);
   const int per_step = P.ndual + 1;
   const bool first_dual = (st.iter % per_step) == 0;
   const bool pending = st.iter > 0;
@@ -263,7 +288,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
       const int ln = tid + j * THREADS;
       const int g = gid[j];
       if (g >= 0) {
-        const long long tag = B.node_bc[g] >= 0 ? (long long)g : -1ll;
+        const long long tag = (long long)g | (B.node_bc[g] >= 0 ? FM_TAG_BC : 0ll);
         s_rec[rec_index(ln, 0)] = make_double2(B.x[g], B.y[g]);
         s_rec[rec_index(ln, 1)] = make_double2(B.z[g], B.su[g]);
         s_rec[rec_index(ln, 2)] = make_double2(B.sv[g], B.sw[g]);
@@ -289,11 +314,8 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   const double nu4 = 4.0 * P.nu;
   __syncthreads();
 
-  // nodes owned by this thread for the accumulation: consecutive local nodes
-  // (which tend to be active in the same chunk) go to different warps,
-  // node = j * THREADS + lane * warps + warp; cur/end walk each one's
-  // incidence list in element order
-  constexpr int WARPS = THREADS / 32;
+  // nodes owned by this thread for the accumulation: j * THREADS + tid;
+  // cur/end walk each one's incidence list in element order
   auto owned_node = [](int t, int j) { return j * THREADS + t; };
   int cur[MAXOWN], endi[MAXOWN];
 #pragma unroll
@@ -337,7 +359,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
 #pragma unroll
       for (int q = 0; q < 12; ++q) sd_in[q] = bs[q * THREADS + tid];
       double lres[4][4];
-      vms_element<MIXED, S>(B, P, tm.elem_begin + le, ln, precise, s_rec, sd_in, pq, pending, first_dual, inv_dt,
+      vms_element<MIXED, S>(B, PC, tm.elem_begin + le, ln, precise, s_rec, sd_in, pq, pending, first_dual, inv_dt,
                             c1nu, nu4, lres);
       if (B.diag_res) {
 #pragma unroll
@@ -411,10 +433,10 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
     if (ln2 >= tm.n_node) break;
     const double acc[4] = {s_a0[ln2], s_a1[ln2], s_a2[ln2], s_a3[ln2]};
     if (ln2 < tm.n_int) {
-      const int g = B.tile_nodes[tm.node_begin + ln2];
       const double2 r1 = s_rec[rec_index(ln2, 1)], r2 = s_rec[rec_index(ln2, 2)], r3 = s_rec[rec_index(ln2, 3)];
+      const int g = (int)(__double_as_longlong(r3.y) & 0x7fffffffll);
       const double post[4] = {r1.y, r2.x, r2.y, r3.x};
-      vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
+      vms_node_update(B, PC, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
     } else {
       const int s = tm.slot_base + (ln2 - tm.n_int);
       B.part[2 * s] = make_double2(acc[0], acc[1]);

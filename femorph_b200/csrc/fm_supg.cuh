@@ -142,6 +142,35 @@ __device__ __forceinline__ double jacobian(const double dN[NPE][3], const double
   return jacobian_at<NPE>([&](int n, int a) { return dN[n][a]; }, sx, sy, sz, ln, inv);
 }
 
+// Per Gauss point (per element for tet4): G = J^-T J^-1
+// (femElement.cpp:192-232), the G:G term of tau, (mu/rho)^2 cI G:G
+// (eval_stabilization, src lines 336-377), and G's cofactor inverse
+// (eval_bulk_modulus, src lines 382-441).
+__device__ __forceinline__ void tet_metric(const double inv[3][3], double nu, double cI, double G[3][3], double& t3,
+                                           double iG[3][3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
+  t3 = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
+  t3 = t3 * nu * nu * cI;
+  const double m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
+               m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
+  const double dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+  const double idg = 1.0 / dG;
+  iG[0][0] = (m11 * m22 - m21 * m12) * idg;
+  iG[0][1] = (m02 * m21 - m01 * m22) * idg;
+  iG[0][2] = (m01 * m12 - m02 * m11) * idg;
+  iG[1][0] = (m12 * m20 - m10 * m22) * idg;
+  iG[1][1] = (m00 * m22 - m02 * m20) * idg;
+  iG[1][2] = (m10 * m02 - m00 * m12) * idg;
+  iG[2][0] = (m10 * m21 - m20 * m11) * idg;
+  iG[2][1] = (m20 * m01 - m00 * m21) * idg;
+  iG[2][2] = (m00 * m11 - m10 * m01) * idg;
+}
+
 // One element: k[a][c] = -dt (sum of the enabled K_i u_e)[a][c].  Coordinates
 // and velocities are read from the tile's shared-memory node arrays through
 // the local ids ln[].  Also returns the element's lambda (volume average) and
@@ -195,6 +224,16 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
 #pragma unroll
     for (int c = 0; c < 3; ++c) Dbar[c] = dsum[c] / bden;
   }
+  // tet4: the local derivatives are constant, so the Jacobian, its inverse,
+  // G = J^-T J^-1, the G:G term of tau and G's inverse are element constants;
+  // they are formed once here (the same expressions as at every Gauss point,
+  // hence the same values) instead of at each of the 4 points
+  auto dN4 = [](int a, int c) -> double { return a == 3 ? -1.0 : (a == c ? 1.0 : 0.0); };
+  double inv4[3][3], det4 = 0.0, G4[3][3], t3_4 = 0.0, iG4[3][3];
+  if constexpr (NPE == 4) {
+    det4 = jacobian_at<NPE>(dN4, sx, sy, sz, ln, inv4);
+    tet_metric(inv4, nu, cI, G4, t3_4, iG4);
+  }
   double vol = 0.0, lam_int = 0.0, reg = 0.0;
 #pragma unroll 1
   for (int g = 0; g < GaussRule<NPE>::n; ++g) {
@@ -209,19 +248,29 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
     }
     auto Nv = [&](int a) -> double { return NPE == 4 ? Nq[a] : tab.N[g][a]; };
     auto dNv = [&](int a, int c) -> double {
-      if (NPE == 4) return a == 3 ? -1.0 : (a == c ? 1.0 : 0.0);
+      if (NPE == 4) return dN4(a, c);
       return tab.dN[g][a][c];
     };
-    double inv[3][3];
-    const double det = NPE == 8 ? jac_inv(g, inv) : jacobian_at<NPE>(dNv, sx, sy, sz, ln, inv);
+    double inv[3][3], G[3][3], t3 = 0.0, iG[3][3];
+    double det;
+    if constexpr (NPE == 4) {
+      det = det4;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          inv[a][b] = inv4[a][b];
+          G[a][b] = G4[a][b];
+          iG[a][b] = iG4[a][b];
+        }
+      t3 = t3_4;
+    } else {
+      det = jac_inv(g, inv);
+      tet_metric(inv, nu, cI, G, t3, iG);
+    }
     auto gdv = [&](int a, int b) -> double {
       return inv[b][0] * dNv(a, 0) + inv[b][1] * dNv(a, 1) + inv[b][2] * dNv(a, 2);
     };
-    double G[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
     // velocity, gradient, divergence at the point
     double u[3] = {0.0, 0.0, 0.0}, gr[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
 #pragma unroll
@@ -239,29 +288,17 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
     const double div = gr[0][0] + gr[1][1] + gr[2][2];
     // eval_stabilization (dt term removed in the reference)
     const double trG = G[0][0] + G[1][1] + G[2][2];
-    double t2 = 0.0, t3 = 0.0;
+    double t2 = 0.0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
-      t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
-    }
-    t3 = t3 * nu * nu * cI;
+    for (int a = 0; a < 3; ++a) t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
     const double tau = 1.0 / sqrt(t2 + t3);
     const double nuC = 1.0 / (trG * tau);
     // eval_bulk_modulus: lambda = alpha * max(mu/rho, sqrt(u^T G^-1 u))
     double lam, regime;
     {
-      const double m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
-                   m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
-      const double dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
-      const double idg = 1.0 / dG;
-      const double i00 = (m11 * m22 - m21 * m12) * idg, i01 = (m02 * m21 - m01 * m22) * idg,
-                   i02 = (m01 * m12 - m02 * m11) * idg, i10 = (m12 * m20 - m10 * m22) * idg,
-                   i11 = (m00 * m22 - m02 * m20) * idg, i12 = (m10 * m02 - m00 * m12) * idg,
-                   i20 = (m10 * m21 - m20 * m11) * idg, i21 = (m20 * m01 - m00 * m21) * idg,
-                   i22 = (m00 * m11 - m10 * m01) * idg;
-      const double l2 = sqrt((i00 * u[0] + i01 * u[1] + i02 * u[2]) * u[0] + (i10 * u[0] + i11 * u[1] + i12 * u[2]) * u[1] +
-                             (i20 * u[0] + i21 * u[1] + i22 * u[2]) * u[2]);
+      const double l2 = sqrt((iG[0][0] * u[0] + iG[0][1] * u[1] + iG[0][2] * u[2]) * u[0] +
+                             (iG[1][0] * u[0] + iG[1][1] * u[1] + iG[1][2] * u[2]) * u[1] +
+                             (iG[2][0] * u[0] + iG[2][1] * u[1] + iG[2][2] * u[2]) * u[2]);
       const double l1 = nu;
       lam = alpha * ((l1 < l2) ? l2 : l1);  // std::max(limit_1, limit_2)
       regime = (l1 > l2) ? 1.0 : 2.0;
@@ -383,6 +420,32 @@ __device__ __forceinline__ float rsqrt_f(float x) {
   return y * fmaf(-0.5f * x, y * y, 1.5f);
 }
 
+// FP32 form of tet_metric.
+__device__ __forceinline__ void metric_f(const float inv[3][3], float nu, float cI, float G[3][3], float& t3,
+                                         float iG[3][3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
+  t3 = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
+  t3 = t3 * nu * nu * cI;
+  const float m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
+              m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
+  const float dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+  const float idg = rcp_f(dG);
+  iG[0][0] = (m11 * m22 - m21 * m12) * idg;
+  iG[0][1] = (m02 * m21 - m01 * m22) * idg;
+  iG[0][2] = (m01 * m12 - m02 * m11) * idg;
+  iG[1][0] = (m12 * m20 - m10 * m22) * idg;
+  iG[1][1] = (m00 * m22 - m02 * m20) * idg;
+  iG[1][2] = (m10 * m02 - m00 * m12) * idg;
+  iG[2][0] = (m10 * m21 - m20 * m11) * idg;
+  iG[2][1] = (m20 * m01 - m00 * m21) * idg;
+  iG[2][2] = (m00 * m11 - m10 * m01) * idg;
+}
+
 template <int NPE>
 __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const ShapeTable<NPE, float>& tab,
                                                    const ShapeTable<NPE, double>& tabd, const float Xr[NPE][3],
@@ -480,11 +543,33 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
 #pragma unroll
       for (int b = 0; b < 3; ++b) sd0[a][b] = num[a][b] * iden;
   }
+  // tet4: inverse Jacobian, G, its G:G term and G's inverse are element
+  // constants, formed once (the same values as at every Gauss point)
+  float inv4[3][3], det4 = 0.0f, G4[3][3], t3_4 = 0.0f, iG4[3][3];
+  if constexpr (NPE == 4) {
+    det4 = geometry(0, inv4);
+    metric_f(inv4, nu, cI, G4, t3_4, iG4);
+  }
   float vol = 0.0f, lam_int = 0.0f, reg = 0.0f;
 #pragma unroll 1
   for (int g = 0; g < GaussRule<NPE>::n; ++g) {
-    float inv[3][3];
-    const float det = geometry(g, inv);
+    float inv[3][3], G[3][3], t3, iG[3][3];
+    float det;
+    if constexpr (NPE == 4) {
+      det = det4;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          inv[a][b] = inv4[a][b];
+          G[a][b] = G4[a][b];
+          iG[a][b] = iG4[a][b];
+        }
+      t3 = t3_4;
+    } else {
+      det = geometry(g, inv);
+      metric_f(inv, nu, cI, G, t3, iG);
+    }
     float gd[NPE][3];
     {
       const float2 i0 = make_float2(inv[0][0], inv[1][0]), i1 = make_float2(inv[0][1], inv[1][1]),
@@ -499,11 +584,6 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
         gd[a][2] = inv[2][0] * d0 + inv[2][1] * d1 + inv[2][2] * d2;
       }
     }
-    float G[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b) G[a][b] = inv[0][a] * inv[0][b] + inv[1][a] * inv[1][b] + inv[2][a] * inv[2][b];
     float u[3], gr[3][3];
     {
       // (u0, u1) and (gr[c][0], gr[c][1]) as pairs
@@ -532,29 +612,17 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
     const float div = gr[0][0] + gr[1][1] + gr[2][2];
     // eval_stabilization (dt term removed in the reference)
     const float trG = G[0][0] + G[1][1] + G[2][2];
-    float t2 = 0.0f, t3 = 0.0f;
+    float t2 = 0.0f;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
-      t3 += G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
-    }
-    t3 = t3 * nu * nu * cI;
+    for (int a = 0; a < 3; ++a) t2 += u[a] * (G[a][0] * u[0] + G[a][1] * u[1] + G[a][2] * u[2]);
     const float tau = rsqrt_f(t2 + t3);
     const float nuC = rcp_f(trG * tau);
     // eval_bulk_modulus: lambda = alpha * max(mu/rho, sqrt(u^T G^-1 u))
     float lam, regime;
     {
-      const float m00 = G[0][0], m01 = G[0][1], m02 = G[0][2], m10 = G[1][0], m11 = G[1][1], m12 = G[1][2],
-                  m20 = G[2][0], m21 = G[2][1], m22 = G[2][2];
-      const float dG = m00 * (m11 * m22 - m21 * m12) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
-      const float idg = rcp_f(dG);
-      const float i00 = (m11 * m22 - m21 * m12) * idg, i01 = (m02 * m21 - m01 * m22) * idg,
-                  i02 = (m01 * m12 - m02 * m11) * idg, i10 = (m12 * m20 - m10 * m22) * idg,
-                  i11 = (m00 * m22 - m02 * m20) * idg, i12 = (m10 * m02 - m00 * m12) * idg,
-                  i20 = (m10 * m21 - m20 * m11) * idg, i21 = (m20 * m01 - m00 * m21) * idg,
-                  i22 = (m00 * m11 - m10 * m01) * idg;
-      const float q2 = (i00 * u[0] + i01 * u[1] + i02 * u[2]) * u[0] + (i10 * u[0] + i11 * u[1] + i12 * u[2]) * u[1] +
-                       (i20 * u[0] + i21 * u[1] + i22 * u[2]) * u[2];
+      const float q2 = (iG[0][0] * u[0] + iG[0][1] * u[1] + iG[0][2] * u[2]) * u[0] +
+                       (iG[1][0] * u[0] + iG[1][1] * u[1] + iG[1][2] * u[2]) * u[1] +
+                       (iG[2][0] * u[0] + iG[2][1] * u[1] + iG[2][2] * u[2]) * u[2];
       const float l2 = q2 > 0.0f ? q2 * rsqrt_f(q2) : sqrtf(q2);  // sqrt; NaN for negative input as sqrt
       const float l1 = nu;
       lam = alpha * ((l1 < l2) ? l2 : l1);  // std::max(limit_1, limit_2)
