@@ -82,6 +82,9 @@ __device__ __forceinline__ void vms_node_update(const DevBatch& B, const PROB& P
 // all eight groups.
 __device__ __forceinline__ int rec_index(int ln, int k) { return ln * 4 + (k ^ ((ln >> 1) & 3)); }
 
+// Brings the line holding *p into L1 (no data returned).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // Node record piece 3 = (p, tag): tag = batch node id, with bit 62 set when
 // the node carries a BC (its pre-BC values are then read from memory).
 constexpr long long FM_TAG_BC = 1ll << 62;
@@ -235,6 +238,16 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   const TileMeta tm = B.tiles[blockIdx.x];
   const int pidx = tm.problem;
   if (pidx < 0) return;  // free tile slot
+  const int tid = threadIdx.x;
+  // this thread's staged nodes: their ids are loaded before the problem
+  // state is checked, so both round trips overlap
+  constexpr int MAXOWN = FM_MAX_TILE_NODES / THREADS;  // the host caps tile_nodes
+  int gid[MAXOWN];
+#pragma unroll
+  for (int j = 0; j < MAXOWN; ++j) {
+    const int ln = tid + j * THREADS;
+    gid[j] = ln < tm.n_node ? B.tile_nodes[tm.node_begin + ln] : -1;
+  }
   const DevProbState st = B.pstate[pidx];
   if (st.iter >= B.target[pidx] || st.status != FM_OK) return;
   const DevProb& P = B.probs[pidx];
@@ -242,7 +255,6 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   const int per_step = P.ndual + 1;
   const bool first_dual = (st.iter % per_step) == 0;
   const bool pending = st.iter > 0;
-  const int tid = threadIdx.x;
   const int64_t E = B.E;
   const S* sdus_g = MIXED ? reinterpret_cast<const S*>(B.sdus32) : reinterpret_cast<const S*>(B.sdus);
   const uint2* conn_g = reinterpret_cast<const uint2*>(B.conn);
@@ -273,16 +285,9 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
     // the stage buffers, which the staging does not touch)
     if (nchunks > 0) issue(0);
   }
-  // node staging: all of this thread's node ids first, then their loads,
-  // so the gathers of its (up to FM_MAX_TILE_NODES / THREADS) nodes overlap
-  constexpr int MAXOWN = FM_MAX_TILE_NODES / THREADS;  // the host caps tile_nodes
+  // node staging: the gathers of this thread's (up to FM_MAX_TILE_NODES /
+  // THREADS) nodes overlap
   {
-    int gid[MAXOWN];
-#pragma unroll
-    for (int j = 0; j < MAXOWN; ++j) {
-      const int ln = tid + j * THREADS;
-      gid[j] = ln < tm.n_node ? B.tile_nodes[tm.node_begin + ln] : -1;
-    }
 #pragma unroll
     for (int j = 0; j < MAXOWN; ++j) {
       const int ln = tid + j * THREADS;
@@ -329,6 +334,19 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
     if (tid == 0 && k + 1 < nchunks) {
       fence_proxy_async_smem();  // buffer (k+1)&1 was last read before the previous barrier
       issue(k + 1);
+    }
+    if (k + 1 == nchunks) {
+      // the node update after the last chunk reads the mass and BC index of
+      // this thread's interior nodes: fetch them into L1 now
+#pragma unroll
+      for (int j = 0; j < MAXOWN; ++j) {
+        const int ln2 = tid + j * THREADS;
+        if (ln2 < tm.n_int) {
+          const int g = (int)(__double_as_longlong(s_rec[rec_index(ln2, 3)].y) & 0x7fffffffll);
+          prefetch_l1(B.mass + g);
+          prefetch_l1(B.node_bc + g);
+        }
+      }
     }
     // each thread waits for the chunk itself (the mbarrier phase makes the
     // bulk-copied bytes visible to it); a timed-out wait skips the chunk and
