@@ -703,7 +703,8 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
     const int64_t inc_end = (int64_t)L.tile_inc.size();
     if (ntile > 0)  // alignment gap after the previous problem's entries
       std::fill(L.tile_inc.begin() + inc_prev, L.tile_inc.begin() + tms[0].inc_begin, 0);
-    // each tile fills its ranges and the padding up to the next tile
+    // each tile fills its ranges and the padding up to the next tile (a few
+    // tiles a block: the per-tile copies are large)
     parallel_blocks(ntile, [&](int64_t tb, int64_t te2, int) {
       for (int64_t t = tb; t < te2; ++t) {
         const TileWork& W = tw[t];
@@ -724,7 +725,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         std::copy(W.eo.begin(), W.eo.end(), eo.begin() + (tm.elem_begin - elem_base));
         std::fill(eo.begin() + (tm.elem_begin - elem_base) + tm.n_elem, eo.begin() + eo_next, -1);
       }
-    });
+    }, 8);
     if (ntile == 0) {
       std::fill(L.conn_local.begin() + (size_t)elem_base * npe, L.conn_local.end(), 0);
       std::fill(eo.begin(), eo.end(), -1);
