@@ -216,11 +216,12 @@ void compute_mass(fm_problem* p) {
 
 // Sorts element indices by (key, index) - the order a stable sort by key
 // gives.  Keys are below 2^63 (3 x 21-bit Morton interleave): the pairs are
-// distributed into 4096 buckets by their top 12 bits (per-worker histograms),
-// then the buckets are sorted in parallel.
+// distributed into 65536 buckets by their top 16 bits (per-worker histograms),
+// then the buckets are sorted in parallel.  The pair array is a trivial type,
+// so it is first touched by the distributing threads, not zeroed first.
 static void sort_by_key(const hvec<uint64_t>& key, hvec<int64_t>& order) {
   const int64_t E = (int64_t)key.size();
-  constexpr int NB = 4096, SHIFT = 63 - 12;
+  constexpr int NB = 1 << 16, SHIFT = 63 - 16;
   const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
   const int64_t nw = std::min<int64_t>(hw, std::max<int64_t>(1, E / 65536));
   std::vector<int64_t> hist((size_t)nw * NB, 0);
@@ -247,10 +248,15 @@ static void sort_by_key(const hvec<uint64_t>& key, hvec<int64_t>& order) {
     }
     start[NB] = acc;
   }
-  hvec<std::pair<uint64_t, int64_t>> kv(E);
+  struct KV {
+    uint64_t k;
+    int64_t i;
+    bool operator<(const KV& o) const { return k < o.k || (k == o.k && i < o.i); }
+  };
+  hvec<KV> kv(E);
   run([&](int64_t w, int64_t b, int64_t e) {
     int64_t* h = &hist[(size_t)w * NB];
-    for (int64_t i = b; i < e; ++i) kv[h[std::min<uint64_t>(key[i] >> SHIFT, NB - 1)]++] = {key[i], i};
+    for (int64_t i = b; i < e; ++i) kv[h[std::min<uint64_t>(key[i] >> SHIFT, NB - 1)]++] = KV{key[i], i};
   });
   {
     std::vector<std::thread> th;
@@ -263,7 +269,7 @@ static void sort_by_key(const hvec<uint64_t>& key, hvec<int64_t>& order) {
   }
   order.resize(E);
   parallel_blocks(E, [&](int64_t b, int64_t e, int) {
-    for (int64_t i = b; i < e; ++i) order[i] = kv[i].second;
+    for (int64_t i = b; i < e; ++i) order[i] = kv[i].i;
   });
 }
 
