@@ -116,18 +116,23 @@ def algorithmic_bytes(E: int, N: int, precision: str, config: str = "cavity") ->
     coordinates, the 4-dof state read and written and the lumped mass.  SUPG
     (Euler, no history): per element connectivity (npe x int32); per node
     coordinates, velocity read and written and the lumped mass.  Geometry is
-    recomputed from coordinates and not counted."""
+    recomputed from coordinates, except in the FP64 hexa8 form, which reads
+    the stored Gauss-point geometry (8 points x 10 FP64 values an element)
+    and no coordinates."""
     if config == "cavity":
         sub = 48 if precision == "mixed" else 96
         return E * (16 + 2 * sub) + N * (24 + 32 + 32 + 8)
     npe = 8 if config == "channel" else 4
+    if npe == 8 and precision != "mixed":
+        return E * (4 * npe + 8 * 10 * 8) + N * (24 + 24 + 8)
     return E * 4 * npe + N * (24 + 24 + 24 + 8)
 
 
 # FP64 operations of one SUPG element-step (matrix-free K u over the Gauss
 # points, counting an FMA as two), from the ncu FP64 instruction counts of
-# the tile kernels (profiles/supg_tile_kernel_*.md).
-SUPG_FLOPS = {"channel": 9187, "supg": 1668}
+# the tile kernels (profiles/supg_tile_kernel_*.md); the hexa8 count is that
+# of the kernel reading the stored Gauss-point geometry.
+SUPG_FLOPS = {"channel": 6419, "supg": 1668}
 
 CONFIG_DEFAULT_N = {"cavity": 96, "supg": 96, "channel": 64}
 
@@ -630,7 +635,7 @@ def main():
                     "traffic": measured_traffic(kernel, pn, E), "peak_source": peak_kind, "kernel": kernel,
                     "algorithmic_bytes_per_launch": ab, "avg_launch_ms": tile_ms,
                     "iface_kernel_avg_ms": r["kprof"]["iface"] / klaunch}
-            if args.config in SUPG_FLOPS:
+            if args.config in SUPG_FLOPS and pn == "fp64":
                 # the SUPG element work is FP64-pipe bound: FLOP rate beside the bytes
                 roof["fp64_tflops"] = SUPG_FLOPS[args.config] * E / (tile_ms * 1e-3) / 1e12
                 roof["fp64_flops_per_element_step"] = SUPG_FLOPS[args.config]

@@ -26,6 +26,7 @@ struct DevBatch {
   double* el_lam;                 // SUPG per-element lambda / regime (diagnostics)
   double* el_reg;
   double* diag_res;               // VMS diagnostics on: [16][E] residual entries of the last iteration (else null)
+  double* geo;                    // SUPG hexa8 FP64: [8 * FM_GEO_PER_GP][E] Gauss-point geometry (else null)
   int64_t E;
   // tiles
   const TileMeta* tiles;

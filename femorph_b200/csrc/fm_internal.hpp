@@ -197,6 +197,9 @@ struct Layout {
 
 // Tiles start at multiples of this many element slots.
 constexpr int ELEM_ALIGN = 32;
+// SUPG hexa8 FP64: stored geometry values per Gauss point (inverse Jacobian
+// and det J), 8 points an element.
+constexpr int FM_GEO_PER_GP = 10;
 // VMS tiles: at most this many nodes (each CTA thread owns up to
 // FM_MAX_TILE_NODES / threads of them during accumulation).
 #define FM_MAX_TILE_NODES 512

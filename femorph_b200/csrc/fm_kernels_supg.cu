@@ -48,11 +48,12 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
   if (status != FM_OK) B.pstate[pidx].status = status;
 }
 
-// MIXED: Gauss-point work in FP32 (supg_element_mixed).  The mixed kernels
-// and the FP64 tet4 kernel are held to ~168 registers a thread so that three
-// 128-thread CTAs fit an SM (FP64 tet4: a small spill, 12% faster than two
-// CTAs at 241 registers); the FP64 hexa8 kernel keeps 255 (three CTAs spill
-// 1 KB a thread and run 30% slower).
+// MIXED: Gauss-point work in FP32 (supg_element_mixed).  All 128-thread
+// kernels are held to 168 registers a thread so that three CTAs fit an SM
+// (FP64 tet4: a small spill, 12% faster than two CTAs at 241 registers;
+// FP64 hexa8 with the stored geometry: ~360 bytes of spill, 10% faster than
+// two CTAs at 255 registers, while forming the geometry in the kernel it
+// spilled 1 KB at three CTAs and ran 30% slower).
 //
 // Accumulation of the element contributions into the tile's nodes, in the
 // order of the elements (colour-sorted) in both schemes, so both give the
@@ -63,10 +64,16 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
 //  - hexa8: one round per colour present in the chunk (elements of one
 //    colour share no node), a barrier after each; the 24 entries a hexa
 //    would stage cost more shared memory than the barriers cost time.
+//
+// The FP64 hexa8 kernel (GEO) reads each Gauss point's inverse Jacobian and
+// det J from the geometry stored at placement (supg_geo_kernel) instead of
+// forming them from the staged coordinates at every step, and stages no
+// coordinates.
 template <int NPE, int THREADS, bool MIXED>
-__global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4) ? 3 : 1)
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
     supg_tile_kernel(DevBatch B, int tn_max, int inc_max) {
   constexpr bool GATHER = NPE == 4;
+  constexpr bool GEO = NPE == 8 && !MIXED;
   extern __shared__ double sm[];
   double* s_x = sm;
   double* s_y = s_x + tn_max;
@@ -96,7 +103,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
   const int tid = threadIdx.x;
   for (int ln = tid; ln < tm.n_node; ln += THREADS) {
     const int g = B.tile_nodes[tm.node_begin + ln];
-    s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
+    if (!GEO) {
+      s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
+    }
     double u = B.su[g], v = B.sv[g], w = B.sw[g];
     mask_fixed(P.glob_fixed, u, v, w);
     s_u[ln] = u; s_v[ln] = v; s_w[ln] = w;
@@ -148,7 +157,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
         }
         supg_element_mixed<NPE>(P, s_shape_f, s_shape, Xr, U0, Ud, precise, s_x, s_y, s_z, ln, k, lam, reg);
       } else {
-        supg_element<NPE>(P, s_shape, s_x, s_y, s_z, s_u, s_v, s_w, ln, k, lam, reg);
+        supg_element<NPE, GEO>(P, s_shape, s_x, s_y, s_z, s_u, s_v, s_w, ln, k, lam, reg, GEO ? B.geo + e : nullptr, E);
       }
       B.el_lam[e] = lam;
       B.el_reg[e] = reg;
@@ -223,6 +232,45 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 && (MIXED || NPE == 4)
     }
   }
   check_exit(B, P, pidx, max_u2, status);
+}
+
+// Stored Gauss-point geometry of the hexa8 tiles [tile0, tile0 + gridDim.x)
+// (geo_at's layout): the tile's coordinates staged in shared memory, then per
+// element and Gauss point the Jacobian inverse and determinant by
+// jacobian_at over the same shape table the element loop reads.  Run once
+// when a problem is placed in a batch.
+__global__ void supg_geo_kernel(DevBatch B, int tile0) {
+  extern __shared__ double sm[];
+  __shared__ ShapeTable<8, double> s_shape;
+  const TileMeta tm = B.tiles[tile0 + blockIdx.x];
+  if (tm.problem < 0) return;
+  double* s_x = sm;
+  double* s_y = s_x + tm.n_node;
+  double* s_z = s_y + tm.n_node;
+  for (int ln = threadIdx.x; ln < tm.n_node; ln += blockDim.x) {
+    const int g = B.tile_nodes[tm.node_begin + ln];
+    s_x[ln] = B.x[g]; s_y[ln] = B.y[g]; s_z[ln] = B.z[g];
+  }
+  fill_shape_table<8, double>(&s_shape);
+  __syncthreads();
+  const int64_t E = B.E;
+  for (int le = threadIdx.x; le < tm.n_elem; le += blockDim.x) {
+    const int64_t e = tm.elem_begin + le;
+    const uint4 cw = __ldg(reinterpret_cast<const uint4*>(B.conn) + e);
+    const int ln[8] = {(int)(cw.x & 0xffff), (int)(cw.x >> 16), (int)(cw.y & 0xffff), (int)(cw.y >> 16),
+                       (int)(cw.z & 0xffff), (int)(cw.z >> 16), (int)(cw.w & 0xffff), (int)(cw.w >> 16)};
+#pragma unroll 1
+    for (int g = 0; g < 8; ++g) {
+      double inv[3][3];
+      const double det = jacobian_at<8>([&](int n, int c) { return s_shape.dN[g][n][c]; }, s_x, s_y, s_z, ln, inv);
+      double* q = B.geo + (int64_t)g * FM_GEO_PER_GP * E + e;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) q[(a * 3 + b) * E] = inv[a][b];
+      q[9 * E] = det;
+    }
+  }
 }
 
 __global__ void supg_iface_kernel(DevBatch B) {
@@ -379,7 +427,8 @@ cudaError_t supg_configure(size_t smem, int npe) {
     if (e == cudaSuccess) e = raise_dyn_smem(supg_pressure_kernel<4>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_stats_kernel<4>, optin);
   } else {
-    e = raise_dyn_smem(supg_tile_kernel<8, 128, false>, optin);
+    e = raise_dyn_smem(supg_geo_kernel, optin);
+    if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 128, false>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256, false>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 128, true>, optin);
     if (e == cudaSuccess) e = raise_dyn_smem(supg_tile_kernel<8, 256, true>, optin);
@@ -414,6 +463,12 @@ cudaError_t launch_supg_step(const DevBatch& B, int tn_max, int inc_max, int thr
   else
     supg_iface_kernel<<<iface_blocks, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[2], s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_supg_geo(const DevBatch& B, int tile0, int ntiles, int tn_max, cudaStream_t s) {
+  if (ntiles <= 0) return cudaSuccess;
+  supg_geo_kernel<<<ntiles, 128, (size_t)tn_max * 3 * sizeof(double), s>>>(B, tile0);
   return cudaGetLastError();
 }
 

@@ -171,15 +171,41 @@ __device__ __forceinline__ void tet_metric(const double inv[3][3], double nu, do
   iG[2][2] = (m00 * m11 - m10 * m01) * idg;
 }
 
+// Gauss-point geometry of one hexa8 element, formed once per placement and
+// kept in HBM: per point g the inverse Jacobian (9 entries) and det J, entry
+// q of point g at geo[(g * FM_GEO_PER_GP + q) * E + e] (coalesced over the
+// tile's consecutive element slots).  The mesh does not move, so these are
+// the values the element loop would form at every step from the same
+// coordinates with the same expressions.
+__device__ __forceinline__ double geo_at(const double* geo, int64_t E, int g, double inv[3][3]) {
+  const double* q = geo + (int64_t)g * FM_GEO_PER_GP * E;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) inv[a][b] = __ldg(q + (a * 3 + b) * E);
+  return __ldg(q + 9 * E);
+}
+
+// Requests point g's ten entries into L1 ahead of their use (the loads of a
+// warp cover consecutive element slots: two 128-byte lines an entry).
+__device__ __forceinline__ void geo_prefetch(const double* geo, int64_t E, int g) {
+  const double* q = geo + (int64_t)g * FM_GEO_PER_GP * E;
+#pragma unroll
+  for (int k = 0; k < FM_GEO_PER_GP; ++k) asm volatile("prefetch.global.L1 [%0];" ::"l"(q + k * E));
+}
+
 // One element: k[a][c] = -dt (sum of the enabled K_i u_e)[a][c].  Coordinates
 // and velocities are read from the tile's shared-memory node arrays through
-// the local ids ln[].  Also returns the element's lambda (volume average) and
-// regime (average of the Gauss-point regimes) for output.
-template <int NPE>
+// the local ids ln[]; with GEO the Gauss-point inverse Jacobians and
+// determinants are read from the stored geometry instead (geo = the
+// element's first entry, E = the row stride).  Also returns the element's
+// lambda (volume average) and regime (average of the Gauss-point regimes)
+// for output.
+template <int NPE, bool GEO = false>
 __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<NPE, double>& tab, const double* sx,
                                              const double* sy, const double* sz, const double* su, const double* sv,
                                              const double* sw, const int ln[NPE], double k[NPE][3], double& lam_el,
-                                             double& reg_el) {
+                                             double& reg_el, const double* geo = nullptr, int64_t E = 0) {
   const double rho = P.rho, mu = P.mu, alpha = P.alpha, cI = P.c_i;
   const double nu = mu / rho;
   const bool bbar = (P.ex_mask & 2) != 0;
@@ -201,6 +227,7 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
   // gr_g[c][c] / V (before the Gauss loop) and sd0[a][c] Q_c, Q_c = sum_g q_c
   // (after it): the 24 averaged derivatives are never held in registers.
   auto jac_inv = [&](int g, double inv[3][3]) -> double {
+    if constexpr (GEO) return geo_at(geo, E, g, inv);
     return jacobian_at<NPE>([&](int n, int c) { return tab.dN[g][n][c]; }, sx, sy, sz, ln, inv);
   };
   double Dbar[3] = {0.0, 0.0, 0.0}, Qb[3] = {0.0, 0.0, 0.0}, bden = 0.0;
@@ -235,6 +262,10 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
     tet_metric(inv4, nu, cI, G4, t3_4, iG4);
   }
   double vol = 0.0, lam_int = 0.0, reg = 0.0;
+  if constexpr (GEO) {
+    geo_prefetch(geo, E, 0);
+    geo_prefetch(geo, E, 1);
+  }
 #pragma unroll 1
   for (int g = 0; g < GaussRule<NPE>::n; ++g) {
     // shape values and local derivatives: tet4 in closed form (constant
@@ -265,24 +296,51 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
         }
       t3 = t3_4;
     } else {
+      if constexpr (GEO) {
+        if (g + 2 < GaussRule<NPE>::n) geo_prefetch(geo, E, g + 2);
+      }
       det = jac_inv(g, inv);
       tet_metric(inv, nu, cI, G, t3, iG);
     }
     auto gdv = [&](int a, int b) -> double {
       return inv[b][0] * dNv(a, 0) + inv[b][1] * dNv(a, 1) + inv[b][2] * dNv(a, 2);
     };
-    // velocity, gradient, divergence at the point
+    // velocity, gradient, divergence at the point.  hexa8: the gradient in
+    // local coordinates first, Lg[c][k] = sum_a dN[a][k] u_a[c], then
+    // gr[c][d] = sum_k inv[d][k] Lg[c][k] (the same sum over the nodes as
+    // sum_a gd[a][d] u_a[c], 99 instead of 144 FLOP a point); tet4's
+    // derivatives are constants, so its global ones cost nothing to form
     double u[3] = {0.0, 0.0, 0.0}, gr[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    if constexpr (NPE == 8) {
+      double Lg[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
 #pragma unroll
-    for (int a = 0; a < NPE; ++a) {
-      const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
-      const double ga[3] = {gdv(a, 0), gdv(a, 1), gdv(a, 2)};
-      const double Na = Nv(a);
+      for (int a = 0; a < NPE; ++a) {
+        const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
+        const double Na = Nv(a);
+        const double da[3] = {dNv(a, 0), dNv(a, 1), dNv(a, 2)};
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        u[c] += Na * ua[c];
+        for (int c = 0; c < 3; ++c) {
+          u[c] += Na * ua[c];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) gr[c][d] += ga[d] * ua[c];
+          for (int kk = 0; kk < 3; ++kk) Lg[c][kk] += da[kk] * ua[c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gr[c][d] = inv[d][0] * Lg[c][0] + inv[d][1] * Lg[c][1] + inv[d][2] * Lg[c][2];
+    } else {
+#pragma unroll
+      for (int a = 0; a < NPE; ++a) {
+        const double ua[3] = {su[ln[a]], sv[ln[a]], sw[ln[a]]};
+        const double ga[3] = {gdv(a, 0), gdv(a, 1), gdv(a, 2)};
+        const double Na = Nv(a);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          u[c] += Na * ua[c];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) gr[c][d] += ga[d] * ua[c];
+        }
       }
     }
     const double div = gr[0][0] + gr[1][1] + gr[2][2];
@@ -340,6 +398,40 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
         sd[c] -= q;
       }
     }
+    if constexpr (NPE == 8) {
+      // hexa8: every term is linear in gd[a] = inv dN[a] (K2: S gd[a] with S
+      // the symmetric matrix of the stress terms above; K4: c4w gd[a]; K3:
+      // u.gd[a]), so inv is folded into one 3x3 matrix and one vector a
+      // point, T = (S + c4w I) inv and ut = inv^T u, and each node takes
+      // T dN[a] and ut.dN[a] (17 instead of ~36 FLOP a node)
+      double S[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+      if (iK2) {
+        S[0][0] = sd[0]; S[1][1] = sd[1]; S[2][2] = sd[2];
+        S[0][1] = S[1][0] = sig[3] * w;
+        S[1][2] = S[2][1] = sig[4] * w;
+        S[0][2] = S[2][0] = sig[5] * w;
+      }
+      if (iK4) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) S[c][c] += c4w;
+      }
+      double T[3][3], ut[3];
+#pragma unroll
+      for (int kk = 0; kk < 3; ++kk) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) T[c][kk] = S[c][0] * inv[0][kk] + S[c][1] * inv[1][kk] + S[c][2] * inv[2][kk];
+        ut[kk] = u[0] * inv[0][kk] + u[1] * inv[1][kk] + u[2] * inv[2][kk];
+      }
+#pragma unroll
+      for (int a = 0; a < NPE; ++a) {
+        const double da[3] = {dNv(a, 0), dNv(a, 1), dNv(a, 2)};
+        double sa = 0.0;
+        if (iK1) sa = c1w * Nv(a);
+        if (iK3) sa += c3w * (ut[0] * da[0] + ut[1] * da[1] + ut[2] * da[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) k[a][c] += T[c][0] * da[0] + T[c][1] * da[1] + T[c][2] * da[2] + sa * conv[c];
+      }
+    } else {
 #pragma unroll
     for (int a = 0; a < NPE; ++a) {
       const double ga[3] = {gdv(a, 0), gdv(a, 1), gdv(a, 2)};
@@ -365,6 +457,7 @@ __device__ __forceinline__ void supg_element(const DevProb& P, const ShapeTable<
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) k[a][c] += f[c];
+    }
     }
   }
   if (NPE == 8 && bbar && iK2) {
