@@ -27,6 +27,7 @@ struct DevBatch {
   double* el_reg;
   double* diag_res;               // VMS diagnostics on: [16][E] residual entries of the last iteration (else null)
   double* geo;                    // SUPG hexa8 FP64: [8 * FM_GEO_PER_GP][E] Gauss-point geometry (else null)
+  float* geo32;                   // SUPG hexa8 mixed: the same, rounded to FP32 (else null)
   int64_t E;
   // tiles
   const TileMeta* tiles;

@@ -51,9 +51,10 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
 // MIXED: Gauss-point work in FP32 (supg_element_mixed).  All 128-thread
 // kernels are held to 168 registers a thread so that three CTAs fit an SM
 // (FP64 tet4: a small spill, 12% faster than two CTAs at 241 registers;
-// FP64 hexa8 with the stored geometry: ~360 bytes of spill, 10% faster than
-// two CTAs at 255 registers, while forming the geometry in the kernel it
-// spilled 1 KB at three CTAs and ran 30% slower).
+// FP64 hexa8 with the stored geometry: ~500 bytes of spill, faster than two
+// CTAs at 255 registers, while forming the geometry in the kernel it spilled
+// 1 KB at three CTAs and ran 30% slower; mixed hexa8 with the stored
+// geometry: no spill, and 2% faster than four CTAs at 128 registers).
 //
 // Accumulation of the element contributions into the tile's nodes, in the
 // order of the elements (colour-sorted) in both schemes, so both give the
@@ -65,15 +66,15 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
 //    colour share no node), a barrier after each; the 24 entries a hexa
 //    would stage cost more shared memory than the barriers cost time.
 //
-// The FP64 hexa8 kernel (GEO) reads each Gauss point's inverse Jacobian and
-// det J from the geometry stored at placement (supg_geo_kernel) instead of
-// forming them from the staged coordinates at every step, and stages no
-// coordinates.
+// The hexa8 kernels (GEO) read each Gauss point's inverse Jacobian and det J
+// from the geometry stored at placement (supg_geo_kernel; FP64, or rounded
+// to FP32 for the mixed form) instead of forming them from the staged
+// coordinates at every step, and stage no coordinates.
 template <int NPE, int THREADS, bool MIXED>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
     supg_tile_kernel(DevBatch B, int tn_max, int inc_max) {
   constexpr bool GATHER = NPE == 4;
-  constexpr bool GEO = NPE == 8 && !MIXED;
+  constexpr bool GEO = NPE == 8;
   extern __shared__ double sm[];
   double* s_x = sm;
   double* s_y = s_x + tn_max;
@@ -147,15 +148,22 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
         const bool precise = (ln[0] & 0x8000) != 0;
         ln[0] &= 0x7fff;
         float Xr[NPE][3], U0[3], Ud[NPE][3];
-        const double x0 = s_x[ln[0]], y0 = s_y[ln[0]], z0 = s_z[ln[0]];
         const double u0 = s_u[ln[0]], v0 = s_v[ln[0]], w0 = s_w[ln[0]];
         U0[0] = (float)u0; U0[1] = (float)v0; U0[2] = (float)w0;
+        if (!GEO) {
+          const double x0 = s_x[ln[0]], y0 = s_y[ln[0]], z0 = s_z[ln[0]];
+#pragma unroll
+          for (int a = 0; a < NPE; ++a) {
+            Xr[a][0] = (float)(s_x[ln[a]] - x0); Xr[a][1] = (float)(s_y[ln[a]] - y0);
+            Xr[a][2] = (float)(s_z[ln[a]] - z0);
+          }
+        }
 #pragma unroll
         for (int a = 0; a < NPE; ++a) {
-          Xr[a][0] = (float)(s_x[ln[a]] - x0); Xr[a][1] = (float)(s_y[ln[a]] - y0); Xr[a][2] = (float)(s_z[ln[a]] - z0);
           Ud[a][0] = (float)(s_u[ln[a]] - u0); Ud[a][1] = (float)(s_v[ln[a]] - v0); Ud[a][2] = (float)(s_w[ln[a]] - w0);
         }
-        supg_element_mixed<NPE>(P, s_shape_f, s_shape, Xr, U0, Ud, precise, s_x, s_y, s_z, ln, k, lam, reg);
+        supg_element_mixed<NPE, GEO>(P, s_shape_f, s_shape, Xr, U0, Ud, precise, s_x, s_y, s_z, ln, k, lam, reg,
+                                     GEO ? B.geo32 + e : nullptr, E);
       } else {
         supg_element<NPE, GEO>(P, s_shape, s_x, s_y, s_z, s_u, s_v, s_w, ln, k, lam, reg, GEO ? B.geo + e : nullptr, E);
       }
@@ -237,8 +245,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
 // Stored Gauss-point geometry of the hexa8 tiles [tile0, tile0 + gridDim.x)
 // (geo_at's layout): the tile's coordinates staged in shared memory, then per
 // element and Gauss point the Jacobian inverse and determinant by
-// jacobian_at over the same shape table the element loop reads.  Run once
-// when a problem is placed in a batch.
+// jacobian_at over the same shape table the element loop reads, stored in
+// FP64 (B.geo) or rounded to FP32 (B.geo32, mixed form).  Run once when a
+// problem is placed in a batch.
 __global__ void supg_geo_kernel(DevBatch B, int tile0) {
   extern __shared__ double sm[];
   __shared__ ShapeTable<8, double> s_shape;
@@ -257,18 +266,28 @@ __global__ void supg_geo_kernel(DevBatch B, int tile0) {
   for (int le = threadIdx.x; le < tm.n_elem; le += blockDim.x) {
     const int64_t e = tm.elem_begin + le;
     const uint4 cw = __ldg(reinterpret_cast<const uint4*>(B.conn) + e);
-    const int ln[8] = {(int)(cw.x & 0xffff), (int)(cw.x >> 16), (int)(cw.y & 0xffff), (int)(cw.y >> 16),
+    // bit 15 of the first id is the mixed form's FP64-Jacobian flag
+    const int ln[8] = {(int)(cw.x & 0x7fff), (int)(cw.x >> 16), (int)(cw.y & 0xffff), (int)(cw.y >> 16),
                        (int)(cw.z & 0xffff), (int)(cw.z >> 16), (int)(cw.w & 0xffff), (int)(cw.w >> 16)};
 #pragma unroll 1
     for (int g = 0; g < 8; ++g) {
       double inv[3][3];
       const double det = jacobian_at<8>([&](int n, int c) { return s_shape.dN[g][n][c]; }, s_x, s_y, s_z, ln, inv);
-      double* q = B.geo + (int64_t)g * FM_GEO_PER_GP * E + e;
+      const int64_t q0 = (int64_t)g * FM_GEO_PER_GP * E + e;
+      if (B.geo) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) q[(a * 3 + b) * E] = inv[a][b];
-      q[9 * E] = det;
+          for (int b = 0; b < 3; ++b) B.geo[q0 + (a * 3 + b) * E] = inv[a][b];
+        B.geo[q0 + 9 * E] = det;
+      }
+      if (B.geo32) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) B.geo32[q0 + (a * 3 + b) * E] = (float)inv[a][b];
+        B.geo32[q0 + 9 * E] = (float)det;
+      }
     }
   }
 }

@@ -378,6 +378,8 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
     }
     if (b->solver == FM_SOLVER_SUPG && b->npe == 8 && b->precision != FM_MIXED)
       A((void**)&D.geo, (size_t)NE * 8 * FM_GEO_PER_GP * sizeof(double));
+    if (b->solver == FM_SOLVER_SUPG && b->npe == 8 && b->precision == FM_MIXED)
+      A((void**)&D.geo32, (size_t)NE * 8 * FM_GEO_PER_GP * sizeof(float));
     if (b->solver == FM_SOLVER_SUPG) {
       A((void**)&D.el_lam, NE * sizeof(double));
       A((void**)&D.el_reg, NE * sizeof(double));
@@ -788,7 +790,7 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
     if (r) return r;
   }
   r = configure(b);
-  if (!r && D.geo) {
+  if (!r && (D.geo || D.geo32)) {
     // the problem's Gauss-point geometry, ahead of its first step on the stream
     cudaError_t e = launch_supg_geo(D, (int)b->slots[ps].off[P_TILE], (int)L.tiles.size(), b->slots[ps].tn_max, s);
     if (e != cudaSuccess) r = fail(FM_ERR_CUDA, std::string("geometry: ") + cudaGetErrorString(e));
@@ -830,7 +832,7 @@ static int64_t pool_bytes(const int64_t cap[P_COUNT], int solver, int npe, int p
   if (solver == FM_SOLVER_VMS && prec == FM_MIXED) b += NE * 12 * 4;
   else if (solver == FM_SOLVER_VMS || history) b += NE * (solver == FM_SOLVER_VMS ? 12 : 3 * npe) * 8;
   if (solver == FM_SOLVER_SUPG) b += NE * 3 * 8;
-  if (solver == FM_SOLVER_SUPG && npe == 8 && prec != FM_MIXED) b += NE * 8 * FM_GEO_PER_GP * 8;
+  if (solver == FM_SOLVER_SUPG && npe == 8) b += NE * 8 * FM_GEO_PER_GP * (prec == FM_MIXED ? 4 : 8);
   b += at_least(cap[P_TILE], 1) * (int64_t)sizeof(TileMeta) + at_least(cap[P_TNODE], 1) * 4 +
        at_least(cap[P_TCOL], 1) * 4 + at_least(cap[P_TINC], 8) * 2 + at_least(cap[P_TOFF], 1) * 2;
   b += at_least(cap[P_SLOT], 1) * 4 * 8 + at_least(cap[P_IFACE], 1) * 4 * 4 + at_least(cap[P_ISLOT], 1) * 4;
@@ -978,7 +980,7 @@ int fm_batch_estimate_bytes(fm_problem* const* probs, int32_t n, const fm_tuning
   // nodes: 12 FP64 arrays + BC index; elements: connectivity + history;
   // tiles, incidence lists and interface partials: ~40 B per element
   const int64_t per_e = (int64_t)npe * 2 + (vms ? (mixed ? 48 : 96) : (3 * npe * 8 + 24)) + 40 +
-                        (!vms && npe == 8 && !mixed ? 8 * FM_GEO_PER_GP * 8 : 0);
+                        (!vms && npe == 8 ? 8 * FM_GEO_PER_GP * (mixed ? 4 : 8) : 0);
   *bytes = N * 100 + E * per_e + (16 << 20);
   return FM_OK;
 }

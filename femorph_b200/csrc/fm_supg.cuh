@@ -187,11 +187,22 @@ __device__ __forceinline__ double geo_at(const double* geo, int64_t E, int g, do
 }
 
 // Requests point g's ten entries into L1 ahead of their use (the loads of a
-// warp cover consecutive element slots: two 128-byte lines an entry).
-__device__ __forceinline__ void geo_prefetch(const double* geo, int64_t E, int g) {
-  const double* q = geo + (int64_t)g * FM_GEO_PER_GP * E;
+// warp cover consecutive element slots: one or two 128-byte lines an entry).
+template <typename T>
+__device__ __forceinline__ void geo_prefetch(const T* geo, int64_t E, int g) {
+  const T* q = geo + (int64_t)g * FM_GEO_PER_GP * E;
 #pragma unroll
   for (int k = 0; k < FM_GEO_PER_GP; ++k) asm volatile("prefetch.global.L1 [%0];" ::"l"(q + k * E));
+}
+
+// The mixed form's copy: the same FP64 values rounded to FP32.
+__device__ __forceinline__ float geo_at_f(const float* geo, int64_t E, int g, float inv[3][3]) {
+  const float* q = geo + (int64_t)g * FM_GEO_PER_GP * E;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) inv[a][b] = __ldg(q + (a * 3 + b) * E);
+  return __ldg(q + 9 * E);
 }
 
 // One element: k[a][c] = -dt (sum of the enabled K_i u_e)[a][c].  Coordinates
@@ -539,13 +550,13 @@ __device__ __forceinline__ void metric_f(const float inv[3][3], float nu, float 
   iG[2][2] = (m00 * m11 - m10 * m01) * idg;
 }
 
-template <int NPE>
+template <int NPE, bool GEO = false>
 __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const ShapeTable<NPE, float>& tab,
                                                    const ShapeTable<NPE, double>& tabd, const float Xr[NPE][3],
                                                    const float U0[3], const float Ud[NPE][3], bool precise,
                                                    const double* sx, const double* sy, const double* sz,
                                                    const int ln[NPE], double k[NPE][3], double& lam_el,
-                                                   double& reg_el) {
+                                                   double& reg_el, const float* geo = nullptr, int64_t E = 0) {
   const float rho = (float)P.rho, mu = (float)P.mu, alpha = (float)P.alpha, cI = (float)P.c_i;
   const float nu = (float)(P.mu / P.rho);
   const bool bbar = (P.ex_mask & 2) != 0;
@@ -569,8 +580,10 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
     }
     return tab.N[g][a];
   };
-  // per Gauss point: inverse Jacobian and det, FP32 or (precise) FP64
+  // per Gauss point: inverse Jacobian and det, FP32 or (precise) FP64; with
+  // GEO read from the stored geometry (formed in FP64 for every element)
   auto geometry = [&](int g, float inv[3][3]) -> float {
+    if constexpr (GEO) return geo_at_f(geo, E, g, inv);
     if (precise) {
       double dN[NPE][3], invd[3][3];
 #pragma unroll
@@ -644,6 +657,10 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
     metric_f(inv4, nu, cI, G4, t3_4, iG4);
   }
   float vol = 0.0f, lam_int = 0.0f, reg = 0.0f;
+  if constexpr (GEO) {
+    geo_prefetch(geo, E, 0);
+    geo_prefetch(geo, E, 1);
+  }
 #pragma unroll 1
   for (int g = 0; g < GaussRule<NPE>::n; ++g) {
     float inv[3][3], G[3][3], t3, iG[3][3];
@@ -660,6 +677,9 @@ __device__ __forceinline__ void supg_element_mixed(const DevProb& P, const Shape
         }
       t3 = t3_4;
     } else {
+      if constexpr (GEO) {
+        if (g + 2 < GaussRule<NPE>::n) geo_prefetch(geo, E, g + 2);
+      }
       det = geometry(g, inv);
       metric_f(inv, nu, cI, G, t3, iG);
     }
