@@ -162,6 +162,13 @@ def test_capacity_bytes_grow_with_capacity_and_static_entry_validates():
     big = api.capacity_bytes(mesh.VMS, 4, 4, 1_000_000, 200_000, api.FM_FP64)
     mixed = api.capacity_bytes(mesh.VMS, 4, 4, 1_000_000, 200_000, api.FM_MIXED)
     assert 0 < small < big and mixed < big
+    # SUPG hexa8 pools hold the stored Gauss-point geometry: 8 points x 10
+    # values an element, FP64 (640 B) or FP32 for the mixed form (320 B)
+    E, N = 1_000_000, 1_100_000
+    h64 = api.capacity_bytes(mesh.SUPG, 8, 1, E, N, api.FM_FP64)
+    h32 = api.capacity_bytes(mesh.SUPG, 8, 1, E, N, api.FM_MIXED)
+    assert h64 - h32 >= 320 * E
+    assert h32 - api.capacity_bytes(mesh.SUPG, 4, 1, E, N, api.FM_MIXED) >= 320 * E
     # the allocation-free entry point checks its inputs before any device work
     L = api.lib()
     s = api.GpuProblem(mesh.cavity(2, seed=0, steps=1, solver=mesh.SUPG))
