@@ -62,6 +62,9 @@ struct DevBatch {
   // polls of a tile CTA's wait for one chunk's bulk copies before it gives
   // up with FM_ERR_TIMEOUT (FM_WAIT_LIMIT unless fm_batch_set_wait_limit)
   uint32_t wait_limit;
+  // VMS tile CTAs ask L2 for tile blockIdx.x + l2_ahead's element rows and
+  // interior-node ranges (0: off)
+  int32_t l2_ahead;
 };
 
 // Sum over the part slices of exchange entry xi (component c).
@@ -86,6 +89,12 @@ __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.p
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+// Asks L2 for bytes (a multiple of 16) from a 16-byte aligned global
+// address; nothing waits for it.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),

@@ -318,6 +318,30 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   const double c1nu = P.c1 * P.nu;
   const double nu4 = 4.0 * P.nu;
   __syncthreads();
+  // one lane asks L2 for a later tile's element rows and interior-node
+  // ranges (contiguous), so that tile's bulk copies and gathers hit L2; the
+  // round-up to 16 bytes reads at most 12 bytes past an array, inside the
+  // batch's single device allocation (another array or the carve padding)
+  if (B.l2_ahead > 0 && tid == THREADS - 32 && blockIdx.x + B.l2_ahead < (unsigned)B.n_tiles) {
+    const TileMeta tn = B.tiles[blockIdx.x + B.l2_ahead];
+    if (tn.problem >= 0 && tn.n_elem > 0) {
+      const int64_t e0 = tn.elem_begin;  // multiple of 32 slots: 16-byte aligned rows
+      const uint32_t bs = ((uint32_t)tn.n_elem * (uint32_t)sizeof(S) + 15u) & ~15u;
+#pragma unroll 1
+      for (int q = 0; q < 12; ++q) bulk_prefetch_l2(sdus_g + (int64_t)q * E + e0, bs);
+      bulk_prefetch_l2(conn_g + e0, ((uint32_t)tn.n_elem * 8u + 15u) & ~15u);
+      bulk_prefetch_l2(B.tile_inc + tn.inc_begin, ((uint32_t)tn.n_elem * 8u + 15u) & ~15u);
+      if (tn.n_int > 0) {
+        const int64_t g0 = tn.node0 & ~1, g1 = ((int64_t)tn.node0 + tn.n_int + 1) & ~1ll;
+        const uint32_t nb = (uint32_t)(g1 - g0) * 8u;
+        bulk_prefetch_l2(B.x + g0, nb); bulk_prefetch_l2(B.y + g0, nb); bulk_prefetch_l2(B.z + g0, nb);
+        bulk_prefetch_l2(B.su + g0, nb); bulk_prefetch_l2(B.sv + g0, nb); bulk_prefetch_l2(B.sw + g0, nb);
+        bulk_prefetch_l2(B.sp + g0, nb); bulk_prefetch_l2(B.mass + g0, nb);
+        const int64_t h0 = tn.node0 & ~3, h1 = ((int64_t)tn.node0 + tn.n_int + 3) & ~3ll;
+        bulk_prefetch_l2(B.node_bc + h0, (uint32_t)(h1 - h0) * 4u);
+      }
+    }
+  }
 
   // nodes owned by this thread for the accumulation: j * THREADS + tid;
   // cur/end walk each one's incidence list in element order
