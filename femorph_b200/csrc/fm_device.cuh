@@ -62,7 +62,7 @@ struct DevBatch {
   // polls of a tile CTA's wait for one chunk's bulk copies before it gives
   // up with FM_ERR_TIMEOUT (FM_WAIT_LIMIT unless fm_batch_set_wait_limit)
   uint32_t wait_limit;
-  // VMS tile CTAs ask L2 for tile blockIdx.x + l2_ahead's element rows and
+  // tile CTAs ask L2 for tile blockIdx.x + l2_ahead's element rows and
   // interior-node ranges (0: off)
   int32_t l2_ahead;
 };

@@ -126,6 +126,32 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
   if (MIXED) fill_shape_table<NPE, float>(&s_shape_f);
   __syncthreads();
   const int64_t E = B.E;
+  // one lane asks L2 for a later tile's connectivity, incidence entries, AB2
+  // history rows and interior-node ranges (see vms_tile_kernel)
+  if (B.l2_ahead > 0 && tid == THREADS - 32 && blockIdx.x + B.l2_ahead < (unsigned)B.n_tiles) {
+    const TileMeta tn = B.tiles[blockIdx.x + B.l2_ahead];
+    if (tn.problem >= 0 && tn.n_elem > 0) {
+      const int64_t e0 = tn.elem_begin;  // multiple of 32 slots: 16-byte aligned rows
+      const uint32_t cb = ((uint32_t)tn.n_elem * NPE * 2u + 15u) & ~15u;
+      bulk_prefetch_l2(B.conn + e0 * NPE, cb);
+      if (GATHER) bulk_prefetch_l2(B.tile_inc + tn.inc_begin, cb);
+      if (B.sdus) {
+#pragma unroll 1
+        for (int q = 0; q < 3 * NPE; ++q) bulk_prefetch_l2(B.sdus + (int64_t)q * E + e0, ((uint32_t)tn.n_elem * 8u + 15u) & ~15u);
+      }
+      if (tn.n_int > 0) {
+        const int64_t g0 = tn.node0 & ~1, g1 = ((int64_t)tn.node0 + tn.n_int + 1) & ~1ll;
+        const uint32_t nb = (uint32_t)(g1 - g0) * 8u;
+        if (!GEO) {
+          bulk_prefetch_l2(B.x + g0, nb); bulk_prefetch_l2(B.y + g0, nb); bulk_prefetch_l2(B.z + g0, nb);
+        }
+        bulk_prefetch_l2(B.su + g0, nb); bulk_prefetch_l2(B.sv + g0, nb); bulk_prefetch_l2(B.sw + g0, nb);
+        bulk_prefetch_l2(B.mass + g0, nb);
+        const int64_t h0 = tn.node0 & ~3, h1 = ((int64_t)tn.node0 + tn.n_int + 3) & ~3ll;
+        bulk_prefetch_l2(B.node_bc + h0, (uint32_t)(h1 - h0) * 4u);
+      }
+    }
+  }
   int c_lo = 0;
   for (int base = 0; base < tm.n_elem; base += THREADS) {
     const int le = base + tid;

@@ -430,14 +430,17 @@ static int allocate(fm_batch* b, const int64_t cap[P_COUNT]) {
   D.recs = recs; D.tab_off = toffs; D.tab_len = tlens; D.tab_rows = rows;
   D.probs = dp; D.pstate = ds; D.target = tg; D.q1p = q1; D.done = done;
   D.wait_limit = FM_WAIT_LIMIT;
-  // mixed VMS tiles ask L2 for the tile two SM-counts of CTAs ahead (measured
-  // at 96^3: 0.460 -> 0.445 ms a step; the FP64 form gains nothing and keeps
-  // it off)
-  if (b->solver == FM_SOLVER_VMS && b->precision == FM_MIXED) {
+  // tile CTAs ask L2 for a tile this many CTAs ahead (measured: mixed VMS
+  // two SM-counts, 0.460 -> 0.444 ms a step at 96^3; SUPG one SM-count, tet4
+  // 96^3 0.797 -> 0.770 ms FP64 and 0.537 -> 0.511 ms mixed, hexa8 channel
+  // -0.3% FP64 and -1.2% mixed; the FP64 VMS form gains nothing and keeps it
+  // off)
+  {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       sms = 148;
-    D.l2_ahead = 2 * sms;
+    if (b->solver == FM_SOLVER_SUPG) D.l2_ahead = sms;
+    else if (b->precision == FM_MIXED) D.l2_ahead = 2 * sms;
   }
   // every slot starts inactive
   CK(cudaMemset(tiles, 0xff, std::max<int64_t>(cap[P_TILE], 1) * sizeof(TileMeta)));
