@@ -389,6 +389,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
     // which costs more than it gains)
     double* R = MIXED ? s_lres_mixed : reinterpret_cast<double*>(buf);
     double2* R2 = reinterpret_cast<double2*>(R);
+    double lres[4][4];
     if (active) {
       const S* bs = reinterpret_cast<const S*>(buf);
       const uint2 cw = reinterpret_cast<const uint2*>(bs + 12 * THREADS)[tid];
@@ -400,24 +401,37 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
       S sd_in[12];
 #pragma unroll
       for (int q = 0; q < 12; ++q) sd_in[q] = bs[q * THREADS + tid];
-      double lres[4][4];
       vms_element<MIXED, S>(B, PC, tm.elem_begin + le, ln, precise, s_rec, sd_in, pq, pending, first_dual, inv_dt,
                             c1nu, nu4, lres);
       if (B.diag_res) {
 #pragma unroll
         for (int r = 0; r < 16; ++r) B.diag_res[(int64_t)r * E + tm.elem_begin + le] = lres[r >> 2][r & 3];
       }
-      if constexpr (MIXED) {
+    }
+    if constexpr (MIXED) {
+      // the mixed form's residual region is its own, so the barrier that lets
+      // it be overwritten (owners of the previous chunk done) comes after
+      // this chunk's element work: warps that finish the previous chunk's
+      // accumulation early go on with their elements instead of waiting
+      if (k > 0) __syncthreads();
+      if (active) {
         double2* Rt = R2 + tid * 8;
 #pragma unroll
         for (int q = 0; q < 8; ++q)
           Rt[q ^ (tid & 7)] = make_double2(lres[q >> 1][2 * (q & 1)], lres[q >> 1][2 * (q & 1) + 1]);
-      } else {
+      }
+      // any timed-out wait aborts here, before the accumulation
+      if (__syncthreads_or(!arrived)) {
+        if (tid == 0) s_abort = 1;
+        break;
+      }
+    } else {
+      if (active) {
 #pragma unroll
         for (int r = 0; r < 16; ++r) R[r * THREADS + tid] = lres[r >> 2][r & 3];
       }
+      __syncthreads();
     }
-    __syncthreads();
     // owners add this chunk's contributions to their nodes, in element order
 #pragma unroll
     for (int j = 0; j < MAXOWN; ++j) {
@@ -451,10 +465,13 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
         s_a0[ln] = a0; s_a1[ln] = a1; s_a2[ln] = a2; s_a3[ln] = a3;
       }
     }
-    // end of chunk: stage buffer k&1 is free again; any timed-out wait aborts
-    if (__syncthreads_or(!arrived)) {
-      if (tid == 0) s_abort = 1;
-      break;
+    // FP64 end of chunk: stage buffer k&1 (holding this chunk's residuals) is
+    // free again; any timed-out wait aborts
+    if constexpr (!MIXED) {
+      if (__syncthreads_or(!arrived)) {
+        if (tid == 0) s_abort = 1;
+        break;
+      }
     }
   }
   __syncthreads();
