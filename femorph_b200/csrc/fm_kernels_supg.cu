@@ -61,7 +61,8 @@ __device__ __forceinline__ void check_exit(const DevBatch& B, const DevProb& P, 
 // same sums:
 //  - tet4 (GATHER): element threads write their 12 entries to shared memory,
 //    then each node's owner thread adds the entries of this chunk's elements
-//    from the node's incidence list (two barriers a chunk);
+//    from the node's incidence list (two barriers a chunk; the one that
+//    frees the staged entries sits after the next chunk's element work);
 //  - hexa8: one round per colour present in the chunk (elements of one
 //    colour share no node), a barrier after each; the 24 entries a hexa
 //    would stage cost more shared memory than the barriers cost time.
@@ -208,6 +209,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
       }
     }
     if constexpr (GATHER) {
+      // the barrier that frees R (owners of the previous chunk done) comes
+      // after this chunk's element work, not at the end of the accumulation
+      if (base > 0) __syncthreads();
       if (active) {
 #pragma unroll
         for (int a = 0; a < NPE; ++a)
@@ -234,7 +238,6 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
         s_cur[n] = (uint16_t)c;
         s_a0[n] = a0; s_a1[n] = a1; s_a2[n] = a2;
       }
-      __syncthreads();
     } else {
       while (c_lo < tm.n_col && s_col[c_lo + 1] <= base) ++c_lo;
       for (int c = c_lo; c < tm.n_col && s_col[c] < base + THREADS; ++c) {
