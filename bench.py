@@ -136,7 +136,7 @@ def stored_geometry_bytes(E: int, precision: str, config: str) -> int:
 # points, counting an FMA as two), from the ncu FP64 instruction counts of
 # the tile kernels (profiles/supg_tile_kernel_*.md); the hexa8 count is that
 # of the kernel reading the stored Gauss-point geometry.
-SUPG_FLOPS = {"channel": 6419, "supg": 1705}
+SUPG_FLOPS = {"channel": 6419, "supg": 1676}
 
 CONFIG_DEFAULT_N = {"cavity": 96, "supg": 96, "channel": 64}
 
