@@ -323,14 +323,15 @@ __global__ void supg_geo_kernel(DevBatch B, int tile0) {
 
 __global__ void supg_iface_kernel(DevBatch B) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
+    // entry fields load together with the problem id (see vms_iface_kernel)
     const int pidx = B.iface_prob[i];
+    const int g = B.iface_node[i];
+    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     if (pidx < 0) continue;  // free interface entry
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
-    const int g = B.iface_node[i];
     double acc[3] = {0.0, 0.0, 0.0};
-    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     for (int kk = k0; kk < k1; ++kk) {
       const int s = B.iface_slots[kk];
       const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];

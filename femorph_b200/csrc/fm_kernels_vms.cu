@@ -507,15 +507,17 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
 
 __global__ void vms_iface_kernel(DevBatch B) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n_iface; i += gridDim.x * blockDim.x) {
+    // the entry's fields load together with its problem id (a free entry's
+    // are read but not used), so they do not wait for the state check
     const int pidx = B.iface_prob[i];
+    const int g = B.iface_node[i];
+    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     if (pidx < 0) continue;  // free interface entry
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     const bool first_dual = (st.iter % (P.ndual + 1)) == 0;
-    const int g = B.iface_node[i];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     for (int k = k0; k < k1; ++k) {
       const int s = B.iface_slots[k];
       const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
