@@ -121,8 +121,8 @@ struct TileMeta {
   int32_t problem;
   int32_t inc_begin;            // node->element incidence entries in tile_inc (multiple of 8)
   int32_t off_begin;            // per-node offsets (n_node+1) into those entries, in tile_off
-  int32_t node0;                // batch id of local node 0 (the interior nodes are consecutive
-                                // batch ids from it); set at placement
+  int32_t node0;                // batch id of local node 0 when the interior nodes are
+                                // consecutive batch ids from it (-1 otherwise); set at placement
 };
 
 struct HostProblem;

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 128 ? 3 : 1)
 #pragma unroll 1
         for (int q = 0; q < 3 * NPE; ++q) bulk_prefetch_l2(B.sdus + (int64_t)q * E + e0, ((uint32_t)tn.n_elem * 8u + 15u) & ~15u);
       }
-      if (tn.n_int > 0) {
+      if (tn.n_int > 0 && tn.node0 >= 0) {
         const int64_t g0 = tn.node0 & ~1, g1 = ((int64_t)tn.node0 + tn.n_int + 1) & ~1ll;
         const uint32_t nb = (uint32_t)(g1 - g0) * 8u;
         if (!GEO) {

@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
       for (int q = 0; q < 12; ++q) bulk_prefetch_l2(sdus_g + (int64_t)q * E + e0, bs);
       bulk_prefetch_l2(conn_g + e0, ((uint32_t)tn.n_elem * 8u + 15u) & ~15u);
       bulk_prefetch_l2(B.tile_inc + tn.inc_begin, ((uint32_t)tn.n_elem * 8u + 15u) & ~15u);
-      if (tn.n_int > 0) {
+      if (tn.n_int > 0 && tn.node0 >= 0) {
         const int64_t g0 = tn.node0 & ~1, g1 = ((int64_t)tn.node0 + tn.n_int + 1) & ~1ll;
         const uint32_t nb = (uint32_t)(g1 - g0) * 8u;
         bulk_prefetch_l2(B.x + g0, nb); bulk_prefetch_l2(B.y + g0, nb); bulk_prefetch_l2(B.z + g0, nb);

@@ -705,7 +705,15 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
       tm.col_begin += (int32_t)pl.off[P_TCOL];
       tm.inc_begin += (int32_t)pl.off[P_TINC];
       tm.off_begin += (int32_t)pl.off[P_TOFF];
-      tm.node0 = tm.n_node > 0 ? L.tile_nodes[tm.node_begin - (int32_t)pl.off[P_TNODE]] + (int32_t)noff : 0;
+      // the look-ahead prefetch reads node0 .. node0 + n_int - 1: checked to
+      // be the tile's interior nodes (consecutive by construction), else -1
+      // (no node prefetch for the tile)
+      {
+        const int32_t* tn = L.tile_nodes.data() + (tm.node_begin - (int32_t)pl.off[P_TNODE]);
+        bool consecutive = tm.n_int > 0;
+        for (int32_t j = 1; j < tm.n_int && consecutive; ++j) consecutive = tn[j] == tn[0] + j;
+        tm.node0 = consecutive ? tn[0] + (int32_t)noff : -1;
+      }
       tm.problem = ps;
       pl.tn_max = std::max(pl.tn_max, tm.n_node);
     }
