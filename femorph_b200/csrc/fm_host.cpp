@@ -432,6 +432,57 @@ void morton_order(const fm_problem* p, hvec<int64_t>& order) {
   sort_by_key(code, order);
 }
 
+// Orders one tile's interface nodes for the node-owner accumulation of the
+// tile kernels, in which the thread p % FM_OWNER_THREADS adds up the
+// contributions of the tile's local node p.  Interior nodes keep positions
+// [0, n_int) (their batch ids are consecutive from local node 0); the
+// interface nodes, heaviest first (incident elements in the tile plus a fixed
+// cost per node), take a free position of the thread with the least work so
+// far (ties: the lowest thread).  Without it the threads that own an
+// interior node (up to 24 incident elements) also own as many interface
+// nodes as the others, and the slowest owner sets the length of every
+// chunk's accumulation.  Each node's sum keeps its element order, so the
+// results do not depend on this order.
+//   w_int / w_ifc: incident elements of the interior / interface nodes (in
+//   their current order); ifc: the interface nodes, reordered in place.
+constexpr int FM_OWNER_THREADS = 128;
+static void balance_owners(const std::vector<int32_t>& w_int, const std::vector<int32_t>& w_ifc,
+                           std::vector<int32_t>& ifc, std::vector<int32_t>& scratch) {
+  const int n_int = (int)w_int.size(), n_ifc = (int)w_ifc.size(), n_node = n_int + n_ifc;
+  constexpr int64_t kNodeCost = 2;  // accumulator load / store and walk set-up, in entry units
+  int64_t load[FM_OWNER_THREADS] = {};
+  int next[FM_OWNER_THREADS];
+  for (int q = 0; q < n_int; ++q) load[q % FM_OWNER_THREADS] += w_int[q] + kNodeCost;
+  // (load, thread) heap of the threads with a free interface position
+  std::vector<std::pair<int64_t, int>> heap;
+  heap.reserve(FM_OWNER_THREADS);
+  for (int t = 0; t < FM_OWNER_THREADS; ++t) {
+    int q = n_int + ((t - n_int % FM_OWNER_THREADS) + FM_OWNER_THREADS) % FM_OWNER_THREADS;
+    next[t] = q;
+    if (q < n_node) heap.push_back({load[t], t});
+  }
+  auto later = [](const std::pair<int64_t, int>& a, const std::pair<int64_t, int>& b) { return a > b; };
+  std::make_heap(heap.begin(), heap.end(), later);
+  std::vector<int32_t>& by_w = scratch;
+  by_w.resize(n_ifc);
+  std::iota(by_w.begin(), by_w.end(), 0);
+  std::stable_sort(by_w.begin(), by_w.end(), [&](int32_t a, int32_t b) { return w_ifc[a] > w_ifc[b]; });
+  std::vector<int32_t> out(n_ifc);
+  for (int32_t i : by_w) {
+    std::pop_heap(heap.begin(), heap.end(), later);
+    auto [l, t] = heap.back();
+    heap.pop_back();
+    out[next[t] - n_int] = ifc[i];
+    next[t] += FM_OWNER_THREADS;
+    l += w_ifc[i] + kNodeCost;
+    if (next[t] < n_node) {
+      heap.push_back({l, t});
+      std::push_heap(heap.begin(), heap.end(), later);
+    }
+  }
+  ifc.swap(out);
+}
+
 // Builds the batch layout:
 //  1. elements of each problem sorted by the Morton code of their centroid;
 //  2. cut greedily into tiles of <= tile_elems elements and <= tile_nodes
@@ -567,7 +618,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         th.emplace_back([&, w] {
           std::vector<int32_t> local(N, -1);
           std::vector<uint64_t> used;                 // per-worker scratch, reused tile by tile
-          std::vector<int32_t> col, idx, cnt, pos;
+          std::vector<int32_t> col, idx, cnt, pos, w_int, w_ifc;
           for (int t = (int)(ntile * w / nw); t < (int)(ntile * (w + 1) / nw); ++t) {
             TileWork& W = tw[t];
             for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
@@ -578,13 +629,25 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
                   (ntiles[c[a]] == 1 ? W.inter : W.ifc).push_back(c[a]);
                 }
             }
-            // interior nodes in their (contiguous) batch order, then interface nodes by id
+            // interior nodes in their (contiguous) batch order, then interface
+            // nodes by id, reordered to balance the owner threads
             std::sort(W.inter.begin(), W.inter.end(), [&](int32_t x, int32_t y) { return nn[x] < nn[y]; });
             std::sort(W.ifc.begin(), W.ifc.end(), [&](int32_t x, int32_t y) { return nn[x] < nn[y]; });
             int32_t li = 0;
             for (int32_t v : W.inter) local[v] = li++;
             for (int32_t v : W.ifc) local[v] = li++;
             const int32_t n_node = li;
+            {
+              cnt.assign(n_node, 0);
+              for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi)
+                for (int a = 0; a < npe; ++a) cnt[local[cs[(size_t)oi * npe + a]]]++;
+              const int n_int = (int)W.inter.size();
+              w_int.assign(cnt.begin(), cnt.begin() + n_int);
+              w_ifc.assign(cnt.begin() + n_int, cnt.end());
+              balance_owners(w_int, w_ifc, W.ifc, idx);
+              li = n_int;
+              for (int32_t v : W.ifc) local[v] = li++;
+            }
             // colouring (greedy, up to 128 colours)
             const int64_t ne = tile_start[t + 1] - tile_start[t];
             used.assign(2 * (size_t)n_node, 0);

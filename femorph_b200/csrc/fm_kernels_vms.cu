@@ -344,14 +344,17 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
   }
 
   // nodes owned by this thread for the accumulation: j * THREADS + tid;
-  // cur/end walk each one's incidence list in element order
+  // cur/end walk each one's incidence list in element order, nxt holds the
+  // entry at cur (loaded one step ahead, so the walk's shared-memory loads
+  // do not wait on each other)
   auto owned_node = [](int t, int j) { return j * THREADS + t; };
-  int cur[MAXOWN], endi[MAXOWN];
+  int cur[MAXOWN], endi[MAXOWN], nxt[MAXOWN];
 #pragma unroll
   for (int j = 0; j < MAXOWN; ++j) {
     const int ln = owned_node(tid, j);
     cur[j] = ln < tm.n_node ? s_off[ln] : 0;
     endi[j] = ln < tm.n_node ? s_off[ln + 1] : 0;
+    nxt[j] = cur[j] < endi[j] ? s_inc[cur[j]] : 0;
   }
   int k = 0;
   for (; k < nchunks; ++k) {
@@ -436,14 +439,16 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
 #pragma unroll
     for (int j = 0; j < MAXOWN; ++j) {
       const int ln = owned_node(tid, j);
-      if (ln < tm.n_node) {
+      int c = cur[j];
+      const int ce = endi[j];
+      int ent = nxt[j];
+      // nodes without an entry in this chunk leave their accumulators alone
+      if (c < ce && (ent >> 2) - base < THREADS) {
         double a0 = s_a0[ln], a1 = s_a1[ln], a2 = s_a2[ln], a3 = s_a3[ln];
-        int c = cur[j];
-        const int ce = endi[j];
         while (c < ce) {
-          const int ent = s_inc[c];
           const int col = (ent >> 2) - base;
           if (col >= THREADS) break;
+          const int ent1 = s_inc[c + 1 < ce ? c + 1 : c];
           if constexpr (MIXED) {
             const double2* Rc = R2 + col * 8;
             const int q0i = 2 * (ent & 3), sw = col & 7;
@@ -459,9 +464,11 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
             a2 += Rp[2 * THREADS];
             a3 += Rp[3 * THREADS];
           }
+          ent = ent1;
           ++c;
         }
         cur[j] = c;
+        nxt[j] = ent;
         s_a0[ln] = a0; s_a1[ln] = a1; s_a2[ln] = a2; s_a3[ln] = a3;
       }
     }
