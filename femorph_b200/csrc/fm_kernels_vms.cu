@@ -445,27 +445,38 @@ __global__ void __launch_bounds__(THREADS, MINB) vms_tile_kernel(DevBatch B, int
       // nodes without an entry in this chunk leave their accumulators alone
       if (c < ce && (ent >> 2) - base < THREADS) {
         double a0 = s_a0[ln], a1 = s_a1[ln], a2 = s_a2[ln], a3 = s_a3[ln];
-        while (c < ce) {
-          const int col = (ent >> 2) - base;
-          if (col >= THREADS) break;
-          const int ent1 = s_inc[c + 1 < ce ? c + 1 : c];
+        // the residual entries of incidence entry e (of this chunk)
+        auto fetch = [&](int e, double v[4]) {
+          const int col = (e >> 2) - base;
           if constexpr (MIXED) {
             const double2* Rc = R2 + col * 8;
-            const int q0i = 2 * (ent & 3), sw = col & 7;
+            const int q0i = 2 * (e & 3), sw = col & 7;
             const double2 q0 = Rc[q0i ^ sw], q1 = Rc[(q0i + 1) ^ sw];
-            a0 += q0.x;
-            a1 += q0.y;
-            a2 += q1.x;
-            a3 += q1.y;
+            v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
           } else {
-            const double* Rp = R + (ent & 3) * 4 * THREADS + col;  // rows 4*corner .. 4*corner+3
-            a0 += Rp[0];
-            a1 += Rp[THREADS];
-            a2 += Rp[2 * THREADS];
-            a3 += Rp[3 * THREADS];
+            const double* Rp = R + (e & 3) * 4 * THREADS + col;  // rows 4*corner .. 4*corner+3
+            v[0] = Rp[0]; v[1] = Rp[THREADS]; v[2] = Rp[2 * THREADS]; v[3] = Rp[3 * THREADS];
           }
-          ent = ent1;
-          ++c;
+        };
+        // two entries a pass (their loads overlap), added in element order;
+        // the entries after them are loaded one pass ahead
+        while (true) {
+          const int ent1 = s_inc[c + 1 < ce ? c + 1 : c];
+          const int ent2 = s_inc[c + 2 < ce ? c + 2 : c];
+          const bool two = c + 1 < ce && (ent1 >> 2) - base < THREADS;
+          double v[4], w[4];
+          fetch(ent, v);
+          fetch(two ? ent1 : ent, w);
+          a0 += v[0]; a1 += v[1]; a2 += v[2]; a3 += v[3];
+          if (!two) {
+            ++c;
+            ent = ent1;
+            break;
+          }
+          a0 += w[0]; a1 += w[1]; a2 += w[2]; a3 += w[3];
+          c += 2;
+          ent = ent2;
+          if (c >= ce || (ent >> 2) - base >= THREADS) break;
         }
         cur[j] = c;
         nxt[j] = ent;
