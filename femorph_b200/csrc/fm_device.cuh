@@ -230,6 +230,32 @@ __device__ __forceinline__ void apply_bc(const DevBatch& B, int32_t rec, double 
   }
 }
 
+// Adds the tile partials of interface slots [k0, k1) to acc in slot (tile)
+// order.  The slot ids, and then the partials, are loaded four at a time
+// (past k1 the first id is loaded again and not added), so that their round
+// trips overlap instead of following one another slot by slot.
+__device__ __forceinline__ void sum_partials(const DevBatch& B, int k0, int k1, double acc[4]) {
+  for (int k = k0; k < k1; k += 4) {
+    int s[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s[i] = B.iface_slots[k + i < k1 ? k + i : k];
+    double2 q[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      q[i][0] = B.part[2 * s[i]];
+      q[i][1] = B.part[2 * s[i] + 1];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (k + i < k1) {
+        acc[0] += q[i][0].x;
+        acc[1] += q[i][0].y;
+        acc[2] += q[i][1].x;
+        acc[3] += q[i][1].y;
+      }
+  }
+}
+
 // Marks the end of one pass over the interface nodes.  The last block to
 // finish (counter pattern: fence, ticket, no waiting) advances every active
 // problem by one iteration and its time at the start of a new step.  A

@@ -328,15 +328,13 @@ __global__ void supg_iface_kernel(DevBatch B) {
     const int g = B.iface_node[i];
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     if (pidx < 0) continue;  // free interface entry
+    // partials loaded before the state check (see vms_iface_kernel); the
+    // fourth component is not used
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    sum_partials(B, k0, k1, acc);
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
-    double acc[3] = {0.0, 0.0, 0.0};
-    for (int kk = k0; kk < k1; ++kk) {
-      const int s = B.iface_slots[kk];
-      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
-      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x;
-    }
     double old[3] = {B.su[g], B.sv[g], B.sw[g]};
     mask_fixed(P.glob_fixed, old[0], old[1], old[2]);
     int32_t status = FM_OK;
@@ -356,13 +354,8 @@ __global__ void supg_xpack_kernel(DevBatch B) {
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
-    double acc[3] = {0.0, 0.0, 0.0};
-    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
-    for (int kk = k0; kk < k1; ++kk) {
-      const int s = B.iface_slots[kk];
-      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
-      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x;
-    }
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};  // the fourth component is not used
+    sum_partials(B, B.iface_slot_beg[i], B.iface_slot_beg[i] + B.iface_slot_cnt[i], acc);
     const int xi = B.iface_xidx[i];
     if (xi >= 0) {
       double* d = B.xsend + ((int64_t)P.xslice * B.x_n + xi) * 4;

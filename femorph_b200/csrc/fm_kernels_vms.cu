@@ -531,16 +531,14 @@ __global__ void vms_iface_kernel(DevBatch B) {
     const int g = B.iface_node[i];
     const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
     if (pidx < 0) continue;  // free interface entry
+    // the partials are loaded before the state check (an active entry's
+    // slots are valid whatever the problem's state)
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    sum_partials(B, k0, k1, acc);
     const DevProbState st = B.pstate[pidx];
     if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     const bool first_dual = (st.iter % (P.ndual + 1)) == 0;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k = k0; k < k1; ++k) {
-      const int s = B.iface_slots[k];
-      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
-      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x; acc[3] += q1.y;
-    }
     const double post[4] = {B.su[g], B.sv[g], B.sw[g], B.sp[g]};
     int32_t status = FM_OK;
     vms_node_update(B, P, pidx, st.iter, st.time, g, post, acc, first_dual, &status);
@@ -560,12 +558,7 @@ __global__ void vms_xpack_kernel(DevBatch B) {
     if (st.iter >= B.target[pidx] || st.status != FM_OK) continue;
     const DevProb& P = B.probs[pidx];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int k0 = B.iface_slot_beg[i], k1 = k0 + B.iface_slot_cnt[i];
-    for (int k = k0; k < k1; ++k) {
-      const int s = B.iface_slots[k];
-      const double2 q0 = B.part[2 * s], q1 = B.part[2 * s + 1];
-      acc[0] += q0.x; acc[1] += q0.y; acc[2] += q1.x; acc[3] += q1.y;
-    }
+    sum_partials(B, B.iface_slot_beg[i], B.iface_slot_beg[i] + B.iface_slot_cnt[i], acc);
     const int xi = B.iface_xidx[i];
     if (xi >= 0) {
       double* d = B.xsend + ((int64_t)P.xslice * B.x_n + xi) * 4;
