@@ -284,6 +284,114 @@ def run_batched(args, rank, world, local_rank, dist):
     return res
 
 
+def run_poisson(args, rank, world, local_rank, dist):
+    """The Poisson solver (femPoissonSolver::solve) on an n^3 Kuhn-tet cube:
+    each timed step is one whole preconditioned-CG solve from x = 0 to a
+    relative residual of 1e-10 on the device (host assembly and upload are
+    outside the timed region, which is what e2e adds)."""
+    from femorph_b200 import api, mesh
+
+    n = args.n or 96
+    p = mesh.poisson_box(n, mesh.TET4, seed=rank)
+    s = api.GpuPoisson(p, device=local_rank)
+    rows, nnz = s.info()
+    for _ in range(max(1, args.warmup)):
+        s.solve(1e-10, 100000)
+    if dist:
+        dist.barrier()
+    iters, dev_ms = 0, 0.0
+    solves = max(1, args.steps)
+    with ClockSampler(local_rank) as clk:
+        for _ in range(solves):
+            it, rr, ms = s.solve(1e-10, 100000)
+            iters += it
+            dev_ms += ms
+    s.close()
+    if dist:
+        import torch
+        t = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    res = dict(n=n, N=p.n_nodes, E=p.n_elems, nnz=nnz, iters=iters, solves=solves, ms=dev_ms, clocks=clk.summary(),
+               rr=rr)
+    if rank == 0:
+        # end to end through the C ABI: host assembly + upload + solve + read-back
+        t0 = time.perf_counter()
+        s2 = api.GpuPoisson(p, device=local_rank)
+        it2, _, _ = s2.solve(1e-10, 100000)
+        x, _ = s2.solution()
+        t1 = time.perf_counter()
+        s2.close()
+        res["e2e_s"], res["e2e_iters"] = t1 - t0, it2
+        res["h2d"] = p.coords.nbytes + p.conn.nbytes + p.diffusivity.nbytes
+        res["d2h"] = x.nbytes
+        if not args.no_cpu:
+            res["cpu"] = poisson_cpu_baseline(p)
+    return res
+
+
+def poisson_cpu_baseline(p, iters: int = 200):
+    """The same Jacobi-preconditioned CG on the host (scipy sparse matrix of
+    the oracle's assembly of the reference's system), a bounded number of
+    iterations."""
+    import scipy.sparse as sp
+    from oracle import oracle_b
+
+    K, b, _ = oracle_b.poisson_system(p)
+    dinv = 1.0 / K.diagonal()
+    x = np.zeros_like(b)
+    r = b.copy()
+    z = dinv * r
+    q = z.copy()
+    rz = r @ z
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        w = K @ q
+        a = rz / (q @ w)
+        x += a * q
+        r -= a * w
+        z = dinv * r
+        rz2 = r @ z
+        q = z + (rz2 / rz) * q
+        rz = rz2
+    dt = time.perf_counter() - t0
+    return {"value": p.n_nodes * iters / dt, "unit": "DOF-iterations/s", "cores": 1, "kind": "port",
+            "sample": f"{iters} Jacobi-PCG iterations on the oracle's assembly of the same system (scipy CSR, "
+                      f"numpy vectors, one host thread)"}
+
+
+def poisson_line(args, world, r):
+    peak, peak_kind = hbm_peak()
+    N, nnz = r["N"], r["nnz"]
+    # compulsory bytes of one CG iteration: the matrix (value + column), row
+    # offsets and the vectors each kernel reads or writes once (p, q in the
+    # product; x, p, r, q, z, D^-1 in the update; z, p in the direction)
+    ab = 12 * nnz + 4 * (N + 1) + 8 * N * 13
+    ms_it = r["ms"] / max(1, r["iters"])
+    achieved = ab / (ms_it * 1e-3) / 1e9
+    value = world * N * r["iters"] / (r["ms"] / 1e3)
+    line = {"metric": "Poisson CG DOF-iterations/s (Jacobi-PCG to 1e-10, n^3 Kuhn-tet cube)", "value": value,
+            "unit": "DOF-iterations/s", "n_gpus": world, "steps": r["solves"], "warmup": args.warmup,
+            "ms_per_step": r["ms"] / r["solves"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"femPoissonSolver on the {r['n']}^3 Kuhn-tet cube ({r['E']} tets, {N} nodes, "
+                                   f"{nnz} matrix entries), anisotropic diffusivity, sources, Neumann and Dirichlet "
+                                   f"faces; a step is one whole CG solve ({r['iters'] // r['solves']} iterations)",
+                       "l2": "matrix and vectors larger than L2 (no flush)",
+                       "parallelism": f"{world} independent solve(s), one per GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind, "kernel": "CG iteration (3 kernels)",
+                         "algorithmic_bytes_per_iteration": ab, "avg_iteration_ms": ms_it},
+            "gpu_launches": 3 * r["iters"] + 3 * r["solves"], "clocks": r["clocks"]}
+    if "e2e_s" in r:
+        line["e2e"] = {"value": N * r["e2e_iters"] / r["e2e_s"], "unit": "DOF-iterations/s",
+                       "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                       "note": "one whole solve through the C ABI: host assembly + upload + CG + read-back, wall clock"}
+    if "cpu" in r:
+        line["cpu_baseline"] = r["cpu"]
+    return line
+
+
 def batched_line(args, world, rb):
     peak, peak_kind = hbm_peak()
     out = {}
@@ -482,6 +590,9 @@ def run_reference(args):
     W warm-up + K timed time steps, parse and setup excluded."""
     from oracle import ref
     from femorph_b200 import mesh
+    if args.config == "poisson":
+        return {"impl": "reference", "unavailable": "the reference solves the Poisson system only through Trilinos "
+                                                    "(src/femSolver.cpp:590-600), which is not in this image"}
     if not ref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/fm_refdrv was not built (reference sources absent)"}
     n = cpu_sample_n(args)
@@ -557,7 +668,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="mesh size (default 96 for cavity/supg, 64 for channel)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--config", default="cavity",
-                    choices=["cavity", "supg", "channel", "batched", "serve", "partitioned"])
+                    choices=["cavity", "supg", "channel", "batched", "serve", "partitioned", "poisson"])
     ap.add_argument("--rates", default="10,30,100,1000", help="serve: arrival rates, requests/s")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
     ap.add_argument("--budget-gb", type=float, default=16.0, help="serve: HBM budget of the pooled batch")
@@ -606,6 +717,14 @@ def main():
         runs = {pn: run_partitioned(args, rank, world, local_rank, dist, pn) for pn in precs}
         if rank == 0:
             print(json.dumps(partitioned_line(args, world, runs)), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.config == "poisson":
+        rp = run_poisson(args, rank, world, local_rank, dist)
+        if rank == 0:
+            print(json.dumps(poisson_line(args, world, rp)), flush=True)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

@@ -35,7 +35,10 @@ SYMBOLS = [
     "fm_problem_write_vtu", "fm_batch_exchange_account", "fm_batch_exchange_buffers", "fm_batch_exchange_begin",
     "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
     "fm_batch_set_diagnostics", "fm_problem_vms_log", "fm_problem_vms_residuals",
+    "fm_poisson_create", "fm_poisson_destroy", "fm_poisson_solve", "fm_poisson_get_solution", "fm_poisson_info",
 ]
+
+FM_POISSON_CLASSIC, FM_POISSON_PPE, FM_POISSON_DISTANCE = 0, 1, 2
 
 
 class FmMesh(C.Structure):
@@ -65,6 +68,15 @@ class FmCapacity(C.Structure):
     _fields_ = [("solver", C.c_int32), ("elem_type", C.c_int32), ("precision", C.c_int32),
                 ("max_problems", C.c_int32), ("max_elems", C.c_int64), ("max_nodes", C.c_int64),
                 ("max_table_rows", C.c_int64), ("reserved", C.c_int64 * 4)]
+
+
+class FmPoissonDesc(C.Structure):
+    _fields_ = [("elem_type", C.c_int32), ("problem", C.c_int32), ("n_nodes", C.c_int64), ("n_elems", C.c_int64),
+                ("coords", C.c_void_p), ("conn", C.c_void_p), ("diffusivity", C.c_void_p),
+                ("n_sources", C.c_int64), ("source_elem", C.c_void_p), ("source_value", C.c_void_p),
+                ("n_neumann", C.c_int64), ("neumann_off", C.c_void_p), ("neumann_nodes", C.c_void_p),
+                ("neumann_value", C.c_void_p), ("n_dirichlet", C.c_int64), ("dir_node", C.c_void_p),
+                ("dir_value", C.c_void_p)]
 
 
 class FmError(RuntimeError):
@@ -133,6 +145,11 @@ def lib():
         L.fm_batch_exchange_end.argtypes = [P, P]
         L.fm_batch_iterations_per_step.argtypes = [P, P]
         L.fm_batch_exchange_account.argtypes = [P, C.c_int32]
+        L.fm_poisson_create.argtypes = [P, C.c_int32, P]
+        L.fm_poisson_destroy.argtypes = [P]
+        L.fm_poisson_solve.argtypes = [P, C.c_double, C.c_int32, P, P, P]
+        L.fm_poisson_get_solution.argtypes = [P, P, P]
+        L.fm_poisson_info.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -493,3 +510,51 @@ def solve(p: "_mesh.Problem", steps: int | None = None, precision: int = FM_FP64
     b.step(p.steps if steps is None else steps)
     b.sync()
     return gp, b
+
+
+class GpuPoisson:
+    """femPoissonSolver::solve (femSolver.cpp:409-654) on the GPU: the system
+    of a `mesh.PoissonProblem` assembled on the host, solved by conjugate
+    gradients on `device`."""
+
+    def __init__(self, pp: "_mesh.PoissonProblem", device: int = 0):
+        self._keep = [np.ascontiguousarray(a) for a in (
+            pp.coords, pp.conn, pp.diffusivity, pp.source_elem, pp.source_value, pp.neumann_off, pp.neumann_nodes,
+            pp.neumann_value, pp.dir_node, pp.dir_value)]
+        co, cn, df, se, sv, no, nn, nv, dn, dv = self._keep
+        d = FmPoissonDesc(int(cn.shape[1]), int(pp.problem), int(co.shape[0]), int(cn.shape[0]), _p(co), _p(cn), _p(df),
+                          int(se.size), _p(se), _p(sv), int(nv.size), _p(no), _p(nn), _p(nv), int(dn.size), _p(dn),
+                          _p(dv))
+        h = C.c_void_p()
+        check(lib().fm_poisson_create(C.byref(d), int(device), C.byref(h)))
+        self.h = h
+        self.n_nodes, self.n_elems, self.problem = int(co.shape[0]), int(cn.shape[0]), int(pp.problem)
+
+    def solve(self, rel_tol: float = 1e-12, max_iter: int = 20000):
+        """Returns (iterations, relative residual, device ms)."""
+        it, rr, ms = C.c_int32(), C.c_double(), C.c_double()
+        check(lib().fm_poisson_solve(self.h, float(rel_tol), int(max_iter), C.byref(it), C.byref(rr), C.byref(ms)))
+        return int(it.value), float(rr.value), float(ms.value)
+
+    def solution(self):
+        """(x, cell distance or None)."""
+        x = np.empty(self.n_nodes)
+        dist = np.empty(self.n_elems) if self.problem == FM_POISSON_DISTANCE else None
+        check(lib().fm_poisson_get_solution(self.h, _p(x), _p(dist)))
+        return x, dist
+
+    def info(self):
+        r, z = C.c_int64(), C.c_int64()
+        check(lib().fm_poisson_info(self.h, C.byref(r), C.byref(z)))
+        return int(r.value), int(z.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fm_poisson_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -279,3 +279,112 @@ def write_dat(p: Problem, path: str, output_prefix: str = "sol", log_file: str =
         f.write(_fmt_rows("NODEVEL ", p.vel_node + 1, p.vel_vals, p.vel_dir))
         f.write(_fmt_rows("NODEDIRBC ", p.dir_node + 1, p.dir_vals))
         f.write(_fmt_rows("NODEPRES ", p.pres_node + 1, p.pres_vals.reshape(-1, 1)))
+
+
+# ---------------------------------------------------------------------------
+# Poisson problems (femPoissonSolver::solve, femSolver.cpp:409-654)
+# ---------------------------------------------------------------------------
+POISSON_CLASSIC, POISSON_PPE, POISSON_DISTANCE = 0, 1, 2
+
+
+@dataclass
+class PoissonProblem:
+    """The femModel fields femPoissonSolver::solve reads: mesh, per-element
+    diffusivity (ELDIFF rows in element order), ELSOURCE rows, FACENEUMANN
+    rows (face node lists in CSR form), NODEDIRBC rows (first value) and the
+    PROBLEM type."""
+    coords: np.ndarray
+    conn: np.ndarray
+    diffusivity: np.ndarray
+    source_elem: np.ndarray
+    source_value: np.ndarray
+    neumann_off: np.ndarray
+    neumann_nodes: np.ndarray
+    neumann_value: np.ndarray
+    dir_node: np.ndarray
+    dir_value: np.ndarray
+    problem: int = POISSON_CLASSIC
+    name: str = "poisson"
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def n_elems(self) -> int:
+        return int(self.conn.shape[0])
+
+
+def poisson_box(n: int, elem_type: int = TET4, problem: int = POISSON_CLASSIC, seed: int = 0,
+                jitter: float = 0.1, anisotropic: bool = True, sources: bool = True, neumann: bool = True,
+                dirichlet: bool = True) -> PoissonProblem:
+    """Unit cube, n^3 cells (6 Kuhn tets or one hexa8 each) with seeded
+    interior jitter; seeded per-element diffusivity (each component in
+    [0.5, 2] when anisotropic, else 1); an ELSOURCE row for every fourth
+    element; FACENEUMANN rows on the x = 1 face (one per boundary face, its
+    3 or 4 nodes); NODEDIRBC on the x = 0 face with a smooth value.  Without
+    Dirichlet rows the system is singular (pure Neumann): the solver then
+    works on the zero-sum part of the right-hand side."""
+    rng = np.random.default_rng(seed + 7919)
+    if elem_type == TET4:
+        X, conn, _ = kuhn_cavity_mesh(n, seed, jitter)
+    else:
+        p = channel(n, n, n, seed=seed, jitter=jitter, steps=1)
+        X = p.coords / np.array([4.0, 1.0, 1.0])  # the channel box scaled to the unit cube
+        conn = p.conn
+    E = conn.shape[0]
+    diff = rng.uniform(0.5, 2.0, (E, 3)) if anisotropic else np.ones((E, 3))
+    if sources:
+        se = np.arange(0, E, 4, dtype=np.int32)
+        sv = rng.uniform(-1.0, 1.0, se.size)
+    else:
+        se, sv = np.zeros(0, np.int32), np.zeros(0)
+    tol = 1e-12
+    on_x1 = X[:, 0] > 1.0 - tol
+    if neumann:
+        # boundary faces on x = 1: element faces whose nodes all lie there
+        faces = []
+        npe = conn.shape[1]
+        face_sets = ([(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)] if npe == 4 else
+                     [(0, 1, 2, 3), (4, 5, 6, 7), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7)])
+        for fs in face_sets:
+            m = np.all(on_x1[conn[:, list(fs)]], axis=1)
+            for e in np.nonzero(m)[0]:
+                faces.append(conn[e, list(fs)])
+        faces.sort(key=lambda f: tuple(sorted(f.tolist())))
+        off = np.zeros(len(faces) + 1, np.int32)
+        off[1:] = np.cumsum([len(f) for f in faces])
+        nodes = np.concatenate(faces).astype(np.int32) if faces else np.zeros(0, np.int32)
+        nval = rng.uniform(0.0, 1.0, len(faces))
+    else:
+        off, nodes, nval = np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)
+    if dirichlet:
+        dn = np.nonzero(X[:, 0] < tol)[0].astype(np.int32)
+        dv = np.sin(np.pi * X[dn, 1]) * np.cos(np.pi * X[dn, 2])
+    else:
+        dn, dv = np.zeros(0, np.int32), np.zeros(0)
+    return PoissonProblem(X, conn.astype(np.int32), diff, se, sv, off, nodes, nval, dn, dv, problem,
+                          name=f"poisson{'tet' if elem_type == TET4 else 'hexa'}{n}_s{seed}")
+
+
+def write_poisson_dat(pp: PoissonProblem, path: str) -> None:
+    """Write ``pp`` as a reference-readable .dat keyword file (PROBLEM, NODE,
+    ELEMENT, ELDIFF, ELSOURCE, FACENEUMANN, NODEDIRBC; femModel.cpp:
+    3719-4213)."""
+    kind = {POISSON_CLASSIC: "POISSON", POISSON_PPE: "PPE", POISSON_DISTANCE: "DISTANCE"}[pp.problem]
+    with open(path, "w") as f:
+        f.write(f"PROBLEM {kind}\n")
+        N, E = pp.n_nodes, pp.n_elems
+        f.write(_fmt_rows("NODE ", np.arange(1, N + 1), pp.coords))
+        et = "TET4" if pp.conn.shape[1] == 4 else "HEXA8"
+        lines = np.char.add(f"ELEMENT {et} ", np.arange(1, E + 1).astype(str))
+        lines = np.char.add(lines, " 1")
+        for c in range(pp.conn.shape[1]):
+            lines = np.char.add(np.char.add(lines, " "), (pp.conn[:, c].astype(np.int64) + 1).astype(str))
+        f.write("\n".join(lines.tolist()) + "\n")
+        f.write(_fmt_rows("ELDIFF ", np.arange(1, E + 1), pp.diffusivity))
+        f.write(_fmt_rows("ELSOURCE ", pp.source_elem + 1, pp.source_value.reshape(-1, 1)))
+        for k in range(pp.neumann_value.size):
+            nodes = pp.neumann_nodes[pp.neumann_off[k]:pp.neumann_off[k + 1]] + 1
+            f.write("FACENEUMANN 1 " + " ".join(str(int(v)) for v in nodes) + " %.17e\n" % pp.neumann_value[k])
+        f.write(_fmt_rows("NODEDIRBC ", pp.dir_node + 1, pp.dir_value.reshape(-1, 1)))

@@ -415,6 +415,74 @@ FM_API int fm_batch_estimate_bytes(fm_problem* const* problems, int32_t n, const
 FM_API int fm_batch_layout(fm_batch* b, int64_t* n_tiles, int64_t* n_iface_nodes, int32_t* max_colors,
                     int64_t* n_slots);
 
+/* ---- Poisson solver (femPoissonSolver::solve, femSolver.cpp:409-654) ----
+ * The implicit neighbour of the explicit path: the same tet4 / hexa8
+ * kinematics (irSecondOrder Gauss points, femElement.cpp:272-354) assemble
+ *   K[a][b] = sum_e sum_g (sum_d diff_e[d] dN_a,d dN_b,d) detJ w_g
+ * (femElement::formPoissonMatrix, femElement.cpp:903-944) and
+ *   f[a] = sum_sources sum_g N_a source detJ w_g
+ * (femElement::formPoissonSource, femElement.cpp:949-981), plus face Neumann
+ * values spread evenly over the face's nodes (femSolver.cpp:546-562); the
+ * Dirichlet rows become identity rows with the value on the right-hand side
+ * (femTrilinosMatrix::applyBlockDirichelet, femTrilinosVector.cpp:109-119).
+ * The reference then solves with Trilinos (its other builds stop: "Solver not
+ * available", femSolver.cpp:590-600); here the system is solved on the GPU by
+ * conjugate gradients with a Jacobi preconditioner on the assembled matrix
+ * (the Dirichlet columns moved to the right-hand side, which keeps it
+ * symmetric and leaves the solution unchanged).  Results: the nodal solution
+ * ("PoissonResult"; its average subtracted for FM_POISSON_PPE,
+ * femSolver.cpp:604-612) and, for FM_POISSON_DISTANCE, the element wall
+ * distance of femPoissonSolver::evalDistanceFromPoissonSolution
+ * (femSolver.cpp:366-403). */
+enum { FM_POISSON_CLASSIC = 0, FM_POISSON_PPE = 1, FM_POISSON_DISTANCE = 2 };
+
+/* femModel fields read by femPoissonSolver::solve (femModel.h): the mesh,
+ * elDiffusivity (one row a element, in ELDIFF row order, femModel.cpp:
+ * 3909-3925), sourceElement / sourceValues (ELSOURCE, femModel.cpp:
+ * 3999-4011), neumannBCFaceNodes / neumannBCValues (FACENEUMANN,
+ * femModel.cpp:4185-4200, face node lists in CSR form), diricheletBCNode and
+ * the first NODEDIRBC value (femModel.cpp:3926-3950), problemType (PROBLEM,
+ * femModel.cpp:4036-4050). */
+typedef struct fm_poisson_desc {
+  int32_t elem_type;             /* FM_TET4 or FM_HEXA8 */
+  int32_t problem;               /* FM_POISSON_* */
+  int64_t n_nodes, n_elems;
+  const double* coords;          /* n_nodes x 3 */
+  const int32_t* conn;           /* n_elems x elem_type, 0-based */
+  const double* diffusivity;     /* n_elems x 3 */
+  int64_t n_sources;
+  const int32_t* source_elem;    /* element of each ELSOURCE row */
+  const double* source_value;
+  int64_t n_neumann;
+  const int32_t* neumann_off;    /* n_neumann + 1 offsets into neumann_nodes */
+  const int32_t* neumann_nodes;  /* face nodes of each FACENEUMANN row */
+  const double* neumann_value;
+  int64_t n_dirichlet;
+  const int32_t* dir_node;
+  const double* dir_value;
+} fm_poisson_desc;
+
+typedef struct fm_poisson fm_poisson;
+
+/* Assembles the system on the host (element matrices in parallel, every
+ * matrix entry and right-hand-side value summed in element order) and
+ * uploads it to `device`.  The descriptor's arrays are copied. */
+FM_API int fm_poisson_create(const fm_poisson_desc* desc, int32_t device, fm_poisson** out);
+FM_API int fm_poisson_destroy(fm_poisson* s);
+/* Preconditioned CG from x = 0 until ||r|| <= rel_tol ||b|| or max_iter
+ * iterations; every reduction is summed in a fixed order, so the iterates
+ * are the same from run to run.  FM_ERR_DIVERGED if the iteration breaks down
+ * (a non-positive curvature or a NaN).  Device time of the solve in
+ * *device_ms (may be NULL). */
+FM_API int fm_poisson_solve(fm_poisson* s, double rel_tol, int32_t max_iter, int32_t* iterations,
+                            double* rel_residual, double* device_ms);
+/* The result fields: x (n_nodes; the average subtracted for
+ * FM_POISSON_PPE) and, when cell_distance is non-NULL and the problem is
+ * FM_POISSON_DISTANCE, the element wall distance (n_elems). */
+FM_API int fm_poisson_get_solution(fm_poisson* s, double* x, double* cell_distance);
+/* Sizes of the assembled system: rows and stored matrix entries. */
+FM_API int fm_poisson_info(const fm_poisson* s, int64_t* rows, int64_t* nonzeros);
+
 #ifdef __cplusplus
 }
 #endif

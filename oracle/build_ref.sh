@@ -39,7 +39,8 @@ LIBDIR=$HERE/../femorph_b200
 if [ -f "$LIBDIR/libfemorph_b200.so" ]; then
   g++ $CXXFLAGS -DFM_WITH_GPU_ADAPTER -I"$LIBDIR/adapter" -I"$HERE/../include" \
     -DFM_EXPORT_SYM="\"$EXPORT_SYM\"" -DFM_SETVEL_SYM="\"$SETVEL_SYM\"" \
-    "$HERE/refdrv.cpp" "$LIBDIR/adapter/femExplicitFluidSolverGPU.cpp" "$OBJ"/*.o -o "$OUT/fm_gpudrv" \
+    "$HERE/refdrv.cpp" "$LIBDIR/adapter/femExplicitFluidSolverGPU.cpp" "$LIBDIR/adapter/femPoissonSolverGPU.cpp" \
+    "$OBJ"/*.o -o "$OUT/fm_gpudrv" \
     -L"$LIBDIR" -lfemorph_b200 -Wl,-rpath,'$ORIGIN/../../femorph_b200' \
     -Wl,--wrap="$EXPORT_SYM" -Wl,--wrap="$SETVEL_SYM"
   echo "built $OUT/fm_gpudrv"

@@ -636,6 +636,114 @@ static void global_deriv(int npe, const double xe[8][3], const double* q, double
       }
 }
 
+/* ------------------------------------------------------------------ */
+/* Poisson (femPoissonSolver::solve, femSolver.cpp:409-654): element   */
+/* matrices and sources of its Gauss loops, and the wall distance.     */
+/* ------------------------------------------------------------------ */
+static void poisson_coords(int npe, const double* x, const int32_t* conn, int64_t e, double xe[8][3]) {
+  for (int a = 0; a < npe; ++a)
+    for (int k = 0; k < 3; ++k) xe[a][k] = x[(int64_t)conn[e * npe + a] * 3 + k];
+}
+
+/* femModel::FixedElementConnectivities (femModel.cpp:3554-3569), which the
+ * Poisson driver runs after reading the model (main.cpp:491): an element
+ * whose smallest Jacobian determinant over the irSecondOrder points
+ * (femElement::checkMinDetJ, femElement.cpp:63-81) is <= 0 gets one swap,
+ * tet4 nodes 0 and 1 (femTetra4.cpp:160-170), hexa8 nodes 2 / 3 and 6 / 7
+ * (femHexa8.cpp:93-103).  conn is modified in place; returns the count. */
+int64_t fmo_poisson_fix(int npe, int64_t E, const double* x, int32_t* conn) {
+  int ngp;
+  double gps[8][3], gpw[8];
+  int64_t fixed = 0;
+  gauss_rule(npe, &ngp, gps, gpw);
+  for (int64_t e = 0; e < E; ++e) {
+    double xe[8][3], gd[8][3], detJ, mn = 1e308;
+    poisson_coords(npe, x, conn, e, xe);
+    for (int g = 0; g < ngp; ++g) {
+      global_deriv(npe, xe, gps[g], &detJ, gd, NULL);
+      if (detJ < mn) mn = detJ;
+    }
+    if (mn <= 0.0) {
+      int32_t* c = conn + e * npe;
+      int32_t t;
+      if (npe == 4) {
+        t = c[1]; c[1] = c[0]; c[0] = t;
+      } else {
+        t = c[2]; c[2] = c[3]; c[3] = t;
+        t = c[6]; c[6] = c[7]; c[7] = t;
+      }
+      ++fixed;
+    }
+  }
+  return fixed;
+}
+
+/* femElement::formPoissonMatrix (femElement.cpp:903-944), irSecondOrder
+ * rule, for elements [0, E): Ke[e][a][b] (npe x npe each). */
+void fmo_poisson_elements(int npe, int64_t E, const double* x, const int32_t* conn, const double* diff, double* Ke) {
+  int ngp;
+  double gps[8][3], gpw[8];
+  gauss_rule(npe, &ngp, gps, gpw);
+  for (int64_t e = 0; e < E; ++e) {
+    double xe[8][3], gd[8][3], detJ;
+    double* K = Ke + e * npe * npe;
+    poisson_coords(npe, x, conn, e, xe);
+    for (int a = 0; a < npe * npe; ++a) K[a] = 0.0;
+    for (int g = 0; g < ngp; ++g) {
+      global_deriv(npe, xe, gps[g], &detJ, gd, NULL);
+      for (int a = 0; a < npe; ++a)
+        for (int b = 0; b < npe; ++b) {
+          double st = 0.0;
+          for (int d = 0; d < 3; ++d) st += diff[e * 3 + d] * gd[a][d] * gd[b][d];
+          K[a * npe + b] += st * detJ * gpw[g];
+        }
+    }
+  }
+}
+
+/* femElement::formPoissonSource (femElement.cpp:949-981): f[a] of element e
+ * with source value `value` (detJ as femElement::evalJacobian,
+ * femElement.cpp:149-186). */
+void fmo_poisson_source(int npe, const double* x, const int32_t* conn, int64_t e, double value, double* f) {
+  int ngp;
+  double gps[8][3], gpw[8], xe[8][3], gd[8][3], N[8], detJ;
+  gauss_rule(npe, &ngp, gps, gpw);
+  poisson_coords(npe, x, conn, e, xe);
+  for (int a = 0; a < npe; ++a) f[a] = 0.0;
+  for (int g = 0; g < ngp; ++g) {
+    shape_fn(npe, gps[g], N);
+    global_deriv(npe, xe, gps[g], &detJ, gd, NULL);
+    for (int a = 0; a < npe; ++a) f[a] += N[a] * value * detJ * gpw[g];
+  }
+}
+
+/* fmo_poisson_source for every ELSOURCE row k (element elems[k], value
+ * values[k]): out[k][a]. */
+void fmo_poisson_sources(int npe, const double* x, const int32_t* conn, int64_t n, const int32_t* elems,
+                         const double* values, double* out) {
+  for (int64_t k = 0; k < n; ++k) fmo_poisson_source(npe, x, conn, elems[k], values[k], out + k * npe);
+}
+
+/* evalDistanceFromPoissonSolution (femSolver.cpp:366-403): per element the
+ * solution and its gradient at local coordinates (0, 0, 0). */
+void fmo_poisson_distance(int npe, int64_t E, const double* x, const int32_t* conn, const double* sol, double* dist) {
+  const double q0[3] = {0.0, 0.0, 0.0};
+  for (int64_t e = 0; e < E; ++e) {
+    double xe[8][3], gd[8][3], N[8], detJ, phi = 0.0, g[3] = {0.0, 0.0, 0.0};
+    poisson_coords(npe, x, conn, e, xe);
+    shape_fn(npe, q0, N);
+    global_deriv(npe, xe, q0, &detJ, gd, NULL);
+    for (int a = 0; a < npe; ++a) {
+      const double u = sol[conn[e * npe + a]];
+      phi += N[a] * u;
+      g[0] += gd[a][0] * u;
+      g[1] += gd[a][1] * u;
+      g[2] += gd[a][2] * u;
+    }
+    dist[e] = -sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) + sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + 2.0 * phi);
+  }
+}
+
 static void elem_coords(fmo_ctx* c, int64_t e, double xe[8][3]) {
   for (int a = 0; a < c->npe; ++a)
     for (int k = 0; k < 3; ++k) xe[a][k] = c->x[(int64_t)c->conn[e * c->npe + a] * 3 + k];

@@ -99,3 +99,101 @@ class OracleSolve:
 
     def __del__(self):
         self.close()
+
+
+# ---------------------------------------------------------------------------
+# Poisson (femPoissonSolver::solve, femSolver.cpp:409-654)
+# ---------------------------------------------------------------------------
+def _vp(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def poisson_fix(pp):
+    """Connectivity after femModel::FixedElementConnectivities (a copy)."""
+    L = lib()
+    L.fmo_poisson_fix.restype = C.c_int64
+    conn = np.ascontiguousarray(pp.conn, dtype=np.int32).copy()
+    L.fmo_poisson_fix(C.c_int(conn.shape[1]), C.c_int64(conn.shape[0]), _vp(np.ascontiguousarray(pp.coords)),
+                      _vp(conn))
+    return conn
+
+
+def poisson_elements(pp, conn):
+    """femElement::formPoissonMatrix of every element: (E, npe, npe)."""
+    E, npe = conn.shape
+    K = np.empty((E, npe, npe))
+    lib().fmo_poisson_elements(C.c_int(npe), C.c_int64(E), _vp(np.ascontiguousarray(pp.coords)), _vp(conn),
+                               _vp(np.ascontiguousarray(pp.diffusivity)), _vp(K))
+    return K
+
+
+def poisson_sources(pp, conn):
+    """femElement::formPoissonSource of every ELSOURCE row: (rows, npe)."""
+    npe = conn.shape[1]
+    out = np.empty((pp.source_elem.size, npe))
+    se = np.ascontiguousarray(pp.source_elem, dtype=np.int32)
+    sv = np.ascontiguousarray(pp.source_value, dtype=np.float64)
+    lib().fmo_poisson_sources(C.c_int(npe), _vp(np.ascontiguousarray(pp.coords)), _vp(conn), C.c_int64(se.size),
+                              _vp(se), _vp(sv), _vp(out))
+    return out
+
+
+def poisson_system(pp):
+    """The reference's assembled system (femSolver.cpp:446-586): K (CSR) and
+    the right-hand side after the sources, the face Neumann values and the
+    Dirichlet rows (identity rows, value on the right-hand side).  Returns
+    (K, b, fixed connectivity)."""
+    import scipy.sparse as sp
+    conn = poisson_fix(pp)
+    E, npe = conn.shape
+    N = pp.n_nodes
+    Ke = poisson_elements(pp, conn)
+    rows = np.repeat(conn, npe, axis=1).ravel()
+    cols = np.tile(conn, (1, npe)).ravel()
+    K = sp.coo_matrix((Ke.ravel(), (rows, cols)), shape=(N, N)).tocsr()
+    b = np.zeros(N)
+    fs = poisson_sources(pp, conn)
+    np.add.at(b, conn[pp.source_elem].ravel(), fs.ravel())  # rows in ELSOURCE order
+    nv = np.zeros(N)
+    cnt = np.diff(pp.neumann_off)
+    share = np.repeat(pp.neumann_value / np.maximum(cnt, 1), cnt)
+    np.add.at(nv, pp.neumann_nodes, share)
+    b += nv
+    if pp.dir_node.size:
+        # identity rows (femTrilinosMatrix::applyBlockDirichelet), the last
+        # NODEDIRBC row of a node wins (ReplaceGlobalValue)
+        keep = np.ones(N, bool)
+        keep[pp.dir_node] = False
+        D = sp.diags(keep.astype(np.float64))
+        K = (D @ K + sp.diags((~keep).astype(np.float64))).tocsr()
+        K.eliminate_zeros()
+        b[pp.dir_node] = pp.dir_value
+    return K, b, conn
+
+
+def poisson_solve(pp):
+    """Direct solution of the reference's system (its Trilinos solve is not
+    available here): x (the average subtracted for PPE) and, for DISTANCE,
+    the element distances of evalDistanceFromPoissonSolution.  Without
+    Dirichlet rows the system is singular: the right-hand side is reduced to
+    its zero-sum part and node 0 is pinned, and the solution is compared up
+    to a constant."""
+    import scipy.sparse.linalg as spla
+    K, b, conn = poisson_system(pp)
+    if pp.dir_node.size == 0:
+        import scipy.sparse as sp
+        b = b - b.mean()
+        keep = np.ones(K.shape[0])
+        keep[0] = 0.0
+        K = (sp.diags(keep) @ K + sp.diags(1.0 - keep)).tocsr()
+        b[0] = 0.0
+    x = spla.spsolve(K.tocsc(), b)
+    if pp.problem == 1:
+        x = x - x.mean()
+    dist = None
+    if pp.problem == 2:
+        E, npe = conn.shape
+        dist = np.empty(E)
+        lib().fmo_poisson_distance(C.c_int(npe), C.c_int64(E), _vp(np.ascontiguousarray(pp.coords)), _vp(conn),
+                                   _vp(np.ascontiguousarray(x)), _vp(dist))
+    return x, dist

@@ -19,6 +19,16 @@
 //
 // Usage: fm_refdrv model.dat vms|supg [--ic f64file ncomp] [--dump dir]
 //                  [--vtk] [--timing file]
+//        fm_refdrv model.dat poisson-elements --dump dir
+//        fm_gpudrv model.dat poisson-gpu --dump dir   (drop-in check build)
+// The second form reads a Poisson model (src/main.cpp:476-490:
+// ReadFromFEMTextFile, FixedElementConnectivities) and writes the reference's
+// own element arithmetic of femPoissonSolver::solve: the element matrix of
+// femElement::formPoissonMatrix for every element (src/femSolver.cpp:
+// 446-459), then the element vector of femElement::formPoissonSource for
+// every ELSOURCE row (src/femSolver.cpp:478-494), irSecondOrder rule, as raw
+// FP64 in dir/poisson_elements.f64.  (The reference solves the system only
+// through Trilinos, src/femSolver.cpp:590-600.)
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -27,6 +37,7 @@
 #include <vector>
 #include <unistd.h>
 
+#include "femIntegrationRule.h"
 #include "femModel.h"
 #include "femSUPGExplicitFluidSolver.h"
 #include "femVMSExplicitFluidSolver.h"
@@ -35,6 +46,7 @@
 // ("vms-gpu", "supg-gpu"), i.e. the reference's reader and VTK exporter
 // around the B200 solver.
 #include "femExplicitFluidSolverGPU.h"
+#include "femPoissonSolverGPU.h"
 #endif
 
 void real_export(femModel*, std::string, bool) __asm__("__real_" FM_EXPORT_SYM);
@@ -150,6 +162,44 @@ int main(int argc, char** argv) {
       double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - g_t0).count();
       fprintf(g_timing, "# parsed %.9f\n", s);
     }
+    if (solver == "poisson-elements") {
+      if (!g_dump) {
+        fprintf(stderr, "poisson-elements needs --dump dir\n");
+        return 2;
+      }
+      model->FixedElementConnectivities();
+      femIntegrationRule* rule = new femIntegrationRule(irSecondOrder);
+      std::string path = g_dump_dir + "/poisson_elements.f64";
+      FILE* f = fopen(path.c_str(), "wb");
+      if (!f) { perror(path.c_str()); return 4; }
+      femDoubleMat elMat(kMaxConnections, femDoubleVec(kMaxConnections, 0.0));
+      for (size_t e = 0; e < model->elementList.size(); ++e) {
+        femElement* el = model->elementList[e];
+        el->formPoissonMatrix(model->nodeList, rule, (femDoubleVec)model->elDiffusivity[e], elMat);
+        const size_t npe = el->elementConnections.size();
+        for (size_t a = 0; a < npe; ++a) fwrite(elMat[a].data(), sizeof(double), npe, f);
+      }
+      femDoubleVec elSrc(kMaxConnections, 0.0);
+      for (size_t k = 0; k < model->sourceElement.size(); ++k) {
+        femElement* el = model->elementList[model->sourceElement[k]];
+        el->formPoissonSource(model->nodeList, rule, model->sourceValues[k], elSrc);
+        fwrite(elSrc.data(), sizeof(double), el->elementConnections.size(), f);
+      }
+      fclose(f);
+      return 0;
+    }
+#ifdef FM_WITH_GPU_ADAPTER
+    if (solver == "poisson-gpu") {
+      // src/main.cpp:476-511 with the B200 adapter in place of femPoissonSolver;
+      // the results go through the export hook (--dump)
+      model->FixedElementConnectivities();
+      femPoissonSolverGPU* s = new femPoissonSolverGPU(0, 1e-14, 100000);
+      femPoissonSolverOptions* o = new femPoissonSolverOptions();
+      s->solve(o, model);
+      model->ExportToVTKLegacy("poisson", false);
+      return 0;
+    }
+#endif
     if (solver == "vms") {
       femVMSExplicitFluidSolver* s = new femVMSExplicitFluidSolver();
       s->solve(model);
