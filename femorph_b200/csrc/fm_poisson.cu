@@ -434,8 +434,7 @@ FM_API int fm_poisson_destroy(fm_poisson* s) {
   return FM_OK;
 }
 
-FM_API int fm_poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson** out) {
-  fm::NvtxRange nv("fm_poisson_create");
+static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson** out) {
   if (!d || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
   const int npe = d->elem_type;
@@ -555,8 +554,12 @@ FM_API int fm_poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisso
       rowlen[v] = std::max<int32_t>(1, (int32_t)(std::unique(cl.begin(), cl.end()) - cl.begin()));
     }
   }, 4096);
-  for (int64_t v = 0; v < N; ++v) rowp[v + 1] = rowp[v] + rowlen[v];
-  const int64_t nnz = rowp[N];
+  int64_t nnz = 0;
+  for (int64_t v = 0; v < N; ++v) {
+    nnz += rowlen[v];
+    if (nnz >= INT32_MAX) return fail(FM_ERR_INVALID, "matrix too large for 32-bit row offsets");
+    rowp[v + 1] = (int32_t)nnz;
+  }
   fm::hvec<int32_t> col(nnz);
   fm::hvec<double> val(nnz);
   std::vector<double> bvec(N), dinv(N);
@@ -715,6 +718,15 @@ FM_API int fm_poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisso
   if (e != cudaSuccess) return fail_free("upload of the Poisson system", e);
   *out = s;
   return FM_OK;
+}
+
+FM_API int fm_poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson** out) {
+  fm::NvtxRange nv("fm_poisson_create");
+  try {
+    return poisson_create(d, device, out);
+  } catch (const std::bad_alloc&) {
+    return fail(FM_ERR_OOM, "host allocation failed while assembling the Poisson system");
+  }
 }
 
 FM_API int fm_poisson_info(const fm_poisson* s, int64_t* rows, int64_t* nonzeros) {
