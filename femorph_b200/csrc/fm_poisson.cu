@@ -271,8 +271,25 @@ __global__ void __launch_bounds__(kThreads) cg_spmv_kernel(Cg c) {
     const int64_t i = base + (threadIdx.x % 32) / kRowLanes;
     double s = 0.0;
     if (i < c.n) {
+      // a lane's entries k0 + lane, + kRowLanes, ... in order, four a pass:
+      // the column ids, then the values and gathers of the pass are loaded
+      // together (one round trip each instead of one an entry)
       const int32_t k0 = c.rowp[i], k1 = c.rowp[i + 1];
-      for (int32_t k = k0 + lane; k < k1; k += kRowLanes) s += c.val[k] * c.p[c.col[k]];
+      for (int32_t kb = k0 + lane; kb < k1; kb += 4 * kRowLanes) {
+        int32_t cj[4];
+        double vj[4], pj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int32_t k = kb + u * kRowLanes;
+          cj[u] = k < k1 ? c.col[k] : 0;
+          vj[u] = k < k1 ? c.val[k] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pj[u] = c.p[cj[u]];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (kb + u * kRowLanes < k1) s += vj[u] * pj[u];
+      }
     }
 #pragma unroll
     for (int o = kRowLanes / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, kRowLanes);
