@@ -120,11 +120,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
-// ---- reciprocal, inverse cube root and square root by Newton-Raphson ----
+// ---- reciprocal, inverse cube root and square root ----
 // Seeds from the PTX approximate FP32 instructions (rcp/lg2/ex2/rsqrt
-// .approx, relative error below 2^-21), then Newton steps in FP64, each of
-// which squares the relative error: two steps leave it below 2^-84, i.e. the
-// results are within about one ulp of the correctly rounded values.
+// .approx, relative error below 2^-21), then one correction in FP64.  With
+// e = 1 - x y0 (reciprocal) or e = 1 - x y0^3 (inverse cube root) the exact
+// result is y0 / (1 - e) = y0 (1 + e + e^2 + ...), resp.
+// y0 (1 - e)^(-1/3) = y0 (1 + e/3 + 2 e^2 / 9 + 14 e^3 / 81 + ...); the
+// series is cut after the e^2 term (Householder's third-order step), which
+// with |e| < 2^-19 leaves a truncation below 2^-57, so the result is within
+// about one ulp of the correctly rounded value in one dependent step less
+// than two Newton steps.  The square root takes a Newton step on its inverse
+// and one on the root itself.
 __device__ __forceinline__ float ptx_rcp_approx(float x) {
   float y;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -150,22 +156,17 @@ __device__ __forceinline__ float ptx_rsqrt_approx(float x) {
 __device__ __forceinline__ double rcp_nr(double x) {
   const double ax = fabs(x);
   if (!(ax > 1e-37 && ax < 1e37)) return 1.0 / x;
-  double y = (double)ptx_rcp_approx((float)x);
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
+  const double y = (double)ptx_rcp_approx((float)x);
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
 }
-// x^(-1/3) for x > 0: Newton on f(y) = y^-3 - x, y <- y + y (1 - x y^3) / 3.
+// x^(-1/3) for x > 0 (third-order step above); the FP32 form below takes
+// one Newton step, y <- y + y (1 - x y^3) / 3.
 __device__ __forceinline__ double rcbrt_nr(double x) {
   if (!(x > 1e-37 && x < 1e37)) return rcbrt(x);
-  double y = (double)ptx_ex2_approx(ptx_lg2_approx((float)x) * (-1.0f / 3.0f));
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const double e = fma(-x, y * y * y, 1.0);
-    y = fma(y * (1.0 / 3.0), e, y);
-  }
-  return y;
+  const double y = (double)ptx_ex2_approx(ptx_lg2_approx((float)x) * (-1.0f / 3.0f));
+  const double e = fma(-x, y * y * y, 1.0);
+  return fma(y, e * fma(e, 2.0 / 9.0, 1.0 / 3.0), y);
 }
 __device__ __forceinline__ float rcbrt_nr(float x) {
   float y = ptx_ex2_approx(ptx_lg2_approx(x) * (-1.0f / 3.0f));
