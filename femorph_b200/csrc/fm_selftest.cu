@@ -1,5 +1,6 @@
-// Self-check of the library's own device arithmetic: the reciprocal, inverse cube root and square root of fm_device.cuh (used by the
-// element kernels in place of CUDA's division, rcbrt and sqrt) evaluated next
+// Self-check of the library's own device arithmetic: the reciprocal, inverse
+// cube root and square root of fm_device.cuh (used by the element kernels
+// in place of CUDA's division, rcbrt and sqrt) evaluated next
 // to CUDA's own operations on the same inputs, so that a test can bound
 // their difference in units in the last place.  No reference counterpart
 // (the reference computes 1.0 / detJ, pow(6V, 1/3) and sqrt on the host,

@@ -1,7 +1,7 @@
 """The element kernels' own reciprocal, inverse cube root and square root
 (fm_device.cuh: a correction step from the PTX approximate FP32 seeds,
-Newton's / Householder's published methods) against CUDA's 1.0/x, rcbrt, sqrt and rcbrtf on the same
-device, over a sweep that crosses the 1e-37 / 1e37 switch points to CUDA's
+Newton's / Householder's published methods) against CUDA's 1.0/x, rcbrt,
+sqrt and rcbrtf on the same device, over a sweep that crosses the 1e-37 / 1e37 switch points to CUDA's
 own operations, with ulp bounds.  (The reference computes these on the host:
 1.0 / detJ, pow(6V, 1/3), sqrt - src/femVMSExplicitFluidSolver.cpp:64, 75,
 585.)"""
