@@ -36,6 +36,7 @@ SYMBOLS = [
     "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
     "fm_batch_set_diagnostics", "fm_problem_vms_log", "fm_problem_vms_residuals",
     "fm_poisson_create", "fm_poisson_destroy", "fm_poisson_solve", "fm_poisson_get_solution", "fm_poisson_info",
+    "fm_poisson_read_dat",
 ]
 
 FM_POISSON_CLASSIC, FM_POISSON_PPE, FM_POISSON_DISTANCE = 0, 1, 2
@@ -150,6 +151,7 @@ def lib():
         L.fm_poisson_solve.argtypes = [P, C.c_double, C.c_int32, P, P, P]
         L.fm_poisson_get_solution.argtypes = [P, P, P]
         L.fm_poisson_info.argtypes = [P, P, P]
+        L.fm_poisson_read_dat.argtypes = [C.c_char_p, C.c_int32, P]
         _lib = L
     return _lib
 
@@ -517,7 +519,14 @@ class GpuPoisson:
     of a `mesh.PoissonProblem` assembled on the host, solved by conjugate
     gradients on `device`."""
 
-    def __init__(self, pp: "_mesh.PoissonProblem", device: int = 0):
+    def __init__(self, pp: "_mesh.PoissonProblem | None", device: int = 0, path: str | None = None):
+        if pp is None:  # from a .dat file (fm_poisson_read_dat)
+            h = C.c_void_p()
+            check(lib().fm_poisson_read_dat(str(path).encode(), int(device), C.byref(h)))
+            self.h = h
+            n, _ = self.info()
+            self.n_nodes, self.problem = n, None
+            return
         self._keep = [np.ascontiguousarray(a) for a in (
             pp.coords, pp.conn, pp.diffusivity, pp.source_elem, pp.source_value, pp.neumann_off, pp.neumann_nodes,
             pp.neumann_value, pp.dir_node, pp.dir_value)]
@@ -535,6 +544,14 @@ class GpuPoisson:
         it, rr, ms = C.c_int32(), C.c_double(), C.c_double()
         check(lib().fm_poisson_solve(self.h, float(rel_tol), int(max_iter), C.byref(it), C.byref(rr), C.byref(ms)))
         return int(it.value), float(rr.value), float(ms.value)
+
+    @classmethod
+    def read_dat(cls, path: str, device: int = 0, n_elems: int = 0, problem: int = FM_POISSON_CLASSIC):
+        """The solver of a .dat file's Poisson model; n_elems and problem are
+        needed only to read the DISTANCE problem's element distances."""
+        s = cls(None, device, path)
+        s.n_elems, s.problem = n_elems, problem
+        return s
 
     def solution(self):
         """(x, cell distance or None)."""

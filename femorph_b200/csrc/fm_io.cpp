@@ -65,6 +65,9 @@ int tint(const Tok* t, int n, int i) { return i < n ? (int)strtol(t[i].b, nullpt
 struct DatBlock {
   std::vector<double> coords, vel_vals, dir_vals, pres_vals;
   std::vector<int32_t> conn, vel_node, vel_dir, dir_node, pres_node;
+  // Poisson keywords (femModel.cpp:3909-3925, 3999-4011, 4185-4200)
+  std::vector<double> diff, src_val, neu_val;
+  std::vector<int32_t> src_el, neu_cnt, neu_nodes;
   int etype = 0;
   int64_t etype_line = -1;              // first ELEMENT line of a handled type (block-local)
   int64_t change_line = -1;             // first ELEMENT line whose type differs from etype
@@ -118,9 +121,22 @@ void parse_block(const char* b, const char* e, DatBlock& B) {
     } else if (tok_is(t[0], "NODEPRES")) {
       B.pres_node.push_back(tint(t, nt, 1) - 1);
       B.pres_vals.push_back(tdbl(t, nt, 2));
+    } else if (tok_is(t[0], "ELDIFF")) {
+      // rows are kept in file order whatever their element number, as the
+      // reference's reader does (femModel.cpp:3909-3925)
+      for (int c = 0; c < 3; ++c) B.diff.push_back(tdbl(t, nt, 2 + c));
+    } else if (tok_is(t[0], "ELSOURCE")) {
+      B.src_el.push_back(tint(t, nt, 1) - 1);
+      B.src_val.push_back(tdbl(t, nt, 2));
+    } else if (tok_is(t[0], "FACENEUMANN")) {
+      // element, face nodes..., value (femModel.cpp:4185-4200)
+      const int k = std::max(0, std::min(n, MT) - 3);
+      for (int i = 0; i < k; ++i) B.neu_nodes.push_back(tint(t, nt, 2 + i) - 1);
+      B.neu_cnt.push_back(k);
+      B.neu_val.push_back(n <= MT ? tdbl(t, nt, n - 1) : 0.0);
     } else if (tok_is(t[0], "NODEDOF") || tok_is(t[0], "TIMESTEP") || tok_is(t[0], "DUALSTEP") ||
                tok_is(t[0], "VMSPROPS") || tok_is(t[0], "EXOPTS") || tok_is(t[0], "EXITCOND") ||
-               tok_is(t[0], "SOLVER") || tok_is(t[0], "PRECISION")) {
+               tok_is(t[0], "SOLVER") || tok_is(t[0], "PRECISION") || tok_is(t[0], "PROBLEM")) {
       std::vector<std::string> v;
       for (int i = 0; i < nt; ++i) v.emplace_back(t[i].b, t[i].e);
       v[0] = tok_upper(t[0]);
@@ -585,4 +601,94 @@ extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
   const bool ok = ferror(f) == 0;
   fclose(f);
   return ok ? FM_OK : fail(FM_ERR_IO, std::string("cannot write ") + path);
+}
+
+// The Poisson model of a .dat file (the keywords femPoissonSolver::solve
+// reads: PROBLEM, NODE, ELEMENT, ELDIFF, ELSOURCE, FACENEUMANN, NODEDIRBC),
+// read like fm_problem_read_dat (blocks parsed on the host threads, joined
+// in file order), then assembled and uploaded by fm_poisson_create.
+extern "C" int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson** out) {
+  NvtxRange nvtx_range("fm_poisson_read_dat");
+  if (!path || !out) return fail(FM_ERR_INVALID, "null argument");
+  *out = nullptr;
+  FILE* fp = fopen(path, "rb");
+  if (!fp) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  fseek(fp, 0, SEEK_END);
+  const long size = ftell(fp);
+  fseek(fp, 0, SEEK_SET);
+  std::vector<char> buf((size_t)std::max(0L, size) + 1, '\0');
+  if (size > 0 && fread(buf.data(), 1, (size_t)size, fp) != (size_t)size) {
+    fclose(fp);
+    return fail(FM_ERR_IO, std::string("cannot read ") + path);
+  }
+  fclose(fp);
+  const char* base = buf.data();
+  const int64_t len = size;
+  const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  const int64_t nb = std::min<int64_t>(hw, std::max<int64_t>(1, len / (1 << 20)));
+  std::vector<int64_t> cut(nb + 1, 0);
+  cut[nb] = len;
+  for (int64_t k = 1; k < nb; ++k) {
+    int64_t c = std::max(cut[k - 1], len * k / nb);
+    while (c < len && base[c - 1] != '\n') ++c;
+    cut[k] = c;
+  }
+  std::vector<DatBlock> blk(nb);
+  {
+    std::vector<std::thread> th;
+    for (int64_t k = 0; k < nb; ++k)
+      th.emplace_back([&, k] { parse_block(base + cut[k], base + cut[k + 1], blk[k]); });
+    for (auto& x : th) x.join();
+  }
+  std::vector<double> coords, diff, src_val, neu_val, dir_val;
+  std::vector<int32_t> conn, src_el, neu_off(1, 0), neu_nodes, dir_node;
+  int etype = 0, problem = FM_POISSON_CLASSIC;
+  auto cat = [](auto& dst, const auto& src) { dst.insert(dst.end(), src.begin(), src.end()); };
+  for (int64_t k = 0; k < nb; ++k) {
+    const DatBlock& B = blk[k];
+    if (B.bad_line >= 0) return fail(FM_ERR_INVALID, "element type " + B.bad_type + " is not handled");
+    if (B.change_line >= 0 || (B.etype && etype && B.etype != etype))
+      return fail(FM_ERR_INVALID, "mixed element types are not supported");
+    if (B.etype) etype = B.etype;
+    cat(coords, B.coords);
+    cat(conn, B.conn);
+    cat(diff, B.diff);
+    cat(src_el, B.src_el);
+    cat(src_val, B.src_val);
+    cat(neu_val, B.neu_val);
+    cat(neu_nodes, B.neu_nodes);
+    for (int32_t c : B.neu_cnt) neu_off.push_back(neu_off.back() + c);
+    cat(dir_node, B.dir_node);
+    for (size_t i = 0; i < B.dir_node.size(); ++i) dir_val.push_back(B.dir_vals[3 * i]);
+    for (const auto& sc : B.scalars)
+      if (sc.second[0] == "PROBLEM") {
+        std::string v = sc.second.size() > 1 ? sc.second[1] : "";
+        for (auto& c : v) c = (char)std::toupper((unsigned char)c);
+        if (v == "POISSON") problem = FM_POISSON_CLASSIC;
+        else if (v == "PPE") problem = FM_POISSON_PPE;
+        else if (v == "DISTANCE") problem = FM_POISSON_DISTANCE;
+        else return fail(FM_ERR_INVALID, "PROBLEM " + v + " is not a Poisson problem");
+      }
+  }
+  const int64_t E = etype ? (int64_t)conn.size() / etype : 0;
+  if ((int64_t)diff.size() < 3 * E) return fail(FM_ERR_INVALID, "fewer ELDIFF rows than elements");
+  fm_poisson_desc d;
+  d.elem_type = etype;
+  d.problem = problem;
+  d.n_nodes = (int64_t)coords.size() / 3;
+  d.n_elems = E;
+  d.coords = coords.data();
+  d.conn = conn.data();
+  d.diffusivity = diff.data();
+  d.n_sources = (int64_t)src_el.size();
+  d.source_elem = src_el.data();
+  d.source_value = src_val.data();
+  d.n_neumann = (int64_t)neu_val.size();
+  d.neumann_off = neu_off.data();
+  d.neumann_nodes = neu_nodes.data();
+  d.neumann_value = neu_val.data();
+  d.n_dirichlet = (int64_t)dir_node.size();
+  d.dir_node = dir_node.data();
+  d.dir_value = dir_val.data();
+  return fm_poisson_create(&d, device, out);
 }

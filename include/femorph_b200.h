@@ -480,6 +480,11 @@ FM_API int fm_poisson_solve(fm_poisson* s, double rel_tol, int32_t max_iter, int
  * FM_POISSON_PPE) and, when cell_distance is non-NULL and the problem is
  * FM_POISSON_DISTANCE, the element wall distance (n_elems). */
 FM_API int fm_poisson_get_solution(fm_poisson* s, double* x, double* cell_distance);
+/* The same from a .dat file: the keywords femPoissonSolver::solve reads
+ * (PROBLEM, NODE, ELEMENT, ELDIFF, ELSOURCE, FACENEUMANN, NODEDIRBC;
+ * femModel::ReadFromFEMTextFile, femModel.cpp:3719-4213, with its token
+ * rules), parsed on the host threads. */
+FM_API int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson** out);
 /* Sizes of the assembled system: rows and stored matrix entries. */
 FM_API int fm_poisson_info(const fm_poisson* s, int64_t* rows, int64_t* nonzeros);
 

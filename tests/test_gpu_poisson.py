@@ -108,3 +108,20 @@ def test_dropin_poisson_adapter(tmp_path):
     d = out["cellDistance"][:, 0]
     ok = np.isfinite(do)
     assert rel(x, xo) <= TOL and rel(d[ok], do[ok]) <= TOL
+
+
+@pytest.mark.parametrize("elem_type,problem", [(mesh.TET4, mesh.POISSON_CLASSIC), (mesh.HEXA8, mesh.POISSON_DISTANCE)])
+def test_read_dat_equals_arrays(tmp_path, elem_type, problem):
+    """The .dat path (fm_poisson_read_dat) builds the same system as the
+    arrays: bitwise the same solution."""
+    p = mesh.poisson_box(5, elem_type=elem_type, problem=problem, seed=9)
+    dat = str(tmp_path / "p.dat")
+    mesh.write_poisson_dat(p, dat)
+    x, d, it, _ = gpu_solve(p)
+    s = api.GpuPoisson.read_dat(dat, n_elems=p.n_elems, problem=problem)
+    it2, _, _ = s.solve(1e-14, 20000)
+    x2, d2 = s.solution()
+    s.close()
+    assert it2 == it and np.array_equal(x2, x)
+    if d is not None:
+        assert np.array_equal(d2, d, equal_nan=True)

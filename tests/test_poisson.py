@@ -86,3 +86,34 @@ def test_poisson_create_rejects_bad_input_and_needs_a_device():
         with pytest.raises(api.FmError) as ei:
             api.GpuPoisson(p)
         assert ei.value.code == api.FM_ERR_NODEVICE
+
+
+def test_poisson_read_dat_input_checks(tmp_path):
+    """fm_poisson_read_dat parses the reference's keywords on the host; bad
+    files are rejected before any device is asked for."""
+    with pytest.raises(api.FmError) as ei:
+        api.GpuPoisson.read_dat(str(tmp_path / "missing.dat"))
+    assert ei.value.code == api.FM_ERR_IO
+    p = mesh.poisson_box(2)
+    good = str(tmp_path / "p.dat")
+    mesh.write_poisson_dat(p, good)
+    txt = open(good).read()
+    bad = str(tmp_path / "bad.dat")
+    open(bad, "w").write(txt.replace("PROBLEM POISSON", "PROBLEM EXPLICITVMS"))
+    with pytest.raises(api.FmError) as ei:
+        api.GpuPoisson.read_dat(bad)
+    assert ei.value.code == api.FM_ERR_INVALID
+    lines = [ln for ln in txt.splitlines() if not ln.startswith("ELDIFF 1 ")]
+    open(bad, "w").write("\n".join(lines) + "\n")
+    with pytest.raises(api.FmError) as ei:
+        api.GpuPoisson.read_dat(bad)
+    assert ei.value.code == api.FM_ERR_INVALID
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if not has_gpu:
+        with pytest.raises(api.FmError) as ei:
+            api.GpuPoisson.read_dat(good)
+        assert ei.value.code == api.FM_ERR_NODEVICE
