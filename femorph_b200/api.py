@@ -36,7 +36,7 @@ SYMBOLS = [
     "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
     "fm_batch_set_diagnostics", "fm_problem_vms_log", "fm_problem_vms_residuals",
     "fm_poisson_create", "fm_poisson_destroy", "fm_poisson_solve", "fm_poisson_get_solution", "fm_poisson_info",
-    "fm_poisson_read_dat",
+    "fm_poisson_read_dat", "fm_poisson_write_vtk",
 ]
 
 FM_POISSON_CLASSIC, FM_POISSON_PPE, FM_POISSON_DISTANCE = 0, 1, 2
@@ -152,6 +152,7 @@ def lib():
         L.fm_poisson_get_solution.argtypes = [P, P, P]
         L.fm_poisson_info.argtypes = [P, P, P]
         L.fm_poisson_read_dat.argtypes = [C.c_char_p, C.c_int32, P]
+        L.fm_poisson_write_vtk.argtypes = [P, C.c_char_p]
         _lib = L
     return _lib
 
@@ -559,6 +560,10 @@ class GpuPoisson:
         dist = np.empty(self.n_elems) if self.problem == FM_POISSON_DISTANCE else None
         check(lib().fm_poisson_get_solution(self.h, _p(x), _p(dist)))
         return x, dist
+
+    def write_vtk(self, path: str) -> None:
+        """The results in the reference exporter's legacy-VTK layout."""
+        check(lib().fm_poisson_write_vtk(self.h, str(path).encode()))
 
     def info(self):
         r, z = C.c_int64(), C.c_int64()

@@ -174,6 +174,22 @@ int resolve_bcs(fm_problem* p);
 void compute_mass(fm_problem* p);
 
 // Host-side layout of a batch (all arrays in batch numbering).
+// Host arrays of a Poisson solver that its VTK writer needs
+// (fm_poisson_write_vtk, fm_io.cpp): the model's coordinates, the fixed
+// connectivity, the diffusivity rows, and the exporter's source, Neumann and
+// Dirichlet fields.
+struct PoissonHostView {
+  int64_t N, E;
+  int npe, problem;
+  const double* coords;
+  const int32_t* conn;
+  const double* diff;
+  const double* src;
+  const double* neu;
+  const double* dir;
+};
+const PoissonHostView* poisson_host_view(const fm_poisson* s);
+
 struct Layout {
   int64_t n_nodes = 0, n_elems = 0;
   std::vector<TileMeta> tiles;

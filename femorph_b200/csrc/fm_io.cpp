@@ -692,3 +692,61 @@ extern "C" int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson*
   d.dir_value = dir_val.data();
   return fm_poisson_create(&d, device, out);
 }
+
+// femModel::ExportToVTKLegacy (femModel.cpp:1294-1530) for the Poisson
+// solver's result list (femSolver.cpp:613-648): POINTS, the connectivity the
+// solver used (after FixedElementConnectivities), DXYZ, "PoissonResult",
+// dirBC, neuBC; CELL_DATA normal (zeros: the Poisson driver builds no face
+// list), diffusivity, source and, for PROBLEM DISTANCE, "cellDistance".
+extern "C" int fm_poisson_write_vtk(fm_poisson* s, const char* path) {
+  NvtxRange nvtx_range("fm_poisson_write_vtk");
+  if (!s || !path) return fail(FM_ERR_INVALID, "null argument");
+  const PoissonHostView* v = poisson_host_view(s);
+  const int64_t N = v->N, E = v->E;
+  const int npe = v->npe;
+  std::vector<double> x(N), dist(v->problem == FM_POISSON_DISTANCE ? E : 0);
+  int r = fm_poisson_get_solution(s, x.data(), dist.empty() ? nullptr : dist.data());
+  if (r) return r;
+  FILE* f = fopen(path, "w");
+  if (!f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  const double* X = v->coords;
+  const int32_t* cn = v->conn;
+  fprintf(f, "# vtk DataFile Version 2.0\nModel Exported from feMorph\nASCII\nDATASET UNSTRUCTURED_GRID\n");
+  fprintf(f, "POINTS %d float\n", (int)N);
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e %e %e\n", X[i * 3], X[i * 3 + 1], X[i * 3 + 2]); });
+  fprintf(f, "CELLS %d %d\n", (int)E, (int)(E * (npe + 1)));
+  write_rows(f, E, [&](int64_t e, char* b) {
+    int k = snprintf(b, 256, "%d ", npe);
+    for (int a = 0; a < npe; ++a) k += snprintf(b + k, 256 - k, "%d ", cn[e * npe + a]);
+    k += snprintf(b + k, 256 - k, "\n");
+    return k;
+  });
+  fprintf(f, "CELL_TYPES %d\n", (int)E);
+  const int ctype = npe == 4 ? 10 : 12;
+  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%d\n", ctype); });
+  fprintf(f, "POINT_DATA %d\n", (int)N);
+  fprintf(f, "VECTORS DXYZ double\n");
+  write_rows(f, N, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e\n", 0.0, 0.0, 0.0); });
+  fprintf(f, "SCALARS PoissonResult double 1\nLOOKUP_TABLE default\n");
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e \n", x[i]); });
+  fprintf(f, "SCALARS dirBC double 1\nLOOKUP_TABLE default\n");
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e\n", v->dir[i]); });
+  fprintf(f, "SCALARS neuBC double\nLOOKUP_TABLE default\n");
+  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e\n", v->neu[i]); });
+  fprintf(f, "CELL_DATA %d\n", (int)E);
+  fprintf(f, "VECTORS normal double\n");
+  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e\n", 0.0, 0.0, 0.0); });
+  fprintf(f, "VECTORS diffusivity double\n");
+  write_rows(f, E, [&](int64_t e, char* b) {
+    return snprintf(b, 256, "%e %e %e\n", v->diff[e * 3], v->diff[e * 3 + 1], v->diff[e * 3 + 2]);
+  });
+  fprintf(f, "SCALARS source double 1\nLOOKUP_TABLE default\n");
+  write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e\n", v->src[e]); });
+  if (!dist.empty()) {
+    fprintf(f, "SCALARS cellDistance double 1\nLOOKUP_TABLE default\n");
+    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", dist[e]); });
+  }
+  const bool ok = ferror(f) == 0;
+  fclose(f);
+  return ok ? FM_OK : fail(FM_ERR_IO, std::string("cannot write ") + path);
+}

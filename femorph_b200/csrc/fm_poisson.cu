@@ -426,6 +426,12 @@ struct fm_poisson {
   int32_t* h_ctl = nullptr;  // pinned copy of the control words
   double* h_scal = nullptr;
   double bb = 0.0;           // |b|^2 of the whole right-hand side
+  // host copies for the VTK writer (fm_poisson_write_vtk): the model's
+  // coordinates, the fixed connectivity, the diffusivity rows and the source,
+  // Neumann and Dirichlet markers of femModel::ExportToVTKLegacy
+  fm::PoissonHostView view{};
+  std::vector<double> h_coords, h_diff, h_src, h_neu, h_dir;
+  std::vector<int32_t> h_conn;
 };
 
 #define PCK(x)                                                                                         \
@@ -666,6 +672,21 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   s->E = E;
   s->nnz = nnz;
   s->bb = bb;
+  // the exporter's fields (femModel.cpp:1400-1500): Dirichlet nodes 1,
+  // Neumann face nodes their row's value, source elements their value (a
+  // later row wins in each)
+  s->h_coords.assign(d->coords, d->coords + N * 3);
+  s->h_conn = cfix;
+  s->h_diff.assign(d->diffusivity, d->diffusivity + E * 3);
+  s->h_src.assign(E, 0.0);
+  for (int64_t k = 0; k < d->n_sources; ++k) s->h_src[d->source_elem[k]] = d->source_value[k];
+  s->h_neu.assign(N, 0.0);
+  for (int64_t k = 0; k < d->n_neumann; ++k)
+    for (int32_t j = d->neumann_off[k]; j < d->neumann_off[k + 1]; ++j) s->h_neu[d->neumann_nodes[j]] = d->neumann_value[k];
+  s->h_dir.assign(N, 0.0);
+  for (int64_t k = 0; k < d->n_dirichlet; ++k) s->h_dir[d->dir_node[k]] = 1.0;
+  s->view = fm::PoissonHostView{N, E, npe, d->problem, s->h_coords.data(), s->h_conn.data(), s->h_diff.data(),
+                                s->h_src.data(), s->h_neu.data(), s->h_dir.data()};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   s->blocks = (int)std::max<int64_t>(1, std::min<int64_t>((N + kThreads - 1) / kThreads, (int64_t)sms * 8));
@@ -831,3 +852,7 @@ FM_API int fm_poisson_get_solution(fm_poisson* s, double* x, double* cell_distan
 }
 
 }  // extern "C"
+
+namespace fm {
+const PoissonHostView* poisson_host_view(const fm_poisson* s) { return s ? &s->view : nullptr; }
+}  // namespace fm

@@ -485,6 +485,12 @@ FM_API int fm_poisson_get_solution(fm_poisson* s, double* x, double* cell_distan
  * femModel::ReadFromFEMTextFile, femModel.cpp:3719-4213, with its token
  * rules), parsed on the host threads. */
 FM_API int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson** out);
+/* The results in femModel::ExportToVTKLegacy's legacy-VTK layout
+ * (femModel.cpp:1294-1530) as the reference's Poisson driver writes them
+ * (src/main.cpp:508-511): mesh with the connectivity the solver used,
+ * "PoissonResult", dirBC, neuBC, diffusivity, source and, for
+ * FM_POISSON_DISTANCE, "cellDistance".  After fm_poisson_solve. */
+FM_API int fm_poisson_write_vtk(fm_poisson* s, const char* path);
 /* Sizes of the assembled system: rows and stored matrix entries. */
 FM_API int fm_poisson_info(const fm_poisson* s, int64_t* rows, int64_t* nonzeros);
 

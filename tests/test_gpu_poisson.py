@@ -125,3 +125,31 @@ def test_read_dat_equals_arrays(tmp_path, elem_type, problem):
     assert it2 == it and np.array_equal(x2, x)
     if d is not None:
         assert np.array_equal(d2, d, equal_nan=True)
+
+
+@pytest.mark.parametrize("problem", [mesh.POISSON_CLASSIC, mesh.POISSON_DISTANCE])
+def test_vtk_writer_matches_reference_exporter(tmp_path, problem):
+    """fm_poisson_write_vtk against the reference's own exporter
+    (femModel::ExportToVTKLegacy) run on the same solution: the adapter
+    behind the reference's reader (oracle/_ref/fm_gpudrv poisson-gpu --vtk)
+    and the library from the same .dat file at the same tolerance give the
+    same bytes."""
+    import os
+    import subprocess
+
+    from oracle import ref
+    gpudrv = os.path.join(os.path.dirname(ref.REFDRV), "fm_gpudrv")
+    if not os.path.exists(gpudrv):
+        pytest.skip("oracle/_ref/fm_gpudrv not built")
+    p = mesh.poisson_box(4, problem=problem, seed=12)
+    dat = str(tmp_path / "p.dat")
+    mesh.write_poisson_dat(p, dat)
+    r = subprocess.run([gpudrv, dat, "poisson-gpu", "--dump", str(tmp_path), "--vtk"], cwd=str(tmp_path),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    s = api.GpuPoisson.read_dat(dat, n_elems=p.n_elems, problem=problem)
+    s.solve(1e-14, 100000)
+    mine = str(tmp_path / "mine.vtk")
+    s.write_vtk(mine)
+    s.close()
+    assert open(mine).read() == open(str(tmp_path / "poisson")).read()
