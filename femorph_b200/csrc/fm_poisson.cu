@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "fm_internal.hpp"
@@ -100,22 +101,40 @@ __host__ __device__ inline void shape_derivs(int npe, const double q[3], double 
     }
   }
 }
-// Jacobian J[a][b] = sum_n dN[n][a] x[n][b] (femElement.cpp:104-127), its
-// cofactor inverse and determinant (femUtils.cpp:716-770), global
-// derivatives gd[n][b] = sum_c inv[b][c] dN[n][c] (femElement.cpp:345-352).
-__host__ __device__ inline double global_derivs(int npe, const double xe[8][3], const double q[3], double gd[8][3]) {
-  double dN[8][3], J[3][3];
-  shape_derivs(npe, q, dN);
+// Jacobian J[a][b] = sum_n dN[n][a] x[n][b] (femElement.cpp:104-127) from
+// the local derivatives dN at the point.
+__host__ __device__ inline void jacobian(int npe, const double xe[8][3], const double dN[8][3], double J[3][3]) {
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
       double t = 0.0;
       for (int n = 0; n < npe; ++n) t += dN[n][a] * xe[n][b];
       J[a][b] = t;
     }
+}
+// Its determinant by the cofactors of the first row (femUtils.cpp:729-731).
+__host__ __device__ inline double det3(const double J[3][3]) {
   const double c00 = J[1][1] * J[2][2] - J[2][1] * J[1][2];
   const double c01 = J[1][0] * J[2][2] - J[1][2] * J[2][0];
   const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-  const double det = J[0][0] * c00 - J[0][1] * c01 + J[0][2] * c02;
+  return J[0][0] * c00 - J[0][1] * c01 + J[0][2] * c02;
+}
+// detJ at local point q alone (femElement::evalJacobian, femElement.cpp:149-186).
+__host__ __device__ inline double jacobian_det(int npe, const double xe[8][3], const double q[3]) {
+  double dN[8][3], J[3][3];
+  shape_derivs(npe, q, dN);
+  jacobian(npe, xe, dN, J);
+  return det3(J);
+}
+// The Jacobian, its cofactor inverse and determinant (femUtils.cpp:716-770),
+// global derivatives gd[n][b] = sum_c inv[b][c] dN[n][c] (femElement.cpp:
+// 345-352).
+__host__ __device__ inline double global_derivs(int npe, const double xe[8][3], const double q[3], double gd[8][3]) {
+  double dN[8][3], J[3][3];
+  shape_derivs(npe, q, dN);
+  jacobian(npe, xe, dN, J);
+  const double c00 = J[1][1] * J[2][2] - J[2][1] * J[1][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = det3(J);
   const double id = 1.0 / det;
   double inv[3][3];
   inv[0][0] = c00 * id;
@@ -137,27 +156,36 @@ __host__ __device__ inline double global_derivs(int npe, const double xe[8][3], 
 }
 
 // Element matrix of femElement::formPoissonMatrix (femElement.cpp:903-944).
+// A tet4's local derivatives do not depend on the point, so its derivatives,
+// determinant and products are the same at every Gauss point: they are
+// formed once and added once a point, which gives the reference loop's sums.
 void element_matrix(int npe, const Rule& r, const double xe[8][3], const double diff[3], double K[8][8]) {
   for (int a = 0; a < npe; ++a)
     for (int b = 0; b < npe; ++b) K[a][b] = 0.0;
+  double gd[8][3], detJ = 0.0, S[8][8];
   for (int g = 0; g < r.ngp; ++g) {
-    double gd[8][3];
-    const double detJ = global_derivs(npe, xe, r.q[g], gd);
+    if (g == 0 || npe == 8) {
+      detJ = global_derivs(npe, xe, r.q[g], gd);
+      for (int a = 0; a < npe; ++a)
+        for (int b = 0; b < npe; ++b) {
+          double s = 0.0;
+          for (int d = 0; d < 3; ++d) s += diff[d] * gd[a][d] * gd[b][d];
+          S[a][b] = s;
+        }
+    }
     for (int a = 0; a < npe; ++a)
-      for (int b = 0; b < npe; ++b) {
-        double s = 0.0;
-        for (int d = 0; d < 3; ++d) s += diff[d] * gd[a][d] * gd[b][d];
-        K[a][b] += s * detJ * r.w[g];
-      }
+      for (int b = 0; b < npe; ++b) K[a][b] += S[a][b] * detJ * r.w[g];
   }
 }
-// Element source of femElement::formPoissonSource (femElement.cpp:949-981).
+// Element source of femElement::formPoissonSource (femElement.cpp:949-981)
+// (a tet4's determinant formed once, as above).
 void element_source(int npe, const Rule& r, const double xe[8][3], double value, double f[8]) {
   for (int a = 0; a < npe; ++a) f[a] = 0.0;
+  double detJ = 0.0;
   for (int g = 0; g < r.ngp; ++g) {
-    double N[8], gd[8][3];
+    double N[8];
     shape_values(npe, r.q[g], N);
-    const double detJ = global_derivs(npe, xe, r.q[g], gd);
+    if (g == 0 || npe == 8) detJ = jacobian_det(npe, xe, r.q[g]);
     for (int a = 0; a < npe; ++a) f[a] += N[a] * value * detJ * r.w[g];
   }
 }
@@ -492,10 +520,11 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   std::vector<int32_t> cfix(d->conn, d->conn + E * npe);
   fm::parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
     for (int64_t e = eb; e < ee; ++e) {
-      double xe[8][3], gd[8][3], mn = 1e308;
+      double xe[8][3], mn = 1e308;
       for (int a = 0; a < npe; ++a)
         for (int k = 0; k < 3; ++k) xe[a][k] = d->coords[3 * (int64_t)cfix[e * npe + a] + k];
-      for (int g = 0; g < rule.ngp; ++g) mn = std::min(mn, global_derivs(npe, xe, rule.q[g], gd));
+      // a tet4's Jacobian is the same at every point
+      for (int g = 0; g < (npe == 4 ? 1 : rule.ngp); ++g) mn = std::min(mn, jacobian_det(npe, xe, rule.q[g]));
       if (mn <= 0.0) {
         int32_t* c = &cfix[e * npe];
         if (npe == 4) {
@@ -536,13 +565,22 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   // right-hand side: sources in row order, then the Neumann vector (its own
   // sums in row order) added node by node (femSolver.cpp:478-558)
   std::vector<double> rhs(N, 0.0);
-  for (int64_t k = 0; k < d->n_sources; ++k) {
-    const int64_t e = d->source_elem[k];
-    double xe[8][3], f[8];
-    for (int a = 0; a < npe; ++a)
-      for (int q = 0; q < 3; ++q) xe[a][q] = d->coords[3 * (int64_t)conn[e * npe + a] + q];
-    element_source(npe, rule, xe, d->source_value[k], f);
-    for (int a = 0; a < npe; ++a) rhs[conn[e * npe + a]] += f[a];
+  {
+    // element vectors in parallel, added in row order
+    fm::hvec<double> fs((size_t)d->n_sources * npe);
+    fm::parallel_blocks(d->n_sources, [&](int64_t kb, int64_t ke, int) {
+      for (int64_t k = kb; k < ke; ++k) {
+        const int64_t e = d->source_elem[k];
+        double xe[8][3];
+        for (int a = 0; a < npe; ++a)
+          for (int q = 0; q < 3; ++q) xe[a][q] = d->coords[3 * (int64_t)conn[e * npe + a] + q];
+        element_source(npe, rule, xe, d->source_value[k], &fs[(size_t)k * npe]);
+      }
+    }, 4096);
+    for (int64_t k = 0; k < d->n_sources; ++k) {
+      const int64_t e = d->source_elem[k];
+      for (int a = 0; a < npe; ++a) rhs[conn[e * npe + a]] += fs[(size_t)k * npe + a];
+    }
   }
   {
     std::vector<double> nv(N, 0.0);
@@ -556,43 +594,25 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   // in element order; Dirichlet rows become identity rows with the value on
   // the right-hand side, and their columns move to the right-hand side of
   // the other rows (same solution, symmetric matrix)
+  // One pass over contiguous row blocks on the host threads: each block
+  // forms its rows' sorted columns and summed values into its own arrays,
+  // which are then placed at the block's offset.
   std::vector<int32_t> rowp(N + 1, 0);
   fm::hvec<int32_t> rowlen(N);
-  fm::parallel_blocks(N, [&](int64_t vb, int64_t ve, int) {
-    std::vector<int32_t> cl;
-    for (int64_t v = vb; v < ve; ++v) {
-      if (dir_of[v] >= 0) {
-        rowlen[v] = 1;
-        continue;
-      }
-      cl.clear();
-      for (int32_t k = ioff[v]; k < ioff[v + 1]; ++k) {
-        const int64_t e = inc[k] / npe;
-        for (int b = 0; b < npe; ++b) {
-          const int32_t w = conn[e * npe + b];
-          if (dir_of[w] < 0) cl.push_back(w);
-        }
-      }
-      std::sort(cl.begin(), cl.end());
-      rowlen[v] = std::max<int32_t>(1, (int32_t)(std::unique(cl.begin(), cl.end()) - cl.begin()));
-    }
-  }, 4096);
-  int64_t nnz = 0;
-  for (int64_t v = 0; v < N; ++v) {
-    nnz += rowlen[v];
-    if (nnz >= INT32_MAX) return fail(FM_ERR_INVALID, "matrix too large for 32-bit row offsets");
-    rowp[v + 1] = (int32_t)nnz;
-  }
-  fm::hvec<int32_t> col(nnz);
-  fm::hvec<double> val(nnz);
   std::vector<double> bvec(N), dinv(N);
-  fm::parallel_blocks(N, [&](int64_t vb, int64_t ve, int) {
+  const int64_t hwt = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
+  const int64_t nblk = std::min<int64_t>(hwt, std::max<int64_t>(1, N / 2048));
+  std::vector<std::vector<int32_t>> bcol(nblk);
+  std::vector<std::vector<double>> bval(nblk);
+  auto rows = [&](int64_t kb) {
+    std::vector<int32_t>& lc = bcol[kb];
+    std::vector<double>& lv = bval[kb];
     std::vector<int32_t> cl;
-    for (int64_t v = vb; v < ve; ++v) {
-      const int32_t r0 = rowp[v];
+    for (int64_t v = N * kb / nblk; v < N * (kb + 1) / nblk; ++v) {
       if (dir_of[v] >= 0) {
-        col[r0] = (int32_t)v;
-        val[r0] = 1.0;
+        lc.push_back((int32_t)v);
+        lv.push_back(1.0);
+        rowlen[v] = 1;
         bvec[v] = d->dir_value[dir_of[v]];
         dinv[v] = 1.0;
         continue;
@@ -608,16 +628,16 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
       std::sort(cl.begin(), cl.end());
       cl.erase(std::unique(cl.begin(), cl.end()), cl.end());
       if (cl.empty()) {  // a node of no element (and not Dirichlet): identity row, value 0
-        col[r0] = (int32_t)v;
-        val[r0] = 1.0;
+        lc.push_back((int32_t)v);
+        lv.push_back(1.0);
+        rowlen[v] = 1;
         bvec[v] = 0.0;
         dinv[v] = 1.0;
         continue;
       }
-      for (size_t j = 0; j < cl.size(); ++j) {
-        col[r0 + j] = cl[j];
-        val[r0 + j] = 0.0;
-      }
+      const size_t r0 = lv.size();
+      lc.insert(lc.end(), cl.begin(), cl.end());
+      lv.resize(r0 + cl.size(), 0.0);
       double bv = rhs[v], diag = 0.0;
       for (int32_t k = ioff[v]; k < ioff[v + 1]; ++k) {
         const int64_t e = inc[k] / npe;
@@ -628,17 +648,43 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
           if (dir_of[w] >= 0) {
             bv -= kv * d->dir_value[dir_of[w]];
           } else {
-            const int32_t j = (int32_t)(std::lower_bound(cl.begin(), cl.end(), w) - cl.begin());
-            val[r0 + j] += kv;
+            const size_t j = (size_t)(std::lower_bound(cl.begin(), cl.end(), w) - cl.begin());
+            lv[r0 + j] += kv;
           }
         }
       }
       for (size_t j = 0; j < cl.size(); ++j)
-        if (cl[j] == v) diag = val[r0 + j];
+        if (cl[j] == v) diag = lv[r0 + j];
+      rowlen[v] = (int32_t)cl.size();
       bvec[v] = bv;
       dinv[v] = diag != 0.0 ? 1.0 / diag : 1.0;
     }
-  }, 2048);
+  };
+  {
+    std::vector<std::thread> th;
+    for (int64_t kb = 0; kb < nblk; ++kb) th.emplace_back(rows, kb);
+    for (auto& x : th) x.join();
+  }
+  int64_t nnz = 0;
+  for (int64_t v = 0; v < N; ++v) {
+    nnz += rowlen[v];
+    if (nnz >= INT32_MAX) return fail(FM_ERR_INVALID, "matrix too large for 32-bit row offsets");
+    rowp[v + 1] = (int32_t)nnz;
+  }
+  fm::hvec<int32_t> col(nnz);
+  fm::hvec<double> val(nnz);
+  {
+    std::vector<std::thread> th;
+    for (int64_t kb = 0; kb < nblk; ++kb)
+      th.emplace_back([&, kb] {
+        const int64_t r0 = rowp[N * kb / nblk];
+        std::copy(bcol[kb].begin(), bcol[kb].end(), col.begin() + r0);
+        std::copy(bval[kb].begin(), bval[kb].end(), val.begin() + r0);
+        std::vector<int32_t>().swap(bcol[kb]);
+        std::vector<double>().swap(bval[kb]);
+      });
+    for (auto& x : th) x.join();
+  }
   // no Dirichlet row: K is singular (constants), so the right-hand side is
   // projected onto its range (zero sum) to make the system consistent
   if (d->n_dirichlet == 0) {
