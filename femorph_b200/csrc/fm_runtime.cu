@@ -518,7 +518,7 @@ static void diag_free(fm_batch* b) {
 }
 
 // The problem's reference-order incidence lists and output array.
-static int diag_prepare_problem(fm_batch* b, Placement& pl) {
+static int diag_prepare_problem(Placement& pl) {
   const fm_problem* p = pl.p;
   const Layout& L = *pl.L;
   const auto& eo = L.elem_old[0];
@@ -807,7 +807,7 @@ static int place(fm_batch* b, fm_problem* p, const std::shared_ptr<Layout>& Lp) 
   b->slots[ps] = std::move(pl);
   refresh_extent(b);
   if (b->diag) {
-    r = diag_prepare_problem(b, b->slots[ps]);
+    r = diag_prepare_problem(b->slots[ps]);
     if (r) return r;
   }
   r = configure(b);
@@ -2030,7 +2030,7 @@ int fm_batch_set_diagnostics(fm_batch* b, int32_t enable) {
   b->diag = true;
   for (Placement& pl : b->slots)
     if (pl.p) {
-      int r = diag_prepare_problem(b, pl);
+      int r = diag_prepare_problem(pl);
       if (r) {
         diag_free(b);
         return r;
