@@ -36,7 +36,7 @@ SYMBOLS = [
     "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
     "fm_batch_set_diagnostics", "fm_problem_vms_log", "fm_problem_vms_residuals",
     "fm_poisson_create", "fm_poisson_destroy", "fm_poisson_solve", "fm_poisson_get_solution", "fm_poisson_info",
-    "fm_poisson_read_dat", "fm_poisson_write_vtk",
+    "fm_poisson_read_dat", "fm_poisson_write_vtk", "fm_problem_check_layout",
 ]
 
 FM_POISSON_CLASSIC, FM_POISSON_PPE, FM_POISSON_DISTANCE = 0, 1, 2
@@ -152,6 +152,7 @@ def lib():
         L.fm_poisson_get_solution.argtypes = [P, P, P]
         L.fm_poisson_info.argtypes = [P, P, P]
         L.fm_poisson_read_dat.argtypes = [C.c_char_p, C.c_int32, P]
+        L.fm_problem_check_layout.argtypes = [P, P]
         L.fm_poisson_write_vtk.argtypes = [P, C.c_char_p]
         _lib = L
     return _lib
@@ -268,6 +269,12 @@ class GpuProblem:
         """Loads a restart file of this mesh and configuration into the
         problem (it must sit in a batch); stepping on continues that solve."""
         check(lib().fm_problem_restore(self.h, path.encode()))
+
+    def check_layout(self, tile_elems=0, tile_nodes=0, threads=0) -> None:
+        """Builds the tile layout for these sizes and checks its invariants
+        (host only); raises FmError naming the first broken one."""
+        t = FmTuning(tile_elems, tile_nodes, threads, 0, 0)
+        check(lib().fm_problem_check_layout(self.h, C.byref(t)))
 
     def prepare(self, tile_elems=0, tile_nodes=0, threads=0) -> None:
         """Builds the tile layout now (host only, thread-safe per problem)."""

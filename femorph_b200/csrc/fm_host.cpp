@@ -889,3 +889,112 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
 }
 
 }  // namespace fm
+
+namespace fm {
+
+// Checks the invariants the tile kernels rely on in one problem's layout
+// (one problem, built by build_layout): local connectivity inside the tile's
+// node list; distinct nodes in a tile, interior ones touched by this tile
+// only; elements of one colour sharing no node (the hexa8 colour rounds add
+// without ordering); every (element, corner) once in its node's incidence
+// list, in element order; each interface node's partial slots, one per
+// touching tile, in tile order; every element and node of the problem once.
+int check_layout(const fm_problem* p, const Layout& L) {
+  auto bad = [](const std::string& m) { return fail(FM_ERR_INVALID, "layout check: " + m); };
+  const int npe = p->etype;
+  const int64_t N = p->N, E = p->E;
+  const std::vector<int32_t>& nn = L.node_new[0];
+  if ((int64_t)nn.size() != N) return bad("node map size");
+  std::vector<int32_t> seen_node(N, 0), tiles_of(N, 0);
+  {
+    std::vector<char> used((size_t)N, 0);
+    for (int64_t v = 0; v < N; ++v) {
+      if (nn[v] < 0 || nn[v] >= N || used[nn[v]]) return bad("node renumbering is not a permutation");
+      used[nn[v]] = 1;
+    }
+  }
+  std::vector<int32_t> old_of(N);
+  for (int64_t v = 0; v < N; ++v) old_of[nn[v]] = (int32_t)v;
+  std::vector<char> elem_seen((size_t)E, 0);
+  std::vector<int32_t> stamp(N, -1), colour_stamp;
+  // slot -> (tile, interface node batch id)
+  std::vector<int32_t> slot_node((size_t)L.n_slots, -1), slot_tile((size_t)L.n_slots, -1);
+  for (size_t t = 0; t < L.tiles.size(); ++t) {
+    const TileMeta& tm = L.tiles[t];
+    const int32_t ne = tm.n_elem, nl = tm.n_node;
+    if (tm.n_int < 0 || tm.n_int > nl) return bad("tile " + std::to_string(t) + ": interior count");
+    const int32_t* tn = &L.tile_nodes[tm.node_begin];
+    for (int32_t l = 0; l < nl; ++l) {
+      const int32_t g = tn[l];
+      if (g < 0 || g >= N) return bad("tile " + std::to_string(t) + ": node id out of range");
+      if (stamp[g] == (int32_t)t) return bad("tile " + std::to_string(t) + ": node listed twice");
+      stamp[g] = (int32_t)t;
+      tiles_of[g]++;
+      if (l < tm.n_int) seen_node[g]++;
+      else {
+        const int64_t s = (int64_t)tm.slot_base + (l - tm.n_int);
+        if (s < 0 || s >= L.n_slots || slot_node[s] >= 0) return bad("tile " + std::to_string(t) + ": slot");
+        slot_node[s] = g;
+        slot_tile[s] = (int32_t)t;
+      }
+    }
+    // local connectivity (bit 15 of the first id flags an FP64-Jacobian
+    // element in the mixed form)
+    const uint16_t* cl = &L.conn_local[(size_t)tm.elem_begin * npe];
+    for (int32_t i = 0; i < ne; ++i) {
+      const int64_t oe = L.elem_old[0][tm.elem_begin + i];
+      if (oe < 0 || oe >= E || elem_seen[oe]) return bad("tile " + std::to_string(t) + ": element map");
+      elem_seen[oe] = 1;
+      for (int a = 0; a < npe; ++a) {
+        const int32_t ln = a == 0 ? (cl[i * npe] & 0x7fff) : cl[i * npe + a];
+        if (ln >= nl) return bad("tile " + std::to_string(t) + ": local node id out of range");
+        if (old_of[tn[ln]] != p->conn[oe * npe + a]) return bad("tile " + std::to_string(t) + ": connectivity");
+      }
+    }
+    // colours
+    const int32_t* co = &L.tile_cols[tm.col_begin];
+    if (co[0] != 0 || co[tm.n_col] != ne) return bad("tile " + std::to_string(t) + ": colour offsets");
+    colour_stamp.assign(nl, -1);
+    for (int32_t c = 0; c < tm.n_col; ++c)
+      for (int32_t i = co[c]; i < co[c + 1]; ++i)
+        for (int a = 0; a < npe; ++a) {
+          const int32_t ln = a == 0 ? (cl[i * npe] & 0x7fff) : cl[i * npe + a];
+          if (colour_stamp[ln] == c) return bad("tile " + std::to_string(t) + ": two elements of a colour share a node");
+          colour_stamp[ln] = c;
+        }
+    // incidence lists
+    const uint16_t* off = &L.tile_off[tm.off_begin];
+    const uint16_t* inc = &L.tile_inc[tm.inc_begin];
+    if (off[0] != 0 || off[nl] != ne * npe) return bad("tile " + std::to_string(t) + ": incidence offsets");
+    for (int32_t l = 0; l < nl; ++l)
+      for (int32_t k = off[l]; k < off[l + 1]; ++k) {
+        const int32_t el = inc[k] / npe, a = inc[k] % npe;
+        if (el >= ne) return bad("tile " + std::to_string(t) + ": incidence element");
+        const int32_t ln = a == 0 ? (cl[el * npe] & 0x7fff) : cl[el * npe + a];
+        if (ln != l) return bad("tile " + std::to_string(t) + ": incidence entry of another node");
+        if (k > off[l] && inc[k - 1] / npe >= el) return bad("tile " + std::to_string(t) + ": incidence order");
+      }
+  }
+  for (int64_t e = 0; e < E; ++e)
+    if (!elem_seen[e]) return bad("element " + std::to_string(e) + " in no tile");
+  for (int64_t g = 0; g < N; ++g) {
+    if (seen_node[g] > 1) return bad("node interior to two tiles");
+    if (seen_node[g] == 1 && tiles_of[g] != 1) return bad("interior node touched by another tile");
+  }
+  // interface lists: node i's slots name the node, one a touching tile, in
+  // tile order, and the slot map of the tiles is a permutation
+  const int64_t NI = (int64_t)L.iface_node.size();
+  for (int64_t i = 0; i < NI; ++i) {
+    const int32_t g = L.iface_node[i];
+    const int32_t k0 = L.iface_slot_beg[i], k1 = L.iface_slot_beg[i + 1];
+    if (k1 - k0 != tiles_of[g] && tiles_of[g] > 0) return bad("interface node slot count");
+    for (int32_t k = k0; k < k1; ++k) {
+      const int32_t s = L.iface_slots[k];
+      if (s < 0 || s >= L.n_slots || slot_node[s] != g) return bad("interface slot of another node");
+      if (k > k0 && slot_tile[L.iface_slots[k - 1]] >= slot_tile[s]) return bad("interface slots not in tile order");
+    }
+  }
+  return FM_OK;
+}
+
+}  // namespace fm

@@ -222,5 +222,6 @@ constexpr int FM_GEO_PER_GP = 10;
 #define FM_MAX_TILE_NODES 512
 
 int build_layout(fm_problem* const* probs, int n, int tile_elems, int tile_nodes, Layout& L);
+int check_layout(const fm_problem* p, const Layout& L);
 void morton_order(const fm_problem* p, hvec<int64_t>& order);
 }  // namespace fm

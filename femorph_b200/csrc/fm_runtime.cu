@@ -987,6 +987,20 @@ int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning) {
   return prepare(p, t.tile_elems, t.tile_nodes, &L);
 }
 
+int fm_problem_check_layout(fm_problem* p, const fm_tuning* tuning) {
+  NvtxRange nvtx_range("fm_problem_check_layout");
+  if (!p) return fail(FM_ERR_INVALID, "null problem");
+  if (p->part >= 0) return fail(FM_ERR_INVALID, "fm_problem_check_layout checks whole problems, not partition parts");
+  fm_tuning t;
+  memset(&t, 0, sizeof(t));
+  if (tuning) t = *tuning;
+  default_tuning(p->params.solver, p->etype, p->params.precision, t);
+  std::shared_ptr<Layout> L;
+  int r = prepare(p, t.tile_elems, t.tile_nodes, &L);
+  if (r) return r;
+  return check_layout(p, *L);
+}
+
 int fm_batch_estimate_bytes(fm_problem* const* probs, int32_t n, const fm_tuning* tuning, int64_t* bytes) {
   if (!probs || n <= 0 || !bytes) return fail(FM_ERR_INVALID, "null argument");
   int64_t N = 0, E = 0;

@@ -178,6 +178,15 @@ FM_API int fm_batch_create_empty(const fm_capacity* cap, const fm_tuning* tuning
 FM_API int fm_batch_add(fm_batch* b, fm_problem* p);
 FM_API int fm_batch_remove(fm_batch* b, fm_problem* p);
 FM_API int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning);
+/* Builds (or reuses) the problem's tile layout for these tile sizes and
+ * checks the invariants the tile kernels rely on: local connectivity inside
+ * each tile's node list, interior nodes touched by one tile only, no two
+ * elements of a colour sharing a node, each (element, corner) once in its
+ * node's incidence list in element order, one partial slot per (tile,
+ * interface node) listed in tile order, every element and node once.
+ * FM_ERR_INVALID names the first broken one.  Host only.  No counterpart in
+ * the reference (its element loop neither tiles nor colours). */
+FM_API int fm_problem_check_layout(fm_problem* p, const fm_tuning* tuning);
 /* Device bytes fm_batch_create_empty allocates for these capacities (HBM
  * budgeting). */
 FM_API int fm_batch_capacity_bytes(const fm_capacity* cap, const fm_tuning* tuning, int64_t* bytes);
