@@ -19,7 +19,7 @@
 //
 // Usage: fm_refdrv model.dat vms|supg [--ic f64file ncomp] [--dump dir]
 //                  [--vtk] [--timing file]
-//        fm_refdrv model.dat poisson-elements --dump dir
+//        fm_refdrv model.dat poisson-elements --dump dir [--sol f64file]
 //        fm_gpudrv model.dat poisson-gpu --dump dir   (drop-in check build)
 // The second form reads a Poisson model (src/main.cpp:476-490:
 // ReadFromFEMTextFile, FixedElementConnectivities) and writes the reference's
@@ -27,7 +27,9 @@
 // femElement::formPoissonMatrix for every element (src/femSolver.cpp:
 // 446-459), then the element vector of femElement::formPoissonSource for
 // every ELSOURCE row (src/femSolver.cpp:478-494), irSecondOrder rule, as raw
-// FP64 in dir/poisson_elements.f64.  (The reference solves the system only
+// FP64 in dir/poisson_elements.f64, followed, with --sol, by the wall
+// distance evalDistanceFromPoissonSolution (src/femSolver.cpp:367-403)
+// computes from that nodal solution.  (The reference solves the system only
 // through Trilinos, src/femSolver.cpp:590-600.)
 #include <chrono>
 #include <cstdio>
@@ -39,6 +41,7 @@
 
 #include "femIntegrationRule.h"
 #include "femModel.h"
+#include "femVector.h"
 #include "femSUPGExplicitFluidSolver.h"
 #include "femVMSExplicitFluidSolver.h"
 #ifdef FM_WITH_GPU_ADAPTER
@@ -54,7 +57,11 @@ void real_setvel(femModel*, double, femDoubleMat&) __asm__("__real_" FM_SETVEL_S
 void wrap_export(femModel*, std::string, bool) __asm__("__wrap_" FM_EXPORT_SYM);
 void wrap_setvel(femModel*, double, femDoubleMat&) __asm__("__wrap_" FM_SETVEL_SYM);
 
+// defined at file scope in src/femSolver.cpp:367-403 (no header declares it)
+void evalDistanceFromPoissonSolution(femVector* femSolution, femModel* model, femDoubleVec& cellDistance);
+
 static std::vector<double> g_ic;
+static std::vector<double> g_sol;
 static int g_ic_ncomp = 0;
 static bool g_ic_done = false;
 static bool g_dump = false;
@@ -144,6 +151,16 @@ int main(int argc, char** argv) {
     } else if (!strcmp(argv[i], "--dump") && i + 1 < argc) {
       g_dump = true;
       g_dump_dir = argv[++i];
+    } else if (!strcmp(argv[i], "--sol") && i + 1 < argc) {
+      FILE* f = fopen(argv[i + 1], "rb");
+      if (!f) { perror(argv[i + 1]); return 2; }
+      fseek(f, 0, SEEK_END);
+      long sz = ftell(f);
+      fseek(f, 0, SEEK_SET);
+      g_sol.resize(sz / sizeof(double));
+      if (fread(g_sol.data(), sizeof(double), g_sol.size(), f) != g_sol.size()) { fclose(f); return 2; }
+      fclose(f);
+      ++i;
     } else if (!strcmp(argv[i], "--vtk")) {
       g_vtk = true;
     } else if (!strcmp(argv[i], "--timing") && i + 1 < argc) {
@@ -184,6 +201,14 @@ int main(int argc, char** argv) {
         femElement* el = model->elementList[model->sourceElement[k]];
         el->formPoissonSource(model->nodeList, rule, model->sourceValues[k], elSrc);
         fwrite(elSrc.data(), sizeof(double), el->elementConnections.size(), f);
+      }
+      // with --sol: the reference's wall distance of that nodal solution
+      if (!g_sol.empty()) {
+        femDenseVector sol((int)g_sol.size());
+        for (size_t i = 0; i < g_sol.size(); ++i) sol.setComponent((int)i, g_sol[i]);
+        femDoubleVec dist;
+        evalDistanceFromPoissonSolution(&sol, model, dist);
+        fwrite(dist.data(), sizeof(double), dist.size(), f);
       }
       fclose(f);
       return 0;

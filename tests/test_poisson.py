@@ -117,3 +117,24 @@ def test_poisson_read_dat_input_checks(tmp_path):
         with pytest.raises(api.FmError) as ei:
             api.GpuPoisson.read_dat(good)
         assert ei.value.code == api.FM_ERR_NODEVICE
+
+
+@pytest.mark.skipif(not os.path.exists(REFDRV), reason="oracle A (compiled reference) not built")
+@pytest.mark.parametrize("elem_type", [mesh.TET4, mesh.HEXA8])
+def test_wall_distance_bitwise_against_reference(tmp_path, elem_type):
+    """evalDistanceFromPoissonSolution of the reference and the oracle's
+    restatement on the same nodal solution: bit for bit."""
+    p = mesh.poisson_box(4, elem_type=elem_type, problem=mesh.POISSON_DISTANCE, seed=13)
+    dat = str(tmp_path / "p.dat")
+    mesh.write_poisson_dat(p, dat)
+    x, d = oracle_b.poisson_solve(p)
+    sol = str(tmp_path / "sol.f64")
+    x.astype(np.float64).tofile(sol)
+    subprocess.run([REFDRV, dat, "poisson-elements", "--dump", str(tmp_path), "--sol", sol], check=True,
+                   capture_output=True)
+    raw = np.fromfile(str(tmp_path / "poisson_elements.f64"))
+    E, npe = p.conn.shape
+    skip = E * npe * npe + p.source_elem.size * npe
+    da = raw[skip:]
+    assert da.size == E
+    assert np.array_equal(da, d, equal_nan=True)
