@@ -5,6 +5,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <thread>
 
@@ -446,38 +447,51 @@ void morton_order(const fm_problem* p, hvec<int64_t>& order) {
 //   w_int / w_ifc: incident elements of the interior / interface nodes (in
 //   their current order); ifc: the interface nodes, reordered in place.
 constexpr int FM_OWNER_THREADS = 128;
+struct BalanceScratch {
+  std::vector<int32_t> by_w, count, out;
+  std::vector<uint64_t> heap;
+};
 static void balance_owners(const std::vector<int32_t>& w_int, const std::vector<int32_t>& w_ifc,
-                           std::vector<int32_t>& ifc, std::vector<int32_t>& scratch) {
+                           std::vector<int32_t>& ifc, BalanceScratch& sc) {
   const int n_int = (int)w_int.size(), n_ifc = (int)w_ifc.size(), n_node = n_int + n_ifc;
   constexpr int64_t kNodeCost = 2;  // accumulator load / store and walk set-up, in entry units
   int64_t load[FM_OWNER_THREADS] = {};
   int next[FM_OWNER_THREADS];
   for (int q = 0; q < n_int; ++q) load[q % FM_OWNER_THREADS] += w_int[q] + kNodeCost;
-  // (load, thread) heap of the threads with a free interface position
-  std::vector<std::pair<int64_t, int>> heap;
-  heap.reserve(FM_OWNER_THREADS);
+  // min-heap of (load, thread) packed as load * 256 + thread (thread < 256,
+  // so the order is that of the pairs) over the threads with a free
+  // interface position
+  std::vector<uint64_t>& heap = sc.heap;
+  heap.clear();
   for (int t = 0; t < FM_OWNER_THREADS; ++t) {
     int q = n_int + ((t - n_int % FM_OWNER_THREADS) + FM_OWNER_THREADS) % FM_OWNER_THREADS;
     next[t] = q;
-    if (q < n_node) heap.push_back({load[t], t});
+    if (q < n_node) heap.push_back((uint64_t)load[t] * 256u + (uint64_t)t);
   }
-  auto later = [](const std::pair<int64_t, int>& a, const std::pair<int64_t, int>& b) { return a > b; };
-  std::make_heap(heap.begin(), heap.end(), later);
-  std::vector<int32_t>& by_w = scratch;
+  std::make_heap(heap.begin(), heap.end(), std::greater<uint64_t>());
+  // interface nodes heaviest first, equal weights in their current order (a
+  // stable counting sort on the weight)
+  int32_t wmax = 0;
+  for (int32_t w : w_ifc) wmax = std::max(wmax, w);
+  std::vector<int32_t>& count = sc.count;
+  count.assign((size_t)wmax + 2, 0);
+  for (int32_t w : w_ifc) count[wmax - w + 1]++;
+  for (int32_t k = 0; k <= wmax; ++k) count[k + 1] += count[k];
+  std::vector<int32_t>& by_w = sc.by_w;
   by_w.resize(n_ifc);
-  std::iota(by_w.begin(), by_w.end(), 0);
-  std::stable_sort(by_w.begin(), by_w.end(), [&](int32_t a, int32_t b) { return w_ifc[a] > w_ifc[b]; });
-  std::vector<int32_t> out(n_ifc);
+  for (int32_t i = 0; i < n_ifc; ++i) by_w[count[wmax - w_ifc[i]]++] = i;
+  std::vector<int32_t>& out = sc.out;
+  out.resize(n_ifc);
   for (int32_t i : by_w) {
-    std::pop_heap(heap.begin(), heap.end(), later);
-    auto [l, t] = heap.back();
+    std::pop_heap(heap.begin(), heap.end(), std::greater<uint64_t>());
+    const uint64_t key = heap.back();
     heap.pop_back();
+    const int t = (int)(key & 255u);
     out[next[t] - n_int] = ifc[i];
     next[t] += FM_OWNER_THREADS;
-    l += w_ifc[i] + kNodeCost;
     if (next[t] < n_node) {
-      heap.push_back({l, t});
-      std::push_heap(heap.begin(), heap.end(), later);
+      heap.push_back(key + (uint64_t)(w_ifc[i] + kNodeCost) * 256u);
+      std::push_heap(heap.begin(), heap.end(), std::greater<uint64_t>());
     }
   }
   ifc.swap(out);
@@ -619,6 +633,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
           std::vector<int32_t> local(N, -1);
           std::vector<uint64_t> used;                 // per-worker scratch, reused tile by tile
           std::vector<int32_t> col, idx, cnt, pos, w_int, w_ifc;
+          BalanceScratch bal;
           for (int t = (int)(ntile * w / nw); t < (int)(ntile * (w + 1) / nw); ++t) {
             TileWork& W = tw[t];
             for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
@@ -644,7 +659,7 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
               const int n_int = (int)W.inter.size();
               w_int.assign(cnt.begin(), cnt.begin() + n_int);
               w_ifc.assign(cnt.begin() + n_int, cnt.end());
-              balance_owners(w_int, w_ifc, W.ifc, idx);
+              balance_owners(w_int, w_ifc, W.ifc, bal);
               li = n_int;
               for (int32_t v : W.ifc) local[v] = li++;
             }
