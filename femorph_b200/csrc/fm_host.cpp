@@ -259,19 +259,18 @@ static void sort_by_key(const hvec<uint64_t>& key, hvec<int64_t>& order) {
     int64_t* h = &hist[(size_t)w * NB];
     for (int64_t i = b; i < e; ++i) kv[h[std::min<uint64_t>(key[i] >> SHIFT, NB - 1)]++] = KV{key[i], i};
   });
+  // each worker sorts its buckets and writes their part of the order
+  order.resize(E);
   {
     std::vector<std::thread> th;
     for (int64_t w = 0; w < nw; ++w)
       th.emplace_back([&, w] {
-        for (int k = (int)(NB * w / nw); k < (int)(NB * (w + 1) / nw); ++k)
-          std::sort(kv.begin() + start[k], kv.begin() + start[k + 1]);
+        const int k0 = (int)(NB * w / nw), k1 = (int)(NB * (w + 1) / nw);
+        for (int k = k0; k < k1; ++k) std::sort(kv.begin() + start[k], kv.begin() + start[k + 1]);
+        for (int64_t i = start[k0]; i < start[k1]; ++i) order[i] = kv[i].i;
       });
     for (auto& x : th) x.join();
   }
-  order.resize(E);
-  parallel_blocks(E, [&](int64_t b, int64_t e, int) {
-    for (int64_t i = b; i < e; ++i) order[i] = kv[i].i;
-  });
 }
 
 // Set of node ids (open addressing, cleared in O(size)), for the distinct
