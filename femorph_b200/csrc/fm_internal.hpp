@@ -94,14 +94,15 @@ struct DevProb {
   int64_t node_begin, n_nodes, elem_begin, n_elems;
 };
 
-// Per-problem progress on the device.  iter counts completed dual
-// iterations (VMS) or steps (SUPG); a pass only works on problems with
-// iter < target[p] (a separate array, set by the host per launch block).  time is the physical time of the step iter belongs to,
-// accumulated by repeated addition like the reference's currentTime.
 // Default polls of a tile CTA's bounded wait for one chunk's bulk copies
 // (each mbarrier try_wait may itself suspend for a bounded time).
 constexpr uint32_t FM_WAIT_LIMIT = 1u << 22;
 
+// Per-problem progress on the device.  iter counts completed dual
+// iterations (VMS) or steps (SUPG); a pass only works on problems with
+// iter < target[p] (a separate array, set by the host per launch block).
+// time is the physical time of the step iter belongs to, accumulated by
+// repeated addition like the reference's currentTime.
 struct DevProbState {
   int32_t iter;
   int32_t status;   // FM_OK or an FM_ERR_* raised on the device
@@ -173,7 +174,6 @@ int fail(int code, const std::string& msg);
 int resolve_bcs(fm_problem* p);
 void compute_mass(fm_problem* p);
 
-// Host-side layout of a batch (all arrays in batch numbering).
 // Host arrays of a Poisson solver that its VTK writer needs
 // (fm_poisson_write_vtk, fm_io.cpp): the model's coordinates, the fixed
 // connectivity, the diffusivity rows, and the exporter's source, Neumann and
@@ -190,6 +190,7 @@ struct PoissonHostView {
 };
 const PoissonHostView* poisson_host_view(const fm_poisson* s);
 
+// Host-side layout of a batch (all arrays in batch numbering).
 struct Layout {
   int64_t n_nodes = 0, n_elems = 0;
   std::vector<TileMeta> tiles;
