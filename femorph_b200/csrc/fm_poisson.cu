@@ -439,7 +439,8 @@ struct DeviceRestore {
 struct fm_poisson {
   int32_t device = 0, npe = 4, problem = 0;
   int64_t N = 0, E = 0, nnz = 0;
-  int blocks = 1;
+  int blocks = 1;   // grid of the CG kernels (rows)
+  int eblocks = 1;  // grid of the element kernel (wall distance)
   bool has_result = false;
   // device arrays (one allocation)
   void* block = nullptr;
@@ -502,6 +503,8 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
     return fail(FM_ERR_INVALID, "null boundary / source array");
   for (int64_t k = 0; k < d->n_sources; ++k)
     if (d->source_elem[k] < 0 || d->source_elem[k] >= E) return fail(FM_ERR_INVALID, "ELSOURCE element out of range");
+  if (d->n_neumann < 0 || d->n_sources < 0 || d->n_dirichlet < 0) return fail(FM_ERR_INVALID, "negative count");
+  if (d->n_neumann > 0 && d->neumann_off[0] < 0) return fail(FM_ERR_INVALID, "FACENEUMANN offsets must start at >= 0");
   for (int64_t k = 0; k < d->n_neumann; ++k) {
     if (d->neumann_off[k + 1] <= d->neumann_off[k]) return fail(FM_ERR_INVALID, "FACENEUMANN row without nodes");
     for (int32_t j = d->neumann_off[k]; j < d->neumann_off[k + 1]; ++j)
@@ -736,6 +739,7 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   s->blocks = (int)std::max<int64_t>(1, std::min<int64_t>((N + kThreads - 1) / kThreads, (int64_t)sms * 8));
+  s->eblocks = (int)std::max<int64_t>(1, std::min<int64_t>((E + kThreads - 1) / kThreads, (int64_t)sms * 8));
   // one device allocation carved into the arrays (256-byte aligned)
   size_t total = 0;
   auto take = [&](size_t bytes) {
@@ -865,10 +869,8 @@ FM_API int fm_poisson_solve(fm_poisson* s, double rel_tol, int32_t max_iter, int
   PCK(cudaEventRecord(s->ev1, st));
   avg_kernel<<<G, kThreads, 0, st>>>(c);
   shift_kernel<<<G, kThreads, 0, st>>>(c.x, c.scal, s->problem == FM_POISSON_PPE, s->N, s->out);
-  if (s->problem == FM_POISSON_DISTANCE) {
-    const int eb = (int)std::max<int64_t>(1, std::min<int64_t>((s->E + kThreads - 1) / kThreads, 148 * 8));
-    distance_kernel<<<eb, kThreads, 0, st>>>(s->coords, s->conn, s->npe, s->E, s->out, s->dist);
-  }
+  if (s->problem == FM_POISSON_DISTANCE)
+    distance_kernel<<<s->eblocks, kThreads, 0, st>>>(s->coords, s->conn, s->npe, s->E, s->out, s->dist);
   PCK(cudaGetLastError());
   PCK(cudaMemcpyAsync(s->h_ctl, c.ctl, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   PCK(cudaMemcpyAsync(s->h_scal, c.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -77,6 +77,18 @@ def test_poisson_create_rejects_bad_input_and_needs_a_device():
     with pytest.raises(api.FmError) as ei:
         api.GpuPoisson(bad)
     assert ei.value.code == api.FM_ERR_INVALID
+    # FACENEUMANN offsets: must start at >= 0 and increase
+    for off0, off1 in ((-1, None), (None, 0)):
+        bad = mesh.poisson_box(2)
+        assert bad.neumann_value.size > 0
+        bad.neumann_off = bad.neumann_off.copy()
+        if off0 is not None:
+            bad.neumann_off[0] = off0
+        if off1 is not None:
+            bad.neumann_off[1] = bad.neumann_off[0]
+        with pytest.raises(api.FmError) as ei:
+            api.GpuPoisson(bad)
+        assert ei.value.code == api.FM_ERR_INVALID
     try:
         import torch
         has_gpu = torch.cuda.is_available()
