@@ -415,6 +415,7 @@ void morton_order(const fm_problem* p, hvec<int64_t>& order) {
   double span = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
   if (!(span > 0)) span = 1.0;
   hvec<uint64_t> code(E);
+  const double inv_npe = 1.0 / npe;  // exact (4 or 8): c * inv_npe equals c / npe
   parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
     for (int64_t e = eb; e < ee; ++e) {
       double c[3] = {0, 0, 0};
@@ -422,7 +423,7 @@ void morton_order(const fm_problem* p, hvec<int64_t>& order) {
         for (int k = 0; k < 3; ++k) c[k] += p->coords[(int64_t)p->conn[e * npe + a] * 3 + k];
       uint64_t q[3];
       for (int k = 0; k < 3; ++k) {
-        double t = (c[k] / npe - lo[k]) / span;
+        double t = (c[k] * inv_npe - lo[k]) / span;
         t = std::min(std::max(t, 0.0), 1.0);
         q[k] = (uint64_t)(t * 2097151.0);
       }
@@ -631,22 +632,30 @@ int build_layout(fm_problem* const* probs, int n, int TE, int TN, Layout& L) {
         th.emplace_back([&, w] {
           std::vector<int32_t> local(N, -1);
           std::vector<uint64_t> used;                 // per-worker scratch, reused tile by tile
-          std::vector<int32_t> col, idx, cnt, pos, w_int, w_ifc;
+          std::vector<int32_t> col, idx, cnt, pos, w_int, w_ifc, own;
           BalanceScratch bal;
           for (int t = (int)(ntile * w / nw); t < (int)(ntile * (w + 1) / nw); ++t) {
             TileWork& W = tw[t];
+            own.clear();
             for (int64_t oi = tile_start[t]; oi < tile_start[t + 1]; ++oi) {
               const int32_t* c = &cs[(size_t)oi * npe];
-              for (int a = 0; a < npe; ++a)
-                if (local[c[a]] != -2 - t) {
-                  local[c[a]] = -2 - t;
-                  (ntiles[c[a]] == 1 ? W.inter : W.ifc).push_back(c[a]);
-                }
+              for (int a = 0; a < npe; ++a) {
+                const int32_t v = c[a];
+                if (local[v] == -2 - t) continue;
+                local[v] = -2 - t;
+                if (ntiles[v] == 1) W.inter.push_back(v);
+                else if (first_tile[v] == t) own.push_back(v);
+                else W.ifc.push_back(v);
+              }
             }
             // interior nodes in their (contiguous) batch order, then interface
-            // nodes by id, reordered to balance the owner threads
-            std::sort(W.inter.begin(), W.inter.end(), [&](int32_t x, int32_t y) { return nn[x] < nn[y]; });
+            // nodes by id, reordered to balance the owner threads.  The
+            // interior nodes and the interface nodes this tile touches first
+            // were numbered in this same first-touch walk, so they arrive in
+            // id order; only the interface nodes of earlier tiles (all with
+            // smaller ids) are sorted
             std::sort(W.ifc.begin(), W.ifc.end(), [&](int32_t x, int32_t y) { return nn[x] < nn[y]; });
+            W.ifc.insert(W.ifc.end(), own.begin(), own.end());
             int32_t li = 0;
             for (int32_t v : W.inter) local[v] = li++;
             for (int32_t v : W.ifc) local[v] = li++;
