@@ -35,7 +35,7 @@ SYMBOLS = [
     "fm_problem_write_vtu", "fm_batch_exchange_account", "fm_batch_exchange_buffers", "fm_batch_exchange_begin",
     "fm_batch_exchange_end", "fm_batch_iterations_per_step", "fm_problem_checkpoint", "fm_problem_restore",
     "fm_batch_set_diagnostics", "fm_problem_vms_log", "fm_problem_vms_residuals",
-    "fm_poisson_create", "fm_poisson_destroy", "fm_poisson_solve", "fm_poisson_get_solution", "fm_poisson_info",
+    "fm_poisson_create", "fm_poisson_destroy", "fm_poisson_solve", "fm_poisson_get_solution", "fm_poisson_info", "fm_poisson_model",
     "fm_poisson_read_dat", "fm_poisson_write_vtk", "fm_problem_check_layout",
 ]
 
@@ -151,6 +151,7 @@ def lib():
         L.fm_poisson_solve.argtypes = [P, C.c_double, C.c_int32, P, P, P]
         L.fm_poisson_get_solution.argtypes = [P, P, P]
         L.fm_poisson_info.argtypes = [P, P, P]
+        L.fm_poisson_model.argtypes = [P, P, P, P, P]
         L.fm_poisson_read_dat.argtypes = [C.c_char_p, C.c_int32, P]
         L.fm_problem_check_layout.argtypes = [P, P]
         L.fm_poisson_write_vtk.argtypes = [P, C.c_char_p]
@@ -532,8 +533,7 @@ class GpuPoisson:
             h = C.c_void_p()
             check(lib().fm_poisson_read_dat(str(path).encode(), int(device), C.byref(h)))
             self.h = h
-            n, _ = self.info()
-            self.n_nodes, self.problem = n, None
+            self.n_nodes, self.n_elems, _, self.problem = self.model()
             return
         self._keep = [np.ascontiguousarray(a) for a in (
             pp.coords, pp.conn, pp.diffusivity, pp.source_elem, pp.source_value, pp.neumann_off, pp.neumann_nodes,
@@ -554,12 +554,15 @@ class GpuPoisson:
         return int(it.value), float(rr.value), float(ms.value)
 
     @classmethod
-    def read_dat(cls, path: str, device: int = 0, n_elems: int = 0, problem: int = FM_POISSON_CLASSIC):
-        """The solver of a .dat file's Poisson model; n_elems and problem are
-        needed only to read the DISTANCE problem's element distances."""
-        s = cls(None, device, path)
-        s.n_elems, s.problem = n_elems, problem
-        return s
+    def read_dat(cls, path: str, device: int = 0):
+        """The solver of a .dat file's Poisson model (fm_poisson_read_dat)."""
+        return cls(None, device, path)
+
+    def model(self):
+        """(nodes, elements, element type, FM_POISSON_* problem) of the model."""
+        n, e, t, pb = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
+        check(lib().fm_poisson_model(self.h, C.byref(n), C.byref(e), C.byref(t), C.byref(pb)))
+        return int(n.value), int(e.value), int(t.value), int(pb.value)
 
     def solution(self):
         """(x, cell distance or None)."""

@@ -824,6 +824,16 @@ FM_API int fm_poisson_info(const fm_poisson* s, int64_t* rows, int64_t* nonzeros
   return FM_OK;
 }
 
+FM_API int fm_poisson_model(const fm_poisson* s, int64_t* n_nodes, int64_t* n_elems, int32_t* elem_type,
+                            int32_t* problem) {
+  if (!s) return fail(FM_ERR_INVALID, "null solver");
+  if (n_nodes) *n_nodes = s->N;
+  if (n_elems) *n_elems = s->E;
+  if (elem_type) *elem_type = s->npe;
+  if (problem) *problem = s->problem;
+  return FM_OK;
+}
+
 FM_API int fm_poisson_solve(fm_poisson* s, double rel_tol, int32_t max_iter, int32_t* iterations,
                             double* rel_residual, double* device_ms) {
   fm::NvtxRange nv("fm_poisson_solve");

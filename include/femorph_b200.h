@@ -502,6 +502,12 @@ FM_API int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson** ou
 FM_API int fm_poisson_write_vtk(fm_poisson* s, const char* path);
 /* Sizes of the assembled system: rows and stored matrix entries. */
 FM_API int fm_poisson_info(const fm_poisson* s, int64_t* rows, int64_t* nonzeros);
+/* The model behind a solver (also one read by fm_poisson_read_dat): node and
+ * element counts, element type (FM_TET4 / FM_HEXA8) and FM_POISSON_* problem
+ * (femModel's nodeList / elementList sizes and problemType).  Null outputs
+ * are skipped. */
+FM_API int fm_poisson_model(const fm_poisson* s, int64_t* n_nodes, int64_t* n_elems, int32_t* elem_type,
+                            int32_t* problem);
 
 #ifdef __cplusplus
 }

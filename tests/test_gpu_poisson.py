@@ -118,7 +118,8 @@ def test_read_dat_equals_arrays(tmp_path, elem_type, problem):
     dat = str(tmp_path / "p.dat")
     mesh.write_poisson_dat(p, dat)
     x, d, it, _ = gpu_solve(p)
-    s = api.GpuPoisson.read_dat(dat, n_elems=p.n_elems, problem=problem)
+    s = api.GpuPoisson.read_dat(dat)
+    assert s.model() == (p.n_nodes, p.n_elems, p.conn.shape[1], problem)
     it2, _, _ = s.solve(1e-14, 20000)
     x2, d2 = s.solution()
     s.close()
@@ -147,7 +148,8 @@ def test_vtk_writer_matches_reference_exporter(tmp_path, problem):
     r = subprocess.run([gpudrv, dat, "poisson-gpu", "--dump", str(tmp_path), "--vtk"], cwd=str(tmp_path),
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
-    s = api.GpuPoisson.read_dat(dat, n_elems=p.n_elems, problem=problem)
+    s = api.GpuPoisson.read_dat(dat)
+    assert s.model() == (p.n_nodes, p.n_elems, p.conn.shape[1], problem)
     s.solve(1e-14, 100000)
     mine = str(tmp_path / "mine.vtk")
     s.write_vtk(mine)
