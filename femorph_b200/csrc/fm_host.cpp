@@ -1004,9 +1004,36 @@ int check_layout(const fm_problem* p, const Layout& L) {
     if (seen_node[g] > 1) return bad("node interior to two tiles");
     if (seen_node[g] == 1 && tiles_of[g] != 1) return bad("interior node touched by another tile");
   }
-  // interface lists: node i's slots name the node, one a touching tile, in
-  // tile order, and the slot map of the tiles is a permutation
+  // interface lists: every node some tile touches but none owns is listed
+  // once (no interior node is); node i's slots name the node, one a touching
+  // tile, in tile order, and the slot map of the tiles is a permutation
   const int64_t NI = (int64_t)L.iface_node.size();
+  if ((int64_t)L.iface_slot_beg.size() != NI + 1) return bad("interface list size");
+  std::vector<char> listed((size_t)N, 0);
+  for (int64_t i = 0; i < NI; ++i) {
+    const int32_t g = L.iface_node[i];
+    if (g < 0 || g >= N || listed[g] || seen_node[g]) return bad("interface node list");
+    listed[g] = 1;
+  }
+  for (int64_t g = 0; g < N; ++g)
+    if (tiles_of[g] > 0 && !seen_node[g] && !listed[g]) return bad("touched node neither interior nor interface");
+  // partition parts: a node shared with another part is never interior, and
+  // its interface entry carries its exchange index (unique in the part, below
+  // the partition's total); other entries carry -1
+  if (p->part >= 0) {
+    if ((int64_t)p->xidx.size() != N || (int64_t)L.iface_xidx.size() != NI) return bad("exchange index size");
+    std::vector<char> xused((size_t)std::max<int64_t>(p->x_total, 0), 0);
+    for (int64_t v = 0; v < N; ++v) {
+      const int32_t x = p->xidx[v];
+      if (x < 0) continue;
+      if (x >= p->x_total || xused[x]) return bad("exchange index out of range or repeated");
+      xused[x] = 1;
+      if (seen_node[nn[v]]) return bad("shared node interior to a tile");
+      if (tiles_of[nn[v]] > 0 && !listed[nn[v]]) return bad("shared node without an interface entry");
+    }
+    for (int64_t i = 0; i < NI; ++i)
+      if (L.iface_xidx[i] != p->xidx[old_of[L.iface_node[i]]]) return bad("interface entry's exchange index");
+  }
   for (int64_t i = 0; i < NI; ++i) {
     const int32_t g = L.iface_node[i];
     const int32_t k0 = L.iface_slot_beg[i], k1 = L.iface_slot_beg[i + 1];

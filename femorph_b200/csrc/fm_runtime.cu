@@ -990,7 +990,6 @@ int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning) {
 int fm_problem_check_layout(fm_problem* p, const fm_tuning* tuning) {
   NvtxRange nvtx_range("fm_problem_check_layout");
   if (!p) return fail(FM_ERR_INVALID, "null problem");
-  if (p->part >= 0) return fail(FM_ERR_INVALID, "fm_problem_check_layout checks whole problems, not partition parts");
   fm_tuning t;
   memset(&t, 0, sizeof(t));
   if (tuning) t = *tuning;

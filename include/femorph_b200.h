@@ -183,7 +183,9 @@ FM_API int fm_problem_prepare(fm_problem* p, const fm_tuning* tuning);
  * each tile's node list, interior nodes touched by one tile only, no two
  * elements of a colour sharing a node, each (element, corner) once in its
  * node's incidence list in element order, one partial slot per (tile,
- * interface node) listed in tile order, every element and node once.
+ * interface node) listed in tile order, every element and node once; for a
+ * partition part (fm_problem_partition) also that shared nodes are interface
+ * nodes carrying their exchange index.
  * FM_ERR_INVALID names the first broken one.  Host only.  No counterpart in
  * the reference (its element loop neither tiles nor colours). */
 FM_API int fm_problem_check_layout(fm_problem* p, const fm_tuning* tuning);

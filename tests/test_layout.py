@@ -1,8 +1,9 @@
 """Host-side checks of the tile layout the kernels rely on
 (fm_problem_check_layout): local connectivity, interior nodes touched by one
 tile only, colours without shared nodes, incidence lists in element order,
-interface slots in tile order, every element and node once - over the mesh
-families, tile sizes and precisions the solvers use (the mixed form flags
+interface slots in tile order, every element and node once, shared nodes of
+partition parts on interface entries - over the mesh families, tile sizes
+and precisions the solvers use (the mixed form flags
 FP64-Jacobian elements in the local connectivity; the interface nodes are
 reordered to balance the owner threads).  No GPU needed."""
 import pytest
@@ -30,11 +31,15 @@ def test_layout_invariants(name, make, prec, tune):
     g.close()
 
 
-def test_layout_check_rejects_partition_parts():
-    g = api.GpuProblem(mesh.cavity(4, seed=1, steps=2))
-    part = g.part(2, 0)
-    with pytest.raises(api.FmError) as ei:
+@pytest.mark.parametrize("solver,n_parts", [(mesh.VMS, 2), (mesh.VMS, 3), (mesh.SUPG, 4)])
+def test_layout_invariants_partition_parts(solver, n_parts):
+    """Every part of a split mesh: the same invariants, and its shared nodes
+    are interface nodes carrying their exchange index."""
+    g = api.GpuProblem(mesh.cavity(10, seed=5, steps=2, solver=solver, cfl=0.05))
+    for k in range(n_parts):
+        part = g.part(n_parts, k)
+        assert (part.xidx >= 0).any()
         part.check_layout()
-    assert ei.value.code == api.FM_ERR_INVALID
-    part.close()
+        part.check_layout(tile_elems=256, tile_nodes=128)
+        part.close()
     g.close()
