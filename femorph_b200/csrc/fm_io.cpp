@@ -1,12 +1,21 @@
 // .dat keyword reader and legacy-VTK writer with the reference's formats.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cctype>
+#include <cerrno>
+#include <charconv>
 #include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "fm_internal.hpp"
@@ -58,8 +67,59 @@ std::string tok_upper(const Tok& t) {
   for (auto& c : s) c = (char)std::toupper((unsigned char)c);
   return s;
 }
-double tdbl(const Tok* t, int n, int i) { return i < n ? strtod(t[i].b, nullptr) : 0.0; }
-int tint(const Tok* t, int n, int i) { return i < n ? (int)strtol(t[i].b, nullptr, 10) : 0; }
+// A token's number as strtod / strtol read it from the token's start.  A
+// token that is exactly a finite decimal number in std::from_chars's grammar
+// (no '+', no hex) takes that path, whose result is the same correctly
+// rounded value; a token of at most nine digits after an optional '-' is
+// summed directly; every other token goes through strtod / strtol.
+double tok_dbl(const Tok& t) {
+  double v = 0.0;
+  const auto r = std::from_chars(t.b, t.e, v);
+  if (r.ec == std::errc() && r.ptr == t.e && std::isfinite(v)) return v;
+  return strtod(t.b, nullptr);
+}
+int tok_int(const Tok& t) {
+  const char* q = t.b + (t.b < t.e && *t.b == '-');
+  const ptrdiff_t nd = t.e - q;
+  if (nd >= 1 && nd <= 9) {
+    int v = 0;
+    for (; q < t.e && *q >= '0' && *q <= '9'; ++q) v = v * 10 + (*q - '0');
+    if (q == t.e) return *t.b == '-' ? -v : v;
+  }
+  return (int)strtol(t.b, nullptr, 10);
+}
+double tdbl(const Tok* t, int n, int i) { return i < n ? tok_dbl(t[i]) : 0.0; }
+int tint(const Tok* t, int n, int i) { return i < n ? tok_int(t[i]) : 0; }
+
+// The whole file in a NUL-terminated host buffer, read in pieces by the host
+// threads (pread; the buffer is not zero-filled first).
+int read_file(const char* path, hvec<char>& buf) {
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) return fail(FM_ERR_IO, std::string("cannot open ") + path);
+  struct stat st;
+  if (fstat(fd, &st) != 0) {
+    close(fd);
+    return fail(FM_ERR_IO, std::string("cannot read ") + path);
+  }
+  const int64_t size = std::max<int64_t>(0, (int64_t)st.st_size);
+  buf.resize((size_t)size + 1);
+  std::atomic<bool> ok{true};
+  parallel_blocks(size, [&](int64_t b, int64_t e, int) {
+    while (b < e) {
+      const ssize_t r = pread(fd, buf.data() + b, (size_t)(e - b), (off_t)b);
+      if (r < 0 && errno == EINTR) continue;
+      if (r <= 0) {
+        ok = false;
+        return;
+      }
+      b += r;
+    }
+  }, 1 << 22);
+  close(fd);
+  buf[(size_t)size] = '\0';
+  if (!ok) return fail(FM_ERR_IO, std::string("cannot read ") + path);
+  return FM_OK;
+}
 
 // Everything one block of lines contributes, in line order.
 struct DatBlock {
@@ -146,6 +206,23 @@ void parse_block(const char* b, const char* e, DatBlock& B) {
   }
 }
 
+// One array of every block, in block order, into dst: sized once, the blocks
+// copied on their own threads and released.
+template <class T, class Get>
+void join_blocks(std::vector<DatBlock>& blk, Get get, hvec<T>& dst) {
+  std::vector<size_t> off(blk.size() + 1, 0);
+  for (size_t k = 0; k < blk.size(); ++k) off[k + 1] = off[k] + get(blk[k]).size();
+  dst.resize(off.back());
+  std::vector<std::thread> th;
+  for (size_t k = 0; k < blk.size(); ++k)
+    th.emplace_back([&, k] {
+      std::vector<T>& v = get(blk[k]);
+      std::copy(v.begin(), v.end(), dst.begin() + (std::ptrdiff_t)off[k]);
+      std::vector<T>().swap(v);
+    });
+  for (auto& x : th) x.join();
+}
+
 }  // namespace
 
 // Reads the whole file, cuts it at line ends into one block per host thread,
@@ -156,19 +233,10 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
   NvtxRange nvtx_range("fm_problem_read_dat");
   if (!path || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
-  FILE* fp = fopen(path, "rb");
-  if (!fp) return fail(FM_ERR_IO, std::string("cannot open ") + path);
-  fseek(fp, 0, SEEK_END);
-  const long size = ftell(fp);
-  fseek(fp, 0, SEEK_SET);
-  std::vector<char> buf((size_t)std::max(0L, size) + 1, '\0');
-  if (size > 0 && fread(buf.data(), 1, (size_t)size, fp) != (size_t)size) {
-    fclose(fp);
-    return fail(FM_ERR_IO, std::string("cannot read ") + path);
-  }
-  fclose(fp);
+  hvec<char> buf;
+  if (int r = read_file(path, buf)) return r;
   const char* base = buf.data();
-  const int64_t len = size;
+  const int64_t len = (int64_t)buf.size() - 1;
   const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
   const int64_t nb = std::min<int64_t>(hw, std::max<int64_t>(1, len / (1 << 20)));
   std::vector<int64_t> cut(nb + 1, 0);
@@ -185,8 +253,8 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
       th.emplace_back([&, k] { parse_block(base + cut[k], base + cut[k + 1], blk[k]); });
     for (auto& x : th) x.join();
   }
-  std::vector<double> coords, vel_vals, dir_vals, pres_vals;
-  std::vector<int32_t> conn, vel_node, vel_dir, dir_node, pres_node;
+  std::vector<double> vel_vals, dir_vals, pres_vals;
+  std::vector<int32_t> vel_node, vel_dir, dir_node, pres_node;
   int etype = 0;
   fm_params prm;
   memset(&prm, 0, sizeof(prm));
@@ -208,7 +276,6 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
                                       " is not handled by the explicit flow solvers");
     if (at_mix < INF) return fail(FM_ERR_INVALID, "mixed element types are not supported");
     if (B.etype) etype = B.etype;
-    cat(coords, B.coords); cat(conn, B.conn);
     cat(vel_node, B.vel_node); cat(vel_vals, B.vel_vals); cat(vel_dir, B.vel_dir);
     cat(dir_node, B.dir_node); cat(dir_vals, B.dir_vals);
     cat(pres_node, B.pres_node); cat(pres_vals, B.pres_vals);
@@ -248,9 +315,11 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
       }
     }
     line0 += B.lines;
-    std::vector<double>().swap(B.coords);  // release as we go
-    std::vector<int32_t>().swap(B.conn);
   }
+  hvec<double> coords;
+  hvec<int32_t> conn;
+  join_blocks(blk, [](DatBlock& B) -> std::vector<double>& { return B.coords; }, coords);
+  join_blocks(blk, [](DatBlock& B) -> std::vector<int32_t>& { return B.conn; }, conn);
   if (glob == "NONE") prm.glob_fixed = FM_FIX_NONE;
   else if (glob == "X") prm.glob_fixed = FM_FIX_X;
   else if (glob == "Y") prm.glob_fixed = FM_FIX_Y;
@@ -611,19 +680,10 @@ extern "C" int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson*
   NvtxRange nvtx_range("fm_poisson_read_dat");
   if (!path || !out) return fail(FM_ERR_INVALID, "null argument");
   *out = nullptr;
-  FILE* fp = fopen(path, "rb");
-  if (!fp) return fail(FM_ERR_IO, std::string("cannot open ") + path);
-  fseek(fp, 0, SEEK_END);
-  const long size = ftell(fp);
-  fseek(fp, 0, SEEK_SET);
-  std::vector<char> buf((size_t)std::max(0L, size) + 1, '\0');
-  if (size > 0 && fread(buf.data(), 1, (size_t)size, fp) != (size_t)size) {
-    fclose(fp);
-    return fail(FM_ERR_IO, std::string("cannot read ") + path);
-  }
-  fclose(fp);
+  hvec<char> buf;
+  if (int r = read_file(path, buf)) return r;
   const char* base = buf.data();
-  const int64_t len = size;
+  const int64_t len = (int64_t)buf.size() - 1;
   const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
   const int64_t nb = std::min<int64_t>(hw, std::max<int64_t>(1, len / (1 << 20)));
   std::vector<int64_t> cut(nb + 1, 0);
@@ -640,8 +700,8 @@ extern "C" int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson*
       th.emplace_back([&, k] { parse_block(base + cut[k], base + cut[k + 1], blk[k]); });
     for (auto& x : th) x.join();
   }
-  std::vector<double> coords, diff, src_val, neu_val, dir_val;
-  std::vector<int32_t> conn, src_el, neu_off(1, 0), neu_nodes, dir_node;
+  std::vector<double> src_val, neu_val, dir_val;
+  std::vector<int32_t> src_el, neu_off(1, 0), neu_nodes, dir_node;
   int etype = 0, problem = FM_POISSON_CLASSIC;
   auto cat = [](auto& dst, const auto& src) { dst.insert(dst.end(), src.begin(), src.end()); };
   for (int64_t k = 0; k < nb; ++k) {
@@ -650,9 +710,6 @@ extern "C" int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson*
     if (B.change_line >= 0 || (B.etype && etype && B.etype != etype))
       return fail(FM_ERR_INVALID, "mixed element types are not supported");
     if (B.etype) etype = B.etype;
-    cat(coords, B.coords);
-    cat(conn, B.conn);
-    cat(diff, B.diff);
     cat(src_el, B.src_el);
     cat(src_val, B.src_val);
     cat(neu_val, B.neu_val);
@@ -670,6 +727,11 @@ extern "C" int fm_poisson_read_dat(const char* path, int32_t device, fm_poisson*
         else return fail(FM_ERR_INVALID, "PROBLEM " + v + " is not a Poisson problem");
       }
   }
+  hvec<double> coords, diff;
+  hvec<int32_t> conn;
+  join_blocks(blk, [](DatBlock& B) -> std::vector<double>& { return B.coords; }, coords);
+  join_blocks(blk, [](DatBlock& B) -> std::vector<int32_t>& { return B.conn; }, conn);
+  join_blocks(blk, [](DatBlock& B) -> std::vector<double>& { return B.diff; }, diff);
   const int64_t E = etype ? (int64_t)conn.size() / etype : 0;
   if ((int64_t)diff.size() < 3 * E) return fail(FM_ERR_INVALID, "fewer ELDIFF rows than elements");
   fm_poisson_desc d;
