@@ -138,7 +138,7 @@ def stored_geometry_bytes(E: int, precision: str, config: str) -> int:
 # of the kernel reading the stored Gauss-point geometry.
 SUPG_FLOPS = {"channel": 6419, "supg": 1676}
 
-CONFIG_DEFAULT_N = {"cavity": 96, "supg": 96, "channel": 64}
+CONFIG_DEFAULT_N = {"cavity": 96, "supg": 96, "channel": 64, "io": 96}
 
 
 def make_problem(args, seed: int, n: int | None = None):
@@ -584,6 +584,116 @@ def cpu_baseline(args, steps: int = 2):
                       f"C restatement of {solver} on {threads} host threads, setup excluded"}
 
 
+def io_file(args):
+    """The cavity workload's input file, written once into a temporary
+    directory (mesh.write_dat: the reference's .dat keywords)."""
+    from femorph_b200 import mesh
+    d = tempfile.mkdtemp(prefix="fm_io_")
+    path = os.path.join(d, f"cavity{args.n}.dat")
+    mesh.write_dat(mesh.cavity(args.n, seed=args.seed, steps=2), path)
+    return d, path
+
+
+def run_io(args):
+    """--config io: the .dat reader (fm_problem_read_dat: the keywords of
+    femModel::ReadFromFEMTextFile, femModel.cpp:3719-4213, parsed in blocks on
+    the host threads) on the cavity's input file; a step is one whole read
+    from the file into a problem (parse, checks, BC resolution, lumped mass).
+    With a device the problem is also placed in a batch and each writer
+    (legacy ASCII VTK, legacy binary VTK, VTU) is timed on its state, the
+    device read-back included."""
+    import ctypes as C
+    import shutil
+    import types
+
+    from femorph_b200 import api
+    d, path = io_file(args)
+    size = os.path.getsize(path)
+    L = api.lib()
+    steps, warm = max(1, min(args.steps, 10)), max(1, min(args.warmup, 3))
+    times, h = [], None
+    try:
+        for k in range(warm + steps):
+            if h is not None:
+                L.fm_problem_destroy(h)
+            h = C.c_void_p()
+            t0 = time.perf_counter()
+            api.check(L.fm_problem_read_dat(path.encode(), 0, api.FM_FP64, C.byref(h)))
+            if k >= warm:
+                times.append(time.perf_counter() - t0)
+        writers = None
+        try:
+            import torch
+            has_gpu = torch.cuda.is_available()
+        except Exception:
+            has_gpu = False
+        if has_gpu:
+            b = api.Batch([types.SimpleNamespace(h=h)])
+            writers = {}
+            for name, fn in (("vtk_ascii", L.fm_problem_write_vtk), ("vtk_binary", L.fm_problem_write_vtk_binary),
+                             ("vtu", L.fm_problem_write_vtu)):
+                out = os.path.join(d, "out." + ("vtu" if name == "vtu" else "vtk"))
+                ws = []
+                for k in range(2):
+                    t0 = time.perf_counter()
+                    api.check(fn(h, out.encode()))
+                    ws.append(time.perf_counter() - t0)
+                osz = os.path.getsize(out)
+                writers[name] = {"bytes": osz, "s": min(ws), "MB_per_s": osz / min(ws) / 1e6}
+                os.remove(out)
+            b.close()
+    finally:
+        if h is not None:
+            L.fm_problem_destroy(h)
+        shutil.rmtree(d, ignore_errors=True)
+    return {"size": size, "times": times, "warm": warm, "writers": writers}
+
+
+def io_reference(args, path):
+    """The reference's own reader (femModel::ReadFromFEMTextFile, compiled
+    here as oracle/_ref/fm_refdrv, mode parse) on the same file: seconds."""
+    from oracle import ref
+    tf = path + ".timing"
+    r = subprocess.run([ref.REFDRV, path, "parse", "--timing", tf], capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    with open(tf) as f:
+        for line in f:
+            if line.startswith("# parsed"):
+                return float(line.split()[2])
+    raise RuntimeError("no parse time recorded")
+
+
+def io_config(args, size):
+    return {"workload": f"reader of the {args.n}^3 Kuhn-tet cavity .dat ({size / 1e6:.1f} MB, "
+                        f"{6 * args.n ** 3} TET4 elements, {(args.n + 1) ** 3} nodes)",
+            "host_threads": os.cpu_count(), "l2": "host-only path"}
+
+
+def io_line(args, world, r):
+    t = np.array(r["times"])
+    sec = float(np.median(t))
+    val = r["size"] / sec / 1e6
+    line = {"metric": ".dat read throughput (file to problem, C ABI)", "value": val, "unit": "MB/s",
+            "n_gpus": world, "steps": len(t), "warmup": r["warm"], "ms_per_step": 1e3 * sec,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": io_config(args, r["size"]), "read_s": {"median": sec, "min": float(t.min())},
+            "writers": r["writers"], "host": host_cpu() | {"cores_used": os.cpu_count()}}
+    if not args.no_cpu:
+        from oracle import ref
+        if ref.available():
+            d, path = io_file(args)
+            try:
+                rs = io_reference(args, path)
+            finally:
+                import shutil
+                shutil.rmtree(d, ignore_errors=True)
+            line["cpu_baseline"] = {"value": r["size"] / rs / 1e6, "unit": "MB/s", "cores": 1, "kind": "reference",
+                                    "sample": "one read of the same file by femModel::ReadFromFEMTextFile "
+                                              "(reference sources, single-threaded)"}
+    return line
+
+
 def run_reference(args):
     """The reference's own CPU solver (oracle A = the reference sources compiled
     in this repository) on a bounded sample of the workload: the full mesh,
@@ -595,6 +705,24 @@ def run_reference(args):
                                                     "(src/femSolver.cpp:590-600), which is not in this image"}
     if not ref.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/fm_refdrv was not built (reference sources absent)"}
+    if args.config == "io":
+        d, path = io_file(args)
+        try:
+            size = os.path.getsize(path)
+            rs = [io_reference(args, path) for _ in range(max(1, min(args.steps, 3)))]
+        finally:
+            import shutil
+            shutil.rmtree(d, ignore_errors=True)
+        sec = float(np.median(rs))
+        val = size / sec / 1e6
+        return {"impl": "reference", "metric": ".dat read throughput (file to problem, C ABI)", "value": val,
+                "unit": "MB/s", "n_gpus": args.gpus, "steps": len(rs), "warmup": 0, "ms_per_step": 1e3 * sec,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": io_config(args, size),
+                "cpu_baseline": {"value": val, "unit": "MB/s", "cores": 1, "kind": "reference",
+                                 "sample": f"{len(rs)} whole reads by femModel::ReadFromFEMTextFile "
+                                           "(reference sources, single-threaded)"},
+                "e2e": {"value": val, "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     n = cpu_sample_n(args)
     steps = max(1, min(args.steps, args.ref_steps))
     warm = max(1, min(args.warmup, 1))
@@ -668,7 +796,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="mesh size (default 96 for cavity/supg, 64 for channel)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--config", default="cavity",
-                    choices=["cavity", "supg", "channel", "batched", "serve", "partitioned", "poisson"])
+                    choices=["cavity", "supg", "channel", "batched", "serve", "partitioned", "poisson", "io"])
     ap.add_argument("--rates", default="10,30,100,1000", help="serve: arrival rates, requests/s")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
     ap.add_argument("--budget-gb", type=float, default=16.0, help="serve: HBM budget of the pooled batch")
@@ -696,6 +824,11 @@ def main():
             print(json.dumps(run_reference(args)), flush=True)
         return
 
+    if args.config == "io":
+        # host path: rank 0 reads (and, with a device, writes); no collective
+        if rank == 0:
+            print(json.dumps(io_line(args, world, run_io(args))), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime

@@ -131,7 +131,7 @@ void wrap_export(femModel* m, std::string name, bool msg) {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: %s model.dat vms|supg [--ic file ncomp] [--dump dir] [--vtk] [--timing file]\n", argv[0]);
+    fprintf(stderr, "usage: %s model.dat vms|supg|parse [--ic file ncomp] [--dump dir] [--vtk] [--timing file]\n", argv[0]);
     return 2;
   }
   std::string model_path = argv[1], solver = argv[2];
@@ -179,6 +179,7 @@ int main(int argc, char** argv) {
       double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - g_t0).count();
       fprintf(g_timing, "# parsed %.9f\n", s);
     }
+    if (solver == "parse") return 0;  // the reader alone (its time under --timing)
     if (solver == "poisson-elements") {
       if (!g_dump) {
         fprintf(stderr, "poisson-elements needs --dump dir\n");
