@@ -360,6 +360,70 @@ extern "C" int fm_problem_read_dat(const char* path, int32_t solver, int32_t pre
 // element loop order and carry no state); they are written as zeros.
 namespace {
 
+// printf("%e") of a double, byte for byte: std::to_chars in scientific form
+// with six digits gives the same correctly rounded digits and layout for
+// finite values; the others go through snprintf.
+inline char* put_e(char* b, double v) {
+  if (std::isfinite(v)) return std::to_chars(b, b + 32, v, std::chars_format::scientific, 6).ptr;
+  return b + snprintf(b, 32, "%e", v);
+}
+inline char* put_d(char* b, int v) { return std::to_chars(b, b + 16, v).ptr; }
+// "%e<end>" and "%e %e %e<end>" rows (end: "\n" or " \n"); returns the length.
+inline int put_e1(char* b, double v, const char* end) {
+  char* q = put_e(b, v);
+  while (*end) *q++ = *end++;
+  return (int)(q - b);
+}
+inline int put_e3(char* b, const double* v, const char* end) {
+  char* q = put_e(b, v[0]);
+  *q++ = ' ';
+  q = put_e(q, v[1]);
+  *q++ = ' ';
+  q = put_e(q, v[2]);
+  while (*end) *q++ = *end++;
+  return (int)(q - b);
+}
+
+// n copies of one row (a section of constant values), written in large
+// pieces.
+void write_const_rows(FILE* f, int64_t n, const std::string& row) {
+  const int64_t per = std::max<int64_t>(1, (1 << 20) / (int64_t)std::max<size_t>(1, row.size()));
+  std::string chunk;
+  chunk.reserve((size_t)std::min(n, per) * row.size());
+  for (int64_t k = 0; k < std::min(n, per); ++k) chunk += row;
+  for (int64_t done = 0; done < n; done += per) {
+    const int64_t m = std::min(per, n - done);
+    fwrite(chunk.data(), 1, (size_t)m * row.size(), f);
+  }
+}
+// The row printf writes for this format and these values.
+template <class... A>
+std::string row_of(const char* fmt, A... a) {
+  char b[256];
+  const int k = snprintf(b, sizeof(b), fmt, a...);
+  return std::string(b, (size_t)k);
+}
+
+// The state the writers export: the device state of a problem in a batch;
+// a problem not yet stepped outside a batch exports the initial state given
+// at fm_problem_create (zeros without one; Dirichlet values are applied at
+// placement) with zero element fields.
+int writer_state(fm_problem* p, std::vector<double>& u, std::vector<double>& pres, std::vector<double>& e3) {
+  const int64_t N = p->N, E = p->E;
+  const bool vms = p->params.solver == FM_SOLVER_VMS;
+  u.assign((size_t)N * 3, 0.0);
+  pres.assign((size_t)(vms ? N : E), 0.0);
+  e3.assign((size_t)(vms ? E * 3 : E * 2), 0.0);
+  if (p->batch) return fm_problem_get_state(p, u.data(), pres.data(), e3.data(), nullptr);
+  if (p->steps_done > 0) return fail(FM_ERR_INVALID, "the problem left its batch after stepping: its state is gone");
+  if (!p->init.empty())
+    for (int64_t i = 0; i < N; ++i) {
+      for (int k = 0; k < 3; ++k) u[i * 3 + k] = p->init[i * 4 + k];
+      if (vms) pres[i] = p->init[i * 4 + 3];
+    }
+  return FM_OK;
+}
+
 // Writes rows 0..n-1, row i formatted by fmt(i, buf) (returns its length,
 // < 256), formatting blocks of rows on host threads and writing the blocks
 // in order: the bytes are those of the sequential fprintf loop.
@@ -401,13 +465,8 @@ extern "C" int fm_problem_write_vtk(fm_problem* p, const char* path) {
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
   const int64_t N = p->N, E = p->E;
   const bool vms = p->params.solver == FM_SOLVER_VMS;
-  std::vector<double> u(N * 3), pres(vms ? N : E), e3(vms ? E * 3 : E * 2);
-  if (p->batch) {
-    int r = fm_problem_get_state(p, u.data(), pres.data(), e3.data(), nullptr);
-    if (r) return r;
-  } else {
-    return fail(FM_ERR_INVALID, "problem is not in a batch");
-  }
+  std::vector<double> u, pres, e3;
+  if (int r = writer_state(p, u, pres, e3)) return r;
   FILE* f = fopen(path, "w");
   if (!f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
   const double* X = p->coords.data();
@@ -415,55 +474,59 @@ extern "C" int fm_problem_write_vtk(fm_problem* p, const char* path) {
   const int32_t* cn = p->conn.data();
   fprintf(f, "# vtk DataFile Version 2.0\nModel Exported from feMorph\nASCII\nDATASET UNSTRUCTURED_GRID\n");
   fprintf(f, "POINTS %d float\n", (int)N);
-  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e %e %e\n", X[i * 3], X[i * 3 + 1], X[i * 3 + 2]); });
+  write_rows(f, N, [&](int64_t i, char* b) { return put_e3(b, X + i * 3, "\n"); });
   fprintf(f, "CELLS %d %d\n", (int)E, (int)(E * (npe + 1)));
   write_rows(f, E, [&](int64_t e, char* b) {
-    int k = snprintf(b, 256, "%d ", npe);
-    for (int a = 0; a < npe; ++a) k += snprintf(b + k, 256 - k, "%d ", cn[e * npe + a]);
-    k += snprintf(b + k, 256 - k, "\n");
-    return k;
+    char* q = put_d(b, npe);
+    *q++ = ' ';
+    for (int a = 0; a < npe; ++a) {
+      q = put_d(q, cn[e * npe + a]);
+      *q++ = ' ';
+    }
+    *q++ = '\n';
+    return (int)(q - b);
   });
   fprintf(f, "CELL_TYPES %d\n", (int)E);
   const int ctype = npe == 4 ? 10 : 12;
-  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%d\n", ctype); });
+  write_const_rows(f, E, row_of("%d\n", ctype));
   fprintf(f, "POINT_DATA %d\n", (int)N);
   fprintf(f, "VECTORS DXYZ double\n");
-  write_rows(f, N, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e\n", 0.0, 0.0, 0.0); });
+  write_const_rows(f, N, row_of("%e %e %e\n", 0.0, 0.0, 0.0));
   fprintf(f, "VECTORS velocity double\n");
-  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e %e %e \n", u[i * 3], u[i * 3 + 1], u[i * 3 + 2]); });
+  write_rows(f, N, [&](int64_t i, char* b) { return put_e3(b, u.data() + i * 3, " \n"); });
   if (vms) {
     fprintf(f, "SCALARS pressure double 1\nLOOKUP_TABLE default\n");
-    write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e \n", pres[i]); });
+    write_rows(f, N, [&](int64_t i, char* b) { return put_e1(b, pres[i], " \n"); });
   }
   std::vector<double> dirbc(N, 0.0);
   for (int32_t n : p->vel_node) dirbc[n] = 2.0;
   for (int32_t n : p->pres_node) dirbc[n] = 3.0;
   for (int32_t n : p->dir_node) dirbc[n] = 1.0;
   fprintf(f, "SCALARS dirBC double 1\nLOOKUP_TABLE default\n");
-  write_rows(f, N, [&](int64_t i, char* b) { return snprintf(b, 256, "%e\n", dirbc[i]); });
+  write_rows(f, N, [&](int64_t i, char* b) { return put_e1(b, dirbc[i], "\n"); });
   fprintf(f, "SCALARS neuBC double\nLOOKUP_TABLE default\n");
-  write_rows(f, N, [&](int64_t, char* b) { return snprintf(b, 256, "%e\n", 0.0); });
+  write_const_rows(f, N, row_of("%e\n", 0.0));
   fprintf(f, "CELL_DATA %d\n", (int)E);
   fprintf(f, "VECTORS normal double\n");
-  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e\n", 0.0, 0.0, 0.0); });
+  write_const_rows(f, E, row_of("%e %e %e\n", 0.0, 0.0, 0.0));
   fprintf(f, "SCALARS source double 1\nLOOKUP_TABLE default\n");
-  write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e\n", 0.0); });
+  write_const_rows(f, E, row_of("%e\n", 0.0));
   if (vms) {
     fprintf(f, "VECTORS res_v double\n");
-    write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e %e %e \n", 0.0, 0.0, 0.0); });
+    write_const_rows(f, E, row_of("%e %e %e \n", 0.0, 0.0, 0.0));
     fprintf(f, "SCALARS res_p double 1\nLOOKUP_TABLE default\n");
-    write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e \n", 0.0); });
+    write_const_rows(f, E, row_of("%e \n", 0.0));
     fprintf(f, "VECTORS subgrid_u double\n");
-    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e %e %e \n", e3[e * 3], e3[e * 3 + 1], e3[e * 3 + 2]); });
+    write_rows(f, E, [&](int64_t e, char* b) { return put_e3(b, e3.data() + e * 3, " \n"); });
     fprintf(f, "SCALARS subgrid_p double 1\nLOOKUP_TABLE default\n");
-    write_rows(f, E, [&](int64_t, char* b) { return snprintf(b, 256, "%e \n", 0.0); });
+    write_const_rows(f, E, row_of("%e \n", 0.0));
   } else {
     fprintf(f, "SCALARS pressure double 1\nLOOKUP_TABLE default\n");
-    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", pres[e]); });
+    write_rows(f, E, [&](int64_t e, char* b) { return put_e1(b, pres[e], " \n"); });
     fprintf(f, "SCALARS lambda double 1\nLOOKUP_TABLE default\n");
-    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", e3[e * 2]); });
+    write_rows(f, E, [&](int64_t e, char* b) { return put_e1(b, e3[e * 2], " \n"); });
     fprintf(f, "SCALARS regime double 1\nLOOKUP_TABLE default\n");
-    write_rows(f, E, [&](int64_t e, char* b) { return snprintf(b, 256, "%e \n", e3[e * 2 + 1]); });
+    write_rows(f, E, [&](int64_t e, char* b) { return put_e1(b, e3[e * 2 + 1], " \n"); });
   }
   const bool ok = ferror(f) == 0;
   fclose(f);
@@ -475,7 +538,7 @@ namespace {
 // Big-endian copies for legacy binary VTK, converted on host threads.
 template <class T>
 void put_be(FILE* f, const T* v, int64_t n) {
-  std::vector<T> o((size_t)n);
+  hvec<T> o((size_t)n);
   const int64_t hw = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
   const int64_t nt = std::min<int64_t>(hw, std::max<int64_t>(1, n / 65536));
   std::vector<std::thread> th;
@@ -492,6 +555,16 @@ void put_be(FILE* f, const T* v, int64_t n) {
   fwrite(o.data(), sizeof(T), (size_t)n, f);
 }
 
+// `bytes` zero bytes (the big-endian form of a section of zeros).
+void put_zeros(FILE* f, int64_t bytes) {
+  static const char z[1 << 16] = {};
+  while (bytes > 0) {
+    const size_t m = (size_t)std::min<int64_t>(bytes, (int64_t)sizeof(z));
+    fwrite(z, 1, m, f);
+    bytes -= (int64_t)m;
+  }
+}
+
 }  // namespace
 
 // The layout of fm_problem_write_vtk in legacy BINARY form (big-endian
@@ -502,12 +575,10 @@ void put_be(FILE* f, const T* v, int64_t n) {
 extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
   NvtxRange nvtx_range("fm_problem_write_vtk_binary");
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
-  if (!p->batch) return fail(FM_ERR_INVALID, "problem is not in a batch");
   const int64_t N = p->N, E = p->E;
   const bool vms = p->params.solver == FM_SOLVER_VMS;
-  std::vector<double> u(N * 3), pres(vms ? N : E), e3(vms ? E * 3 : E * 2);
-  int r = fm_problem_get_state(p, u.data(), pres.data(), e3.data(), nullptr);
-  if (r) return r;
+  std::vector<double> u, pres, e3;
+  if (int r = writer_state(p, u, pres, e3)) return r;
   FILE* f = fopen(path, "wb");
   if (!f) return fail(FM_ERR_IO, std::string("cannot open ") + path);
   const int npe = p->etype;
@@ -520,11 +591,13 @@ extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
   }
   fprintf(f, "\nCELLS %d %d\n", (int)E, (int)(E * (npe + 1)));
   {
-    std::vector<int32_t> c((size_t)E * (npe + 1));
-    for (int64_t e = 0; e < E; ++e) {
-      c[e * (npe + 1)] = npe;
-      for (int a = 0; a < npe; ++a) c[e * (npe + 1) + 1 + a] = p->conn[e * npe + a];
-    }
+    hvec<int32_t> c((size_t)E * (npe + 1));
+    parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
+      for (int64_t e = eb; e < ee; ++e) {
+        c[e * (npe + 1)] = npe;
+        for (int a = 0; a < npe; ++a) c[e * (npe + 1) + 1 + a] = p->conn[e * npe + a];
+      }
+    }, 1 << 16);
     put_be(f, c.data(), (int64_t)c.size());
   }
   fprintf(f, "\nCELL_TYPES %d\n", (int)E);
@@ -532,17 +605,19 @@ extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
     std::vector<int32_t> t((size_t)E, npe == 4 ? 10 : 12);
     put_be(f, t.data(), E);
   }
-  std::vector<double> zero((size_t)std::max(N, E) * 3, 0.0);
+  // v == nullptr: a section of zeros
   auto vec = [&](const char* name, const double* v, int64_t n) {
     fprintf(f, "\nVECTORS %s double\n", name);
-    put_be(f, v, n * 3);
+    if (v) put_be(f, v, n * 3);
+    else put_zeros(f, n * 3 * (int64_t)sizeof(double));
   };
   auto sca = [&](const char* name, const double* v, int64_t n) {
     fprintf(f, "\nSCALARS %s double 1\nLOOKUP_TABLE default\n", name);
-    put_be(f, v, n);
+    if (v) put_be(f, v, n);
+    else put_zeros(f, n * (int64_t)sizeof(double));
   };
   fprintf(f, "\nPOINT_DATA %d", (int)N);
-  vec("DXYZ", zero.data(), N);
+  vec("DXYZ", nullptr, N);
   vec("velocity", u.data(), N);
   if (vms) sca("pressure", pres.data(), N);
   std::vector<double> dirbc(N, 0.0);
@@ -550,15 +625,15 @@ extern "C" int fm_problem_write_vtk_binary(fm_problem* p, const char* path) {
   for (int32_t n : p->pres_node) dirbc[n] = 3.0;
   for (int32_t n : p->dir_node) dirbc[n] = 1.0;
   sca("dirBC", dirbc.data(), N);
-  sca("neuBC", zero.data(), N);
+  sca("neuBC", nullptr, N);
   fprintf(f, "\nCELL_DATA %d", (int)E);
-  vec("normal", zero.data(), E);
-  sca("source", zero.data(), E);
+  vec("normal", nullptr, E);
+  sca("source", nullptr, E);
   if (vms) {
-    vec("res_v", zero.data(), E);
-    sca("res_p", zero.data(), E);
+    vec("res_v", nullptr, E);
+    sca("res_p", nullptr, E);
     vec("subgrid_u", e3.data(), E);
-    sca("subgrid_p", zero.data(), E);
+    sca("subgrid_p", nullptr, E);
   } else {
     std::vector<double> lam(E), reg(E);
     for (int64_t e = 0; e < E; ++e) {
@@ -583,13 +658,11 @@ extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
   NvtxRange nvtx_range("fm_problem_write_vtu");
   static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "the VTU writer emits little-endian data");
   if (!p || !path) return fail(FM_ERR_INVALID, "null argument");
-  if (!p->batch) return fail(FM_ERR_INVALID, "problem is not in a batch");
   const int64_t N = p->N, E = p->E;
   const int npe = p->etype;
   const bool vms = p->params.solver == FM_SOLVER_VMS;
-  std::vector<double> u(N * 3), pres(vms ? N : E), e3(vms ? E * 3 : E * 2);
-  int r = fm_problem_get_state(p, u.data(), pres.data(), e3.data(), nullptr);
-  if (r) return r;
+  std::vector<double> u, pres, e3;
+  if (int r = writer_state(p, u, pres, e3)) return r;
   std::vector<double> zero((size_t)std::max(N, E) * 3, 0.0), dirbc(N, 0.0), lam, reg;
   for (int32_t n : p->vel_node) dirbc[n] = 2.0;
   for (int32_t n : p->pres_node) dirbc[n] = 3.0;

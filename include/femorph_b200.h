@@ -361,7 +361,12 @@ FM_API int fm_problem_status(fm_problem* p);
 FM_API int fm_problem_get_state(fm_problem* p, double* u, double* pres, double* elem3, double* sdus);
 
 /* Writes the problem's current state as legacy ASCII VTK in the layout of
- * femModel::ExportToVTKLegacy (femModel.cpp:1294-1530). */
+ * femModel::ExportToVTKLegacy (femModel.cpp:1294-1530).  The three writers
+ * export the state of a problem in a batch; a problem not yet placed (or
+ * placed and removed without a step) exports the initial state given at
+ * fm_problem_create (zeros without one, before the Dirichlet values that
+ * placement applies) with zero element fields; one that left its batch
+ * after stepping is refused (FM_ERR_INVALID). */
 FM_API int fm_problem_write_vtk(fm_problem* p, const char* path);
 /* The same sections in legacy BINARY VTK (big-endian float32 points, int32
  * cells, float64 data); no counterpart in the reference, which writes ASCII
