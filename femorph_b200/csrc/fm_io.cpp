@@ -15,7 +15,6 @@
 #include <cstring>
 #include <string>
 #include <thread>
-#include <type_traits>
 #include <vector>
 
 #include "fm_internal.hpp"
