@@ -520,9 +520,10 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   // hexa8 nodes 2 / 3 and 6 / 7 (femHexa8.cpp:93-103)
   Rule rule;
   make_rule(npe, rule);
-  std::vector<int32_t> cfix(d->conn, d->conn + E * npe);
+  fm::hvec<int32_t> cfix((size_t)(E * npe));
   fm::parallel_blocks(E, [&](int64_t eb, int64_t ee, int) {
     for (int64_t e = eb; e < ee; ++e) {
+      for (int a = 0; a < npe; ++a) cfix[e * npe + a] = d->conn[e * npe + a];
       double xe[8][3], mn = 1e308;
       for (int a = 0; a < npe; ++a)
         for (int k = 0; k < 3; ++k) xe[a][k] = d->coords[3 * (int64_t)cfix[e * npe + a] + k];
@@ -553,14 +554,45 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
         for (int b = 0; b < npe; ++b) Ke[(size_t)e * m2 + a * npe + b] = K[a][b];
     }
   }, 1024);
-  // node -> incident (element, corner) in element order
+  // node -> incident (element, corner) in element order: counts per
+  // contiguous element range, each range's entries of a node placed after
+  // those of the ranges before it, the ranges filled on the host threads
+  const int64_t hwt = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
   std::vector<int32_t> ioff(N + 1, 0);
-  for (int64_t i = 0; i < E * npe; ++i) ioff[conn[i] + 1]++;
-  for (int64_t v = 0; v < N; ++v) ioff[v + 1] += ioff[v];
   std::vector<int32_t> inc(E * npe);
   {
-    std::vector<int32_t> pos(ioff.begin(), ioff.end() - 1);
-    for (int64_t i = 0; i < E * npe; ++i) inc[pos[conn[i]]++] = (int32_t)i;
+    const int64_t nr = std::min<int64_t>(hwt, std::max<int64_t>(1, E / 65536));
+    std::vector<std::vector<int32_t>> at(nr);
+    auto ranges = [&](auto&& f) {
+      std::vector<std::thread> th;
+      for (int64_t r = 0; r < nr; ++r) th.emplace_back([&, r] { f(r, E * r / nr * npe, E * (r + 1) / nr * npe); });
+      for (auto& x : th) x.join();
+    };
+    ranges([&](int64_t r, int64_t i0, int64_t i1) {
+      at[r].assign(N, 0);
+      for (int64_t i = i0; i < i1; ++i) at[r][conn[i]]++;
+    });
+    fm::parallel_blocks(N, [&](int64_t vb, int64_t ve, int) {
+      for (int64_t v = vb; v < ve; ++v) {
+        int32_t c = 0;
+        for (int64_t r = 0; r < nr; ++r) c += at[r][v];
+        ioff[v + 1] = c;
+      }
+    }, 1 << 14);
+    for (int64_t v = 0; v < N; ++v) ioff[v + 1] += ioff[v];
+    fm::parallel_blocks(N, [&](int64_t vb, int64_t ve, int) {
+      for (int64_t v = vb; v < ve; ++v) {
+        int32_t pos = ioff[v];
+        for (int64_t r = 0; r < nr; ++r) {
+          const int32_t c = at[r][v];
+          at[r][v] = pos;
+          pos += c;
+        }
+      }
+    }, 1 << 14);
+    ranges([&](int64_t r, int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; ++i) inc[at[r][conn[i]]++] = (int32_t)i;
+    });
   }
   // Dirichlet rows (a later row of the same node wins, as ReplaceGlobalValue)
   std::vector<int32_t> dir_of(N, -1);
@@ -603,7 +635,6 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   std::vector<int32_t> rowp(N + 1, 0);
   fm::hvec<int32_t> rowlen(N);
   std::vector<double> bvec(N), dinv(N);
-  const int64_t hwt = std::max<int64_t>(1, std::min<int64_t>(32, std::thread::hardware_concurrency()));
   const int64_t nblk = std::min<int64_t>(hwt, std::max<int64_t>(1, N / 2048));
   std::vector<std::vector<int32_t>> bcol(nblk);
   std::vector<std::vector<double>> bval(nblk);
@@ -725,7 +756,7 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
   // Neumann face nodes their row's value, source elements their value (a
   // later row wins in each)
   s->h_coords.assign(d->coords, d->coords + N * 3);
-  s->h_conn = cfix;
+  s->h_conn.assign(cfix.begin(), cfix.end());
   s->h_diff.assign(d->diffusivity, d->diffusivity + E * 3);
   s->h_src.assign(E, 0.0);
   for (int64_t k = 0; k < d->n_sources; ++k) s->h_src[d->source_elem[k]] = d->source_value[k];
