@@ -642,6 +642,15 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
     std::vector<int32_t>& lc = bcol[kb];
     std::vector<double>& lv = bval[kb];
     std::vector<int32_t> cl;
+    // the row's distinct columns (open addressing, at most half full) with
+    // their positions in the sorted row
+    std::vector<int32_t> hkey(64, -1), hval(64), hused;
+    uint32_t hmask = 63;
+    auto hslot = [&](int32_t w) {
+      uint32_t h = ((uint32_t)w * 2654435761u) & hmask;
+      while (hkey[h] != w && hkey[h] >= 0) h = (h + 1) & hmask;
+      return h;
+    };
     for (int64_t v = N * kb / nblk; v < N * (kb + 1) / nblk; ++v) {
       if (dir_of[v] >= 0) {
         lc.push_back((int32_t)v);
@@ -651,16 +660,30 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
         dinv[v] = 1.0;
         continue;
       }
+      const uint32_t raw = (uint32_t)(ioff[v + 1] - ioff[v]) * (uint32_t)npe;
+      if (2 * raw + 2 > hmask + 1) {
+        uint32_t cap = hmask + 1;
+        while (cap < 2 * raw + 2) cap <<= 1;
+        hkey.assign(cap, -1);
+        hval.resize(cap);
+        hmask = cap - 1;
+      }
       cl.clear();
       for (int32_t k = ioff[v]; k < ioff[v + 1]; ++k) {
         const int64_t e = inc[k] / npe;
         for (int b = 0; b < npe; ++b) {
           const int32_t w = conn[e * npe + b];
-          if (dir_of[w] < 0) cl.push_back(w);
+          if (dir_of[w] >= 0) continue;
+          const uint32_t h = hslot(w);
+          if (hkey[h] < 0) {
+            hkey[h] = w;
+            hused.push_back((int32_t)h);
+            cl.push_back(w);
+          }
         }
       }
       std::sort(cl.begin(), cl.end());
-      cl.erase(std::unique(cl.begin(), cl.end()), cl.end());
+      for (size_t j = 0; j < cl.size(); ++j) hval[hslot(cl[j])] = (int32_t)j;
       if (cl.empty()) {  // a node of no element (and not Dirichlet): identity row, value 0
         lc.push_back((int32_t)v);
         lv.push_back(1.0);
@@ -682,11 +705,12 @@ static int poisson_create(const fm_poisson_desc* d, int32_t device, fm_poisson**
           if (dir_of[w] >= 0) {
             bv -= kv * d->dir_value[dir_of[w]];
           } else {
-            const size_t j = (size_t)(std::lower_bound(cl.begin(), cl.end(), w) - cl.begin());
-            lv[r0 + j] += kv;
+            lv[r0 + (size_t)hval[hslot(w)]] += kv;
           }
         }
       }
+      for (int32_t h : hused) hkey[h] = -1;
+      hused.clear();
       for (size_t j = 0; j < cl.size(); ++j)
         if (cl[j] == v) diag = lv[r0 + j];
       rowlen[v] = (int32_t)cl.size();
