@@ -212,3 +212,40 @@ def test_unknown_register_budget_rejected_before_device():
             api.Batch([g], threads=threads, ctas_per_sm=ctas)
         assert ei.value.code == api.FM_ERR_INVALID
     g.close()
+
+
+def test_dat_reader_number_forms(tmp_path):
+    """NODE coordinates written in the forms strtod accepts (leading '+',
+    upper-case exponents, short decimals, leading zeros, tabs before the line
+    end, comma separators, CRLF line ends, no final newline) read to the
+    correctly rounded values: the lumped masses equal those of the same mesh
+    built from the values parsed here (Python's float is correctly rounded
+    like strtod)."""
+    p = mesh.cavity(4, seed=8, steps=2)
+    path = str(tmp_path / "m.dat")
+    mesh.write_dat(p, path)
+    forms = [lambda v: "+%.17e" % v if v >= 0 else "%.17e" % v, lambda v: "%.17E" % v, lambda v: "%.4f" % v,
+             lambda v: "%.9g" % v, lambda v: ("0" + "%.12f" % v) if v >= 0 else "%.12f" % v]
+    coords = np.array(p.coords, dtype=np.float64)
+    out, k = [], 0
+    for line in open(path).read().splitlines():
+        t = line.split(" ")
+        if t[0] == "NODE":
+            i = int(t[1]) - 1
+            txt = [forms[(k + c) % len(forms)](coords[i, c]) for c in range(3)]
+            coords[i] = [float(x) for x in txt]
+            sep = "," if k % 3 == 0 else " "
+            line = sep.join(t[:2] + txt) + ("\t" if k % 4 == 1 else "")
+            k += 1
+        out.append(line + ("\r" if k % 5 == 2 else ""))
+    with open(path, "w") as f:
+        f.write("\n".join(out))
+    h = C.c_void_p()
+    api.check(api.lib().fm_problem_read_dat(path.encode(), 0, 0, C.byref(h)))
+    m = np.zeros(p.n_nodes)
+    api.check(api.lib().fm_problem_get_mass(h, m.ctypes.data))
+    api.lib().fm_problem_destroy(h)
+    q = mesh.cavity(4, seed=8, steps=2)
+    q.coords = coords
+    assert not np.array_equal(coords, np.asarray(p.coords))  # the short forms round some coordinates
+    assert np.array_equal(m, api.GpuProblem(q).mass())
