@@ -37,3 +37,27 @@ def test_writers_export_the_initial_state_before_placement(tmp_path, case):
     assert np.allclose(np.array(A["VECTORS velocity"]), init[:, :3], rtol=2e-6, atol=1e-300)
     assert np.array_equal(np.array(A["SCALARS dirBC"]).ravel(), V["dirBC"])
     assert len(A["VECTORS normal"]) == p.n_elems and not np.array(A["VECTORS normal"]).any()
+
+
+def test_ascii_writer_prints_percent_e(tmp_path):
+    """Every number of the velocity and pressure sections is printf's "%e" of
+    the value (checked against Python's correctly rounded %-formatting) over
+    the whole exponent range, signed zeros, halfway cases and infinities."""
+    p = mesh.cavity(4, seed=9, steps=2)
+    rng = np.random.default_rng(11)
+    init = rng.standard_normal((p.n_nodes, 4)) * 10.0 ** rng.integers(-307, 307, (p.n_nodes, 4))
+    specials = [0.0, -0.0, 5e-324, -2.2250738585072014e-308, 1.7976931348623157e308, 0.5, 2.5e-7, 1234565.0,
+                9.9999995, 999999.5, np.inf, -np.inf]
+    init.ravel()[:len(specials)] = specials
+    p.init_state = init
+    g = api.GpuProblem(p)
+    path = str(tmp_path / "a.vtk")
+    g.write_vtk(path)
+    g.close()
+    lines = open(path).read().split("\n")
+    k = lines.index("VECTORS velocity double") + 1
+    for i in range(p.n_nodes):
+        assert lines[k + i] == " ".join("%e" % v for v in init[i, :3]) + " ", (i, lines[k + i])
+    k = lines.index("SCALARS pressure double 1") + 2
+    for i in range(p.n_nodes):
+        assert lines[k + i] == "%e " % init[i, 3], (i, lines[k + i])
