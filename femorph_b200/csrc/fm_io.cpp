@@ -662,7 +662,7 @@ extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
   const bool vms = p->params.solver == FM_SOLVER_VMS;
   std::vector<double> u, pres, e3;
   if (int r = writer_state(p, u, pres, e3)) return r;
-  std::vector<double> zero((size_t)std::max(N, E) * 3, 0.0), dirbc(N, 0.0), lam, reg;
+  std::vector<double> dirbc(N, 0.0), lam, reg;
   for (int32_t n : p->vel_node) dirbc[n] = 2.0;
   for (int32_t n : p->pres_node) dirbc[n] = 3.0;
   for (int32_t n : p->dir_node) dirbc[n] = 1.0;
@@ -690,18 +690,18 @@ extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
   };
   std::vector<Block> pd, cd, pts, cells;
   const uint64_t n8 = (uint64_t)N * 8, e8 = (uint64_t)E * 8;
-  pd.push_back(arr("Float64", "DXYZ", 3, zero.data(), n8 * 3));
+  pd.push_back(arr("Float64", "DXYZ", 3, nullptr, n8 * 3));
   pd.push_back(arr("Float64", "velocity", 3, u.data(), n8 * 3));
   if (vms) pd.push_back(arr("Float64", "pressure", 1, pres.data(), n8));
   pd.push_back(arr("Float64", "dirBC", 1, dirbc.data(), n8));
-  pd.push_back(arr("Float64", "neuBC", 1, zero.data(), n8));
-  cd.push_back(arr("Float64", "normal", 3, zero.data(), e8 * 3));
-  cd.push_back(arr("Float64", "source", 1, zero.data(), e8));
+  pd.push_back(arr("Float64", "neuBC", 1, nullptr, n8));
+  cd.push_back(arr("Float64", "normal", 3, nullptr, e8 * 3));
+  cd.push_back(arr("Float64", "source", 1, nullptr, e8));
   if (vms) {
-    cd.push_back(arr("Float64", "res_v", 3, zero.data(), e8 * 3));
-    cd.push_back(arr("Float64", "res_p", 1, zero.data(), e8));
+    cd.push_back(arr("Float64", "res_v", 3, nullptr, e8 * 3));
+    cd.push_back(arr("Float64", "res_p", 1, nullptr, e8));
     cd.push_back(arr("Float64", "subgrid_u", 3, e3.data(), e8 * 3));
-    cd.push_back(arr("Float64", "subgrid_p", 1, zero.data(), e8));
+    cd.push_back(arr("Float64", "subgrid_p", 1, nullptr, e8));
   } else {
     cd.push_back(arr("Float64", "pressure", 1, pres.data(), e8));
     cd.push_back(arr("Float64", "lambda", 1, lam.data(), e8));
@@ -736,7 +736,8 @@ extern "C" int fm_problem_write_vtu(fm_problem* p, const char* path) {
   fprintf(f, "    </Piece>\n  </UnstructuredGrid>\n  <AppendedData encoding=\"raw\">\n   _");
   for (const Block* b : order) {
     fwrite(&b->bytes, 8, 1, f);
-    fwrite(b->data, 1, b->bytes, f);
+    if (b->data) fwrite(b->data, 1, b->bytes, f);
+    else put_zeros(f, (int64_t)b->bytes);  // a section of zeros
   }
   fprintf(f, "\n  </AppendedData>\n</VTKFile>\n");
   const bool ok = ferror(f) == 0;
