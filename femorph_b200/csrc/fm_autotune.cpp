@@ -1,6 +1,8 @@
 // Launch-shape autotuner with a persisted cache: tile size (elements per
 // CTA), threads per CTA and, for VMS, the register budget (the tile kernel
 // variant compiled for 3 or 4 resident 128-thread CTAs an SM, ...).
+#include <unistd.h>
+
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -67,8 +69,20 @@ void cache_store(const char* path, const std::string& key, const fm_tuning& t) {
   std::ostringstream l;
   l << key << " " << t.tile_elems << " " << t.tile_nodes << " " << t.threads << " " << t.ctas_per_sm;
   lines.push_back(l.str());
-  std::ofstream f(path, std::ios::trunc);
-  for (auto& s : lines) f << s << "\n";
+  // written whole to a file of this process and renamed over the cache, so
+  // a reader (or another rank storing at the same time) sees an old or a new
+  // complete file, never a partial one
+  const std::string tmp = std::string(path) + ".tmp" + std::to_string((long long)getpid());
+  {
+    std::ofstream f(tmp, std::ios::trunc);
+    for (auto& s : lines) f << s << "\n";
+    if (!f.good()) {
+      f.close();
+      std::remove(tmp.c_str());
+      return;
+    }
+  }
+  if (std::rename(tmp.c_str(), path) != 0) std::remove(tmp.c_str());
 }
 
 }  // namespace

@@ -249,3 +249,31 @@ def test_dat_reader_number_forms(tmp_path):
     q.coords = coords
     assert not np.array_equal(coords, np.asarray(p.coords))  # the short forms round some coordinates
     assert np.array_equal(m, api.GpuProblem(q).mass())
+
+
+def test_autotune_cache_lookup_without_device(tmp_path):
+    """fm_autotune answers from its cache file before it touches a device:
+    the line whose key names the problem class (GPU model - "unknown" without
+    a device -, solver, element type, precision, batch or single, log2 of the
+    element count) gives the launch shape; a line written before the
+    register budget was tuned (four fields) reads with ctas_per_sm 0; other
+    lines are skipped.  Without a matching line and without a device the call
+    fails loudly."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present (the key would name it)")
+    except Exception:
+        pass
+    p = mesh.cavity(6, seed=1, steps=2)           # 1296 tets: 2^10 <= E < 2^11
+    g = api.GpuProblem(p)
+    cache = tmp_path / "tune.txt"
+    key = "unknown/s0/e4/p0/n0/E2^10"
+    cache.write_text("not a tuning line\nunknown/s0/e4/p1/n0/E2^10 256 128 128 5\n" + key + " 384 160 128 4\n")
+    assert api.autotune([g], cache_path=str(cache)) == dict(tile_elems=384, tile_nodes=160, threads=128, ctas_per_sm=4)
+    cache.write_text(key + " 512 256 256\n")
+    assert api.autotune([g], cache_path=str(cache)) == dict(tile_elems=512, tile_nodes=256, threads=256, ctas_per_sm=0)
+    cache.write_text("unknown/s0/e4/p0/n0/E2^11 512 256 128 3\n")
+    with pytest.raises(api.FmError):
+        api.autotune([g], cache_path=str(cache))
+    g.close()
